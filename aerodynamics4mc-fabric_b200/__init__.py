@@ -1,0 +1,337 @@
+"""Python binding of libaero_lbm_b200.so (the B200 lattice-Boltzmann brick step).
+
+This is a thin ctypes mirror of the library's C ABI (include/aero_lbm_b200.h),
+which itself mirrors the reference mod's native ABI (aero_lbm_*, aero_solver_*).
+It is how the reference's own Python tools drive the native step, so the same
+calls work against this library. No PyTorch is involved; buffers are numpy
+arrays or raw pointers.
+
+The library runs only on a CUDA device (sm_100a). Loading fails loudly if the
+shared library has not been built; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PACKAGE_DIR = Path(__file__).resolve().parent
+LIB_PATH = PACKAGE_DIR / "libaero_lbm_b200.so"
+HEADER_PATH = PACKAGE_DIR.parent / "include" / "aero_lbm_b200.h"
+
+# ---------------------------------------------------------------- enums
+BENCHMARK_PRESET_NONE = 0
+HYDRO_INHERIT_GAME = 0
+HYDRO_PERIODIC = 1
+HYDRO_BOUNCE_BACK = 2
+HYDRO_MOVING_WALL = 3
+HYDRO_VELOCITY = 4
+HYDRO_PRESSURE = 5
+HYDRO_CONVECTIVE = 6
+HYDRO_SYMMETRY = 7
+
+FLAG_DISABLE_FAN_FORCING = 1 << 0
+FLAG_DISABLE_FAN_NOISE = 1 << 1
+FLAG_DISABLE_SPONGE = 1 << 2
+FLAG_DISABLE_CONVECTIVE_OUTFLOW = 1 << 3
+FLAG_DISABLE_OBSTACLE_BOUNCE_BLEND = 1 << 4
+FLAG_DISABLE_SGS = 1 << 5
+FLAG_DISABLE_INTERNAL_THERMAL_SOURCE = 1 << 6
+FLAG_DISABLE_BUOYANCY = 1 << 7
+
+SOLVER_BOUNDARY_WIND_TUNNEL = 1
+SOLVER_BOUNDARY_WIND_TUNNEL_PRESSURE_OUTLET = 2
+SOLVER_BOUNDARY_CLOSED = 3
+SOLVER_BOUNDARY_PERIODIC = 4
+SOLVER_FLOW_CHANNELS = 4
+
+PACKET_CHANNELS = 11
+
+
+# ---------------------------------------------------------------- structs
+class AeroLbmBoundaryFaceConfig(ctypes.Structure):
+    _fields_ = [
+        ("hydrodynamic_kind", ctypes.c_int),
+        ("thermal_kind", ctypes.c_int),
+        ("velocity", ctypes.c_float * 3),
+        ("pressure", ctypes.c_float),
+        ("temperature", ctypes.c_float),
+        ("heat_flux", ctypes.c_float),
+    ]
+
+
+class AeroLbmBenchmarkConfig(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32),
+        ("struct_size", ctypes.c_uint32),
+        ("flags", ctypes.c_uint32),
+        ("enabled", ctypes.c_int),
+        ("preset", ctypes.c_int),
+        ("reserved0", ctypes.c_int),
+        ("reynolds_number", ctypes.c_float),
+        ("rayleigh_number", ctypes.c_float),
+        ("prandtl_number", ctypes.c_float),
+        ("mach_number", ctypes.c_float),
+        ("reference_density", ctypes.c_float),
+        ("reference_temperature", ctypes.c_float),
+        ("reference_length", ctypes.c_float),
+        ("body_force", ctypes.c_float * 3),
+        ("gravity", ctypes.c_float * 3),
+        ("initial_velocity", ctypes.c_float * 3),
+        ("initial_pressure", ctypes.c_float),
+        ("initial_temperature", ctypes.c_float),
+        ("x_min", AeroLbmBoundaryFaceConfig),
+        ("x_max", AeroLbmBoundaryFaceConfig),
+        ("y_min", AeroLbmBoundaryFaceConfig),
+        ("y_max", AeroLbmBoundaryFaceConfig),
+        ("z_min", AeroLbmBoundaryFaceConfig),
+        ("z_max", AeroLbmBoundaryFaceConfig),
+        ("reserved", ctypes.c_uint32 * 8),
+    ]
+
+    FACE_NAMES = ("x_min", "x_max", "y_min", "y_max", "z_min", "z_max")
+
+    def faces(self):
+        return [getattr(self, n) for n in self.FACE_NAMES]
+
+
+class AeroLbmTimingSnapshot(ctypes.Structure):
+    _fields_ = [
+        ("ticks", ctypes.c_uint64),
+        ("last_payload_copy_ms", ctypes.c_double),
+        ("last_solver_ms", ctypes.c_double),
+        ("last_readback_ms", ctypes.c_double),
+        ("last_total_ms", ctypes.c_double),
+        ("avg_payload_copy_ms", ctypes.c_double),
+        ("avg_solver_ms", ctypes.c_double),
+        ("avg_readback_ms", ctypes.c_double),
+        ("avg_total_ms", ctypes.c_double),
+    ]
+
+
+class AeroGridDesc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("dx", ctypes.c_float), ("dt", ctypes.c_float)]
+
+
+class AeroBoundaryDesc(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int),
+        ("inlet_vx", ctypes.c_float),
+        ("inlet_vy", ctypes.c_float),
+        ("inlet_vz", ctypes.c_float),
+        ("outlet_pressure", ctypes.c_float),
+        ("density", ctypes.c_float),
+        ("viscosity", ctypes.c_float),
+    ]
+
+
+class AeroStepInput(ctypes.Structure):
+    _fields_ = [
+        ("solid_mask", ctypes.POINTER(ctypes.c_uint8)),
+        ("prev_flow", ctypes.POINTER(ctypes.c_float)),
+        ("grid", AeroGridDesc),
+        ("boundary", AeroBoundaryDesc),
+        ("steps", ctypes.c_int),
+    ]
+
+
+class AeroStepOutput(ctypes.Structure):
+    _fields_ = [("flow_out", ctypes.POINTER(ctypes.c_float)), ("max_velocity", ctypes.c_float), ("status", ctypes.c_int)]
+
+
+# ---------------------------------------------------------------- loading
+_P = ctypes.c_void_p
+_F32P = ctypes.POINTER(ctypes.c_float)
+_I16P = ctypes.POINTER(ctypes.c_int16)
+_U8P = ctypes.POINTER(ctypes.c_uint8)
+_I32P = ctypes.POINTER(ctypes.c_int)
+_LL = ctypes.c_longlong
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+SIGNATURES = {
+    # per-context ABI
+    "aero_lbm_init": (_I, [_I, _I, _I]),
+    "aero_lbm_step": (_I, [_F32P, _I, _LL, _F32P]),
+    "aero_lbm_init_rect": (_I, [_I, _I, _I, _I, _I]),
+    "aero_lbm_step_rect": (_I, [_F32P, _I, _I, _I, _LL, _F32P]),
+    "aero_lbm_step_rect_scaled": (_I, [_F32P, _I, _I, _I, _LL, _F, _F32P]),
+    "aero_lbm_step_rect_cached": (_I, [_I, _I, _I, _LL, _F32P]),
+    "aero_lbm_step_rect_cached_scaled": (_I, [_I, _I, _I, _LL, _F, _F32P]),
+    "aero_lbm_has_context": (_I, [_LL]),
+    "aero_lbm_context_realtime_cached_initialized": (_I, [_LL]),
+    "aero_lbm_get_temperature_state_rect": (_I, [_I, _I, _I, _LL, _F32P]),
+    "aero_lbm_extract_flow_atlas_rect": (_I, [_I, _I, _I, _LL, _I, _F32P, _I]),
+    "aero_lbm_get_flow_state_rect": (_I, [_I, _I, _I, _LL, _F32P]),
+    "aero_lbm_set_temperature_state_rect": (_I, [_I, _I, _I, _LL, _F32P]),
+    "aero_lbm_release_context": (None, [_LL]),
+    "aero_lbm_shutdown": (None, []),
+    "aero_lbm_runtime_info": (ctypes.c_char_p, []),
+    "aero_lbm_last_error": (ctypes.c_char_p, []),
+    "aero_lbm_timing_info": (ctypes.c_char_p, []),
+    "aero_lbm_reset_timing": (None, []),
+    "aero_lbm_set_realtime_solver_mode": (None, [_I]),
+    "aero_lbm_finish": (_I, []),
+    "aero_lbm_get_timing_snapshot": (_I, [ctypes.POINTER(AeroLbmTimingSnapshot)]),
+    "aero_lbm_benchmark_default_config": (None, [ctypes.POINTER(AeroLbmBenchmarkConfig)]),
+    "aero_lbm_benchmark_default_preset_config": (_I, [_I, ctypes.POINTER(AeroLbmBenchmarkConfig)]),
+    "aero_lbm_benchmark_set_config": (_I, [ctypes.POINTER(AeroLbmBenchmarkConfig)]),
+    "aero_lbm_benchmark_get_config": (_I, [ctypes.POINTER(AeroLbmBenchmarkConfig)]),
+    "aero_lbm_benchmark_reset_config": (None, []),
+    "aero_lbm_benchmark_info": (ctypes.c_char_p, []),
+    # device-resident extensions
+    "aero_lbm_b200_set_stream": (None, [_P]),
+    "aero_lbm_b200_launch_count": (ctypes.c_ulonglong, []),
+    "aero_lbm_b200_advance_rect": (_I, [_LL, _I]),
+    "aero_lbm_b200_set_streaming_mode": (_I, [_I]),
+    "aero_lbm_b200_set_force_field": (_I, [_LL, _F32P, _I]),
+    "aero_lbm_b200_set_physics_overrides": (None, [_F, _F, _I]),
+    # wind-tunnel ABI
+    "aero_solver_default_grid": (None, [ctypes.POINTER(AeroGridDesc)]),
+    "aero_solver_default_boundary": (None, [ctypes.POINTER(AeroBoundaryDesc)]),
+    "aero_solver_create": (_I, [_I, _I, _I, _F, _F, ctypes.POINTER(_LL)]),
+    "aero_solver_create_with_grid": (_I, [ctypes.POINTER(AeroGridDesc), ctypes.POINTER(_LL)]),
+    "aero_solver_set_solid_mask": (_I, [_LL, _U8P, _I]),
+    "aero_solver_set_flow_state": (_I, [_LL, _F32P, _I]),
+    "aero_solver_step_wind_tunnel": (_I, [_LL, ctypes.POINTER(AeroBoundaryDesc), _I, _F32P, _I]),
+    "aero_solver_advance_wind_tunnel": (_I, [_LL, ctypes.POINTER(AeroBoundaryDesc), _I]),
+    "aero_solver_run_wind_tunnel": (_I, [ctypes.POINTER(AeroStepInput), ctypes.POINTER(AeroStepOutput)]),
+    "aero_solver_destroy": (None, [_LL]),
+    "aero_solver_last_error": (ctypes.c_char_p, []),
+    "aero_solver_runtime_info": (ctypes.c_char_p, []),
+    "aero_solver_finish": (_I, []),
+}
+
+_lib = None
+
+
+def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
+    """Load libaero_lbm_b200.so and attach argument/return types.
+
+    Raises FileNotFoundError when the library has not been built (run
+    build.py): the product has no fallback implementation.
+    """
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: build it with `python {PACKAGE_DIR / 'build.py'}`")
+    lib = ctypes.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def last_error(lib: ctypes.CDLL | None = None) -> str:
+    lib = lib or load_library()
+    msg = lib.aero_lbm_last_error()
+    return msg.decode("utf-8", "replace") if msg else ""
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_F32P)
+
+
+def u8ptr(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags.c_contiguous
+    return a.ctypes.data_as(_U8P)
+
+
+def build_packet(obstacle: np.ndarray, ux=None, uy=None, uz=None, pressure=None, temperature=None,
+                 channels: int = PACKET_CHANNELS) -> np.ndarray:
+    """AoS step packet in the reference's channel order (obstacle, fan mask,
+    fan v, state v, pressure proxy, thermal source, temperature)."""
+    cells = obstacle.size
+    pk = np.zeros((cells, channels), dtype=np.float32)
+    pk[:, 0] = (obstacle.reshape(-1) != 0).astype(np.float32)
+    for ch, v in ((5, ux), (6, uy), (7, uz), (8, pressure)):
+        if v is not None:
+            pk[:, ch] = np.asarray(v, dtype=np.float32).reshape(-1)
+    if temperature is not None and channels > 10:
+        pk[:, 10] = np.asarray(temperature, dtype=np.float32).reshape(-1)
+    return np.ascontiguousarray(pk)
+
+
+def default_config(lib: ctypes.CDLL | None = None) -> AeroLbmBenchmarkConfig:
+    lib = lib or load_library()
+    cfg = AeroLbmBenchmarkConfig()
+    lib.aero_lbm_benchmark_default_config(ctypes.byref(cfg))
+    return cfg
+
+
+def declared_symbols(header: Path = HEADER_PATH) -> list[str]:
+    """Function names declared in include/aero_lbm_b200.h."""
+    import re
+
+    text = "\n".join(l for l in header.read_text().splitlines() if not l.lstrip().startswith("#"))
+    return sorted(set(re.findall(r"AERO_LBM_B200_EXPORT\s+[^;(]*?\b(\w+)\s*\(", text)))
+
+
+class LbmContext:
+    """One brick/grid context of the per-context ABI (aero_lbm_init_rect +
+    aero_lbm_step_rect...), the calls the reference's brick runtime makes."""
+
+    def __init__(self, dims, input_channels: int = PACKET_CHANNELS, output_channels: int = 4, key: int = 1,
+                 lib: ctypes.CDLL | None = None, init: bool = True):
+        self.lib = lib or load_library()
+        self.dims = tuple(int(d) for d in dims)
+        self.cells = int(np.prod(self.dims))
+        self.key = int(key)
+        self.in_ch = input_channels
+        self.out_ch = output_channels
+        if init and not self.lib.aero_lbm_init_rect(*self.dims, input_channels, output_channels):
+            raise RuntimeError(f"aero_lbm_init_rect failed: {last_error(self.lib)}")
+
+    def configure(self, cfg: AeroLbmBenchmarkConfig) -> None:
+        if not self.lib.aero_lbm_benchmark_set_config(ctypes.byref(cfg)):
+            raise RuntimeError("aero_lbm_benchmark_set_config failed")
+
+    def step(self, packet: np.ndarray | None, output: bool = True, scale: float = 1.0) -> np.ndarray | None:
+        out = np.zeros(self.cells * self.out_ch, dtype=np.float32) if output else None
+        optr = fptr(out) if output else None
+        if packet is None:
+            ok = self.lib.aero_lbm_step_rect_cached_scaled(*self.dims, self.key, scale, optr)
+        else:
+            pk = np.ascontiguousarray(packet, dtype=np.float32)
+            if pk.size != self.cells * self.in_ch:
+                raise ValueError("packet size does not match dims x input_channels")
+            ok = self.lib.aero_lbm_step_rect_scaled(fptr(pk), *self.dims, self.key, scale, optr)
+        if not ok:
+            raise RuntimeError(f"step failed: {last_error(self.lib)}")
+        return out.reshape(self.cells, self.out_ch) if output else None
+
+    def advance(self, steps: int) -> None:
+        """Device-resident steps (no host copies, no synchronisation)."""
+        if not self.lib.aero_lbm_b200_advance_rect(self.key, int(steps)):
+            raise RuntimeError(f"advance failed: {last_error(self.lib)}")
+
+    def atlas(self, stride: int) -> np.ndarray:
+        n = [(d + stride - 1) // stride for d in self.dims]
+        out = np.zeros(int(np.prod(n)) * 4, dtype=np.float32)
+        if not self.lib.aero_lbm_extract_flow_atlas_rect(*self.dims, self.key, stride, fptr(out), out.size):
+            raise RuntimeError(f"extract failed: {last_error(self.lib)}")
+        return out.reshape(-1, 4)
+
+    def flow_state(self) -> np.ndarray:
+        out = np.zeros(self.cells * 4, dtype=np.float32)
+        if not self.lib.aero_lbm_get_flow_state_rect(*self.dims, self.key, fptr(out)):
+            raise RuntimeError(f"get_flow_state failed: {last_error(self.lib)}")
+        return out.reshape(self.cells, 4)
+
+    def set_force_field(self, fx, fy, fz) -> None:
+        soa = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float32).reshape(-1) for a in (fx, fy, fz)]))
+        if not self.lib.aero_lbm_b200_set_force_field(self.key, fptr(soa), soa.size):
+            raise RuntimeError(f"set_force_field failed: {last_error(self.lib)}")
+
+    def release(self) -> None:
+        self.lib.aero_lbm_release_context(self.key)

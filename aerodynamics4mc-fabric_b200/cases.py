@@ -1,0 +1,125 @@
+"""Seeded synthetic inputs for the benchmark configurations of the brick step.
+
+Each builder returns plain numpy arrays (obstacle mask, initial velocity,
+temperature) plus the boundary/physics settings, in the packet conventions of
+the C ABI (cell = (x*ny + y)*nz + z, z up). Nothing here runs on the GPU.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PERIODIC, BOUNCE_BACK, MOVING_WALL, VELOCITY, PRESSURE, CONVECTIVE, SYMMETRY = 1, 2, 3, 4, 5, 6, 7
+
+
+@dataclass
+class BrickCase:
+    name: str
+    dims: tuple
+    obstacle: np.ndarray            # uint8 (nx, ny, nz)
+    u: tuple                        # three float32 arrays (nx, ny, nz)
+    temperature: np.ndarray | None  # float32 (nx, ny, nz) or None
+    faces: list                     # 6 dicts: kind, velocity, pressure
+    tau: float
+    u_ref: tuple
+    sgs: bool = True
+    smagorinsky_c: float = 0.025
+    buoyancy: bool = False
+    buoyancy_beta: float = 0.0
+    gravity_axis: int = 2
+    steps: int = 1000
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def cells(self) -> int:
+        return int(np.prod(self.dims))
+
+    def config_dict(self) -> dict:
+        """Dict form understood by the parity tooling (Reynolds number chosen so
+        that the effective shear tau equals ``tau``)."""
+        speed = float(np.linalg.norm(np.asarray(self.u_ref, np.float64)))
+        for fc in self.faces:
+            speed = max(speed, float(np.linalg.norm(np.asarray(fc.get("velocity", (0, 0, 0)), np.float64))))
+        nu = (self.tau - 0.5) / 3.0
+        return {
+            "reynolds": speed / nu,
+            "reference_length": 1.0,
+            "initial_velocity": tuple(float(v) for v in self.u_ref),
+            "faces": self.faces,
+            "sgs": self.sgs,
+            "buoyancy": self.buoyancy,
+            "smagorinsky_c": self.smagorinsky_c,
+            "buoyancy_beta": self.buoyancy_beta,
+            "gravity_axis": self.gravity_axis,
+        }
+
+    def packet(self, channels: int = 11) -> np.ndarray:
+        pk = np.zeros((self.cells, channels), dtype=np.float32)
+        pk[:, 0] = (self.obstacle.reshape(-1) != 0)
+        for a in range(3):
+            pk[:, 5 + a] = self.u[a].reshape(-1)
+        if self.temperature is not None and channels > 10:
+            pk[:, 10] = self.temperature.reshape(-1)
+        return pk
+
+
+def value_noise_heightmap(n_x: int, n_y: int, octaves: int, amplitude: float, seed: int) -> np.ndarray:
+    """Fractal value noise: octave k is a (4*2^k + 1)^2 random lattice
+    bilinearly interpolated to the grid, weight 2^-k; rescaled to [0, amplitude]."""
+    rng = np.random.default_rng(seed)
+    h = np.zeros((n_x, n_y), np.float64)
+    for k in range(octaves):
+        m = 4 * 2 ** k + 1
+        lat = rng.random((m, m))
+        gx = np.linspace(0, m - 1, n_x)
+        gy = np.linspace(0, m - 1, n_y)
+        ix = np.minimum(gx.astype(int), m - 2)
+        iy = np.minimum(gy.astype(int), m - 2)
+        fx = (gx - ix)[:, None]
+        fy = (gy - iy)[None, :]
+        a = lat[ix][:, iy]
+        b = lat[ix + 1][:, iy]
+        c = lat[ix][:, iy + 1]
+        d = lat[ix + 1][:, iy + 1]
+        h += 0.5 ** k * ((1 - fx) * (1 - fy) * a + fx * (1 - fy) * b + (1 - fx) * fy * c + fx * fy * d)
+    h -= h.min()
+    if h.max() > 0:
+        h *= amplitude / h.max()
+    return h
+
+
+def c1_plain_fp32(n: int = 32, seed: int = 1234, tau: float = 0.55, steps: int = 1000) -> BrickCase:
+    """One n^3 brick, periodic x/y, bounce-back floor z=0 (solid plane and
+    face), Bernoulli(0.05) interior solids, u = (0.05,0,0) + U(-0.005,0.005)."""
+    rng = np.random.default_rng(seed)
+    obstacle = (rng.random((n, n, n)) < 0.05).astype(np.uint8)
+    obstacle[:, :, 0] = 1
+    u0 = (0.05, 0.0, 0.0)
+    u = tuple(np.float32(u0[a]) + rng.uniform(-0.005, 0.005, size=(n, n, n)).astype(np.float32) for a in range(3))
+    faces = [{"kind": PERIODIC}] * 4 + [{"kind": BOUNCE_BACK}] * 2
+    return BrickCase("c1-plain-fp32", (n, n, n), obstacle, u, None, faces, tau, u0, sgs=True, steps=steps)
+
+
+def c2_terrain_boussinesq(n: int = 128, seed: int = 2024, tau: float = 0.55, steps: int = 1000) -> BrickCase:
+    """One n^3 brick over a seeded 4-octave heightmap (amplitude 24 cells at
+    n=128, scaled with n), inflow u=(0.08,0.02,0) at x=0, far-field
+    equilibrium outflow at x=n-1 and on the lid, periodic y, bounce-back
+    ground. Boussinesq along +z with g*beta = 1e-4 and T = -1e-3 z plus a
+    Gaussian warm bubble (amplitude 0.01, radius 8, centre (n/2, n/2, 20))."""
+    s = n / 128.0
+    h = value_noise_heightmap(n, n, 4, 24.0 * s, seed)
+    z = np.arange(n)[None, None, :]
+    obstacle = (z < h[:, :, None]).astype(np.uint8)
+    obstacle[:, :, 0] = 1
+    u_in = (0.08, 0.02, 0.0)
+    fluid = obstacle == 0
+    u = tuple(np.where(fluid, np.float32(u_in[a]), np.float32(0)).astype(np.float32) for a in range(3))
+    g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1).astype(np.float64)
+    centre = np.array([n / 2, n / 2, 20.0 * s])
+    r2 = np.sum((g - centre) ** 2, -1)
+    temp = (-1e-3 * g[..., 2] + 0.01 * np.exp(-r2 / (2 * (8.0 * s) ** 2))).astype(np.float32)
+    far = {"kind": VELOCITY, "velocity": u_in}
+    faces = [far, far, {"kind": PERIODIC}, {"kind": PERIODIC}, {"kind": BOUNCE_BACK}, far]
+    return BrickCase("c2-terrain-boussinesq", (n, n, n), obstacle, u, temp, faces, tau, u_in, sgs=True,
+                     smagorinsky_c=0.1, buoyancy=True, buoyancy_beta=1e-4, gravity_axis=2, steps=steps)

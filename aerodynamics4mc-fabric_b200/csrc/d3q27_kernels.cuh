@@ -1,0 +1,75 @@
+// Kernel interface of the FP32 D3Q27 brick step (device buffers only).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "collide27.cuh"
+
+namespace aero {
+
+// Face configuration the pull of one step uses (a snapshot: the pull of call
+// n+1 streams with the faces of call n, as the reference streams at the end of
+// call n).
+struct FaceParams {
+    int kind[6];            // HydroKind per face (x-, x+, y-, y+, z-, z+)
+    float velocity[6][3];   // Dirichlet / moving-wall velocity (lattice units)
+    float pressure[6];      // pressure-Dirichlet proxy (rho - 1)
+    int periodic_mask;      // bit a: axis a wraps (both faces periodic on that side)
+    int wrap_lo[3];         // per axis: the min face wraps
+    int wrap_hi[3];         // per axis: the max face wraps
+    int disable_convective; // INHERIT_GAME faces use bounce-back instead of convective outflow
+    float max_speed;
+};
+
+struct BrickDims {
+    int nx, ny, nz;
+    int pad;
+    long long cells;
+};
+
+// Input channels of the reference packet (native/src/aero_lbm_jni.cpp:64-81).
+constexpr int kChObstacle = 0;
+constexpr int kChFanMask = 1;
+constexpr int kChFanVx = 2;
+constexpr int kChStateVx = 5;
+constexpr int kChStateVy = 6;
+constexpr int kChStateVz = 7;
+constexpr int kChStateP = 8;
+constexpr int kChThermalSource = 9;
+constexpr int kChStateTemp = 10;
+
+struct CellFields {
+    uint8_t* obstacle;    // 1 = solid
+    float* ref_ux;
+    float* ref_uy;
+    float* ref_uz;
+    float* ref_p;         // clamped pressure proxy
+    float* temperature;   // clamped reference temperature (static buoyancy field)
+};
+
+struct ForceField {
+    const float* fx;      // optional per-cell force density (SoA); null = none
+    const float* fy;
+    const float* fz;
+};
+
+// Launch helpers (all asynchronous on `stream`; return the launch error).
+cudaError_t launch_ingest_packet(const float* packet, int in_channels, BrickDims d, CellFields out, cudaStream_t stream);
+cudaError_t launch_build_flags(const uint8_t* obstacle, BrickDims d, FaceParams face, uint32_t* flags, cudaStream_t stream);
+cudaError_t launch_init_collide(BrickDims d, CellFields cur, ForceField force, CollideParams cp, float* g_out,
+                                cudaStream_t stream);
+cudaError_t launch_step_ab(BrickDims d, const float* g_in, float* g_out, const uint32_t* flags_prev,
+                           const uint8_t* obstacle_prev, const float* ref_p_prev, const FaceParams* face_prev,
+                           CellFields cur, ForceField force, CollideParams cp, cudaStream_t stream);
+// Macro output of the streamed state S(g): write_output semantics
+// (AoS, out_channels per cell; ux,uy,uz scaled; clamp(rho - 1)).
+// `face` points to device memory.
+cudaError_t launch_output_ab(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
+                             const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                             float velocity_scale, float* out, cudaStream_t stream);
+
+uint64_t kernel_launch_count();
+void count_launch();
+
+}  // namespace aero

@@ -1,0 +1,926 @@
+// Host runtime of the per-context LBM C ABI: context registry, benchmark /
+// boundary configuration, parameter derivation, step dispatch, output.
+//
+// Behaviour follows the reference runtime (native/src/aero_lbm_jni.cpp):
+// contexts keyed by a caller-chosen long long (jni.cpp:516-611), a process
+// global boundary configuration (jni.cpp:229-489), the effective-parameter
+// rules (jni.cpp:722-1118), init/step/extract entry points (jni.cpp:8592-10368).
+// There is no CPU fallback: every path runs the CUDA kernels and reports
+// failure through aero_lbm_last_error().
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+
+#include "../../include/aero_lbm_b200.h"
+#include "d3q27_kernels.cuh"
+#include "runtime_internal.h"
+
+namespace aero {
+
+// ------------------------------------------------------------------ globals
+namespace {
+
+struct RuntimeConfig {
+    bool initialized = false;
+    int nx = 0, ny = 0, nz = 0;
+    int input_channels = 0, output_channels = 0;
+    std::string runtime_info = "uninitialized";
+};
+
+struct TimingStats {
+    uint64_t ticks = 0;
+    double last_copy = 0, last_solver = 0, last_readback = 0, last_total = 0;
+    double sum_copy = 0, sum_solver = 0, sum_readback = 0, sum_total = 0;
+    uint64_t full_packet_steps = 0, cached_steps = 0;
+};
+
+RuntimeConfig g_cfg;
+std::recursive_mutex g_mutex;  // guards every entry point (the caller is one worker thread)
+std::unordered_map<long long, std::unique_ptr<Context>> g_contexts;
+std::string g_last_error;
+std::string g_timing_text;
+std::string g_bench_text;
+TimingStats g_timing;
+AeroLbmBenchmarkConfig g_bench{};
+bool g_bench_ready = false;
+cudaStream_t g_stream = nullptr;
+bool g_own_stream = false;
+int g_stream_mode = 0;  // 0 auto, 1 two-buffer, 2 in-place
+float g_smagorinsky_c = -1.0f;
+float g_buoyancy_beta_override = -1.0f;
+int g_gravity_axis = -1;
+int g_realtime_solver_mode = AERO_LBM_REALTIME_SOLVER_AUTO;
+
+using Clock = std::chrono::steady_clock;
+double ms_since(Clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+inline float finite_or(float v, float fb) { return std::isfinite(v) ? v : fb; }
+inline float clampf_h(float v, float lo, float hi) { return std::min(hi, std::max(lo, v)); }
+
+// Reference runtime constants (jni.cpp:83-168), evaluated in float.
+constexpr float kCs2 = 1.0f / 3.0f;
+constexpr float kRuntimeMolecularNu0 = 1.50e-5f * (1.0f / 20.0f) / (1.0f * 1.0f);
+constexpr float kNuMin = 1.0e-8f;
+constexpr float kNuMax = (0.95f - 0.5f) / 3.0f;
+constexpr float kTauMinH = 0.5f + 3.0f * 1.0e-8f;
+constexpr float kTauMaxH = 0.95f;
+constexpr float kTauNormalGame = 0.5f + 3.0f * kRuntimeMolecularNu0;
+constexpr float kSgsCDefault = 0.025f;
+constexpr float kSgsNutToNu0Max = 5.0f;
+constexpr float kSgsBulkCoupling = 0.30f;
+constexpr float kBoussinesqBeta = 9.81f * (1.0f / 300.0f) * 20.0f * ((1.0f / 20.0f) * (1.0f / 20.0f) / 1.0f);
+constexpr float kBoussinesqForceMax = 0.02f;
+constexpr float kMaxSpeed = 0.57735026919f * 0.60f;
+constexpr uint32_t kKnownFlags = 0xffu;
+
+AeroLbmBoundaryFaceConfig make_face(int hydro, int thermal) {
+    AeroLbmBoundaryFaceConfig f{};
+    f.hydrodynamic_kind = hydro;
+    f.thermal_kind = thermal;
+    return f;
+}
+
+void set_all_faces(AeroLbmBenchmarkConfig& c, int hydro, int thermal) {
+    c.x_min = c.x_max = c.y_min = c.y_max = c.z_min = c.z_max = make_face(hydro, thermal);
+}
+
+// make_default_benchmark_config (jni.cpp:304-338)
+AeroLbmBenchmarkConfig default_config() {
+    AeroLbmBenchmarkConfig c{};
+    c.abi_version = AERO_LBM_BENCHMARK_ABI_VERSION;
+    c.struct_size = sizeof(AeroLbmBenchmarkConfig);
+    c.flags = AERO_LBM_BENCHMARK_FLAG_DISABLE_FAN_FORCING | AERO_LBM_BENCHMARK_FLAG_DISABLE_FAN_NOISE |
+              AERO_LBM_BENCHMARK_FLAG_DISABLE_SPONGE | AERO_LBM_BENCHMARK_FLAG_DISABLE_OBSTACLE_BOUNCE_BLEND |
+              AERO_LBM_BENCHMARK_FLAG_DISABLE_SGS;
+    c.enabled = 0;
+    c.preset = AERO_LBM_BENCHMARK_PRESET_NONE;
+    c.reynolds_number = 100.0f;
+    c.rayleigh_number = 1.0e5f;
+    c.prandtl_number = 0.71f;
+    c.mach_number = 0.05f;
+    c.reference_density = 1.0f;
+    c.reference_temperature = 0.0f;
+    c.reference_length = 1.0f;
+    c.gravity[1] = -1.0f;
+    set_all_faces(c, AERO_LBM_HYDRO_BOUNDARY_INHERIT_GAME, AERO_LBM_THERMAL_BOUNDARY_INHERIT_GAME);
+    return c;
+}
+
+bool valid_preset(int p) { return p >= AERO_LBM_BENCHMARK_PRESET_NONE && p <= AERO_LBM_BENCHMARK_PRESET_DIFFERENTIALLY_HEATED_CAVITY_3D; }
+bool valid_hydro(int k) { return k >= 0 && k <= 7; }
+bool valid_thermal(int k) { return k >= 0 && k <= 5; }
+
+void sanitize_face(AeroLbmBoundaryFaceConfig& f) {
+    if (!valid_hydro(f.hydrodynamic_kind)) f.hydrodynamic_kind = AERO_LBM_HYDRO_BOUNDARY_INHERIT_GAME;
+    if (!valid_thermal(f.thermal_kind)) f.thermal_kind = AERO_LBM_THERMAL_BOUNDARY_INHERIT_GAME;
+    for (float& v : f.velocity) v = finite_or(v, 0.0f);
+    f.pressure = finite_or(f.pressure, 0.0f);
+    f.temperature = finite_or(f.temperature, 0.0f);
+    f.heat_flux = finite_or(f.heat_flux, 0.0f);
+}
+
+// sanitize_benchmark_config (jni.cpp:408-440)
+void sanitize(AeroLbmBenchmarkConfig& c) {
+    c.abi_version = AERO_LBM_BENCHMARK_ABI_VERSION;
+    c.struct_size = sizeof(AeroLbmBenchmarkConfig);
+    c.flags &= kKnownFlags;
+    c.enabled = c.enabled != 0 ? 1 : 0;
+    if (!valid_preset(c.preset)) c.preset = AERO_LBM_BENCHMARK_PRESET_NONE;
+    c.reynolds_number = finite_or(c.reynolds_number, 100.0f);
+    c.rayleigh_number = finite_or(c.rayleigh_number, 1.0e5f);
+    c.prandtl_number = finite_or(c.prandtl_number, 0.71f);
+    c.mach_number = clampf_h(finite_or(c.mach_number, 0.05f), 1.0e-4f, 0.30f);
+    c.reference_density = finite_or(c.reference_density, 1.0f);
+    c.reference_temperature = finite_or(c.reference_temperature, 0.0f);
+    c.reference_length = std::max(1.0e-6f, finite_or(c.reference_length, 1.0f));
+    for (float& v : c.body_force) v = finite_or(v, 0.0f);
+    c.gravity[0] = finite_or(c.gravity[0], 0.0f);
+    c.gravity[1] = finite_or(c.gravity[1], -1.0f);
+    c.gravity[2] = finite_or(c.gravity[2], 0.0f);
+    for (float& v : c.initial_velocity) v = finite_or(v, 0.0f);
+    c.initial_pressure = finite_or(c.initial_pressure, 0.0f);
+    c.initial_temperature = finite_or(c.initial_temperature, 0.0f);
+    sanitize_face(c.x_min); sanitize_face(c.x_max);
+    sanitize_face(c.y_min); sanitize_face(c.y_max);
+    sanitize_face(c.z_min); sanitize_face(c.z_max);
+}
+
+// apply_benchmark_preset_defaults (jni.cpp:340-407)
+AeroLbmBenchmarkConfig preset_config(int preset) {
+    AeroLbmBenchmarkConfig c = default_config();
+    c.enabled = 1;
+    c.preset = preset;
+    switch (preset) {
+        case AERO_LBM_BENCHMARK_PRESET_TAYLOR_GREEN_3D:
+            c.flags |= AERO_LBM_BENCHMARK_FLAG_DISABLE_CONVECTIVE_OUTFLOW | AERO_LBM_BENCHMARK_FLAG_DISABLE_INTERNAL_THERMAL_SOURCE |
+                       AERO_LBM_BENCHMARK_FLAG_DISABLE_BUOYANCY;
+            set_all_faces(c, AERO_LBM_HYDRO_BOUNDARY_PERIODIC, AERO_LBM_THERMAL_BOUNDARY_DISABLED);
+            break;
+        case AERO_LBM_BENCHMARK_PRESET_LID_DRIVEN_CAVITY_2D:
+        case AERO_LBM_BENCHMARK_PRESET_LID_DRIVEN_CAVITY_3D:
+            c.reynolds_number = 1000.0f;
+            set_all_faces(c, AERO_LBM_HYDRO_BOUNDARY_BOUNCE_BACK, AERO_LBM_THERMAL_BOUNDARY_ADIABATIC);
+            c.y_max = make_face(AERO_LBM_HYDRO_BOUNDARY_MOVING_WALL, AERO_LBM_THERMAL_BOUNDARY_ADIABATIC);
+            c.y_max.velocity[0] = 0.10f;
+            c.flags |= AERO_LBM_BENCHMARK_FLAG_DISABLE_INTERNAL_THERMAL_SOURCE | AERO_LBM_BENCHMARK_FLAG_DISABLE_BUOYANCY;
+            if (preset == AERO_LBM_BENCHMARK_PRESET_LID_DRIVEN_CAVITY_2D) {
+                c.z_min = make_face(AERO_LBM_HYDRO_BOUNDARY_PERIODIC, AERO_LBM_THERMAL_BOUNDARY_PERIODIC);
+                c.z_max = make_face(AERO_LBM_HYDRO_BOUNDARY_PERIODIC, AERO_LBM_THERMAL_BOUNDARY_PERIODIC);
+            }
+            break;
+        case AERO_LBM_BENCHMARK_PRESET_CYLINDER_CROSSFLOW_2D:
+            c.reynolds_number = 100.0f;
+            c.flags |= AERO_LBM_BENCHMARK_FLAG_DISABLE_INTERNAL_THERMAL_SOURCE | AERO_LBM_BENCHMARK_FLAG_DISABLE_BUOYANCY;
+            set_all_faces(c, AERO_LBM_HYDRO_BOUNDARY_BOUNCE_BACK, AERO_LBM_THERMAL_BOUNDARY_DISABLED);
+            c.x_min = make_face(AERO_LBM_HYDRO_BOUNDARY_VELOCITY_DIRICHLET, AERO_LBM_THERMAL_BOUNDARY_DISABLED);
+            c.initial_velocity[0] = 0.08f;
+            c.x_min.velocity[0] = 1.5f * 0.08f;
+            c.x_max = make_face(AERO_LBM_HYDRO_BOUNDARY_CONVECTIVE_OUTFLOW, AERO_LBM_THERMAL_BOUNDARY_DISABLED);
+            c.z_min = make_face(AERO_LBM_HYDRO_BOUNDARY_PERIODIC, AERO_LBM_THERMAL_BOUNDARY_PERIODIC);
+            c.z_max = make_face(AERO_LBM_HYDRO_BOUNDARY_PERIODIC, AERO_LBM_THERMAL_BOUNDARY_PERIODIC);
+            break;
+        case AERO_LBM_BENCHMARK_PRESET_DIFFERENTIALLY_HEATED_CAVITY_2D:
+        case AERO_LBM_BENCHMARK_PRESET_DIFFERENTIALLY_HEATED_CAVITY_3D:
+            c.rayleigh_number = 1.0e5f;
+            c.prandtl_number = 0.71f;
+            c.mach_number = 0.15f;
+            c.flags |= AERO_LBM_BENCHMARK_FLAG_DISABLE_INTERNAL_THERMAL_SOURCE;
+            set_all_faces(c, AERO_LBM_HYDRO_BOUNDARY_BOUNCE_BACK, AERO_LBM_THERMAL_BOUNDARY_ADIABATIC);
+            c.x_min = make_face(AERO_LBM_HYDRO_BOUNDARY_BOUNCE_BACK, AERO_LBM_THERMAL_BOUNDARY_TEMPERATURE_DIRICHLET);
+            c.x_min.temperature = 0.5f;
+            c.x_max = make_face(AERO_LBM_HYDRO_BOUNDARY_BOUNCE_BACK, AERO_LBM_THERMAL_BOUNDARY_TEMPERATURE_DIRICHLET);
+            c.x_max.temperature = -0.5f;
+            if (preset == AERO_LBM_BENCHMARK_PRESET_DIFFERENTIALLY_HEATED_CAVITY_2D) {
+                c.z_min = make_face(AERO_LBM_HYDRO_BOUNDARY_PERIODIC, AERO_LBM_THERMAL_BOUNDARY_PERIODIC);
+                c.z_max = make_face(AERO_LBM_HYDRO_BOUNDARY_PERIODIC, AERO_LBM_THERMAL_BOUNDARY_PERIODIC);
+            }
+            break;
+        default:
+            c.enabled = 0;
+            c.preset = AERO_LBM_BENCHMARK_PRESET_NONE;
+            break;
+    }
+    return c;
+}
+
+void ensure_bench() {
+    if (!g_bench_ready) {
+        g_bench = default_config();
+        g_bench_ready = true;
+    }
+}
+
+bool bench_active() { return g_bench.enabled != 0; }
+bool bench_flag(uint32_t flag) { return bench_active() && (g_bench.flags & flag) != 0; }
+bool heated_cavity() {
+    return bench_active() && (g_bench.preset == AERO_LBM_BENCHMARK_PRESET_DIFFERENTIALLY_HEATED_CAVITY_2D ||
+                              g_bench.preset == AERO_LBM_BENCHMARK_PRESET_DIFFERENTIALLY_HEATED_CAVITY_3D);
+}
+float norm3(const float* v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+const AeroLbmBoundaryFaceConfig& face_cfg(int i) {
+    switch (i) {
+        case 0: return g_bench.x_min;
+        case 1: return g_bench.x_max;
+        case 2: return g_bench.y_min;
+        case 3: return g_bench.y_max;
+        case 4: return g_bench.z_min;
+        default: return g_bench.z_max;
+    }
+}
+
+// benchmark_reference_speed (jni.cpp:831-871)
+float reference_speed() {
+    if (!bench_active()) return 0.0f;
+    if (heated_cavity()) return clampf_h(finite_or(g_bench.mach_number, 0.05f), 1.0e-4f, 0.30f) * std::sqrt(kCs2);
+    if (g_bench.preset == AERO_LBM_BENCHMARK_PRESET_CYLINDER_CROSSFLOW_2D) {
+        const float s = norm3(g_bench.initial_velocity);
+        if (s > 1.0e-8f) return s;
+        return (2.0f / 3.0f) * norm3(g_bench.x_min.velocity);
+    }
+    float s = norm3(g_bench.initial_velocity);
+    for (int i = 0; i < 6; ++i) s = std::max(s, norm3(face_cfg(i).velocity));
+    return s;
+}
+
+float clamp_nu(float nu) { return clampf_h(nu, kNuMin, kNuMax); }
+
+// effective_base_nu_shear (jni.cpp:947-961)
+float base_nu_shear() {
+    if (!bench_active()) return clamp_nu(kRuntimeMolecularNu0);
+    if (heated_cavity()) {
+        const float ra = std::max(1.0e-6f, finite_or(g_bench.rayleigh_number, 1.0e5f));
+        const float pr = std::max(1.0e-6f, finite_or(g_bench.prandtl_number, 0.71f));
+        const float len = std::max(1.0e-6f, finite_or(g_bench.reference_length, 1.0f));
+        return clamp_nu(reference_speed() * len * std::sqrt(pr / ra));
+    }
+    const float re = finite_or(g_bench.reynolds_number, 0.0f);
+    const float sp = reference_speed();
+    const float len = std::max(1.0e-6f, finite_or(g_bench.reference_length, 1.0f));
+    if (re <= 1.0e-6f || sp <= 1.0e-8f) return clamp_nu(kRuntimeMolecularNu0);
+    return clamp_nu(sp * len / re);
+}
+
+float tau_shear_base() { return clampf_h(0.5f + 3.0f * clamp_nu(base_nu_shear()), kTauMinH, kTauMaxH); }
+float tau_normal_base() {
+    if (!bench_active()) return clampf_h(kTauNormalGame, kTauMinH, kTauMaxH);
+    return clampf_h(0.5f + 3.0f * clamp_nu(clamp_nu(base_nu_shear())), kTauMinH, kTauMaxH);
+}
+
+// effective_boussinesq_beta (jni.cpp:1023-1031)
+float boussinesq_beta() {
+    if (g_buoyancy_beta_override >= 0.0f) return g_buoyancy_beta_override;
+    if (!heated_cavity()) return kBoussinesqBeta;
+    const float sp = reference_speed();
+    const float len = std::max(1.0e-6f, finite_or(g_bench.reference_length, 1.0f));
+    float tmin = 1.0e9f, tmax = -1.0e9f;
+    bool any = false;
+    for (int i = 0; i < 6; ++i) {
+        const auto& f = face_cfg(i);
+        if (f.thermal_kind != AERO_LBM_THERMAL_BOUNDARY_TEMPERATURE_DIRICHLET) continue;
+        any = true;
+        tmin = std::min(tmin, f.temperature);
+        tmax = std::max(tmax, f.temperature);
+    }
+    const float span = any ? std::max(1.0e-6f, tmax - tmin) : 1.0f;
+    return (sp * sp) / std::max(1.0e-6f, len * span);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ shared helpers
+std::recursive_mutex& runtime_mutex() { return g_mutex; }
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+const std::string& last_error() { return g_last_error; }
+
+cudaStream_t current_stream() {
+    if (!g_stream) {
+        if (cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking) == cudaSuccess) g_own_stream = true;
+        else g_stream = nullptr;
+    }
+    return g_stream;
+}
+
+bool cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+CollideParams current_collide_params() {
+    ensure_bench();
+    CollideParams p{};
+    p.tau_shear_base = tau_shear_base();
+    p.tau_normal_base = tau_normal_base();
+    p.nu0 = std::max(1e-6f, base_nu_shear());
+    const float c = g_smagorinsky_c >= 0.0f ? g_smagorinsky_c : kSgsCDefault;
+    p.sgs_c2 = c * c;
+    p.sgs_nut_cap = kSgsNutToNu0Max * p.nu0;
+    p.sgs_bulk = kSgsBulkCoupling;
+    p.buoy_beta = boussinesq_beta();
+    p.buoy_fmax = kBoussinesqForceMax;
+    p.body_force[0] = p.body_force[1] = p.body_force[2] = 0.0f;
+    if (bench_active()) {
+        // The reference sanitises but never applies body_force; here it is a
+        // uniform force density on every fluid cell.
+        p.body_force[0] = g_bench.body_force[0];
+        p.body_force[1] = g_bench.body_force[1];
+        p.body_force[2] = g_bench.body_force[2];
+    }
+    p.max_speed = kMaxSpeed;
+    p.enable_sgs = !bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_SGS);
+    p.enable_buoyancy = !bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_BUOYANCY);
+    p.gravity_axis = g_gravity_axis >= 0 ? g_gravity_axis : 1;
+    return p;
+}
+
+FaceParams current_face_params() {
+    ensure_bench();
+    FaceParams f{};
+    for (int i = 0; i < 6; ++i) {
+        const auto& c = face_cfg(i);
+        f.kind[i] = c.hydrodynamic_kind;
+        f.velocity[i][0] = c.velocity[0];
+        f.velocity[i][1] = c.velocity[1];
+        f.velocity[i][2] = c.velocity[2];
+        f.pressure[i] = c.pressure;
+    }
+    for (int a = 0; a < 3; ++a) {
+        f.wrap_lo[a] = f.kind[2 * a] == kHydroPeriodic;
+        f.wrap_hi[a] = f.kind[2 * a + 1] == kHydroPeriodic;
+        if (f.wrap_lo[a] && f.wrap_hi[a]) f.periodic_mask |= 1 << a;
+    }
+    f.disable_convective = bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_CONVECTIVE_OUTFLOW) ? 1 : 0;
+    f.max_speed = kMaxSpeed;
+    return f;
+}
+
+int streaming_mode_setting() { return g_stream_mode; }
+int realtime_solver_mode() { return g_realtime_solver_mode; }
+
+// ------------------------------------------------------------------ contexts
+Context::~Context() { release_device(); }
+
+void Context::release_device() {
+    auto fr = [](void*& p) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    };
+    for (int i = 0; i < 2; ++i) {
+        fr(reinterpret_cast<void*&>(g[i]));
+        fr(reinterpret_cast<void*&>(obstacle[i]));
+        fr(reinterpret_cast<void*&>(ref_p[i]));
+        fr(reinterpret_cast<void*&>(flags[i]));
+        fr(reinterpret_cast<void*&>(d_face[i]));
+    }
+    fr(reinterpret_cast<void*&>(ref_ux));
+    fr(reinterpret_cast<void*&>(ref_uy));
+    fr(reinterpret_cast<void*&>(ref_uz));
+    fr(reinterpret_cast<void*&>(temperature));
+    fr(reinterpret_cast<void*&>(packet));
+    fr(reinterpret_cast<void*&>(out));
+    fr(reinterpret_cast<void*&>(force));
+    packet_cap = out_cap = 0;
+    allocated = false;
+    initialized = false;
+}
+
+bool Context::allocate(int nx_, int ny_, int nz_) {
+    release_device();
+    nx = nx_; ny = ny_; nz = nz_;
+    cells = (long long)nx * ny * nz;
+    const size_t c = (size_t)cells;
+    auto al = [&](void** p, size_t bytes) { return cuda_ok(cudaMalloc(p, bytes), "cudaMalloc"); };
+    bool ok = true;
+    for (int i = 0; i < 2 && ok; ++i) {
+        ok = ok && al(reinterpret_cast<void**>(&g[i]), c * 27 * sizeof(float));
+        ok = ok && al(reinterpret_cast<void**>(&obstacle[i]), c);
+        ok = ok && al(reinterpret_cast<void**>(&ref_p[i]), c * sizeof(float));
+        ok = ok && al(reinterpret_cast<void**>(&flags[i]), c * sizeof(uint32_t));
+        ok = ok && al(reinterpret_cast<void**>(&d_face[i]), sizeof(FaceParams));
+    }
+    ok = ok && al(reinterpret_cast<void**>(&ref_ux), c * sizeof(float));
+    ok = ok && al(reinterpret_cast<void**>(&ref_uy), c * sizeof(float));
+    ok = ok && al(reinterpret_cast<void**>(&ref_uz), c * sizeof(float));
+    ok = ok && al(reinterpret_cast<void**>(&temperature), c * sizeof(float));
+    if (!ok) {
+        release_device();
+        return false;
+    }
+    allocated = true;
+    initialized = false;
+    slot = 0;
+    cur = 0;
+    step_counter = 0;
+    return true;
+}
+
+CellFields Context::fields(int s) const {
+    return CellFields{obstacle[s], ref_ux, ref_uy, ref_uz, ref_p[s], temperature};
+}
+
+ForceField Context::force_field() const {
+    if (!force) return ForceField{nullptr, nullptr, nullptr};
+    return ForceField{force, force + cells, force + 2 * cells};
+}
+
+Context* find_context(long long key) {
+    auto it = g_contexts.find(key);
+    return it == g_contexts.end() ? nullptr : it->second.get();
+}
+
+Context* get_or_create_context(long long key, int nx, int ny, int nz) {
+    auto& slot = g_contexts[key];
+    if (!slot) slot = std::make_unique<Context>();
+    Context* c = slot.get();
+    if (!c->allocated || c->nx != nx || c->ny != ny || c->nz != nz) {
+        if (!c->allocate(nx, ny, nz)) {
+            g_contexts.erase(key);
+            return nullptr;
+        }
+    }
+    return c;
+}
+
+void release_all_contexts() {
+    g_contexts.clear();
+}
+
+const RuntimeView runtime_view() {
+    return RuntimeView{g_cfg.initialized, g_cfg.nx, g_cfg.ny, g_cfg.nz, g_cfg.input_channels, g_cfg.output_channels};
+}
+
+// Build the pull classification of `slot` for faces `face` and keep a device
+// copy of the faces for the kernels that stream with this slot.
+static bool classify(Context& ctx, int slot, const FaceParams& face, const BrickDims& d, cudaStream_t s) {
+    ctx.h_face[slot] = face;
+    if (!cuda_ok(cudaMemcpyAsync(ctx.d_face[slot], &ctx.h_face[slot], sizeof(FaceParams), cudaMemcpyHostToDevice, s),
+                 "upload faces")) return false;
+    return cuda_ok(launch_build_flags(ctx.obstacle[slot], d, face, ctx.flags[slot], s), "build_flags");
+}
+
+// One step of a context. packet may be null (cached step); out may be null.
+bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet) {
+    cudaStream_t s = current_stream();
+    const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
+    const FaceParams face_now = current_face_params();
+    const CollideParams cp = current_collide_params();
+    const int in_ch = g_cfg.input_channels;
+    const bool have_packet = packet != nullptr;
+    if (!have_packet && !ctx.has_inputs) {
+        set_error("cached step requested before any packet was uploaded for this context");
+        return false;
+    }
+
+    int new_slot = ctx.slot;
+    const bool face_changed = std::memcmp(&face_now, &ctx.face_prev, sizeof(FaceParams)) != 0;
+    if (have_packet) {
+        new_slot = ctx.initialized ? 1 - ctx.slot : ctx.slot;
+        const size_t bytes = (size_t)ctx.cells * in_ch * sizeof(float);
+        if (ctx.packet_cap < bytes) {
+            if (ctx.packet) cudaFree(ctx.packet);
+            ctx.packet = nullptr;
+            ctx.packet_cap = 0;
+            if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.packet), bytes), "cudaMalloc(packet)")) return false;
+            ctx.packet_cap = bytes;
+        }
+        if (host_packet) {
+            if (!cuda_ok(cudaMemcpyAsync(ctx.packet, packet, bytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(packet)")) return false;
+        } else {
+            if (!cuda_ok(cudaMemcpyAsync(ctx.packet, packet, bytes, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync(packet)")) return false;
+        }
+        if (!cuda_ok(launch_ingest_packet(ctx.packet, in_ch, d, ctx.fields(new_slot), s), "ingest_packet")) return false;
+        if (!classify(ctx, new_slot, face_now, d, s)) return false;
+        ctx.has_inputs = true;
+    } else if (face_changed && ctx.initialized) {
+        // Same inputs, new faces: rebuild the classification into the other slot.
+        new_slot = 1 - ctx.slot;
+        if (!cuda_ok(cudaMemcpyAsync(ctx.obstacle[new_slot], ctx.obstacle[ctx.slot], (size_t)ctx.cells, cudaMemcpyDeviceToDevice, s), "copy obstacle")) return false;
+        if (!cuda_ok(cudaMemcpyAsync(ctx.ref_p[new_slot], ctx.ref_p[ctx.slot], (size_t)ctx.cells * sizeof(float), cudaMemcpyDeviceToDevice, s), "copy ref_p")) return false;
+        if (!classify(ctx, new_slot, face_now, d, s)) return false;
+    } else if (face_changed) {
+        if (!classify(ctx, new_slot, face_now, d, s)) return false;
+    }
+
+    float* g_next = ctx.g[1 - ctx.cur];
+    if (!ctx.initialized) {
+        if (!cuda_ok(launch_init_collide(d, ctx.fields(new_slot), ctx.force_field(), cp, g_next, s), "init_collide")) return false;
+    } else {
+        if (!cuda_ok(launch_step_ab(d, ctx.g[ctx.cur], g_next, ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
+                                    ctx.d_face[ctx.slot], ctx.fields(new_slot), ctx.force_field(), cp, s),
+                     "step_ab")) return false;
+    }
+    ctx.cur = 1 - ctx.cur;
+    ctx.slot = new_slot;
+    ctx.face_prev = face_now;
+    ctx.initialized = true;
+    ctx.step_counter += 1;
+
+    if (out) return read_output(ctx, 1, g_cfg.output_channels, scale, out);
+    return true;
+}
+
+bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out) {
+    cudaStream_t s = current_stream();
+    const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
+    const int sx = (ctx.nx + stride - 1) / stride, sy = (ctx.ny + stride - 1) / stride, sz = (ctx.nz + stride - 1) / stride;
+    const size_t bytes = (size_t)sx * sy * sz * out_ch * sizeof(float);
+    if (ctx.out_cap < bytes) {
+        if (ctx.out) cudaFree(ctx.out);
+        ctx.out = nullptr;
+        ctx.out_cap = 0;
+        if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.out), bytes), "cudaMalloc(output)")) return false;
+        ctx.out_cap = bytes;
+    }
+    if (!cuda_ok(launch_output_ab(d, ctx.g[ctx.cur], ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
+                                  ctx.d_face[ctx.slot], stride, out_ch, scale, ctx.out, s),
+                 "output")) return false;
+    if (!cuda_ok(cudaMemcpyAsync(host_out, ctx.out, bytes, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(output)")) return false;
+    return cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize(output)");
+}
+
+void record_timing(double copy_ms, double solver_ms, double readback_ms, double total_ms, bool cached) {
+    g_timing.ticks += 1;
+    g_timing.last_copy = copy_ms; g_timing.last_solver = solver_ms;
+    g_timing.last_readback = readback_ms; g_timing.last_total = total_ms;
+    g_timing.sum_copy += copy_ms; g_timing.sum_solver += solver_ms;
+    g_timing.sum_readback += readback_ms; g_timing.sum_total += total_ms;
+    if (cached) g_timing.cached_steps += 1;
+    else g_timing.full_packet_steps += 1;
+}
+
+}  // namespace aero
+
+// ====================================================================== C ABI
+using namespace aero;
+
+namespace {
+
+bool do_init(int nx, int ny, int nz, int in_ch, int out_ch) {
+    release_all_contexts();
+    g_timing = TimingStats{};
+    if (nx <= 0 || ny <= 0 || nz <= 0 || in_ch < 9 || out_ch < 4) {
+        g_cfg = RuntimeConfig{};
+        set_error("aero_lbm_init_rect: invalid dimensions or channel counts");
+        return false;
+    }
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count <= 0) {
+        g_cfg = RuntimeConfig{};
+        set_error("aero_lbm_init_rect: no CUDA device available (this library has no CPU path)");
+        return false;
+    }
+    if (!current_stream()) {
+        g_cfg = RuntimeConfig{};
+        set_error("aero_lbm_init_rect: cudaStreamCreate failed");
+        return false;
+    }
+    g_cfg.initialized = true;
+    g_cfg.nx = nx; g_cfg.ny = ny; g_cfg.nz = nz;
+    g_cfg.input_channels = in_ch;
+    g_cfg.output_channels = out_ch;
+    cudaDeviceProp prop{};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaGetDeviceProperties(&prop, dev);
+    g_cfg.runtime_info = std::string("cuda|cumulant-d3q27+sgs+bouss:") + prop.name;
+    return true;
+}
+
+bool step_impl(const float* packet, int nx, int ny, int nz, long long key, float* out, float scale, bool cached) {
+    const auto t0 = Clock::now();
+    clear_error();
+    if (!g_cfg.initialized) {
+        set_error("native_step_raw_dims: runtime not initialized");
+        return false;
+    }
+    if (!cached && !packet) {
+        set_error("native_step_raw_dims: missing packet");
+        return false;
+    }
+    if (nx <= 0 || ny <= 0 || nz <= 0) {
+        set_error("native_step_raw_dims: invalid dimensions");
+        return false;
+    }
+    if (!std::isfinite(scale)) scale = 1.0f;
+    Context* ctx = cached ? find_context(key) : get_or_create_context(key, nx, ny, nz);
+    if (!ctx) {
+        if (g_last_error.empty()) {
+            set_error(cached ? "cached solver step requested before context initialization"
+                             : "native_step_raw_dims: failed to allocate or acquire context");
+        }
+        return false;
+    }
+    if (cached && (ctx->nx != nx || ctx->ny != ny || ctx->nz != nz)) {
+        set_error("cached solver step: dimensions differ from the resident context");
+        return false;
+    }
+    const bool ok = step_context(*ctx, cached ? nullptr : packet, out, scale, true);
+    if (!ok && g_last_error.empty()) set_error("native_step_raw_dims: step failed");
+    record_timing(0.0, 0.0, 0.0, ms_since(t0), cached);
+    return ok;
+}
+
+}  // namespace
+
+extern "C" {
+
+AERO_LBM_B200_EXPORT int aero_lbm_init_rect(int nx, int ny, int nz, int input_channels, int output_channels) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    ensure_bench();
+    return do_init(nx, ny, nz, input_channels, output_channels) ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_init(int grid_size, int input_channels, int output_channels) {
+    return aero_lbm_init_rect(grid_size, grid_size, grid_size, input_channels, output_channels);
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect(const float* packet, int nx, int ny, int nz, long long key, float* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    return step_impl(packet, nx, ny, nz, key, out, 1.0f, false) ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect_scaled(const float* packet, int nx, int ny, int nz, long long key, float scale,
+                                                   float* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    return step_impl(packet, nx, ny, nz, key, out, scale, false) ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_step(const float* packet, int grid_size, long long key, float* out) {
+    return aero_lbm_step_rect(packet, grid_size, grid_size, grid_size, key, out);
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect_cached(int nx, int ny, int nz, long long key, float* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    return step_impl(nullptr, nx, ny, nz, key, out, 1.0f, true) ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect_cached_scaled(int nx, int ny, int nz, long long key, float scale, float* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    return step_impl(nullptr, nx, ny, nz, key, out, scale, true) ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_has_context(long long key) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    return find_context(key) ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_context_realtime_cached_initialized(long long key) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    Context* c = find_context(key);
+    return (c && c->initialized) ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_extract_flow_atlas_rect(int nx, int ny, int nz, long long key, int stride, float* out,
+                                                          int value_count) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_cfg.initialized || !out || stride <= 0 || nx <= 0 || ny <= 0 || nz <= 0) {
+        set_error("extract_flow_atlas: invalid arguments or runtime not initialized");
+        return 0;
+    }
+    const long long sx = (nx + stride - 1) / stride, sy = (ny + stride - 1) / stride, sz = (nz + stride - 1) / stride;
+    if (sx * sy * sz <= 0 || (long long)value_count != sx * sy * sz * 4) {
+        set_error("extract_flow_atlas: value_count does not match the atlas size");
+        return 0;
+    }
+    Context* c = find_context(key);
+    if (!c || !c->initialized || c->nx != nx || c->ny != ny || c->nz != nz) {
+        set_error("extract_flow_atlas: no initialized context of these dimensions");
+        return 0;
+    }
+    return read_output(*c, stride, 4, 1.0f, out) ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_get_flow_state_rect(int nx, int ny, int nz, long long key, float* out) {
+    if (nx <= 0 || ny <= 0 || nz <= 0) return 0;
+    const long long v = (long long)nx * ny * nz * 4;
+    if (v > 0x7fffffffLL) return 0;
+    return aero_lbm_extract_flow_atlas_rect(nx, ny, nz, key, 1, out, (int)v);
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_get_temperature_state_rect(int nx, int ny, int nz, long long key, float* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    Context* c = find_context(key);
+    if (!c || !out || !c->has_inputs || c->nx != nx || c->ny != ny || c->nz != nz) {
+        set_error("get_temperature_state: no context of these dimensions");
+        return 0;
+    }
+    cudaStream_t s = current_stream();
+    if (!cuda_ok(cudaMemcpyAsync(out, c->temperature, (size_t)c->cells * sizeof(float), cudaMemcpyDeviceToHost, s), "copy temperature")) return 0;
+    return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_set_temperature_state_rect(int nx, int ny, int nz, long long key, const float* t) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    Context* c = find_context(key);
+    if (!c || !t || c->nx != nx || c->ny != ny || c->nz != nz) {
+        set_error("set_temperature_state: no context of these dimensions");
+        return 0;
+    }
+    std::unique_ptr<float[]> tmp(new float[(size_t)c->cells]);
+    for (long long i = 0; i < c->cells; ++i) tmp[i] = clampf_h(t[i], -1.0f, 1.0f);
+    cudaStream_t s = current_stream();
+    if (!cuda_ok(cudaMemcpyAsync(c->temperature, tmp.get(), (size_t)c->cells * sizeof(float), cudaMemcpyHostToDevice, s), "copy temperature")) return 0;
+    return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_release_context(long long key) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    g_contexts.erase(key);
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_shutdown(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    release_all_contexts();
+    g_cfg = RuntimeConfig{};
+    g_timing = TimingStats{};
+}
+
+AERO_LBM_B200_EXPORT const char* aero_lbm_runtime_info(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    return g_cfg.runtime_info.c_str();
+}
+
+AERO_LBM_B200_EXPORT const char* aero_lbm_last_error(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    return g_last_error.c_str();
+}
+
+AERO_LBM_B200_EXPORT const char* aero_lbm_timing_info(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (g_timing.ticks == 0) {
+        g_timing_text = "ticks=0";
+        return g_timing_text.c_str();
+    }
+    const double inv = 1.0 / double(g_timing.ticks);
+    std::ostringstream o;
+    o.setf(std::ios::fixed);
+    o.precision(3);
+    o << "ticks=" << g_timing.ticks << " path=cuda last_ms(total=" << g_timing.last_total << ")"
+      << " avg_ms(total=" << g_timing.sum_total * inv << ")"
+      << " steps(full_packet=" << g_timing.full_packet_steps << ",cached=" << g_timing.cached_steps << ")"
+      << " launches=" << kernel_launch_count();
+    g_timing_text = o.str();
+    return g_timing_text.c_str();
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_reset_timing(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    g_timing = TimingStats{};
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_set_realtime_solver_mode(int mode) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    g_realtime_solver_mode = (mode >= 0 && mode <= 3) ? mode : AERO_LBM_REALTIME_SOLVER_AUTO;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_finish(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_stream) return 1;
+    return cuda_ok(cudaStreamSynchronize(g_stream), "aero_lbm_finish") ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_get_timing_snapshot(AeroLbmTimingSnapshot* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (!out) return 0;
+    AeroLbmTimingSnapshot s{};
+    s.ticks = g_timing.ticks;
+    s.last_payload_copy_ms = g_timing.last_copy;
+    s.last_solver_ms = g_timing.last_solver;
+    s.last_readback_ms = g_timing.last_readback;
+    s.last_total_ms = g_timing.last_total;
+    if (g_timing.ticks) {
+        const double inv = 1.0 / double(g_timing.ticks);
+        s.avg_payload_copy_ms = g_timing.sum_copy * inv;
+        s.avg_solver_ms = g_timing.sum_solver * inv;
+        s.avg_readback_ms = g_timing.sum_readback * inv;
+        s.avg_total_ms = g_timing.sum_total * inv;
+    }
+    *out = s;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_benchmark_default_config(AeroLbmBenchmarkConfig* out) {
+    if (out) *out = default_config();
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_benchmark_default_preset_config(int preset, AeroLbmBenchmarkConfig* out) {
+    if (!out || !valid_preset(preset)) return 0;
+    *out = preset_config(preset);
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_benchmark_set_config(const AeroLbmBenchmarkConfig* config) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (!config) return 0;
+    AeroLbmBenchmarkConfig c = *config;
+    sanitize(c);
+    g_bench = c;
+    g_bench_ready = true;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_benchmark_get_config(AeroLbmBenchmarkConfig* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (!out) return 0;
+    ensure_bench();
+    *out = g_bench;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_benchmark_reset_config(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    g_bench = default_config();
+    g_bench_ready = true;
+}
+
+AERO_LBM_B200_EXPORT const char* aero_lbm_benchmark_info(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    ensure_bench();
+    std::ostringstream o;
+    o << "enabled=" << g_bench.enabled << " preset=" << g_bench.preset << " flags=0x" << std::hex << g_bench.flags << std::dec
+      << " Re=" << g_bench.reynolds_number << " tau_shear=" << tau_shear_base() << " tau_normal=" << tau_normal_base();
+    g_bench_text = o.str();
+    return g_bench_text.c_str();
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_b200_set_stream(void* stream) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (g_own_stream && g_stream) cudaStreamDestroy(g_stream);
+    g_own_stream = false;
+    g_stream = static_cast<cudaStream_t>(stream);
+    if (!g_stream) current_stream();
+}
+
+AERO_LBM_B200_EXPORT unsigned long long aero_lbm_b200_launch_count(void) { return kernel_launch_count(); }
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_advance_rect(long long key, int steps) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (steps < 0) {
+        set_error("advance_rect: negative step count");
+        return 0;
+    }
+    Context* c = find_context(key);
+    if (!c || !c->has_inputs) {
+        set_error("advance_rect: context has no resident inputs");
+        return 0;
+    }
+    for (int i = 0; i < steps; ++i)
+        if (!step_context(*c, nullptr, nullptr, 1.0f, true)) return 0;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streaming_mode(int mode) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (mode < 0 || mode > 2) return 0;
+    g_stream_mode = mode;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_force_field(long long key, const float* force_soa, int value_count) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    Context* c = find_context(key);
+    if (!c) {
+        set_error("set_force_field: unknown context");
+        return 0;
+    }
+    if (!force_soa) {
+        if (c->force) cudaFree(c->force);
+        c->force = nullptr;
+        return 1;
+    }
+    if ((long long)value_count != 3 * c->cells) {
+        set_error("set_force_field: value_count must be 3 * cells");
+        return 0;
+    }
+    if (!c->force && !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&c->force), (size_t)c->cells * 3 * sizeof(float)), "cudaMalloc(force)")) return 0;
+    cudaStream_t s = current_stream();
+    if (!cuda_ok(cudaMemcpyAsync(c->force, force_soa, (size_t)c->cells * 3 * sizeof(float), cudaMemcpyHostToDevice, s), "copy force")) return 0;
+    return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_b200_set_physics_overrides(float smagorinsky_c, float buoyancy_beta, int gravity_axis) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    g_smagorinsky_c = std::isfinite(smagorinsky_c) ? smagorinsky_c : -1.0f;
+    g_buoyancy_beta_override = std::isfinite(buoyancy_beta) ? buoyancy_beta : -1.0f;
+    g_gravity_axis = (gravity_axis >= 0 && gravity_axis <= 2) ? gravity_axis : -1;
+}
+
+}  // extern "C"

@@ -1,0 +1,80 @@
+// Internal interface between the runtime translation units.
+#pragma once
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "d3q27_kernels.cuh"
+
+namespace aero {
+
+// Device state of one context (one brick / grid).
+//
+// g[cur] holds the post-collision populations of the last call. obstacle,
+// ref_p and flags are double-buffered: index `slot` holds the inputs and pull
+// classification of the last call, which the next call's fused kernel streams
+// with (the reference streams at the end of each call with that call's mask).
+struct Context {
+    int nx = 0, ny = 0, nz = 0;
+    long long cells = 0;
+    float* g[2] = {nullptr, nullptr};
+    uint8_t* obstacle[2] = {nullptr, nullptr};
+    float* ref_p[2] = {nullptr, nullptr};
+    uint32_t* flags[2] = {nullptr, nullptr};
+    FaceParams* d_face[2] = {nullptr, nullptr};  // device copy of the faces each slot was classified with
+    float* ref_ux = nullptr;
+    float* ref_uy = nullptr;
+    float* ref_uz = nullptr;
+    float* temperature = nullptr;
+    float* packet = nullptr;
+    size_t packet_cap = 0;
+    float* out = nullptr;
+    size_t out_cap = 0;
+    float* force = nullptr;  // optional per-cell force density, SoA (3 * cells)
+    FaceParams face_prev{};
+    FaceParams h_face[2]{};  // host copies (source of the async uploads; must outlive them)
+    int cur = 0;
+    int slot = 0;
+    bool allocated = false;
+    bool initialized = false;
+    bool has_inputs = false;
+    uint64_t step_counter = 0;
+
+    Context() = default;
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
+    ~Context();
+    bool allocate(int nx, int ny, int nz);
+    void release_device();
+    CellFields fields(int s) const;
+    ForceField force_field() const;
+};
+
+struct RuntimeView {
+    bool initialized;
+    int nx, ny, nz;
+    int input_channels, output_channels;
+};
+
+std::recursive_mutex& runtime_mutex();
+void set_error(const std::string& msg);
+void clear_error();
+const std::string& last_error();
+cudaStream_t current_stream();
+bool cuda_ok(cudaError_t e, const char* what);
+CollideParams current_collide_params();
+FaceParams current_face_params();
+int streaming_mode_setting();
+int realtime_solver_mode();
+
+Context* find_context(long long key);
+Context* get_or_create_context(long long key, int nx, int ny, int nz);
+void release_all_contexts();
+const RuntimeView runtime_view();
+bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet);
+bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out);
+
+}  // namespace aero

@@ -1,0 +1,290 @@
+/*
+ * aero_lbm_b200 — C ABI of the B200 (sm_100a) lattice-Boltzmann brick step.
+ *
+ * This header is the drop-in boundary: the entry points below carry the same
+ * names, argument meaning, return convention (1 = ok, 0 = error, message via
+ * *_last_error) and struct layouts as the reference library's C ABI, so the
+ * reference's Java JNI layer, its ctypes tools and its brick runtime can bind
+ * this library instead. Each declaration names the reference interface it
+ * replaces as file:line in the reference project.
+ *
+ * Entry points prefixed aero_lbm_b200_* have no reference counterpart; they
+ * expose the device-resident paths (batched bricks, FP16 storage, stream
+ * selection, conservation sums) that the reference does not have.
+ *
+ * Struct layouts must stay byte-identical to the reference's
+ * (native/include/aero_lbm_capi.h:15-111, native/include/aero_solver_capi.h:12-56).
+ */
+#ifndef AERO_LBM_B200_H
+#define AERO_LBM_B200_H
+
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define AERO_LBM_B200_EXPORT __declspec(dllexport)
+#else
+#define AERO_LBM_B200_EXPORT __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enums and structs (native/include/aero_lbm_capi.h:15-111) ---- */
+enum {
+    AERO_LBM_BENCHMARK_ABI_VERSION = 1,
+    AERO_LBM_MESOSCALE_ABI_VERSION = 3,
+    AERO_LBM_SIMULATION_ABI_VERSION = 1,
+    AERO_LBM_MESOSCALE_FORCING_CHANNELS = 25,
+    AERO_LBM_MESOSCALE_STATE_CHANNELS = 6,
+    AERO_LBM_SIMULATION_FLOW_STATE_CHANNELS = 4,
+    AERO_LBM_SIMULATION_PACKED_ATLAS_CHANNELS = 4,
+    AERO_LBM_SIMULATION_PLAYER_PROBE_CHANNELS = 6,
+    AERO_LBM_SIMULATION_BRICK_RUNTIME_STATUS_FIELDS = 8
+};
+
+enum {
+    AERO_LBM_REALTIME_SOLVER_AUTO = 0,
+    AERO_LBM_REALTIME_SOLVER_CLASSIC_D3Q27 = 1,
+    AERO_LBM_REALTIME_SOLVER_COMPACT_EXPERIMENTAL = 2,
+    AERO_LBM_REALTIME_SOLVER_D3Q27_FP16_INPLACE_EXPERIMENTAL = 3
+};
+
+typedef enum AeroLbmBenchmarkPreset {
+    AERO_LBM_BENCHMARK_PRESET_NONE = 0,
+    AERO_LBM_BENCHMARK_PRESET_TAYLOR_GREEN_3D = 1,
+    AERO_LBM_BENCHMARK_PRESET_LID_DRIVEN_CAVITY_2D = 2,
+    AERO_LBM_BENCHMARK_PRESET_LID_DRIVEN_CAVITY_3D = 3,
+    AERO_LBM_BENCHMARK_PRESET_CYLINDER_CROSSFLOW_2D = 4,
+    AERO_LBM_BENCHMARK_PRESET_DIFFERENTIALLY_HEATED_CAVITY_2D = 5,
+    AERO_LBM_BENCHMARK_PRESET_DIFFERENTIALLY_HEATED_CAVITY_3D = 6
+} AeroLbmBenchmarkPreset;
+
+typedef enum AeroLbmHydrodynamicBoundaryKind {
+    AERO_LBM_HYDRO_BOUNDARY_INHERIT_GAME = 0,
+    AERO_LBM_HYDRO_BOUNDARY_PERIODIC = 1,
+    AERO_LBM_HYDRO_BOUNDARY_BOUNCE_BACK = 2,
+    AERO_LBM_HYDRO_BOUNDARY_MOVING_WALL = 3,
+    AERO_LBM_HYDRO_BOUNDARY_VELOCITY_DIRICHLET = 4,
+    AERO_LBM_HYDRO_BOUNDARY_PRESSURE_DIRICHLET = 5,
+    AERO_LBM_HYDRO_BOUNDARY_CONVECTIVE_OUTFLOW = 6,
+    AERO_LBM_HYDRO_BOUNDARY_SYMMETRY = 7
+} AeroLbmHydrodynamicBoundaryKind;
+
+typedef enum AeroLbmThermalBoundaryKind {
+    AERO_LBM_THERMAL_BOUNDARY_INHERIT_GAME = 0,
+    AERO_LBM_THERMAL_BOUNDARY_DISABLED = 1,
+    AERO_LBM_THERMAL_BOUNDARY_PERIODIC = 2,
+    AERO_LBM_THERMAL_BOUNDARY_ADIABATIC = 3,
+    AERO_LBM_THERMAL_BOUNDARY_TEMPERATURE_DIRICHLET = 4,
+    AERO_LBM_THERMAL_BOUNDARY_HEAT_FLUX_NEUMANN = 5
+} AeroLbmThermalBoundaryKind;
+
+typedef enum AeroLbmBenchmarkFlags {
+    AERO_LBM_BENCHMARK_FLAG_DISABLE_FAN_FORCING = 1u << 0,
+    AERO_LBM_BENCHMARK_FLAG_DISABLE_FAN_NOISE = 1u << 1,
+    AERO_LBM_BENCHMARK_FLAG_DISABLE_SPONGE = 1u << 2,
+    AERO_LBM_BENCHMARK_FLAG_DISABLE_CONVECTIVE_OUTFLOW = 1u << 3,
+    AERO_LBM_BENCHMARK_FLAG_DISABLE_OBSTACLE_BOUNCE_BLEND = 1u << 4,
+    AERO_LBM_BENCHMARK_FLAG_DISABLE_SGS = 1u << 5,
+    AERO_LBM_BENCHMARK_FLAG_DISABLE_INTERNAL_THERMAL_SOURCE = 1u << 6,
+    AERO_LBM_BENCHMARK_FLAG_DISABLE_BUOYANCY = 1u << 7
+} AeroLbmBenchmarkFlags;
+
+typedef struct AeroLbmBoundaryFaceConfig {
+    int hydrodynamic_kind;
+    int thermal_kind;
+    float velocity[3];
+    float pressure;
+    float temperature;
+    float heat_flux;
+} AeroLbmBoundaryFaceConfig;
+
+typedef struct AeroLbmBenchmarkConfig {
+    uint32_t abi_version;
+    uint32_t struct_size;
+    uint32_t flags;
+    int enabled;
+    int preset;
+    int reserved0;
+    float reynolds_number;
+    float rayleigh_number;
+    float prandtl_number;
+    float mach_number;
+    float reference_density;
+    float reference_temperature;
+    float reference_length;
+    float body_force[3];
+    float gravity[3];
+    float initial_velocity[3];
+    float initial_pressure;
+    float initial_temperature;
+    AeroLbmBoundaryFaceConfig x_min;
+    AeroLbmBoundaryFaceConfig x_max;
+    AeroLbmBoundaryFaceConfig y_min;
+    AeroLbmBoundaryFaceConfig y_max;
+    AeroLbmBoundaryFaceConfig z_min;
+    AeroLbmBoundaryFaceConfig z_max;
+    uint32_t reserved[8];
+} AeroLbmBenchmarkConfig;
+
+typedef struct AeroLbmTimingSnapshot {
+    uint64_t ticks;
+    double last_payload_copy_ms;
+    double last_solver_ms;
+    double last_readback_ms;
+    double last_total_ms;
+    double avg_payload_copy_ms;
+    double avg_solver_ms;
+    double avg_readback_ms;
+    double avg_total_ms;
+} AeroLbmTimingSnapshot;
+
+/* ---- per-context LBM ABI (native/include/aero_lbm_capi.h:166-302) ---- */
+
+/* native/include/aero_lbm_capi.h:166 (jni.cpp:8625) — square grid init. */
+AERO_LBM_B200_EXPORT int aero_lbm_init(int grid_size, int input_channels, int output_channels);
+/* native/include/aero_lbm_capi.h:167 — square-grid step. */
+AERO_LBM_B200_EXPORT int aero_lbm_step(const float* packet, int grid_size, long long context_key, float* output_flow);
+/* native/include/aero_lbm_capi.h:168 (jni.cpp:8592-8624) — global reset of all contexts,
+ * input_channels >= 9, output_channels >= 4. */
+AERO_LBM_B200_EXPORT int aero_lbm_init_rect(int nx, int ny, int nz, int input_channels, int output_channels);
+/* native/include/aero_lbm_capi.h:169 (jni.cpp:8630-8684) — one step from an AoS packet
+ * (input_channels floats per cell, cell = (x*ny+y)*nz+z); output_flow may be null. */
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect(const float* packet, int nx, int ny, int nz, long long context_key, float* output_flow);
+/* native/include/aero_lbm_capi.h:170 — as step_rect, output velocity scaled. */
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect_scaled(const float* packet, int nx, int ny, int nz, long long context_key,
+                                                   float output_velocity_scale, float* output_flow);
+/* native/include/aero_lbm_capi.h:171 (jni.cpp:8534-8582) — step with the resident packet. */
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect_cached(int nx, int ny, int nz, long long context_key, float* output_flow);
+/* native/include/aero_lbm_capi.h:172 */
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect_cached_scaled(int nx, int ny, int nz, long long context_key,
+                                                          float output_velocity_scale, float* output_flow);
+/* native/include/aero_lbm_capi.h:218 */
+AERO_LBM_B200_EXPORT int aero_lbm_has_context(long long context_key);
+/* native/include/aero_lbm_capi.h:220 */
+AERO_LBM_B200_EXPORT int aero_lbm_context_realtime_cached_initialized(long long context_key);
+/* native/include/aero_lbm_capi.h:241 */
+AERO_LBM_B200_EXPORT int aero_lbm_get_temperature_state_rect(int nx, int ny, int nz, long long context_key, float* out_temperature);
+/* native/include/aero_lbm_capi.h:262 (jni.cpp:9246-9450) — sample every stride cells
+ * (min(n-1, a*stride)), 4 floats per atlas cell; value_count must equal ceil(n/stride)^3*4. */
+AERO_LBM_B200_EXPORT int aero_lbm_extract_flow_atlas_rect(int nx, int ny, int nz, long long context_key, int stride,
+                                                          float* out_flow_atlas, int value_count);
+/* native/include/aero_lbm_capi.h:285 (jni.cpp:9528) — stride-1 flow state, 4 floats per cell. */
+AERO_LBM_B200_EXPORT int aero_lbm_get_flow_state_rect(int nx, int ny, int nz, long long context_key, float* out_flow);
+/* native/include/aero_lbm_capi.h:286 */
+AERO_LBM_B200_EXPORT int aero_lbm_set_temperature_state_rect(int nx, int ny, int nz, long long context_key, const float* temperature);
+/* native/include/aero_lbm_capi.h:288 */
+AERO_LBM_B200_EXPORT void aero_lbm_release_context(long long context_key);
+/* native/include/aero_lbm_capi.h:289 */
+AERO_LBM_B200_EXPORT void aero_lbm_shutdown(void);
+/* native/include/aero_lbm_capi.h:290-292 */
+AERO_LBM_B200_EXPORT const char* aero_lbm_runtime_info(void);
+AERO_LBM_B200_EXPORT const char* aero_lbm_last_error(void);
+AERO_LBM_B200_EXPORT const char* aero_lbm_timing_info(void);
+/* native/include/aero_lbm_capi.h:294 */
+AERO_LBM_B200_EXPORT void aero_lbm_reset_timing(void);
+/* native/include/aero_lbm_capi.h:295 */
+AERO_LBM_B200_EXPORT void aero_lbm_set_realtime_solver_mode(int solver_mode);
+/* native/include/aero_lbm_capi.h:296 — waits for all queued device work. */
+AERO_LBM_B200_EXPORT int aero_lbm_finish(void);
+/* native/include/aero_lbm_capi.h:297 */
+AERO_LBM_B200_EXPORT int aero_lbm_get_timing_snapshot(AeroLbmTimingSnapshot* out_snapshot);
+
+/* ---- benchmark/boundary configuration (native/include/aero_lbm_capi.h:698-703) ---- */
+AERO_LBM_B200_EXPORT void aero_lbm_benchmark_default_config(AeroLbmBenchmarkConfig* out_config);
+AERO_LBM_B200_EXPORT int aero_lbm_benchmark_default_preset_config(int preset, AeroLbmBenchmarkConfig* out_config);
+AERO_LBM_B200_EXPORT int aero_lbm_benchmark_set_config(const AeroLbmBenchmarkConfig* config);
+AERO_LBM_B200_EXPORT int aero_lbm_benchmark_get_config(AeroLbmBenchmarkConfig* out_config);
+AERO_LBM_B200_EXPORT void aero_lbm_benchmark_reset_config(void);
+AERO_LBM_B200_EXPORT const char* aero_lbm_benchmark_info(void);
+
+/* ---- device-resident extensions (no reference counterpart) ---- */
+
+/* Queue all kernels of this library on `stream` (a cudaStream_t; null = the
+ * library's own stream). */
+AERO_LBM_B200_EXPORT void aero_lbm_b200_set_stream(void* stream);
+/* Number of kernels this library has launched since load. */
+AERO_LBM_B200_EXPORT unsigned long long aero_lbm_b200_launch_count(void);
+/* Advance a context `steps` times with its resident inputs, no host copies and
+ * no synchronisation (the device-resident form of step_rect_cached). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_advance_rect(long long context_key, int steps);
+/* Select the streaming scheme of a context: 0 automatic (in-place when every
+ * face is local), 1 two-buffer pull, 2 in-place esoteric pull. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streaming_mode(int mode);
+/* Per-cell force density field for a context (3 x cells floats, SoA order
+ * fx[cells], fy[cells], fz[cells]; host pointer; null clears). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_force_field(long long context_key, const float* force_soa, int value_count);
+/* Smagorinsky constant C (reference hard-codes 0.025) and buoyancy
+ * coefficient/axis (reference: beta from its runtime constants, +y). A
+ * negative value keeps the reference default. */
+AERO_LBM_B200_EXPORT void aero_lbm_b200_set_physics_overrides(float smagorinsky_c, float buoyancy_beta, int gravity_axis);
+
+/* ---- wind-tunnel ABI (native/include/aero_solver_capi.h:1-115) ---- */
+enum {
+    AERO_SOLVER_ABI_VERSION = 1,
+    AERO_SOLVER_FLOW_CHANNELS = 4,
+    AERO_SOLVER_STATUS_OK = 1,
+    AERO_SOLVER_STATUS_ERROR = 0
+};
+
+typedef enum AeroSolverBoundaryMode {
+    AERO_SOLVER_BOUNDARY_WIND_TUNNEL = 1,
+    AERO_SOLVER_BOUNDARY_WIND_TUNNEL_PRESSURE_OUTLET = 2,
+    AERO_SOLVER_BOUNDARY_CLOSED = 3,
+    AERO_SOLVER_BOUNDARY_PERIODIC = 4
+} AeroSolverBoundaryMode;
+
+typedef struct AeroGridDesc {
+    int nx;
+    int ny;
+    int nz;
+    float dx;
+    float dt;
+} AeroGridDesc;
+
+typedef struct AeroBoundaryDesc {
+    int mode;
+    float inlet_vx;
+    float inlet_vy;
+    float inlet_vz;
+    float outlet_pressure;
+    float density;
+    float viscosity;
+} AeroBoundaryDesc;
+
+typedef struct AeroStepInput {
+    const uint8_t* solid_mask;
+    const float* prev_flow;
+    AeroGridDesc grid;
+    AeroBoundaryDesc boundary;
+    int steps;
+} AeroStepInput;
+
+typedef struct AeroStepOutput {
+    float* flow_out;
+    float max_velocity;
+    int status;
+} AeroStepOutput;
+
+/* native/include/aero_solver_capi.h:58-109 (aero_solver_capi.cpp:333-587) */
+AERO_LBM_B200_EXPORT void aero_solver_default_grid(AeroGridDesc* out_grid);
+AERO_LBM_B200_EXPORT void aero_solver_default_boundary(AeroBoundaryDesc* out_boundary);
+AERO_LBM_B200_EXPORT int aero_solver_create(int nx, int ny, int nz, float dx, float dt, long long* out_handle);
+AERO_LBM_B200_EXPORT int aero_solver_create_with_grid(const AeroGridDesc* grid, long long* out_handle);
+AERO_LBM_B200_EXPORT int aero_solver_set_solid_mask(long long handle, const uint8_t* solid_mask, int cell_count);
+AERO_LBM_B200_EXPORT int aero_solver_set_flow_state(long long handle, const float* flow, int value_count);
+AERO_LBM_B200_EXPORT int aero_solver_step_wind_tunnel(long long handle, const AeroBoundaryDesc* boundary, int steps,
+                                                      float* out_flow, int out_value_count);
+AERO_LBM_B200_EXPORT int aero_solver_advance_wind_tunnel(long long handle, const AeroBoundaryDesc* boundary, int steps);
+AERO_LBM_B200_EXPORT int aero_solver_run_wind_tunnel(const AeroStepInput* input, AeroStepOutput* output);
+AERO_LBM_B200_EXPORT void aero_solver_destroy(long long handle);
+AERO_LBM_B200_EXPORT const char* aero_solver_last_error(void);
+AERO_LBM_B200_EXPORT const char* aero_solver_runtime_info(void);
+AERO_LBM_B200_EXPORT int aero_solver_finish(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

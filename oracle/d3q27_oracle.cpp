@@ -1,0 +1,688 @@
+// ORACLE — test infrastructure only. Not part of the product.
+//
+// CPU restatement of the reference's D3Q27 cumulant LBM step (benchmark mode),
+// templated on the arithmetic type so that the float instantiation reproduces
+// the reference CPU step operation-for-operation (pinned bit-exact against the
+// reference library built from its own sources into oracle/_ref) and the double
+// instantiation is the FP64 run of the same scheme.
+//
+// It follows, in order:
+//   lattice tables          native/include/aero_lbm_hydro_core.h:7-90
+//   equilibrium             native/src/aero_lbm_hydro_core.cpp:48-52
+//   Guo source              native/src/aero_lbm_jni.cpp:1270-1281
+//   moment transforms       native/src/aero_lbm_jni.cpp:1335-1473
+//   bounce/boundary values  native/src/aero_lbm_jni.cpp:1475-1602
+//   payload ingest          native/src/aero_lbm_jni.cpp:1671-1694
+//   initialisation          native/src/aero_lbm_jni.cpp:1752-1781
+//   collide                 native/src/aero_lbm_jni.cpp:2209-2413
+//   stream_and_bounce       native/src/aero_lbm_jni.cpp:2415-2452
+//   write_output            native/src/aero_lbm_jni.cpp:2535-2581
+//   strided atlas extract   native/src/aero_lbm_jni.cpp:9246-9450
+//
+// Knobs the reference hard-codes are parameters here (Smagorinsky constant,
+// buoyancy coefficient and axis, a uniform or per-cell body force); with the
+// reference's values they reduce to the reference step. Temperature is a
+// static per-cell field (the reference's scalar transport is not restated).
+//
+// Driven from Python with ctypes (tests/ and bench.py's CPU baseline only).
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+namespace {
+
+enum FaceKind {
+    kInheritGame = 0,
+    kPeriodic = 1,
+    kBounceBack = 2,
+    kMovingWall = 3,
+    kVelocityDirichlet = 4,
+    kPressureDirichlet = 5,
+    kConvectiveOutflow = 6,
+    kSymmetry = 7,
+};
+
+}  // namespace
+
+extern "C" {
+
+// Parameters of one oracle context; doubles so that both instantiations
+// receive the same values (the float one narrows them).
+typedef struct OracleD3Q27Params {
+    double tau_shear;          // effective base shear tau
+    double tau_normal;         // effective base normal tau
+    double nu0;                // SGS base viscosity (max(1e-6, base nu))
+    double sgs_c2;             // Smagorinsky C^2 (reference: 0.025^2)
+    double sgs_nut_max_ratio;  // cap nu_t <= ratio * nu0 (reference: 5)
+    double sgs_bulk_coupling;  // reference: 0.3
+    double buoyancy_beta;      // force = rho * clamp(beta * T, +-force_max)
+    double buoyancy_force_max; // reference: 0.02
+    double body_force[3];      // uniform force density added to every fluid cell
+    double max_speed;          // reference: 0.57735026919 * 0.6 (float product)
+    double face_velocity[6][3];
+    double face_pressure[6];
+    int face_kind[6];          // x-, x+, y-, y+, z-, z+
+    int enable_sgs;
+    int enable_buoyancy;
+    int gravity_axis;          // 0,1,2: axis the buoyancy force acts along (+)
+    int disable_convective_outflow;  // flag for INHERIT_GAME faces
+    int reserved;
+} OracleD3Q27Params;
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+struct Lattice {
+    int cx[27], cy[27], cz[27], opp[27];
+    T w[27];
+    Lattice() {
+        const int v1[3] = {-1, 0, 1};
+        const T w1[3] = {T(1.0) / T(6.0), T(2.0) / T(3.0), T(1.0) / T(6.0)};
+        for (int ix = 0; ix < 3; ++ix)
+            for (int iy = 0; iy < 3; ++iy)
+                for (int iz = 0; iz < 3; ++iz) {
+                    const int q = (ix * 3 + iy) * 3 + iz;
+                    cx[q] = v1[ix];
+                    cy[q] = v1[iy];
+                    cz[q] = v1[iz];
+                    opp[q] = ((2 - ix) * 3 + (2 - iy)) * 3 + (2 - iz);
+                    w[q] = w1[ix] * w1[iy] * w1[iz];
+                }
+    }
+};
+
+template <typename T>
+inline T clampv(T v, T lo, T hi) { return std::min(hi, std::max(lo, v)); }
+
+template <typename T>
+struct D3Q27Oracle {
+    using Arr = std::array<T, 27>;
+    Lattice<T> L;
+    int nx = 0, ny = 0, nz = 0;
+    size_t cells = 0;
+    OracleD3Q27Params p{};
+    // constants mirrored from the reference (native/src/aero_lbm_jni.cpp:83-168)
+    T cs2 = T(1.0) / T(3.0);
+    T rho_min = T(0.97), rho_max = T(1.03);
+    T p_min = T(-0.03), p_max = T(0.03);
+    T nu_shear_min = T(1.0e-8), nu_shear_max = (T(0.95) - T(0.5)) / T(3.0);
+    T tau_shear_min = T(0.5) + T(3.0) * T(1.0e-8), tau_shear_max = T(0.95);
+    T tau_normal_min = T(0.5) + T(3.0) * T(1.0e-8), tau_normal_max = T(0.95);
+    T conv_beta = T(0.15);
+
+    std::vector<T> f, f_post, rho, ux, uy, uz;
+    std::vector<T> ref_ux, ref_uy, ref_uz, ref_p, temperature;
+    std::vector<T> force_x, force_y, force_z;  // optional per-cell force density
+    std::vector<uint8_t> obstacle;
+    bool initialized = false;
+    uint64_t steps_done = 0;
+
+    size_t cell_index(int x, int y, int z) const { return (size_t(x) * ny + y) * nz + z; }
+    size_t di(size_t cell, int q) const { return size_t(q) * cells + cell; }
+
+    void allocate(int nx_, int ny_, int nz_) {
+        nx = nx_; ny = ny_; nz = nz_;
+        cells = size_t(nx) * ny * nz;
+        f.assign(cells * 27, T(0));
+        f_post.assign(cells * 27, T(0));
+        rho.assign(cells, T(1));
+        ux.assign(cells, T(0)); uy.assign(cells, T(0)); uz.assign(cells, T(0));
+        ref_ux.assign(cells, T(0)); ref_uy.assign(cells, T(0)); ref_uz.assign(cells, T(0));
+        ref_p.assign(cells, T(0));
+        temperature.assign(cells, T(0));
+        obstacle.assign(cells, 0);
+        force_x.clear(); force_y.clear(); force_z.clear();
+    }
+
+    T feq(int q, T r, T vx, T vy, T vz) const {
+        const T cu = T(3.0) * (T(L.cx[q]) * vx + T(L.cy[q]) * vy + T(L.cz[q]) * vz);
+        const T uu = vx * vx + vy * vy + vz * vz;
+        return L.w[q] * r * (T(1.0) + cu + T(0.5) * cu * cu - T(1.5) * uu);
+    }
+
+    T guo(int q, T vx, T vy, T vz, T fx, T fy, T fz, T omega) const {
+        const T cxq = T(L.cx[q]), cyq = T(L.cy[q]), czq = T(L.cz[q]);
+        const T cu = cxq * vx + cyq * vy + czq * vz;
+        const T c_force = cxq * fx + cyq * fy + czq * fz;
+        const T u_force = vx * fx + vy * fy + vz * fz;
+        const T inv_cs2 = T(1.0) / cs2;
+        const T inv_cs4 = inv_cs2 * inv_cs2;
+        const T pref = std::max(T(0.0), T(1.0) - T(0.5) * clampv(omega, T(0.0), T(1.999)));
+        return pref * L.w[q] * ((c_force - u_force) * inv_cs2 + cu * c_force * inv_cs4);
+    }
+
+    // ---- boundary helpers (native/src/aero_lbm_jni.cpp:739-777, 1475-1602)
+    bool wrap_axis(int& c, int dim, int min_face, int max_face) const {
+        if (c >= 0 && c < dim) return false;
+        const int face = c < 0 ? min_face : max_face;
+        if (p.face_kind[face] != kPeriodic) return false;
+        c %= dim;
+        if (c < 0) c += dim;
+        return true;
+    }
+    void remap(int& x, int& y, int& z) const {
+        wrap_axis(x, nx, 0, 1);
+        wrap_axis(y, ny, 2, 3);
+        wrap_axis(z, nz, 4, 5);
+    }
+    int oob_face(int x, int y, int z) const {
+        if (x < 0) return 0;
+        if (x >= nx) return 1;
+        if (y < 0) return 2;
+        if (y >= ny) return 3;
+        if (z < 0) return 4;
+        if (z >= nz) return 5;
+        return -1;
+    }
+    T bounce_value(size_t cell, int q) const { return f_post[di(cell, L.opp[q])]; }
+
+    T convective_value(size_t cell, int x, int y, int z, int q, int sx, int sy, int sz) const {
+        const int dx = (sx < 0 || sx >= nx) ? L.cx[q] : 0;
+        const int dy = (sy < 0 || sy >= ny) ? L.cy[q] : 0;
+        const int dz = (sz < 0 || sz >= nz) ? L.cz[q] : 0;
+        const int i1x = std::clamp(x + dx, 0, nx - 1);
+        const int i1y = std::clamp(y + dy, 0, ny - 1);
+        const int i1z = std::clamp(z + dz, 0, nz - 1);
+        const size_t src1 = cell_index(i1x, i1y, i1z);
+        if (obstacle[src1]) return bounce_value(cell, q);
+        const T f1 = f_post[di(src1, q)];
+        const int i2x = std::clamp(x + 2 * dx, 0, nx - 1);
+        const int i2y = std::clamp(y + 2 * dy, 0, ny - 1);
+        const int i2z = std::clamp(z + 2 * dz, 0, nz - 1);
+        const size_t src2 = cell_index(i2x, i2y, i2z);
+        if (obstacle[src2]) return f1;
+        const T f2 = f_post[di(src2, q)];
+        return f1 + conv_beta * (f1 - f2);
+    }
+
+    T equilibrium_value(size_t cell, int q, int face) const {
+        T r = T(1.0) + clampv(ref_p[cell], p_min, p_max);
+        T vx = T(0), vy = T(0), vz = T(0);
+        const int kind = p.face_kind[face];
+        if (kind == kMovingWall || kind == kVelocityDirichlet) {
+            vx = T(p.face_velocity[face][0]);
+            vy = T(p.face_velocity[face][1]);
+            vz = T(p.face_velocity[face][2]);
+        } else if (kind == kPressureDirichlet) {
+            r = T(1.0) + clampv(T(p.face_pressure[face]), p_min, p_max);
+        }
+        r = clampv(r, rho_min, rho_max);
+        const T ms = T(p.max_speed);
+        const T s2 = vx * vx + vy * vy + vz * vz;
+        if (s2 > ms * ms && s2 > T(0)) {
+            const T scale = ms / std::sqrt(s2);
+            vx *= scale; vy *= scale; vz *= scale;
+        }
+        return feq(q, r, vx, vy, vz);
+    }
+
+    T face_value(size_t cell, int x, int y, int z, int q, int sx, int sy, int sz) const {
+        const int face = oob_face(sx, sy, sz);
+        const int kind = face >= 0 ? p.face_kind[face] : kInheritGame;
+        switch (kind) {
+            case kBounceBack:
+                return bounce_value(cell, q);
+            case kMovingWall:
+            case kVelocityDirichlet:
+            case kPressureDirichlet:
+                return equilibrium_value(cell, q, face);
+            case kSymmetry: {
+                const int ix = std::clamp(sx, 0, nx - 1);
+                const int iy = std::clamp(sy, 0, ny - 1);
+                const int iz = std::clamp(sz, 0, nz - 1);
+                const size_t src = cell_index(ix, iy, iz);
+                return obstacle[src] ? bounce_value(cell, q) : f_post[di(src, q)];
+            }
+            case kConvectiveOutflow:
+                return convective_value(cell, x, y, z, q, sx, sy, sz);
+            case kPeriodic:
+                break;
+            default:
+                if (p.disable_convective_outflow) return bounce_value(cell, q);
+                return convective_value(cell, x, y, z, q, sx, sy, sz);
+        }
+        return convective_value(cell, x, y, z, q, sx, sy, sz);
+    }
+
+    // ---- state set-up (payload ingest + initialize_distributions)
+    void initialize() {
+        for (size_t cell = 0; cell < cells; ++cell) {
+            if (obstacle[cell]) {
+                rho[cell] = T(1); ux[cell] = uy[cell] = uz[cell] = T(0);
+            } else {
+                rho[cell] = clampv(T(1.0) + ref_p[cell], rho_min, rho_max);
+                ux[cell] = ref_ux[cell]; uy[cell] = ref_uy[cell]; uz[cell] = ref_uz[cell];
+            }
+            for (int q = 0; q < 27; ++q) {
+                const T eq = feq(q, rho[cell], ux[cell], uy[cell], uz[cell]);
+                f[di(cell, q)] = eq;
+                f_post[di(cell, q)] = eq;
+            }
+        }
+        initialized = true;
+    }
+
+    void reseed(size_t cell) {
+        const T pr = clampv(std::isfinite(ref_p[cell]) ? ref_p[cell] : T(0), p_min, p_max);
+        const T r = clampv(T(1.0) + pr, rho_min, rho_max);
+        T vx = std::isfinite(ref_ux[cell]) ? ref_ux[cell] : T(0);
+        T vy = std::isfinite(ref_uy[cell]) ? ref_uy[cell] : T(0);
+        T vz = std::isfinite(ref_uz[cell]) ? ref_uz[cell] : T(0);
+        const T ms = T(p.max_speed);
+        const T s2 = vx * vx + vy * vy + vz * vz;
+        if (!std::isfinite(s2) || s2 > ms * ms) {
+            if (!std::isfinite(s2) || s2 <= T(0)) {
+                vx = vy = vz = T(0);
+            } else {
+                const T scale = ms / std::sqrt(s2);
+                vx *= scale; vy *= scale; vz *= scale;
+            }
+        }
+        rho[cell] = r; ux[cell] = vx; uy[cell] = vy; uz[cell] = vz;
+        for (int q = 0; q < 27; ++q) f_post[di(cell, q)] = feq(q, r, vx, vy, vz);
+    }
+
+    // ---- moment transforms (native/src/aero_lbm_jni.cpp:1335-1473)
+    static int binom(int n, int k) {
+        if (k < 0 || k > n) return 0;
+        if (n <= 1 || k == 0 || k == n) return 1;
+        return 2;
+    }
+    void raw_moments(const Arr& fl, T raw[3][3][3]) const {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) raw[a][b][c] = T(0);
+        for (int q = 0; q < 27; ++q) {
+            const T fq = fl[q];
+            const T px[3] = {T(1), T(L.cx[q]), T(L.cx[q] * L.cx[q])};
+            const T py[3] = {T(1), T(L.cy[q]), T(L.cy[q] * L.cy[q])};
+            const T pz[3] = {T(1), T(L.cz[q]), T(L.cz[q] * L.cz[q])};
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int c = 0; c < 3; ++c) raw[a][b][c] += fq * px[a] * py[b] * pz[c];
+        }
+    }
+    static void shift_moments(const T in[3][3][3], const T sx[3], const T sy[3], const T sz[3], T out[3][3][3]) {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) {
+                    T sum = T(0);
+                    for (int i = 0; i <= a; ++i)
+                        for (int j = 0; j <= b; ++j)
+                            for (int k = 0; k <= c; ++k) {
+                                const T coeff = T(binom(a, i) * binom(b, j) * binom(c, k));
+                                sum += coeff * sx[a - i] * sy[b - j] * sz[c - k] * in[i][j][k];
+                            }
+                    out[a][b][c] = sum;
+                }
+    }
+    void relax(T r, const T cin[3][3][3], T om_diag, T om_off, T cout[3][3][3]) const {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) cout[a][b][c] = T(0);
+        cout[0][0][0] = r;
+        const T eq2 = r * cs2;
+        const T sd = clampv(om_diag, T(0.0), T(1.95));
+        const T so = clampv(om_off, T(0.0), T(1.95));
+        cout[2][0][0] = cin[2][0][0] + sd * (eq2 - cin[2][0][0]);
+        cout[0][2][0] = cin[0][2][0] + sd * (eq2 - cin[0][2][0]);
+        cout[0][0][2] = cin[0][0][2] + sd * (eq2 - cin[0][0][2]);
+        cout[1][1][0] = (T(1.0) - so) * cin[1][1][0];
+        cout[1][0][1] = (T(1.0) - so) * cin[1][0][1];
+        cout[0][1][1] = (T(1.0) - so) * cin[0][1][1];
+        const T c200 = cout[2][0][0], c020 = cout[0][2][0], c002 = cout[0][0][2];
+        const T c110 = cout[1][1][0], c101 = cout[1][0][1], c011 = cout[0][1][1];
+        const T ir = T(1.0) / std::max(T(1e-6), r);
+        cout[2][2][0] = c200 * c020 * ir + T(2.0) * c110 * c110 * ir;
+        cout[2][0][2] = c200 * c002 * ir + T(2.0) * c101 * c101 * ir;
+        cout[0][2][2] = c020 * c002 * ir + T(2.0) * c011 * c011 * ir;
+        cout[2][1][1] = (c200 * c011 + T(2.0) * c110 * c101) * ir;
+        cout[1][2][1] = (c020 * c101 + T(2.0) * c110 * c011) * ir;
+        cout[1][1][2] = (c002 * c110 + T(2.0) * c101 * c011) * ir;
+        cout[2][2][2] = (c200 * c020 * c002 + T(2.0) * c110 * c110 * c002 + T(2.0) * c101 * c101 * c020 +
+                         T(2.0) * c011 * c011 * c200 + T(8.0) * c110 * c101 * c011) * ir * ir;
+    }
+    void raw_to_pop(const T raw[3][3][3], Arr& out) const {
+        const T inv1[3][3] = {{T(0.0), T(-0.5), T(0.5)}, {T(1.0), T(0.0), T(-1.0)}, {T(0.0), T(0.5), T(0.5)}};
+        for (int ix = 0; ix < 3; ++ix)
+            for (int iy = 0; iy < 3; ++iy)
+                for (int iz = 0; iz < 3; ++iz) {
+                    T sum = T(0);
+                    for (int a = 0; a < 3; ++a)
+                        for (int b = 0; b < 3; ++b)
+                            for (int c = 0; c < 3; ++c) sum += inv1[ix][a] * inv1[iy][b] * inv1[iz][c] * raw[a][b][c];
+                    out[(ix * 3 + iy) * 3 + iz] = sum;
+                }
+    }
+
+    // ---- collide (native/src/aero_lbm_jni.cpp:2209-2413, benchmark mode: no fan, nudge or sponge)
+    void collide() {
+        const T ms = T(p.max_speed);
+        const T tau_s_base = T(p.tau_shear), tau_n_base = T(p.tau_normal);
+        const T sgs_c2 = T(p.sgs_c2);
+        for (size_t cell = 0; cell < cells; ++cell) {
+            if (obstacle[cell]) {
+                rho[cell] = T(1); ux[cell] = uy[cell] = uz[cell] = T(0);
+                for (int q = 0; q < 27; ++q) f_post[di(cell, q)] = f[di(cell, q)];
+                continue;
+            }
+            Arr fl{};
+            T r = T(0), mx = T(0), my = T(0), mz = T(0);
+            bool bad = false;
+            for (int q = 0; q < 27; ++q) {
+                const T fq = f[di(cell, q)];
+                if (!std::isfinite(fq)) { bad = true; break; }
+                fl[q] = fq;
+                r += fq;
+                mx += fq * T(L.cx[q]);
+                my += fq * T(L.cy[q]);
+                mz += fq * T(L.cz[q]);
+            }
+            if (bad || !std::isfinite(r) || !std::isfinite(mx) || !std::isfinite(my) || !std::isfinite(mz)) {
+                reseed(cell);
+                continue;
+            }
+            const T rs = std::max(T(1e-6), r);
+            const T ir = T(1.0) / rs;
+            T vx = mx * ir, vy = my * ir, vz = mz * ir;
+            if (!std::isfinite(rs) || !std::isfinite(ir) || !std::isfinite(vx) || !std::isfinite(vy) || !std::isfinite(vz)) {
+                reseed(cell);
+                continue;
+            }
+            T fx = T(0), fy = T(0), fz = T(0);
+            if (p.enable_buoyancy) {
+                const T b = clampv(T(p.buoyancy_beta) * temperature[cell], -T(p.buoyancy_force_max), T(p.buoyancy_force_max));
+                const T add = rs * b;
+                if (p.gravity_axis == 0) fx += add;
+                else if (p.gravity_axis == 1) fy += add;
+                else fz += add;
+            }
+            // body force density (parameter; zero reproduces the reference)
+            if (p.body_force[0] != 0.0 || p.body_force[1] != 0.0 || p.body_force[2] != 0.0) {
+                fx += T(p.body_force[0]); fy += T(p.body_force[1]); fz += T(p.body_force[2]);
+            }
+            if (!force_x.empty()) {
+                fx += force_x[cell]; fy += force_y[cell]; fz += force_z[cell];
+            }
+            const T dux = fx * ir, duy = fy * ir, duz = fz * ir;
+            vx += T(0.5) * dux;
+            vy += T(0.5) * duy;
+            vz += T(0.5) * duz;
+            const T s2 = vx * vx + vy * vy + vz * vz;
+            if (!std::isfinite(s2)) { reseed(cell); continue; }
+            if (s2 > ms * ms) {
+                const T scale = ms / std::sqrt(s2);
+                vx *= scale; vy *= scale; vz *= scale;
+            }
+            rho[cell] = r; ux[cell] = vx; uy[cell] = vy; uz[cell] = vz;
+
+            T raw[3][3][3], cpre[3][3][3], cpost[3][3][3], rpost[3][3][3];
+            raw_moments(fl, raw);
+            {
+                const T sx[3] = {T(1.0), -vx, vx * vx};
+                const T sy[3] = {T(1.0), -vy, vy * vy};
+                const T sz[3] = {T(1.0), -vz, vz * vz};
+                shift_moments(raw, sx, sy, sz, cpre);
+            }
+            T tau_s = tau_s_base, tau_n = tau_n_base;
+            if (p.enable_sgs) {
+                const T nu0 = std::max(T(1e-6), T(p.nu0));
+                const T nxx = cpre[2][0][0] - rs * cs2;
+                const T nyy = cpre[0][2][0] - rs * cs2;
+                const T nzz = cpre[0][0][2] - rs * cs2;
+                const T nxy = cpre[1][1][0], nxz = cpre[1][0][1], nyz = cpre[0][1][1];
+                const T qn2 = nxx * nxx + nyy * nyy + nzz * nzz + T(2.0) * (nxy * nxy + nxz * nxz + nyz * nyz);
+                const T qm = std::sqrt(std::max(T(0.0), qn2));
+                const T sm = qm / std::max(T(1e-6), T(2.0) * rs * nu0);
+                T nut = sgs_c2 * sm;
+                nut = std::min(nut, T(p.sgs_nut_max_ratio) * nu0);
+                tau_s = clampv(T(0.5) + T(3.0) * clampv(nu0 + nut, nu_shear_min, nu_shear_max), tau_shear_min, tau_shear_max);
+                tau_n = clampv(tau_n_base + (tau_s - tau_s_base) * T(p.sgs_bulk_coupling), tau_normal_min, tau_normal_max);
+            }
+            const T om_d = T(1.0) / tau_n;
+            const T om_o = T(1.0) / tau_s;
+            relax(rs, cpre, om_d, om_o, cpost);
+            {
+                const T sx[3] = {T(1.0), vx, vx * vx};
+                const T sy[3] = {T(1.0), vy, vy * vy};
+                const T sz[3] = {T(1.0), vz, vz * vz};
+                shift_moments(cpost, sx, sy, sz, rpost);
+            }
+            Arr fc{};
+            raw_to_pop(rpost, fc);
+            T rc = T(0), mxc = T(0), myc = T(0), mzc = T(0);
+            for (int q = 0; q < 27; ++q) {
+                const T fq = fc[q];
+                rc += fq;
+                mxc += fq * T(L.cx[q]);
+                myc += fq * T(L.cy[q]);
+                mzc += fq * T(L.cz[q]);
+            }
+            const T rcs = std::max(T(1e-6), rc);
+            const T uxc = mxc / rcs, uyc = myc / rcs, uzc = mzc / rcs;
+            for (int q = 0; q < 27; ++q) fc[q] += feq(q, rs, vx, vy, vz) - feq(q, rcs, uxc, uyc, uzc);
+            for (int q = 0; q < 27; ++q) f_post[di(cell, q)] = fc[q] + guo(q, vx, vy, vz, fx, fy, fz, om_o);
+        }
+    }
+
+    // ---- stream_and_bounce (native/src/aero_lbm_jni.cpp:2415-2452)
+    void stream() {
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    const size_t cell = cell_index(x, y, z);
+                    Arr fl{};
+                    if (obstacle[cell]) {
+                        for (int q = 0; q < 27; ++q) fl[q] = f_post[di(cell, L.opp[q])];
+                    } else {
+                        for (int q = 0; q < 27; ++q) {
+                            int sx = x - L.cx[q], sy = y - L.cy[q], sz = z - L.cz[q];
+                            remap(sx, sy, sz);
+                            if (sx < 0 || sy < 0 || sz < 0 || sx >= nx || sy >= ny || sz >= nz) {
+                                fl[q] = face_value(cell, x, y, z, q, sx, sy, sz);
+                                continue;
+                            }
+                            const size_t src = cell_index(sx, sy, sz);
+                            fl[q] = obstacle[src] ? bounce_value(cell, q) : f_post[di(src, q)];
+                        }
+                    }
+                    for (int q = 0; q < 27; ++q) f[di(cell, q)] = fl[q];
+                }
+    }
+
+    // macro readout used by write_output / extract (native/src/aero_lbm_jni.cpp:2535-2581, 9385-9446)
+    void cell_output(size_t cell, T scale, float* o) const {
+        if (obstacle[cell]) { o[0] = o[1] = o[2] = o[3] = 0.0f; return; }
+        T r = T(0), vx = T(0), vy = T(0), vz = T(0);
+        for (int q = 0; q < 27; ++q) {
+            const T fq = f[di(cell, q)];
+            if (!std::isfinite(fq)) { o[0] = o[1] = o[2] = o[3] = 0.0f; return; }
+            r += fq;
+            vx += fq * T(L.cx[q]); vy += fq * T(L.cy[q]); vz += fq * T(L.cz[q]);
+        }
+        if (!std::isfinite(r) || !std::isfinite(vx) || !std::isfinite(vy) || !std::isfinite(vz)) {
+            o[0] = o[1] = o[2] = o[3] = 0.0f; return;
+        }
+        r = clampv(r, rho_min, rho_max);
+        if (!std::isfinite(r) || r <= T(1e-6)) { o[0] = o[1] = o[2] = o[3] = 0.0f; return; }
+        vx /= r; vy /= r; vz /= r;
+        if (!std::isfinite(vx) || !std::isfinite(vy) || !std::isfinite(vz)) vx = vy = vz = T(0);
+        if (std::fabs(r - T(1.0)) < T(1e-6)) r = T(1.0);
+        if (std::fabs(vx) < T(1e-7)) vx = T(0);
+        if (std::fabs(vy) < T(1e-7)) vy = T(0);
+        if (std::fabs(vz) < T(1e-7)) vz = T(0);
+        o[0] = float(vx * scale);
+        o[1] = float(vy * scale);
+        o[2] = float(vz * scale);
+        o[3] = float(clampv(r - T(1.0), p_min, p_max));
+    }
+
+    // rho and u from f without any output clamp (used for error statistics)
+    void raw_macro(size_t cell, double* o) const {
+        T r = T(0), vx = T(0), vy = T(0), vz = T(0);
+        for (int q = 0; q < 27; ++q) {
+            const T fq = f[di(cell, q)];
+            r += fq;
+            vx += fq * T(L.cx[q]); vy += fq * T(L.cy[q]); vz += fq * T(L.cz[q]);
+        }
+        o[0] = double(r);
+        o[1] = double(vx / r); o[2] = double(vy / r); o[3] = double(vz / r);
+    }
+
+    void step() {
+        if (!initialized) initialize();
+        collide();
+        stream();
+        ++steps_done;
+    }
+};
+
+struct Handle {
+    int precision = 0;  // 0 float, 1 double
+    std::unique_ptr<D3Q27Oracle<float>> f32;
+    std::unique_ptr<D3Q27Oracle<double>> f64;
+};
+
+template <typename T>
+void load_fields(D3Q27Oracle<T>& o, const uint8_t* obstacle, const float* ux, const float* uy, const float* uz,
+                 const float* pressure, const float* temperature) {
+    for (size_t c = 0; c < o.cells; ++c) {
+        o.obstacle[c] = obstacle ? (obstacle[c] ? 1 : 0) : 0;
+        o.ref_ux[c] = ux ? T(std::isfinite(ux[c]) ? ux[c] : 0.0f) : T(0);
+        o.ref_uy[c] = uy ? T(std::isfinite(uy[c]) ? uy[c] : 0.0f) : T(0);
+        o.ref_uz[c] = uz ? T(std::isfinite(uz[c]) ? uz[c] : 0.0f) : T(0);
+        const float pv = pressure ? pressure[c] : 0.0f;
+        o.ref_p[c] = T(std::min(0.03f, std::max(-0.03f, pv)));
+        const float tv = temperature ? temperature[c] : 0.0f;
+        o.temperature[c] = T(std::min(1.0f, std::max(-1.0f, tv)));
+    }
+}
+
+template <typename T>
+void set_force(D3Q27Oracle<T>& o, const float* fx, const float* fy, const float* fz) {
+    if (!fx || !fy || !fz) { o.force_x.clear(); o.force_y.clear(); o.force_z.clear(); return; }
+    o.force_x.resize(o.cells); o.force_y.resize(o.cells); o.force_z.resize(o.cells);
+    for (size_t c = 0; c < o.cells; ++c) { o.force_x[c] = T(fx[c]); o.force_y[c] = T(fy[c]); o.force_z[c] = T(fz[c]); }
+}
+
+}  // namespace
+
+extern "C" {
+
+void* oracle_d3q27_create(int nx, int ny, int nz, int precision, const OracleD3Q27Params* params) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !params) return nullptr;
+    auto* h = new Handle();
+    h->precision = precision;
+    if (precision == 0) {
+        h->f32 = std::make_unique<D3Q27Oracle<float>>();
+        h->f32->allocate(nx, ny, nz);
+        h->f32->p = *params;
+    } else {
+        h->f64 = std::make_unique<D3Q27Oracle<double>>();
+        h->f64->allocate(nx, ny, nz);
+        h->f64->p = *params;
+    }
+    return h;
+}
+
+void oracle_d3q27_destroy(void* handle) { delete static_cast<Handle*>(handle); }
+
+// Per-cell inputs in reference packet semantics: obstacle (nonzero = solid),
+// initial/reference velocity (lattice units), pressure proxy (rho - 1, clamped
+// to +-0.03) and temperature (clamped to +-1). Any pointer may be null (zeros).
+int oracle_d3q27_set_fields(void* handle, const uint8_t* obstacle, const float* ux, const float* uy, const float* uz,
+                            const float* pressure, const float* temperature) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h) return 0;
+    if (h->f32) load_fields(*h->f32, obstacle, ux, uy, uz, pressure, temperature);
+    else load_fields(*h->f64, obstacle, ux, uy, uz, pressure, temperature);
+    return 1;
+}
+
+// Optional per-cell force density field (3 x cells, SoA); null clears it.
+int oracle_d3q27_set_force_field(void* handle, const float* fx, const float* fy, const float* fz) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h) return 0;
+    if (h->f32) set_force(*h->f32, fx, fy, fz);
+    else set_force(*h->f64, fx, fy, fz);
+    return 1;
+}
+
+int oracle_d3q27_set_params(void* handle, const OracleD3Q27Params* params) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !params) return 0;
+    if (h->f32) h->f32->p = *params;
+    else h->f64->p = *params;
+    return 1;
+}
+
+int oracle_d3q27_step(void* handle, int steps) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || steps < 0) return 0;
+    for (int s = 0; s < steps; ++s) {
+        if (h->f32) h->f32->step();
+        else h->f64->step();
+    }
+    return 1;
+}
+
+// write_output semantics: cells x 4 floats (ux, uy, uz scaled; clamped rho - 1).
+int oracle_d3q27_output(void* handle, float scale, float* out) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !out) return 0;
+    if (h->f32) {
+        for (size_t c = 0; c < h->f32->cells; ++c) h->f32->cell_output(c, float(scale), out + 4 * c);
+    } else {
+        for (size_t c = 0; c < h->f64->cells; ++c) h->f64->cell_output(c, double(scale), out + 4 * c);
+    }
+    return 1;
+}
+
+// Strided atlas (aero_lbm_extract_flow_atlas_rect semantics, scale 1).
+int oracle_d3q27_extract_atlas(void* handle, int stride, float* out, int value_count) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !out || stride <= 0) return 0;
+    auto run = [&](auto& o) -> int {
+        const int sx = (o.nx + stride - 1) / stride, sy = (o.ny + stride - 1) / stride, sz = (o.nz + stride - 1) / stride;
+        if (value_count != sx * sy * sz * 4) return 0;
+        int dst = 0;
+        for (int ax = 0; ax < sx; ++ax)
+            for (int ay = 0; ay < sy; ++ay)
+                for (int az = 0; az < sz; ++az) {
+                    const int gx = std::min(o.nx - 1, ax * stride);
+                    const int gy = std::min(o.ny - 1, ay * stride);
+                    const int gz = std::min(o.nz - 1, az * stride);
+                    o.cell_output(o.cell_index(gx, gy, gz), 1, out + dst);
+                    dst += 4;
+                }
+        return 1;
+    };
+    return h->f32 ? run(*h->f32) : run(*h->f64);
+}
+
+// Unclamped rho, ux, uy, uz per cell (cells x 4 doubles); solids included.
+int oracle_d3q27_macro(void* handle, double* out) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !out) return 0;
+    if (h->f32) for (size_t c = 0; c < h->f32->cells; ++c) h->f32->raw_macro(c, out + 4 * c);
+    else for (size_t c = 0; c < h->f64->cells; ++c) h->f64->raw_macro(c, out + 4 * c);
+    return 1;
+}
+
+// Current pre-collision populations (f, SoA q-major) as doubles.
+int oracle_d3q27_get_f(void* handle, double* out) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !out) return 0;
+    if (h->f32) for (size_t i = 0; i < h->f32->f.size(); ++i) out[i] = h->f32->f[i];
+    else for (size_t i = 0; i < h->f64->f.size(); ++i) out[i] = h->f64->f[i];
+    return 1;
+}
+
+}  // extern "C"

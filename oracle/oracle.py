@@ -1,0 +1,353 @@
+"""ORACLE — test infrastructure only (imported by tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline leg; never by the product).
+
+Two checkers live here:
+
+* ``RefLib`` drives the reference library itself (the unmodified reference CPU
+  path compiled by ``make ref`` into oracle/_ref/libaero_lbm_ref.so) through its
+  C ABI, like the reference's own ctypes tools do.
+* ``Oracle`` drives liboracle.so, the C++ restatement of the reference step
+  (d3q27_oracle.cpp), in float (bit-exact with the reference) or double (the
+  FP64 run of the same scheme), with the knobs the reference hard-codes.
+
+``derive_params`` restates, in float32, how the reference turns its boundary
+configuration into relaxation times (native/src/aero_lbm_jni.cpp:831-1031).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libaero_lbm_ref.so"
+REFERENCE_SOURCE = Path(os.environ.get("AERO_REFERENCE_NATIVE", "/root/reference/native"))
+
+f32 = np.float32
+
+# Face kinds / flags (same numbering as the C ABI).
+PERIODIC, BOUNCE_BACK, MOVING_WALL, VELOCITY, PRESSURE, CONVECTIVE, SYMMETRY = 1, 2, 3, 4, 5, 6, 7
+INHERIT_GAME = 0
+FLAG_DISABLE_CONVECTIVE_OUTFLOW = 1 << 3
+FLAG_DISABLE_SGS = 1 << 5
+FLAG_DISABLE_BUOYANCY = 1 << 7
+
+
+def build(ref: bool | None = None) -> None:
+    """Compile liboracle.so (always) and the reference library (when its
+    sources are present and ``ref`` is not False)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    if ref is None:
+        ref = REFERENCE_SOURCE.exists()
+    if ref:
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REFERENCE_SOURCE}"], check=True)
+
+
+# ---------------------------------------------------------------- parameter derivation
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("tau_shear", ctypes.c_double),
+        ("tau_normal", ctypes.c_double),
+        ("nu0", ctypes.c_double),
+        ("sgs_c2", ctypes.c_double),
+        ("sgs_nut_max_ratio", ctypes.c_double),
+        ("sgs_bulk_coupling", ctypes.c_double),
+        ("buoyancy_beta", ctypes.c_double),
+        ("buoyancy_force_max", ctypes.c_double),
+        ("body_force", ctypes.c_double * 3),
+        ("max_speed", ctypes.c_double),
+        ("face_velocity", (ctypes.c_double * 3) * 6),
+        ("face_pressure", ctypes.c_double * 6),
+        ("face_kind", ctypes.c_int * 6),
+        ("enable_sgs", ctypes.c_int),
+        ("enable_buoyancy", ctypes.c_int),
+        ("gravity_axis", ctypes.c_int),
+        ("disable_convective_outflow", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+    ]
+
+
+def _clamp(v, lo, hi):
+    return f32(min(f32(hi), max(f32(lo), f32(v))))
+
+
+NU_MIN = f32(1.0e-8)
+NU_MAX = (f32(0.95) - f32(0.5)) / f32(3.0)
+TAU_MIN = f32(0.5) + f32(3.0) * f32(1.0e-8)
+TAU_MAX = f32(0.95)
+MAX_SPEED = f32(0.57735026919) * f32(0.60)
+RUNTIME_NU0 = f32(1.50e-5) * (f32(1.0) / f32(20.0)) / (f32(1.0) * f32(1.0))
+BOUSSINESQ_BETA = f32(9.81) * (f32(1.0) / f32(300.0)) * f32(20.0) * ((f32(1.0) / f32(20.0)) * (f32(1.0) / f32(20.0)) / f32(1.0))
+
+
+def _norm(v):
+    """sqrt(x*x + y*y + z*z) evaluated left to right in float32."""
+    x, y, z = (f32(a) for a in v)
+    return f32(np.sqrt(f32(f32(x * x + y * y) + z * z)))
+
+
+def derive_params(cfg: dict) -> OracleParams:
+    """Benchmark-mode effective parameters, restated from
+    native/src/aero_lbm_jni.cpp:831-871 (reference speed), 947-979 (nu, tau),
+    1023-1031 (beta). ``cfg`` keys: reynolds, reference_length,
+    initial_velocity, faces (list of 6 dicts: kind, velocity, pressure),
+    sgs (bool), buoyancy (bool), smagorinsky_c, buoyancy_beta, gravity_axis,
+    body_force, disable_convective."""
+    faces = cfg["faces"]
+    speed = _norm(cfg.get("initial_velocity", (0, 0, 0)))
+    for fc in faces:
+        speed = max(speed, _norm(fc.get("velocity", (0, 0, 0))))
+    re = f32(cfg.get("reynolds", 100.0))
+    length = max(f32(1.0e-6), f32(cfg.get("reference_length", 1.0)))
+    if re <= f32(1.0e-6) or speed <= f32(1.0e-8):
+        nu = _clamp(RUNTIME_NU0, NU_MIN, NU_MAX)
+    else:
+        nu = _clamp(f32(speed * length) / re, NU_MIN, NU_MAX)
+    tau_s = _clamp(f32(0.5) + f32(3.0) * _clamp(nu, NU_MIN, NU_MAX), TAU_MIN, TAU_MAX)
+    tau_n = _clamp(f32(0.5) + f32(3.0) * _clamp(_clamp(nu, NU_MIN, NU_MAX), NU_MIN, NU_MAX), TAU_MIN, TAU_MAX)
+    p = OracleParams()
+    p.tau_shear = float(tau_s)
+    p.tau_normal = float(tau_n)
+    p.nu0 = float(max(f32(1e-6), nu))
+    c = f32(cfg.get("smagorinsky_c", 0.025))
+    p.sgs_c2 = float(f32(c * c))
+    p.sgs_nut_max_ratio = 5.0
+    p.sgs_bulk_coupling = float(f32(0.30))
+    p.buoyancy_beta = float(f32(cfg.get("buoyancy_beta", BOUSSINESQ_BETA)))
+    p.buoyancy_force_max = float(f32(0.02))
+    for i, v in enumerate(cfg.get("body_force", (0.0, 0.0, 0.0))):
+        p.body_force[i] = float(f32(v))
+    p.max_speed = float(MAX_SPEED)
+    for i, fc in enumerate(faces):
+        p.face_kind[i] = int(fc.get("kind", INHERIT_GAME))
+        for a, v in enumerate(fc.get("velocity", (0, 0, 0))):
+            p.face_velocity[i][a] = float(f32(v))
+        p.face_pressure[i] = float(f32(fc.get("pressure", 0.0)))
+    p.enable_sgs = 1 if cfg.get("sgs", False) else 0
+    p.enable_buoyancy = 1 if cfg.get("buoyancy", False) else 0
+    p.gravity_axis = int(cfg.get("gravity_axis", 1))
+    p.disable_convective_outflow = 1 if cfg.get("disable_convective", False) else 0
+    return p
+
+
+# ---------------------------------------------------------------- oracle (restatement)
+class Oracle:
+    """CPU restatement of the reference D3Q27 step; precision 'f32' or 'f64'."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls) -> ctypes.CDLL:
+        if cls._lib is None:
+            if not ORACLE_LIB.exists():
+                build(ref=False)
+            lib = ctypes.CDLL(str(ORACLE_LIB))
+            lib.oracle_d3q27_create.restype = ctypes.c_void_p
+            lib.oracle_d3q27_create.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(OracleParams)]
+            lib.oracle_d3q27_destroy.argtypes = [ctypes.c_void_p]
+            lib.oracle_d3q27_set_fields.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 6
+            lib.oracle_d3q27_set_force_field.argtypes = [ctypes.c_void_p] * 4
+            lib.oracle_d3q27_set_params.argtypes = [ctypes.c_void_p, ctypes.POINTER(OracleParams)]
+            lib.oracle_d3q27_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            lib.oracle_d3q27_output.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p]
+            lib.oracle_d3q27_extract_atlas.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+            lib.oracle_d3q27_macro.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.oracle_d3q27_get_f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, dims, params: OracleParams, precision: str = "f32"):
+        self.dims = tuple(int(d) for d in dims)
+        self.cells = int(np.prod(self.dims))
+        self.h = self.lib().oracle_d3q27_create(*self.dims, 0 if precision == "f32" else 1, ctypes.byref(params))
+        if not self.h:
+            raise ValueError("oracle_d3q27_create failed")
+        self._keep = []
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib().oracle_d3q27_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def _p(a, dtype):
+        if a is None:
+            return None, None
+        arr = np.ascontiguousarray(np.asarray(a, dtype=dtype).reshape(-1))
+        return arr, arr.ctypes.data
+
+    def set_fields(self, obstacle, ux=None, uy=None, uz=None, pressure=None, temperature=None):
+        arrs = [self._p(obstacle, np.uint8)] + [self._p(v, np.float32) for v in (ux, uy, uz, pressure, temperature)]
+        self._keep = [a for a, _ in arrs]
+        self.lib().oracle_d3q27_set_fields(self.h, *[p for _, p in arrs])
+
+    def set_force_field(self, fx, fy, fz):
+        arrs = [self._p(v, np.float32) for v in (fx, fy, fz)]
+        self.lib().oracle_d3q27_set_force_field(self.h, *[p for _, p in arrs])
+
+    def set_params(self, params: OracleParams):
+        self.lib().oracle_d3q27_set_params(self.h, ctypes.byref(params))
+
+    def step(self, n: int = 1):
+        if not self.lib().oracle_d3q27_step(self.h, int(n)):
+            raise RuntimeError("oracle step failed")
+
+    def output(self, scale: float = 1.0) -> np.ndarray:
+        out = np.zeros(self.cells * 4, dtype=np.float32)
+        self.lib().oracle_d3q27_output(self.h, ctypes.c_float(scale), out.ctypes.data)
+        return out.reshape(self.cells, 4)
+
+    def atlas(self, stride: int) -> np.ndarray:
+        n = [(d + stride - 1) // stride for d in self.dims]
+        out = np.zeros(int(np.prod(n)) * 4, dtype=np.float32)
+        if not self.lib().oracle_d3q27_extract_atlas(self.h, stride, out.ctypes.data, out.size):
+            raise RuntimeError("atlas extraction failed")
+        return out.reshape(-1, 4)
+
+    def macro(self) -> np.ndarray:
+        out = np.zeros(self.cells * 4, dtype=np.float64)
+        self.lib().oracle_d3q27_macro(self.h, out.ctypes.data)
+        return out.reshape(self.cells, 4)
+
+    def populations(self) -> np.ndarray:
+        out = np.zeros(self.cells * 27, dtype=np.float64)
+        self.lib().oracle_d3q27_get_f(self.h, out.ctypes.data)
+        return out.reshape(27, self.cells)
+
+
+# ---------------------------------------------------------------- the reference library itself
+class _Face(ctypes.Structure):
+    _fields_ = [("hydrodynamic_kind", ctypes.c_int), ("thermal_kind", ctypes.c_int), ("velocity", ctypes.c_float * 3),
+                ("pressure", ctypes.c_float), ("temperature", ctypes.c_float), ("heat_flux", ctypes.c_float)]
+
+
+class RefBenchmarkConfig(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32), ("struct_size", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+        ("enabled", ctypes.c_int), ("preset", ctypes.c_int), ("reserved0", ctypes.c_int),
+        ("reynolds_number", ctypes.c_float), ("rayleigh_number", ctypes.c_float), ("prandtl_number", ctypes.c_float),
+        ("mach_number", ctypes.c_float), ("reference_density", ctypes.c_float), ("reference_temperature", ctypes.c_float),
+        ("reference_length", ctypes.c_float), ("body_force", ctypes.c_float * 3), ("gravity", ctypes.c_float * 3),
+        ("initial_velocity", ctypes.c_float * 3), ("initial_pressure", ctypes.c_float), ("initial_temperature", ctypes.c_float),
+        ("x_min", _Face), ("x_max", _Face), ("y_min", _Face), ("y_max", _Face), ("z_min", _Face), ("z_max", _Face),
+        ("reserved", ctypes.c_uint32 * 8),
+    ]
+
+
+def config_struct(struct_type, cfg: dict, default_fn):
+    """Fill a reference-layout benchmark config from the dict form used by
+    derive_params, starting from the library's own default config."""
+    c = struct_type()
+    default_fn(ctypes.byref(c))
+    c.enabled = 1
+    c.preset = 0
+    flags = c.flags
+    flags = (flags & ~FLAG_DISABLE_SGS) if cfg.get("sgs", False) else (flags | FLAG_DISABLE_SGS)
+    flags = (flags & ~FLAG_DISABLE_BUOYANCY) if cfg.get("buoyancy", False) else (flags | FLAG_DISABLE_BUOYANCY)
+    flags |= 1 << 6  # DISABLE_INTERNAL_THERMAL_SOURCE
+    if cfg.get("disable_convective", False):
+        flags |= FLAG_DISABLE_CONVECTIVE_OUTFLOW
+    c.flags = flags
+    c.reynolds_number = cfg.get("reynolds", 100.0)
+    c.reference_length = cfg.get("reference_length", 1.0)
+    for i, v in enumerate(cfg.get("initial_velocity", (0, 0, 0))):
+        c.initial_velocity[i] = v
+    for i, v in enumerate(cfg.get("body_force", (0, 0, 0))):
+        c.body_force[i] = v
+    for name, fc in zip(("x_min", "x_max", "y_min", "y_max", "z_min", "z_max"), cfg["faces"]):
+        face = getattr(c, name)
+        face.hydrodynamic_kind = int(fc.get("kind", INHERIT_GAME))
+        face.thermal_kind = 1
+        for a, v in enumerate(fc.get("velocity", (0, 0, 0))):
+            face.velocity[a] = v
+        face.pressure = fc.get("pressure", 0.0)
+    return c
+
+
+class RefLib:
+    """The reference's CPU library (oracle/_ref), driven through its C ABI."""
+
+    def __init__(self, path: Path = REF_LIB):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} missing (build with `make -C oracle ref`)")
+        lib = ctypes.CDLL(str(path))
+        lib.aero_lbm_init_rect.argtypes = [ctypes.c_int] * 5
+        lib.aero_lbm_init_rect.restype = ctypes.c_int
+        lib.aero_lbm_step_rect.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p]
+        lib.aero_lbm_step_rect.restype = ctypes.c_int
+        lib.aero_lbm_extract_flow_atlas_rect.argtypes = [ctypes.c_int] * 3 + [ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        lib.aero_lbm_extract_flow_atlas_rect.restype = ctypes.c_int
+        lib.aero_lbm_benchmark_default_config.argtypes = [ctypes.c_void_p]
+        lib.aero_lbm_benchmark_set_config.argtypes = [ctypes.c_void_p]
+        lib.aero_lbm_benchmark_set_config.restype = ctypes.c_int
+        lib.aero_lbm_last_error.restype = ctypes.c_char_p
+        lib.aero_lbm_runtime_info.restype = ctypes.c_char_p
+        self.lib = lib
+
+    def run(self, dims, cfg: dict, packet: np.ndarray, steps: int, out_every: int | None = None, key: int = 1):
+        """Initialise, configure and step; returns the final write_output
+        (cells x 4) from the last step."""
+        nx, ny, nz = dims
+        lib = self.lib
+        if not lib.aero_lbm_init_rect(nx, ny, nz, packet.shape[1], 4):
+            raise RuntimeError(lib.aero_lbm_last_error())
+        c = config_struct(RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
+        if not lib.aero_lbm_benchmark_set_config(ctypes.byref(c)):
+            raise RuntimeError("set_config failed")
+        out = np.zeros(nx * ny * nz * 4, dtype=np.float32)
+        pk = np.ascontiguousarray(packet, dtype=np.float32)
+        for s in range(steps):
+            want = (s + 1 == steps) or (out_every and (s + 1) % out_every == 0)
+            if not lib.aero_lbm_step_rect(pk.ctypes.data, nx, ny, nz, key, out.ctypes.data if want else None):
+                raise RuntimeError(lib.aero_lbm_last_error())
+        return out.reshape(-1, 4)
+
+
+# ---------------------------------------------------------------- configs
+def c1_inputs(seed: int = 1234, n: int = 32, solid_p: float = 0.05, u0=(0.05, 0.0, 0.0), noise: float = 0.005):
+    """Plain FP32 brick (32^3): solid floor z=0 + Bernoulli(p) interior,
+    u = u0 + U(-noise, noise) per component, rho = 1."""
+    rng = np.random.default_rng(seed)
+    obstacle = (rng.random((n, n, n)) < solid_p).astype(np.uint8)
+    obstacle[:, :, 0] = 1
+    u = [np.float32(u0[a]) + rng.uniform(-noise, noise, size=(n, n, n)).astype(np.float32) for a in range(3)]
+    return obstacle, u
+
+
+def c1_config(tau: float = 0.55, u0: float = 0.05, sgs: bool = True) -> dict:
+    nu = (tau - 0.5) / 3.0
+    return {
+        "reynolds": u0 / nu,
+        "reference_length": 1.0,
+        "initial_velocity": (u0, 0.0, 0.0),
+        "faces": [{"kind": PERIODIC}, {"kind": PERIODIC}, {"kind": PERIODIC}, {"kind": PERIODIC},
+                  {"kind": BOUNCE_BACK}, {"kind": BOUNCE_BACK}],
+        "sgs": sgs,
+        "buoyancy": False,
+    }
+
+
+def packet_from(obstacle, ux, uy, uz, pressure=None, temperature=None, channels: int = 11) -> np.ndarray:
+    cells = obstacle.size
+    pk = np.zeros((cells, channels), dtype=np.float32)
+    pk[:, 0] = (obstacle.reshape(-1) != 0)
+    pk[:, 5] = np.asarray(ux, np.float32).reshape(-1)
+    pk[:, 6] = np.asarray(uy, np.float32).reshape(-1)
+    pk[:, 7] = np.asarray(uz, np.float32).reshape(-1)
+    if pressure is not None:
+        pk[:, 8] = np.asarray(pressure, np.float32).reshape(-1)
+    if temperature is not None and channels > 10:
+        pk[:, 10] = np.asarray(temperature, np.float32).reshape(-1)
+    return pk
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    """max |a - b| / max |b| (normwise max-relative error)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    den = float(np.max(np.abs(b)))
+    return float(np.max(np.abs(a - b))) / (den if den > 0 else 1.0)

@@ -1,0 +1,84 @@
+"""Generate the golden fixtures in this directory from the reference library.
+
+The reference's own CPU step (compiled from its sources into
+oracle/_ref/libaero_lbm_ref.so by `make -C oracle ref`) is driven through its C
+ABI on seeded inputs; its write_output results are saved as .npz together with
+the seed and a checksum of the inputs. Run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Fixtures:
+  c1_32_1000.npz  plain FP32 brick 32^3, periodic x/y, bounce-back z, solid
+                  floor z=0 + Bernoulli(0.05) interior, tau 0.55, SGS on,
+                  u = (0.05,0,0) + U(-0.005,0.005); 1000 steps.
+  c1_16_200.npz   the same set-up at 16^3, 200 steps.
+  tunnel_16_60.npz wind-tunnel faces (velocity inlet x-, convective outflow
+                  x+, symmetry y/z), sphere obstacle, SGS off; 60 steps.
+"""
+from __future__ import annotations
+
+import hashlib
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT / "oracle"))
+import oracle as O  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def digest(*arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def tunnel_case(n: int = 16):
+    """Sphere in a wind tunnel (the reference tools' check geometry)."""
+    obst = np.zeros((n, n, n), np.uint8)
+    c = np.array([n // 3, n // 2, n // 2])
+    r = max(1.0, n * 0.12)
+    g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1)
+    obst[np.sum((g - c) ** 2, -1) <= r * r] = 1
+    u_in = 0.1
+    ux = np.where(obst == 0, np.float32(u_in), np.float32(0)).astype(np.float32)
+    zero = np.zeros_like(ux)
+    cfg = {
+        "reynolds": u_in / 0.01,
+        "initial_velocity": (u_in, 0.0, 0.0),
+        "faces": [{"kind": O.VELOCITY, "velocity": (u_in, 0.0, 0.0)}, {"kind": O.CONVECTIVE},
+                  {"kind": O.SYMMETRY}, {"kind": O.SYMMETRY}, {"kind": O.SYMMETRY}, {"kind": O.SYMMETRY}],
+        "sgs": False,
+        "buoyancy": False,
+    }
+    return obst, (ux, zero, zero.copy()), cfg
+
+
+def main() -> int:
+    O.build(ref=True)
+    ref = O.RefLib()
+    for name, n, steps in (("c1_16_200", 16, 200), ("c1_32_1000", 32, 1000)):
+        seed = 1234
+        obst, u = O.c1_inputs(seed=seed, n=n)
+        cfg = O.c1_config()
+        pk = O.packet_from(obst, *u)
+        t0 = time.time()
+        out = ref.run((n, n, n), cfg, pk, steps)
+        print(f"{name}: reference {steps} steps in {time.time() - t0:.1f}s")
+        np.savez_compressed(OUT / f"{name}.npz", out=out, seed=seed, n=n, steps=steps,
+                            input_sha256=digest(pk))
+    obst, u, cfg = tunnel_case(16)
+    pk = O.packet_from(obst, *u)
+    out = ref.run((16, 16, 16), cfg, pk, 60)
+    np.savez_compressed(OUT / "tunnel_16_60.npz", out=out, obstacle=obst, steps=60, input_sha256=digest(pk))
+    print("tunnel_16_60 written")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

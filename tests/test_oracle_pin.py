@@ -1,0 +1,86 @@
+"""Pin the oracle: its float restatement must reproduce the reference CPU step
+bit-for-bit (against the committed golden fixtures made by the reference
+library, and live against oracle/_ref when that library is present)."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+import lbm_cases
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _build_oracle():
+    O.build(ref=False)
+
+
+def _bits_equal(a, b) -> bool:
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
+
+
+def test_oracle_f32_matches_golden_c1_16():
+    g = np.load(GOLDEN / "c1_16_200.npz")
+    n, steps = int(g["n"]), int(g["steps"])
+    obst, u = O.c1_inputs(seed=int(g["seed"]), n=n)
+    o = O.Oracle((n, n, n), O.derive_params(O.c1_config()), "f32")
+    o.set_fields(obst, *u)
+    o.step(steps)
+    assert _bits_equal(o.output(), g["out"])
+
+
+def test_oracle_f32_matches_golden_tunnel():
+    g = np.load(GOLDEN / "tunnel_16_60.npz")
+    obst, u, cfg = lbm_cases.tunnel_case(16)
+    assert np.array_equal(obst, g["obstacle"])
+    o = O.Oracle((16, 16, 16), O.derive_params(cfg), "f32")
+    o.set_fields(obst, *u)
+    o.step(int(g["steps"]))
+    assert _bits_equal(o.output(), g["out"])
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("faces", [
+    "pressure_outlet", "closed", "periodic_all", "inherit_game", "inherit_bounce",
+])
+def test_oracle_f32_matches_reference_live(faces):
+    n = 12
+    rng = np.random.default_rng(7)
+    obst = (rng.random((n, n, n)) < 0.08).astype(np.uint8)
+    u = [np.float32(0.04) + rng.uniform(-0.01, 0.01, (n, n, n)).astype(np.float32),
+         rng.uniform(-0.01, 0.01, (n, n, n)).astype(np.float32),
+         rng.uniform(-0.01, 0.01, (n, n, n)).astype(np.float32)]
+    p = rng.uniform(-0.01, 0.01, (n, n, n)).astype(np.float32)
+    table = {
+        "pressure_outlet": [{"kind": O.VELOCITY, "velocity": (0.04, 0.0, 0.0)}, {"kind": O.PRESSURE, "pressure": 0.002}]
+                           + [{"kind": O.SYMMETRY}] * 4,
+        "closed": [{"kind": O.BOUNCE_BACK}] * 5 + [{"kind": O.MOVING_WALL, "velocity": (0.05, 0.0, 0.0)}],
+        "periodic_all": [{"kind": O.PERIODIC}] * 6,
+        "inherit_game": [{"kind": O.INHERIT_GAME}] * 6,
+        "inherit_bounce": [{"kind": O.INHERIT_GAME}] * 6,
+    }
+    cfg = {"reynolds": 60.0, "initial_velocity": (0.04, 0.0, 0.0), "faces": table[faces], "sgs": True,
+           "buoyancy": False, "disable_convective": faces == "inherit_bounce"}
+    pk = O.packet_from(obst, *u, pressure=p)
+    ref = O.RefLib().run((n, n, n), cfg, pk, 25)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+    o.set_fields(obst, *u, pressure=p)
+    o.step(25)
+    assert _bits_equal(o.output(), ref)
+
+
+def test_oracle_f64_is_the_same_scheme():
+    """The FP64 run differs from FP32 only by rounding over a short horizon."""
+    n = 12
+    obst, u = O.c1_inputs(seed=3, n=n)
+    p = O.derive_params(O.c1_config())
+    a = O.Oracle((n, n, n), p, "f32")
+    b = O.Oracle((n, n, n), p, "f64")
+    for o in (a, b):
+        o.set_fields(obst, *u)
+        o.step(50)
+    assert O.rel_err(a.macro()[:, 1:], b.macro()[:, 1:]) < 1e-5
