@@ -186,6 +186,7 @@ SIGNATURES = {
     "aero_lbm_b200_launch_count": (ctypes.c_ulonglong, []),
     "aero_lbm_b200_advance_rect": (_I, [_LL, _I]),
     "aero_lbm_b200_set_streaming_mode": (_I, [_I]),
+    "aero_lbm_b200_set_collision_mode": (_I, [_I]),
     "aero_lbm_b200_set_force_field": (_I, [_LL, _F32P, _I]),
     "aero_lbm_b200_set_physics_overrides": (None, [_F, _F, _I]),
     # wind-tunnel ABI

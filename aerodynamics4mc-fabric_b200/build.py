@@ -41,8 +41,14 @@ def headers() -> list[Path]:
     return sorted(p for p in CSRC.iterdir() if p.suffix in (".cuh", ".h")) + sorted(INCLUDE.glob("*.h"))
 
 
+def per_file_flags(src: Path) -> list[str]:
+    # Reference-order kernels must not contract multiply-adds (bit parity).
+    return ["--fmad=false"] if src.stem.endswith("_exact") else []
+
+
 def compile_one(src: Path, force: bool, extra: list[str]) -> Path:
     obj = BUILD / (src.name + ".o")
+    extra = [*extra, *per_file_flags(src)]
     newest_dep = max([src.stat().st_mtime] + [h.stat().st_mtime for h in headers()])
     if not force and obj.exists() and obj.stat().st_mtime >= newest_dep:
         return obj

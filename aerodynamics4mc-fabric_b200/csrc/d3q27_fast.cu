@@ -1,0 +1,26 @@
+// Instantiation of the brick-step kernels with the factorised collision
+// (multiply-add contraction allowed).
+#include "d3q27_step.cuh"
+
+namespace aero {
+
+cudaError_t launch_init_collide_fast(BrickDims d, CellFields cur, ForceField force, CollideParams cp, float* g_out,
+                                   cudaStream_t stream) {
+    return launch_init_collide_t<false>(d, cur, force, cp, g_out, stream);
+}
+
+cudaError_t launch_step_ab_fast(BrickDims d, const float* g_in, float* g_out, const uint32_t* flags_prev,
+                              const uint8_t* obstacle_prev, const float* ref_p_prev, const FaceParams* face_prev,
+                              CellFields cur, ForceField force, CollideParams cp, cudaStream_t stream) {
+    return launch_step_ab_t<false>(d, g_in, g_out, flags_prev, obstacle_prev, ref_p_prev, face_prev, cur, force, cp,
+                                   stream);
+}
+
+cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
+                                const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                                float velocity_scale, float* out, cudaStream_t stream) {
+    return launch_output_ab_t<false>(d, g, flags, obstacle, ref_p, face, stride, out_channels, velocity_scale, out,
+                                     stream);
+}
+
+}  // namespace aero

@@ -57,17 +57,27 @@ struct ForceField {
 // Launch helpers (all asynchronous on `stream`; return the launch error).
 cudaError_t launch_ingest_packet(const float* packet, int in_channels, BrickDims d, CellFields out, cudaStream_t stream);
 cudaError_t launch_build_flags(const uint8_t* obstacle, BrickDims d, FaceParams face, uint32_t* flags, cudaStream_t stream);
-cudaError_t launch_init_collide(BrickDims d, CellFields cur, ForceField force, CollideParams cp, float* g_out,
-                                cudaStream_t stream);
-cudaError_t launch_step_ab(BrickDims d, const float* g_in, float* g_out, const uint32_t* flags_prev,
-                           const uint8_t* obstacle_prev, const float* ref_p_prev, const FaceParams* face_prev,
-                           CellFields cur, ForceField force, CollideParams cp, cudaStream_t stream);
+// *_exact: reference-order collision (bit-identical to the reference CPU step);
+// *_fast: factorised collision (agrees to FP32 rounding).
+cudaError_t launch_init_collide_exact(BrickDims d, CellFields cur, ForceField force, CollideParams cp, float* g_out,
+                                      cudaStream_t stream);
+cudaError_t launch_init_collide_fast(BrickDims d, CellFields cur, ForceField force, CollideParams cp, float* g_out,
+                                     cudaStream_t stream);
+cudaError_t launch_step_ab_exact(BrickDims d, const float* g_in, float* g_out, const uint32_t* flags_prev,
+                                 const uint8_t* obstacle_prev, const float* ref_p_prev, const FaceParams* face_prev,
+                                 CellFields cur, ForceField force, CollideParams cp, cudaStream_t stream);
+cudaError_t launch_step_ab_fast(BrickDims d, const float* g_in, float* g_out, const uint32_t* flags_prev,
+                                const uint8_t* obstacle_prev, const float* ref_p_prev, const FaceParams* face_prev,
+                                CellFields cur, ForceField force, CollideParams cp, cudaStream_t stream);
 // Macro output of the streamed state S(g): write_output semantics
 // (AoS, out_channels per cell; ux,uy,uz scaled; clamp(rho - 1)).
 // `face` points to device memory.
-cudaError_t launch_output_ab(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
-                             const float* ref_p, const FaceParams* face, int stride, int out_channels,
-                             float velocity_scale, float* out, cudaStream_t stream);
+cudaError_t launch_output_ab_exact(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
+                                   const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                                   float velocity_scale, float* out, cudaStream_t stream);
+cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
+                                  const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                                  float velocity_scale, float* out, cudaStream_t stream);
 
 uint64_t kernel_launch_count();
 void count_launch();

@@ -52,6 +52,7 @@ bool g_bench_ready = false;
 cudaStream_t g_stream = nullptr;
 bool g_own_stream = false;
 int g_stream_mode = 0;  // 0 auto, 1 two-buffer, 2 in-place
+int g_collision_mode = 0;  // 0 reference-order (bit-exact), 1 factorised
 float g_smagorinsky_c = -1.0f;
 float g_buoyancy_beta_override = -1.0f;
 int g_gravity_axis = -1;
@@ -514,10 +515,12 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
 
     float* g_next = ctx.g[1 - ctx.cur];
     if (!ctx.initialized) {
-        if (!cuda_ok(launch_init_collide(d, ctx.fields(new_slot), ctx.force_field(), cp, g_next, s), "init_collide")) return false;
+        auto launch = g_collision_mode == 0 ? launch_init_collide_exact : launch_init_collide_fast;
+        if (!cuda_ok(launch(d, ctx.fields(new_slot), ctx.force_field(), cp, g_next, s), "init_collide")) return false;
     } else {
-        if (!cuda_ok(launch_step_ab(d, ctx.g[ctx.cur], g_next, ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
-                                    ctx.d_face[ctx.slot], ctx.fields(new_slot), ctx.force_field(), cp, s),
+        auto launch = g_collision_mode == 0 ? launch_step_ab_exact : launch_step_ab_fast;
+        if (!cuda_ok(launch(d, ctx.g[ctx.cur], g_next, ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
+                            ctx.d_face[ctx.slot], ctx.fields(new_slot), ctx.force_field(), cp, s),
                      "step_ab")) return false;
     }
     ctx.cur = 1 - ctx.cur;
@@ -542,8 +545,9 @@ bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_
         if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.out), bytes), "cudaMalloc(output)")) return false;
         ctx.out_cap = bytes;
     }
-    if (!cuda_ok(launch_output_ab(d, ctx.g[ctx.cur], ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
-                                  ctx.d_face[ctx.slot], stride, out_ch, scale, ctx.out, s),
+    auto launch = g_collision_mode == 0 ? launch_output_ab_exact : launch_output_ab_fast;
+    if (!cuda_ok(launch(d, ctx.g[ctx.cur], ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
+                        ctx.d_face[ctx.slot], stride, out_ch, scale, ctx.out, s),
                  "output")) return false;
     if (!cuda_ok(cudaMemcpyAsync(host_out, ctx.out, bytes, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(output)")) return false;
     return cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize(output)");
@@ -890,6 +894,13 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streaming_mode(int mode) {
     std::lock_guard<std::recursive_mutex> lk(g_mutex);
     if (mode < 0 || mode > 2) return 0;
     g_stream_mode = mode;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_collision_mode(int mode) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (mode < 0 || mode > 1) return 0;
+    g_collision_mode = mode;
     return 1;
 }
 

@@ -212,6 +212,11 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_advance_rect(long long context_key, int s
 /* Select the streaming scheme of a context: 0 automatic (in-place when every
  * face is local), 1 two-buffer pull, 2 in-place esoteric pull. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streaming_mode(int mode);
+/* FP32 collision arithmetic: 0 = the reference's operation order, no
+ * multiply-add contraction (bit-identical to the reference CPU step; default),
+ * 1 = factorised moment transforms with contraction (same scheme, fewer flops,
+ * agrees to FP32 rounding per step). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_collision_mode(int mode);
 /* Per-cell force density field for a context (3 x cells floats, SoA order
  * fx[cells], fy[cells], fz[cells]; host pointer; null clears). */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_force_field(long long context_key, const float* force_soa, int value_count);

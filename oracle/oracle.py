@@ -351,3 +351,19 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> float:
     b = np.asarray(b, np.float64)
     den = float(np.max(np.abs(b)))
     return float(np.max(np.abs(a - b))) / (den if den > 0 else 1.0)
+
+
+def flow_errors(out: np.ndarray, ref: np.ndarray) -> dict:
+    """Parity metric on write_output-style arrays (cells x 4: ux, uy, uz, rho-1).
+
+    u   : max over cells and components |u - u_ref| / max cell speed of ref
+    rho : max |rho - rho_ref| / max rho_ref, with rho = 1 + channel 3
+    (velocity error relative to the flow speed scale and density error relative
+    to the density; the pressure proxy rho - 1 is ~1e-3, so its own relative
+    error would only measure FP32 rounding of rho ~ 1)."""
+    out = np.asarray(out, np.float64)
+    ref = np.asarray(ref, np.float64)
+    speed = float(np.max(np.linalg.norm(ref[:, :3], axis=1)))
+    u = float(np.max(np.abs(out[:, :3] - ref[:, :3]))) / (speed if speed > 0 else 1.0)
+    rho = float(np.max(np.abs(out[:, 3] - ref[:, 3]))) / float(np.max(1.0 + ref[:, 3]))
+    return {"u": u, "rho": rho}

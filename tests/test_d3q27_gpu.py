@@ -1,9 +1,14 @@
 """FP32 D3Q27 brick step on the GPU against the reference (golden fixtures made
 by the reference library) and the oracle.
 
-Tolerance: max |gpu - ref| / max |ref| <= 1e-5 per output channel (velocity
-components and the pressure proxy) after the stated number of steps; masks,
-solid outputs and atlas indexing are exact."""
+The default FP32 collision (collision mode 0) performs the reference's
+operations in the reference's order, so its outputs must be bit-identical to
+the reference's: these tests compare bits. The factorised collision (mode 1)
+is the same scheme with different rounding; the porous C1 flow amplifies
+rounding differences exponentially (the reference's own FP32 and FP64 runs
+separate by ~1e-4 after 300 steps), so mode 1 is checked with
+oracle.flow_errors <= 1e-5 (velocity relative to the max speed, density
+relative to rho) over a 30-step horizon."""
 from __future__ import annotations
 
 import ctypes
@@ -22,38 +27,56 @@ TOL = 1e-5
 
 
 def channel_errors(out, ref):
-    return [O.rel_err(out[:, c], ref[:, c]) for c in range(4)]
+    e = O.flow_errors(out, ref)
+    return [e["u"], e["rho"]]
+
+
+def assert_bits(out, ref):
+    a = np.asarray(out, np.float32)
+    b = np.asarray(ref, np.float32)
+    diff = np.nonzero(a.view(np.uint32) != b.view(np.uint32))
+    assert diff[0].size == 0, (f"{diff[0].size} values differ; first at {diff[0][0]},{diff[1][0]}: "
+                               f"{a[diff][0]!r} vs {b[diff][0]!r}; errors {channel_errors(a, b)}")
 
 
 @pytest.mark.parametrize("mode", [1, 0])
-def test_c1_16_matches_reference(gpu, mode):
+def test_c1_16_bit_identical_to_reference(gpu, mode):
     g = np.load(GOLDEN / "c1_16_200.npz")
     n, steps = int(g["n"]), int(g["steps"])
     obst, u = O.c1_inputs(seed=int(g["seed"]), n=n)
     out, ctx = lbm_cases.run_product(gpu, (n, n, n), O.c1_config(), O.packet_from(obst, *u), steps, streaming_mode=mode)
-    ref = g["out"]
-    errs = channel_errors(out, ref)
-    assert max(errs) <= TOL, errs
+    assert_bits(out, g["out"])
     solid = obst.reshape(-1) != 0
     assert np.all(out[solid] == 0.0)
 
 
 @pytest.mark.parametrize("mode", [1, 0])
-def test_c1_32_1000_matches_reference(gpu, mode):
+def test_c1_32_1000_bit_identical_to_reference(gpu, mode):
     g = np.load(GOLDEN / "c1_32_1000.npz")
     n, steps = int(g["n"]), int(g["steps"])
     obst, u = O.c1_inputs(seed=int(g["seed"]), n=n)
     out, ctx = lbm_cases.run_product(gpu, (n, n, n), O.c1_config(), O.packet_from(obst, *u), steps, streaming_mode=mode)
-    errs = channel_errors(out, g["out"])
-    assert max(errs) <= TOL, errs
+    assert_bits(out, g["out"])
 
 
-def test_tunnel_matches_reference(gpu):
+def test_tunnel_bit_identical_to_reference(gpu):
     g = np.load(GOLDEN / "tunnel_16_60.npz")
     obst, u, cfg = lbm_cases.tunnel_case(16)
     out, ctx = lbm_cases.run_product(gpu, (16, 16, 16), cfg, O.packet_from(obst, *u), int(g["steps"]))
-    errs = channel_errors(out, g["out"])
+    assert_bits(out, g["out"])
+
+
+def test_factorised_collision_within_tolerance(gpu):
+    n, steps = 16, 30
+    obst, u = O.c1_inputs(seed=77, n=n)
+    cfg = O.c1_config()
+    out, ctx = lbm_cases.run_product(gpu, (n, n, n), cfg, O.packet_from(obst, *u), steps, collision_mode=1)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+    o.set_fields(obst, *u)
+    o.step(steps)
+    errs = channel_errors(out, o.output())
     assert max(errs) <= TOL, errs
+    gpu.aero_lbm_b200_set_collision_mode(0)
 
 
 @pytest.mark.parametrize("faces", ["pressure_outlet", "closed", "inherit_game", "periodic_all"])
@@ -78,8 +101,7 @@ def test_faces_match_oracle(gpu, faces):
     o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
     o.set_fields(obst, *u, pressure=p)
     o.step(40)
-    errs = channel_errors(out, o.output())
-    assert max(errs) <= TOL, errs
+    assert_bits(out, o.output())
 
 
 def test_atlas_and_flow_state_match_oracle(gpu):
@@ -94,10 +116,8 @@ def test_atlas_and_flow_state_match_oracle(gpu):
         a = ctx.atlas(stride)
         b = o.atlas(stride)
         assert a.shape == b.shape
-        assert max(channel_errors(a, b)) <= TOL
-        # solid samples are exactly zero at the same atlas positions
-        assert np.array_equal(np.all(a == 0, axis=1) & np.all(b == 0, axis=1), np.all(b == 0, axis=1))
-    assert max(channel_errors(ctx.flow_state(), o.output())) <= TOL
+        assert_bits(a, b)
+    assert_bits(ctx.flow_state(), o.output())
 
 
 def test_cached_step_equals_packet_step(gpu):
