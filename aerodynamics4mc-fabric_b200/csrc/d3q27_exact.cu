@@ -1,7 +1,7 @@
 // Instantiation of the brick-step kernels with the reference-order collision.
 // Built with --fmad=false (see build.py): no multiply-add contraction, so the
 // collision and output round exactly like the reference CPU step.
-#include "d3q27_step.cuh"
+#include "ip_launch.h"
 
 namespace aero {
 
@@ -22,6 +22,15 @@ cudaError_t launch_output_ab_exact(BrickDims d, const float* g, const uint32_t* 
                                 float velocity_scale, float* out, cudaStream_t stream) {
     return launch_output_ab_t<true>(d, g, flags, obstacle, ref_p, face, stride, out_channels, velocity_scale, out,
                                      stream);
+}
+
+
+cudaError_t ip_init_f32_exact(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, true>::init(f, a, s); }
+cudaError_t ip_step_f32_exact(float* f, const IpArgs& a, bool transitions, cudaStream_t s) {
+    return IpLaunch<StoreF32, true>::step(f, a, transitions, s);
+}
+cudaError_t ip_output_f32_exact(const float* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
+    return IpLaunch<StoreF32, true>::output(f, a, stride, out_ch, scale, out, s);
 }
 
 }  // namespace aero

@@ -1,6 +1,6 @@
 // Instantiation of the brick-step kernels with the factorised collision
 // (multiply-add contraction allowed).
-#include "d3q27_step.cuh"
+#include "ip_launch.h"
 
 namespace aero {
 
@@ -21,6 +21,23 @@ cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* f
                                 float velocity_scale, float* out, cudaStream_t stream) {
     return launch_output_ab_t<false>(d, g, flags, obstacle, ref_p, face, stride, out_channels, velocity_scale, out,
                                      stream);
+}
+
+
+cudaError_t ip_init_f32_fast(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, false>::init(f, a, s); }
+cudaError_t ip_step_f32_fast(float* f, const IpArgs& a, bool transitions, cudaStream_t s) {
+    return IpLaunch<StoreF32, false>::step(f, a, transitions, s);
+}
+cudaError_t ip_output_f32_fast(const float* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
+    return IpLaunch<StoreF32, false>::output(f, a, stride, out_ch, scale, out, s);
+}
+
+cudaError_t ip_init_f16_fast(__half* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF16Dev, false>::init(f, a, s); }
+cudaError_t ip_step_f16_fast(__half* f, const IpArgs& a, bool transitions, cudaStream_t s) {
+    return IpLaunch<StoreF16Dev, false>::step(f, a, transitions, s);
+}
+cudaError_t ip_output_f16_fast(const __half* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
+    return IpLaunch<StoreF16Dev, false>::output(f, a, stride, out_ch, scale, out, s);
 }
 
 }  // namespace aero

@@ -1,0 +1,220 @@
+// In-place (esoteric pull) D3Q27 brick step kernels, templated on the
+// population storage (FP32 or FP16 deviation) and the collision arithmetic
+// (reference order or factorised). See inplace27.cuh for the slot maps.
+//
+// The in-place layout supports the faces whose pulled value is local to the
+// pulling cell: periodic, bounce-back and the equilibrium faces (velocity,
+// pressure, moving wall). Symmetry and convective outflow read other cells'
+// post-collision populations, which the in-place update overwrites within the
+// step; contexts with such faces use the two-buffer kernels.
+#pragma once
+
+#include "d3q27_step.cuh"
+#include "inplace27.cuh"
+
+namespace aero {
+
+struct IpArgs {
+    PadGeom g;
+    int parity;                      // parity of this step's slot maps
+    const uint32_t* flags_prev;      // pull classification of the streaming call
+    const uint8_t* obstacle_cur;     // mask of this call (collide / skip)
+    const float* ref_p_prev;         // pressure proxy of the streaming call (equilibrium faces)
+    const FaceParams* face_prev;     // faces of the streaming call (device memory)
+    CellFields cur;
+    ForceField force;
+    CollideParams cp;
+    Fp16Scale sc;
+};
+
+// Equilibrium value of a face (velocity / pressure / moving wall), the only
+// non-bounce-back faces the in-place layout accepts
+// (boundary_equilibrium_value, jni.cpp:1519-1561).
+__device__ __forceinline__ float ip_face_equilibrium(const FaceParams& F, int q, float ref_p, int sx, int sy, int sz,
+                                                     int nx, int ny, int nz) {
+    const int face = oob_face(sx, sy, sz, nx, ny, nz);
+    const int kind = F.kind[face];
+    float rho = 1.0f + clampf_dev(ref_p, -0.03f, 0.03f);
+    float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+    if (kind == kHydroPressure) {
+        rho = 1.0f + clampf_dev(F.pressure[face], -0.03f, 0.03f);
+    } else {
+        ux = F.velocity[face][0]; uy = F.velocity[face][1]; uz = F.velocity[face][2];
+    }
+    rho = clampf_dev(rho, 0.97f, 1.03f);
+    const float s2 = ux * ux + uy * uy + uz * uz;
+    if (s2 > F.max_speed * F.max_speed && s2 > 0.0f) {
+        const float sc = F.max_speed / sqrtf(s2);
+        ux *= sc; uy *= sc; uz *= sc;
+    }
+    return feq27(q, rho, ux, uy, uz);
+}
+
+// Incoming populations of a fluid cell at parity p.
+template <class S>
+__device__ __forceinline__ void ip_pull(const typename S::T* __restrict__ f, const IpArgs& a, const PadGeom& G,
+                                        const NeighbourOffsets& o, int own, uint32_t w, long long cell, int x, int y,
+                                        int z, int p, const float* ref_p, const FaceParams* F, float (&fl)[27]) {
+    if (!(w & kFlagFaceSpecial)) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            int c, d;
+            incoming_slot(o, own, q, p, (w >> q) & 1u, c, d);
+            fl[q] = S::load(f + (long long)d * G.pcells + c, q, a.sc);
+        }
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const bool bb = (w >> q) & 1u;
+        const int sx = x - q_cx(q), sy = y - q_cy(q), sz = z - q_cz(q);
+        const bool oob = (!G.wrap[0] && (sx < 0 || sx >= G.nx)) || (!G.wrap[1] && (sy < 0 || sy >= G.ny)) ||
+                         (!G.wrap[2] && (sz < 0 || sz >= G.nz));
+        if (!bb && oob) {
+            fl[q] = ip_face_equilibrium(*F, q, ref_p[cell], sx, sy, sz, G.nx, G.ny, G.nz);
+        } else {
+            int c, d;
+            incoming_slot(o, own, q, p, bb, c, d);
+            fl[q] = S::load(f + (long long)d * G.pcells + c, q, a.sc);
+        }
+    }
+}
+
+template <class S>
+__device__ __forceinline__ void ip_push(typename S::T* __restrict__ f, const IpArgs& a, const PadGeom& G,
+                                        const NeighbourOffsets& o, int own, int p, const float (&fl)[27]) {
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        int c, d;
+        outgoing_slot(o, own, q, p, c, d);
+        S::store(f + (long long)d * G.pcells + c, q, fl[q], a.sc);
+    }
+}
+
+__device__ __forceinline__ void cell_coords(const PadGeom& G, long long cell, int& x, int& y, int& z) {
+    z = (int)(cell % G.nz);
+    y = (int)((cell / G.nz) % G.ny);
+    x = (int)(cell / ((long long)G.ny * G.nz));
+}
+
+// Fused pull-stream + collide + push of one step.
+template <class S, bool kExact>
+__global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
+    const PadGeom G = a.g;
+    const long long cells = (long long)G.nx * G.ny * G.nz;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= cells) return;
+    const uint32_t w = a.flags_prev[cell];
+    if (w & kFlagSelfSolid) return;  // memory of a solid cell is link storage; transitions run separately
+    int x, y, z;
+    cell_coords(G, cell, x, y, z);
+    const int own = pad_index(G, x, y, z);
+    const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
+    float fl[27];
+    ip_pull<S>(f, a, G, o, own, w, cell, x, y, z, a.parity, a.ref_p_prev, a.face_prev, fl);
+    if (!a.obstacle_cur[cell]) collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell);
+    ip_push<S>(f, a, G, o, own, a.parity, fl);
+}
+
+// Cells that were solid at the streaming call and are fluid now: start from
+// the rest equilibrium (the state a cell holds while solid since
+// initialisation), collide and push. Runs after step_ip_kernel of the same
+// parity; the slots it writes were only read (as bounce-back) by that launch.
+template <class S, bool kExact>
+__global__ void __launch_bounds__(128) transition_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
+    const PadGeom G = a.g;
+    const long long cells = (long long)G.nx * G.ny * G.nz;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= cells) return;
+    if (!(a.flags_prev[cell] & kFlagSelfSolid) || a.obstacle_cur[cell]) return;
+    int x, y, z;
+    cell_coords(G, cell, x, y, z);
+    const int own = pad_index(G, x, y, z);
+    const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
+    float fl[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) fl[q] = q_w(q);
+    collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell);
+    ip_push<S>(f, a, G, o, own, a.parity, fl);
+}
+
+// First call: populations from the reference state (initialize_distributions,
+// jni.cpp:1752-1781), collide, push with parity 0. Solid cells hold nothing.
+template <class S, bool kExact>
+__global__ void __launch_bounds__(128) init_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
+    const PadGeom G = a.g;
+    const long long cells = (long long)G.nx * G.ny * G.nz;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= cells) return;
+    if (a.cur.obstacle[cell]) return;
+    int x, y, z;
+    cell_coords(G, cell, x, y, z);
+    const int own = pad_index(G, x, y, z);
+    const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
+    const float rho = clampf_dev(1.0f + a.cur.ref_p[cell], 0.97f, 1.03f);
+    const float ux = a.cur.ref_ux[cell], uy = a.cur.ref_uy[cell], uz = a.cur.ref_uz[cell];
+    float fl[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) fl[q] = feq27(q, rho, ux, uy, uz);
+    collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell);
+    ip_push<S>(f, a, G, o, own, 0, fl);
+}
+
+// Macro output of the streamed state (what the next step would pull), with
+// write_output / strided-extract semantics. Read-only.
+template <class S, bool kExact>
+__global__ void output_ip_kernel(const typename S::T* __restrict__ f, IpArgs a, int stride, int ax_n, int ay_n, int az_n,
+                                 int out_ch, float scale, float* __restrict__ out) {
+    const PadGeom G = a.g;
+    const long long n_out = (long long)ax_n * ay_n * az_n;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_out) return;
+    const int az = (int)(i % az_n);
+    const int ay = (int)((i / az_n) % ay_n);
+    const int ax = (int)(i / ((long long)ay_n * az_n));
+    const int x = min(G.nx - 1, ax * stride), y = min(G.ny - 1, ay * stride), z = min(G.nz - 1, az * stride);
+    const long long cell = ((long long)x * G.ny + y) * G.nz + z;
+    const uint32_t w = a.flags_prev[cell];
+    float o4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (!(w & kFlagSelfSolid)) {
+        const int own = pad_index(G, x, y, z);
+        const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
+        float fl[27];
+        ip_pull<S>(f, a, G, o, own, w, cell, x, y, z, a.parity, a.ref_p_prev, a.face_prev, fl);
+        if (kExact) exact::macro_out_exact(fl, false, scale, o4);
+        else macro_out(fl, false, scale, o4);
+    }
+    float* dst = out + i * out_ch;
+    dst[0] = o4[0]; dst[1] = o4[1]; dst[2] = o4[2]; dst[3] = o4[3];
+    for (int c = 4; c < out_ch; ++c) dst[c] = 0.0f;
+}
+
+template <class S, bool kExact>
+struct IpLaunch {
+    static cudaError_t init(typename S::T* f, const IpArgs& a, cudaStream_t s) {
+        const long long cells = (long long)a.g.nx * a.g.ny * a.g.nz;
+        init_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
+        count_launch();
+        return cudaGetLastError();
+    }
+    static cudaError_t step(typename S::T* f, const IpArgs& a, bool transitions, cudaStream_t s) {
+        const long long cells = (long long)a.g.nx * a.g.ny * a.g.nz;
+        step_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
+        count_launch();
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess || !transitions) return e;
+        transition_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
+        count_launch();
+        return cudaGetLastError();
+    }
+    static cudaError_t output(const typename S::T* f, const IpArgs& a, int stride, int out_ch, float scale, float* out,
+                              cudaStream_t s) {
+        const int sx = (a.g.nx + stride - 1) / stride, sy = (a.g.ny + stride - 1) / stride, sz = (a.g.nz + stride - 1) / stride;
+        const long long n = (long long)sx * sy * sz;
+        output_ip_kernel<S, kExact><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a, stride, sx, sy, sz, out_ch, scale, out);
+        count_launch();
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace aero

@@ -1,0 +1,135 @@
+// In-place ("esoteric pull") D3Q27 storage: one population array updated in
+// place, alternating between two slot maps on even and odd steps
+// (Lehmann et al., "Esoteric Pull and Esoteric Push", Computation 10(6) 2022).
+//
+// Directions are paired (q, 26 - q); q > 13 is the "positive" member. Every
+// link x -> x + c (c positive) keeps its two in-transit populations in the
+// memory of the cell at the link's positive end. With parity p of the step:
+//   incoming f_q, q positive : own cell,        slot (p == 0 ? opp(q) : q)
+//   incoming f_q, q negative : cell x - c_q,    slot (p == 0 ? opp(q) : q)
+//   outgoing f*_q, q positive: cell x + c_q,    slot (p == 0 ? q : opp(q))
+//   outgoing f*_q, q negative: own cell,        slot (p == 0 ? q : opp(q))
+//   rest q = 13              : own cell, slot 13
+// Every slot is read and then overwritten by exactly one cell per step, so the
+// update is race-free with a single array. Half-way bounce-back of direction q
+// (its source is solid, or outside a bounce-back face) reads the same cell's
+// slot with the parity flipped: that slot holds the cell's own outgoing
+// opp(q) population of the previous step, which no other cell touches.
+//
+// Storage is padded by one ghost cell on every side: ghost cells are never
+// updated and hold the in-transit populations of links that cross a
+// non-periodic face (bounce-back faces read them back; equilibrium faces
+// ignore them). Periodic axes wrap instead. Padded index:
+//   p(x, y, z) = ((x + 1) * (ny + 2) + (y + 1)) * (nz + 2) + (z + 1).
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include "lattice.cuh"
+
+namespace aero {
+
+__host__ __device__ constexpr bool q_positive(int q) { return q > 13; }
+
+// Per-brick FP16 storage scale (deviation from the rest weights).
+struct Fp16Scale {
+    float scale;      // S: stored half = (f - w_q) * S / w_q
+};
+
+// Population storage policies.
+struct StoreF32 {
+    using T = float;
+    __device__ __forceinline__ static float load(const float* __restrict__ a, int q, const Fp16Scale&) {
+        (void)q;
+        return __ldg(a);
+    }
+    __device__ __forceinline__ static void store(float* __restrict__ a, int q, float v, const Fp16Scale&) {
+        (void)q;
+        *a = v;
+    }
+};
+
+// FP16 deviation storage: h = (f - w_q) * (S / w_q), f = w_q + h * (w_q / S).
+// Stored values are clamped to the finite FP16 range before rounding.
+struct StoreF16Dev {
+    using T = __half;
+    __device__ __forceinline__ static float load(const __half* __restrict__ a, int q, const Fp16Scale& s) {
+        const float h = __half2float(__ldg(a));
+        return fmaf(h, q_w(q) / s.scale, q_w(q));
+    }
+    __device__ __forceinline__ static void store(__half* __restrict__ a, int q, float v, const Fp16Scale& s) {
+        const float d = (v - q_w(q)) * (s.scale / q_w(q));
+        *a = __float2half_rn(fminf(65504.0f, fmaxf(-65504.0f, d)));
+    }
+};
+
+// Geometry of one padded brick and the per-axis wrap rule.
+struct PadGeom {
+    int nx, ny, nz;
+    int py, pz;            // padded ny + 2, nz + 2
+    int pcells;            // (nx + 2) (ny + 2) (nz + 2)
+    int wrap[3];           // axis wraps (periodic on both faces)
+};
+
+__host__ __device__ inline PadGeom make_pad_geom(int nx, int ny, int nz, int periodic_mask) {
+    PadGeom g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    g.py = ny + 2; g.pz = nz + 2;
+    g.pcells = (nx + 2) * (ny + 2) * (nz + 2);
+    g.wrap[0] = (periodic_mask >> 0) & 1;
+    g.wrap[1] = (periodic_mask >> 1) & 1;
+    g.wrap[2] = (periodic_mask >> 2) & 1;
+    return g;
+}
+
+__device__ __forceinline__ int pad_index(const PadGeom& g, int x, int y, int z) {
+    return ((x + 1) * g.py + (y + 1)) * g.pz + (z + 1);
+}
+
+// Neighbour coordinate along one axis: wrapped on periodic axes, else may be
+// -1 or n (a ghost cell).
+__device__ __forceinline__ int axis_neighbour(int c, int d, int n, int wrap) {
+    int v = c + d;
+    if (wrap) v = v < 0 ? v + n : (v >= n ? v - n : v);
+    return v;
+}
+
+// Offsets of the three neighbour positions (-1, 0, +1) per axis in padded
+// index units, so that the padded index of x + c is X[cx+1] + Y[cy+1] + Z[cz+1].
+struct NeighbourOffsets {
+    int X[3], Y[3], Z[3];
+};
+
+__device__ __forceinline__ NeighbourOffsets neighbour_offsets(const PadGeom& g, int x, int y, int z) {
+    NeighbourOffsets o;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        o.X[k] = (axis_neighbour(x, k - 1, g.nx, g.wrap[0]) + 1) * g.py * g.pz;
+        o.Y[k] = (axis_neighbour(y, k - 1, g.ny, g.wrap[1]) + 1) * g.pz;
+        o.Z[k] = axis_neighbour(z, k - 1, g.nz, g.wrap[2]) + 1;
+    }
+    return o;
+}
+
+// Padded index of x + d*c_q (d = +1 destination, -1 source).
+__device__ __forceinline__ int link_cell(const NeighbourOffsets& o, int q, int d) {
+    const int ix = 1 + d * q_cx(q), iy = 1 + d * q_cy(q), iz = 1 + d * q_cz(q);
+    return o.X[ix] + o.Y[iy] + o.Z[iz];
+}
+
+// Memory cell and slot direction of incoming population q at parity p
+// (bounce = read the flipped slot).
+__device__ __forceinline__ void incoming_slot(const NeighbourOffsets& o, int own, int q, int p, bool bounce,
+                                              int& cell, int& dir) {
+    const bool even = (p == 0) != bounce;
+    dir = q == kRest27 ? kRest27 : (even ? q_opp(q) : q);
+    cell = (q == kRest27 || q_positive(q)) ? own : link_cell(o, q, -1);
+}
+
+// Memory cell and slot direction of outgoing population q at parity p.
+__device__ __forceinline__ void outgoing_slot(const NeighbourOffsets& o, int own, int q, int p, int& cell, int& dir) {
+    dir = q == kRest27 ? kRest27 : (p == 0 ? q : q_opp(q));
+    cell = (q == kRest27 || !q_positive(q)) ? own : link_cell(o, q, +1);
+}
+
+}  // namespace aero

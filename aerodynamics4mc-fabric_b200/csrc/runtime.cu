@@ -19,6 +19,7 @@
 
 #include "../../include/aero_lbm_b200.h"
 #include "d3q27_kernels.cuh"
+#include "ip_launch.h"
 #include "runtime_internal.h"
 
 namespace aero {
@@ -391,7 +392,10 @@ void Context::release_device() {
     fr(reinterpret_cast<void*&>(packet));
     fr(reinterpret_cast<void*&>(out));
     fr(reinterpret_cast<void*&>(force));
+    fr(ip);
     packet_cap = out_cap = 0;
+    layout = 0;
+    parity = 0;
     allocated = false;
     initialized = false;
 }
@@ -404,7 +408,6 @@ bool Context::allocate(int nx_, int ny_, int nz_) {
     auto al = [&](void** p, size_t bytes) { return cuda_ok(cudaMalloc(p, bytes), "cudaMalloc"); };
     bool ok = true;
     for (int i = 0; i < 2 && ok; ++i) {
-        ok = ok && al(reinterpret_cast<void**>(&g[i]), c * 27 * sizeof(float));
         ok = ok && al(reinterpret_cast<void**>(&obstacle[i]), c);
         ok = ok && al(reinterpret_cast<void**>(&ref_p[i]), c * sizeof(float));
         ok = ok && al(reinterpret_cast<void**>(&flags[i]), c * sizeof(uint32_t));
@@ -461,6 +464,102 @@ const RuntimeView runtime_view() {
     return RuntimeView{g_cfg.initialized, g_cfg.nx, g_cfg.ny, g_cfg.nz, g_cfg.input_channels, g_cfg.output_channels};
 }
 
+// The in-place layout needs faces whose pulled value is local to the pulling
+// cell (periodic on both sides of an axis, bounce-back, equilibrium faces).
+static bool inplace_faces_ok(const FaceParams& f) {
+    for (int a = 0; a < 3; ++a)
+        if (f.wrap_lo[a] != f.wrap_hi[a]) return false;
+    for (int i = 0; i < 6; ++i) {
+        const int k = f.kind[i];
+        if (k == kHydroPeriodic || k == kHydroBounceBack || k == kHydroVelocity || k == kHydroPressure ||
+            k == kHydroMovingWall)
+            continue;
+        if (k == kHydroInheritGame && f.disable_convective) continue;
+        return false;
+    }
+    return true;
+}
+
+static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const CollideParams& cp) {
+    IpArgs a{};
+    a.g = make_pad_geom(ctx.nx, ctx.ny, ctx.nz, ctx.periodic_mask);
+    a.flags_prev = ctx.flags[stream_slot];
+    a.obstacle_cur = ctx.obstacle[cur_slot];
+    a.ref_p_prev = ctx.ref_p[stream_slot];
+    a.face_prev = ctx.d_face[stream_slot];
+    a.cur = ctx.fields(cur_slot);
+    a.force = ctx.force_field();
+    a.cp = cp;
+    a.sc = Fp16Scale{ctx.fp16_scale};
+    return a;
+}
+
+// Per-brick FP16 scale: a power of two S such that the normalised deviation
+// (f - w)/w of the largest expected state (reference speed u, |rho - 1| <= 0.03,
+// a non-equilibrium margin of 0.5) times S stays below 2^14.
+static float fp16_scale_for_speed(float umax) {
+    umax = std::min(std::max(umax, 0.0f), 0.57735026919f * 0.6f);
+    const float dev = 0.03f + 3.0f * 1.7320508f * umax + 15.0f * umax * umax + 0.5f;
+    float s = 1.0f;
+    while (s * 2.0f * dev < 16384.0f && s < 65536.0f) s *= 2.0f;
+    return s;
+}
+
+// First step of a context: pick the layout, the in-place variant and allocate.
+static bool choose_layout(Context& ctx, const FaceParams& face, const float* packet, bool host_packet) {
+    const bool local = inplace_faces_ok(face);
+    const bool want_fp16 = g_realtime_solver_mode == AERO_LBM_REALTIME_SOLVER_D3Q27_FP16_INPLACE_EXPERIMENTAL;
+    int layout = 0;
+    if (g_stream_mode == 2) {
+        if (!local) {
+            set_error("in-place streaming requested but a face is symmetry or convective outflow (non-local)");
+            return false;
+        }
+        layout = 1;
+    } else if (g_stream_mode == 0) {
+        layout = local ? 1 : 0;
+    }
+    if (want_fp16 && local) layout = 1;
+    ctx.layout = layout;
+    const size_t c = (size_t)ctx.cells;
+    if (layout == 0) {
+        for (int i = 0; i < 2; ++i)
+            if (!ctx.g[i] && !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.g[i]), c * 27 * sizeof(float)), "cudaMalloc(populations)"))
+                return false;
+        ctx.bytes_per_step = (uint64_t)c * (27ull * 4 * 2 + 1);
+        return true;
+    }
+    ctx.periodic_mask = face.periodic_mask;
+    ctx.ip_variant = want_fp16 ? kIpF16Fast : (g_collision_mode == 0 ? kIpF32Exact : kIpF32Fast);
+    const PadGeom g = make_pad_geom(ctx.nx, ctx.ny, ctx.nz, ctx.periodic_mask);
+    const size_t elem = ctx.ip_variant == kIpF16Fast ? 2 : 4;
+    const size_t bytes = (size_t)g.pcells * 27 * elem;
+    if ((long long)g.pcells * 27 >= (1LL << 31)) {
+        set_error("in-place layout: brick too large for 32-bit slot indexing");
+        return false;
+    }
+    if (!cuda_ok(cudaMalloc(&ctx.ip, bytes), "cudaMalloc(in-place populations)")) return false;
+    if (!cuda_ok(cudaMemsetAsync(ctx.ip, 0, bytes, current_stream()), "cudaMemset(in-place)")) return false;
+    ctx.bytes_per_step = (uint64_t)c * (27ull * elem * 2 + 1);
+    if (ctx.ip_variant == kIpF16Fast) {
+        float umax = 0.0f;
+        for (int i = 0; i < 6; ++i)
+            umax = std::max(umax, std::sqrt(face.velocity[i][0] * face.velocity[i][0] + face.velocity[i][1] * face.velocity[i][1] +
+                                            face.velocity[i][2] * face.velocity[i][2]));
+        if (packet && host_packet) {
+            const int in_ch = g_cfg.input_channels;
+            for (size_t i = 0; i < c; ++i) {
+                const float* p = packet + i * in_ch;
+                if (p[0] > 0.5f) continue;
+                const float s2 = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
+                if (std::isfinite(s2)) umax = std::max(umax, std::sqrt(s2));
+            }
+        }
+        ctx.fp16_scale = fp16_scale_for_speed(umax);
+    }
+    return true;
+}
+
 // Build the pull classification of `slot` for faces `face` and keep a device
 // copy of the faces for the kernels that stream with this slot.
 static bool classify(Context& ctx, int slot, const FaceParams& face, const BrickDims& d, cudaStream_t s) {
@@ -513,17 +612,36 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         if (!classify(ctx, new_slot, face_now, d, s)) return false;
     }
 
-    float* g_next = ctx.g[1 - ctx.cur];
-    if (!ctx.initialized) {
-        auto launch = g_collision_mode == 0 ? launch_init_collide_exact : launch_init_collide_fast;
-        if (!cuda_ok(launch(d, ctx.fields(new_slot), ctx.force_field(), cp, g_next, s), "init_collide")) return false;
+    if (!ctx.initialized && !choose_layout(ctx, face_now, packet, host_packet)) return false;
+    if (ctx.layout == 0) {
+        float* g_next = ctx.g[1 - ctx.cur];
+        if (!ctx.initialized) {
+            auto launch = g_collision_mode == 0 ? launch_init_collide_exact : launch_init_collide_fast;
+            if (!cuda_ok(launch(d, ctx.fields(new_slot), ctx.force_field(), cp, g_next, s), "init_collide")) return false;
+        } else {
+            auto launch = g_collision_mode == 0 ? launch_step_ab_exact : launch_step_ab_fast;
+            if (!cuda_ok(launch(d, ctx.g[ctx.cur], g_next, ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
+                                ctx.d_face[ctx.slot], ctx.fields(new_slot), ctx.force_field(), cp, s),
+                         "step_ab")) return false;
+        }
+        ctx.cur = 1 - ctx.cur;
     } else {
-        auto launch = g_collision_mode == 0 ? launch_step_ab_exact : launch_step_ab_fast;
-        if (!cuda_ok(launch(d, ctx.g[ctx.cur], g_next, ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
-                            ctx.d_face[ctx.slot], ctx.fields(new_slot), ctx.force_field(), cp, s),
-                     "step_ab")) return false;
+        if (ctx.initialized && !inplace_faces_ok(face_now)) {
+            set_error("in-place context: the faces changed to a kind that needs the two-buffer layout "
+                      "(symmetry or convective outflow); release and re-create the context");
+            return false;
+        }
+        IpArgs a = ip_args(ctx, ctx.slot, new_slot, cp);
+        if (!ctx.initialized) {
+            a.parity = 0;
+            if (!cuda_ok(ip_init(ctx.ip_variant, ctx.ip, a, s), "init_inplace")) return false;
+            ctx.parity = 1;
+        } else {
+            a.parity = ctx.parity;
+            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, have_packet, s), "step_inplace")) return false;
+            ctx.parity ^= 1;
+        }
     }
-    ctx.cur = 1 - ctx.cur;
     ctx.slot = new_slot;
     ctx.face_prev = face_now;
     ctx.initialized = true;
@@ -533,9 +651,22 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     return true;
 }
 
-bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out) {
+bool output_device(Context& ctx, int stride, int out_ch, float scale, float* dev_out) {
     cudaStream_t s = current_stream();
     const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
+    if (ctx.layout == 0) {
+        auto launch = g_collision_mode == 0 ? launch_output_ab_exact : launch_output_ab_fast;
+        return cuda_ok(launch(d, ctx.g[ctx.cur], ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
+                              ctx.d_face[ctx.slot], stride, out_ch, scale, dev_out, s),
+                       "output");
+    }
+    IpArgs a = ip_args(ctx, ctx.slot, ctx.slot, current_collide_params());
+    a.parity = ctx.parity;
+    return cuda_ok(ip_output(ctx.ip_variant, ctx.ip, a, stride, out_ch, scale, dev_out, s), "output_inplace");
+}
+
+bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out) {
+    cudaStream_t s = current_stream();
     const int sx = (ctx.nx + stride - 1) / stride, sy = (ctx.ny + stride - 1) / stride, sz = (ctx.nz + stride - 1) / stride;
     const size_t bytes = (size_t)sx * sy * sz * out_ch * sizeof(float);
     if (ctx.out_cap < bytes) {
@@ -545,10 +676,7 @@ bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_
         if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.out), bytes), "cudaMalloc(output)")) return false;
         ctx.out_cap = bytes;
     }
-    auto launch = g_collision_mode == 0 ? launch_output_ab_exact : launch_output_ab_fast;
-    if (!cuda_ok(launch(d, ctx.g[ctx.cur], ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
-                        ctx.d_face[ctx.slot], stride, out_ch, scale, ctx.out, s),
-                 "output")) return false;
+    if (!output_device(ctx, stride, out_ch, scale, ctx.out)) return false;
     if (!cuda_ok(cudaMemcpyAsync(host_out, ctx.out, bytes, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(output)")) return false;
     return cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize(output)");
 }

@@ -36,6 +36,15 @@ struct Context {
     float* force = nullptr;  // optional per-cell force density, SoA (3 * cells)
     FaceParams face_prev{};
     FaceParams h_face[2]{};  // host copies (source of the async uploads; must outlive them)
+    // Layout chosen at the first step: 0 two-buffer pull (g[0], g[1]),
+    // 1 in-place esoteric pull (ip, padded by one ghost cell per side).
+    int layout = 0;
+    int ip_variant = 0;      // IpVariant when layout == 1
+    void* ip = nullptr;      // padded population array (float or __half)
+    int parity = 0;          // slot-map parity of the next in-place step
+    int periodic_mask = 0;   // axes wrapped by the in-place layout
+    float fp16_scale = 0.0f; // per-brick FP16 deviation scale
+    uint64_t bytes_per_step = 0;  // algorithmic population bytes per cell-step x cells
     int cur = 0;
     int slot = 0;
     bool allocated = false;
@@ -76,5 +85,7 @@ void release_all_contexts();
 const RuntimeView runtime_view();
 bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet);
 bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out);
+// Device-side output into `dev_out` (no copy, no synchronisation).
+bool output_device(Context& ctx, int stride, int out_ch, float scale, float* dev_out);
 
 }  // namespace aero

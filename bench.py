@@ -235,7 +235,11 @@ def run_ours(args) -> dict | None:
     aero = load_pkg()
     cases = load_cases()
     lib = aero.load_library()
-    stream = torch.cuda.current_stream(dev)
+    # A dedicated stream: the library queues every kernel on it and the CUDA
+    # events below are recorded on it (a null handle would select the
+    # library's own stream instead).
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     lib.aero_lbm_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
 
     case = cases.c2_terrain_boussinesq(args.n)
@@ -353,7 +357,7 @@ def run_ours(args) -> dict | None:
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=128)
