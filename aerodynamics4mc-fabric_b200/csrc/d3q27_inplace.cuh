@@ -67,9 +67,12 @@ __device__ __forceinline__ void ip_pull(const typename S::T* __restrict__ f, con
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const bool bb = (w >> q) & 1u;
-        const int sx = x - q_cx(q), sy = y - q_cy(q), sz = z - q_cz(q);
-        const bool oob = (!G.wrap[0] && (sx < 0 || sx >= G.nx)) || (!G.wrap[1] && (sy < 0 || sy >= G.ny)) ||
-                         (!G.wrap[2] && (sz < 0 || sz >= G.nz));
+        // Periodic axes wrap first, then the first axis still outside picks
+        // the face (remap_hydrodynamic_coords + hydrodynamic_face_for_oob).
+        const int sx = axis_neighbour(x, -q_cx(q), G.nx, G.wrap[0]);
+        const int sy = axis_neighbour(y, -q_cy(q), G.ny, G.wrap[1]);
+        const int sz = axis_neighbour(z, -q_cz(q), G.nz, G.wrap[2]);
+        const bool oob = sx < 0 || sx >= G.nx || sy < 0 || sy >= G.ny || sz < 0 || sz >= G.nz;
         if (!bb && oob) {
             fl[q] = ip_face_equilibrium(*F, q, ref_p[cell], sx, sy, sz, G.nx, G.ny, G.nz);
         } else {

@@ -220,6 +220,46 @@ def cpu_baseline_single(seconds: float = 15.0) -> dict | None:
 
 
 # ---------------------------------------------------------------- our arm
+VARIANTS = {
+    # name: (realtime solver mode, collision mode, bytes per cell-step, storage note)
+    "fp16": (3, 1, 27 * 2 * 2 + 1, "fp16 deviation storage, in-place esoteric pull, factorised collision"),
+    "fp32_exact": (0, 0, 27 * 4 * 2 + 1, "fp32, in-place esoteric pull, reference-order collision (bit-exact)"),
+    "fp32_fast": (0, 1, 27 * 4 * 2 + 1, "fp32, in-place esoteric pull, factorised collision"),
+}
+
+
+def setup_context(aero, lib, case, variant: str, key: int, streaming: int):
+    import torch
+
+    solver_mode, collision, _, _ = VARIANTS[variant]
+    lib.aero_lbm_set_realtime_solver_mode(solver_mode)
+    lib.aero_lbm_b200_set_collision_mode(collision)
+    lib.aero_lbm_b200_set_physics_overrides(case.smagorinsky_c, case.buoyancy_beta, case.gravity_axis)
+    lib.aero_lbm_b200_set_streaming_mode(streaming)
+    n = case.dims[0]
+    ctx = aero.LbmContext(case.dims, key=key, lib=lib, init=False)
+    cfgd = case.config_dict()
+    cfg = aero.default_config(lib)
+    cfg.enabled = 1
+    cfg.flags = cfg.flags & ~aero.FLAG_DISABLE_SGS & ~aero.FLAG_DISABLE_BUOYANCY | aero.FLAG_DISABLE_INTERNAL_THERMAL_SOURCE
+    cfg.reynolds_number = cfgd["reynolds"]
+    for i, v in enumerate(case.u_ref):
+        cfg.initial_velocity[i] = v
+    for face, fc in zip(cfg.faces(), case.faces):
+        face.hydrodynamic_kind = fc["kind"]
+        face.thermal_kind = 1
+        for a, v in enumerate(fc.get("velocity", (0, 0, 0))):
+            face.velocity[a] = v
+    ctx.configure(cfg)
+    packet = torch.from_numpy(case.packet()).pin_memory()
+    pk_ptr = ctypes.cast(packet.data_ptr(), ctypes.POINTER(ctypes.c_float))
+    if not lib.aero_lbm_step_rect(pk_ptr, n, n, n, key, None):
+        raise RuntimeError(aero.last_error(lib))
+    lib.aero_lbm_set_realtime_solver_mode(0)
+    lib.aero_lbm_b200_set_collision_mode(0)
+    return ctx, packet, pk_ptr
+
+
 def run_ours(args) -> dict | None:
     import torch
     import torch.distributed as dist
@@ -241,59 +281,60 @@ def run_ours(args) -> dict | None:
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     lib.aero_lbm_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    if not lib.aero_lbm_init_rect(args.n, args.n, args.n, 11, 4):
+        raise RuntimeError(aero.last_error(lib))
 
     case = cases.c2_terrain_boussinesq(args.n)
     n = args.n
     cells = case.cells
-    lib.aero_lbm_b200_set_physics_overrides(case.smagorinsky_c, case.buoyancy_beta, case.gravity_axis)
-    lib.aero_lbm_b200_set_streaming_mode(args.streaming)
-    ctx = aero.LbmContext(case.dims, key=1 + rank, lib=lib)
-    sys.path.insert(0, str(ROOT / "oracle"))
-    cfgd = case.config_dict()
-    cfg = aero.default_config(lib)
-    cfg.enabled = 1
-    cfg.flags = cfg.flags & ~aero.FLAG_DISABLE_SGS & ~aero.FLAG_DISABLE_BUOYANCY | aero.FLAG_DISABLE_INTERNAL_THERMAL_SOURCE
-    cfg.reynolds_number = cfgd["reynolds"]
-    for i, v in enumerate(case.u_ref):
-        cfg.initial_velocity[i] = v
-    for face, fc in zip(cfg.faces(), case.faces):
-        face.hydrodynamic_kind = fc["kind"]
-        face.thermal_kind = 1
-        for a, v in enumerate(fc.get("velocity", (0, 0, 0))):
-            face.velocity[a] = v
-    ctx.configure(cfg)
-
-    packet = torch.from_numpy(case.packet()).pin_memory()
-    pk_ptr = ctypes.cast(packet.data_ptr(), ctypes.POINTER(ctypes.c_float))
-    if not lib.aero_lbm_step_rect(pk_ptr, n, n, n, ctx.key, None):
-        raise RuntimeError(aero.last_error(lib))
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    for _ in range(args.warmup):
-        ctx.advance(1)
-    barrier()
-    launches0 = lib.aero_lbm_b200_launch_count()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        start.record(stream)
-        for _ in range(args.steps):
-            ctx.advance(1)
-        end.record(stream)
-        barrier()
-    launches = lib.aero_lbm_b200_launch_count() - launches0
-    ms = start.elapsed_time(end)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_per_step = ms / args.steps
-    value = cells * world * args.steps / (ms * 1e-3) / 1e6
+        return float(t.item())
 
-    # e2e through the C ABI with host buffers
+    def timed(variant: str, key: int, steps: int, sample_clocks: bool):
+        ctx, packet, pk_ptr = setup_context(aero, lib, case, variant, key, args.streaming)
+        for _ in range(args.warmup):
+            ctx.advance(1)
+        barrier()
+        launches0 = lib.aero_lbm_b200_launch_count()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            start.record(stream)
+            for _ in range(steps):
+                ctx.advance(1)
+            end.record(stream)
+            barrier()
+        launches = lib.aero_lbm_b200_launch_count() - launches0
+        ms = max_over_ranks(start.elapsed_time(end))
+        return ctx, packet, pk_ptr, ms, launches, clk.summary() if sample_clocks else None
+
+    results = {}
+    head_ctx = None
+    for variant in ("fp16", "fp32_exact", "fp32_fast"):
+        steps = args.steps if variant == "fp16" else max(10, args.steps // 2)
+        ctx, packet, pk_ptr, ms, launches, clocks = timed(variant, 1 + rank * 8 + len(results), steps, variant == "fp16")
+        ms_step = ms / steps
+        results[variant] = {"mlups": cells * world * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms_step,
+                            "launches": launches, "clocks": clocks, "steps": steps,
+                            "achieved_gbs": VARIANTS[variant][2] * cells / (ms_step * 1e-3) / 1e9}
+        if variant == "fp16":
+            head_ctx = (ctx, packet, pk_ptr)
+        else:
+            ctx.release()
+
+    # e2e through the C ABI with host buffers (FP16 brick): per step the
+    # pinned 11-channel packet goes up (aero_lbm_step_rect) and the stride-4
+    # velocity atlas comes back (aero_lbm_extract_flow_atlas_rect).
+    ctx, packet, pk_ptr = head_ctx
     stride = 4
     atlas = np.zeros(((n + stride - 1) // stride) ** 3 * 4, np.float32)
     e2e_steps = max(3, min(args.steps, 50))
@@ -308,12 +349,25 @@ def run_ours(args) -> dict | None:
         if not lib.aero_lbm_extract_flow_atlas_rect(n, n, n, ctx.key, stride, aero.fptr(atlas), atlas.size):
             raise RuntimeError(aero.last_error(lib))
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = cells * world * e2e_steps / e2e_s / 1e6
+    ctx.release()
+
+    # Accuracy leg: FP16 storage against the bit-exact FP32 step after the
+    # same number of steps from the same inputs.
+    acc = None
+    if args.accuracy_steps > 0:
+        outs = {}
+        for variant, key in (("fp16", 90 + rank), ("fp32_exact", 95 + rank)):
+            c, _, _ = setup_context(aero, lib, case, variant, key, args.streaming)
+            c.advance(args.accuracy_steps - 1)
+            outs[variant] = c.flow_state()
+            c.release()
+        ref = outs["fp32_exact"].astype(np.float64)
+        speed = float(np.max(np.linalg.norm(ref[:, :3], axis=1)))
+        acc = {"steps": args.accuracy_steps,
+               "fp16_vs_fp32_u": float(np.max(np.abs(outs["fp16"][:, :3] - ref[:, :3]))) / speed,
+               "fp16_vs_fp32_rho": float(np.max(np.abs(outs["fp16"][:, 3] - ref[:, 3]))) / float(np.max(1 + ref[:, 3]))}
 
     if world > 1:
         dist.barrier()
@@ -322,32 +376,40 @@ def run_ours(args) -> dict | None:
         return None
 
     peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_CELL_FP32 * cells / (ms_per_step * 1e-3) / 1e9
-    traffic = traffic_record("step_ab_kernel@128")
+    h = results["fp16"]
+    achieved = h["achieved_gbs"]
     out = {
         "metric": METRIC,
-        "value": value,
+        "value": h["mlups"],
         "unit": "MLUPS",
         "n_gpus": world,
-        "steps": args.steps,
+        "steps": h["steps"],
         "warmup": args.warmup,
-        "ms_per_step": ms_per_step,
+        "ms_per_step": h["ms_per_step"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": "fp16-store/f32-compute",
         "data": "synthetic (seeded 4-octave terrain, temperature lapse + warm bubble)",
-        "config": {"workload": f"d3q27-cumulant-fp32 {n}^3 terrain brick, SGS C=0.1, Boussinesq g*beta=1e-4",
-                   "bricks_per_gpu": 1, "cells_per_gpu": cells, "storage": "fp32 populations, two-buffer pull",
-                   "l2": "state (2 x 226 MB) larger than L2; no flush needed", "parallelism": f"bricks x{world}"},
+        "config": {"workload": f"d3q27-cumulant {n}^3 terrain brick, SGS C=0.1, Boussinesq g*beta=1e-4, FP16 in-place",
+                   "bricks_per_gpu": 1, "cells_per_gpu": cells, "storage": VARIANTS["fp16"][3],
+                   "l2": "inputs larger than L2 (fp16 state 119 MB + fields; fp32 state 238 MB); no flush",
+                   "parallelism": f"bricks x{world}",
+                   "fp32_exact_mlups": results["fp32_exact"]["mlups"],
+                   "fp32_fast_mlups": results["fp32_fast"]["mlups"],
+                   "fp16_over_fp32_exact": h["mlups"] / results["fp32_exact"]["mlups"],
+                   "fp16_over_fp32_fast": h["mlups"] / results["fp32_fast"]["mlups"],
+                   "fp32_exact_frac_of_peak": results["fp32_exact"]["achieved_gbs"] / peak,
+                   "fp32_fast_frac_of_peak": results["fp32_fast"]["achieved_gbs"] / peak,
+                   "accuracy": acc},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind,
-                     "bytes_per_cell": BYTES_PER_CELL_FP32},
+                     "traffic": traffic_record(f"step_ip_fp16@{n}"), "peak_source": peak_kind,
+                     "bytes_per_cell": VARIANTS["fp16"][2], "kernel": "step_ip_kernel<StoreF16Dev, fast>"},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": int(packet.numel() * 4),
                 "d2h_bytes_per_step": int(atlas.nbytes), "steps": e2e_steps,
                 "api": "aero_lbm_step_rect (pinned packet) + aero_lbm_extract_flow_atlas_rect(stride 4)"},
-        "gpu_launches": int(launches),
-        "clocks": clk.summary(),
+        "gpu_launches": int(h["launches"]),
+        "clocks": h["clocks"],
     }
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_single()
@@ -363,6 +425,8 @@ def main() -> int:
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--streaming", type=int, default=0, help="0 auto, 1 two-buffer, 2 in-place")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="steps of the FP16-vs-FP32 accuracy leg (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
