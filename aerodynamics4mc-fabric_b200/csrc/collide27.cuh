@@ -160,24 +160,42 @@ struct ReseedSource {
     long long cell;
 };
 
-__device__ __forceinline__ void reseed_from(float (&f)[27], const ReseedSource& r, float max_speed, CollideOut& out) {
-    reseed27(f, r.ref_p[r.cell], r.ref_ux[r.cell], r.ref_uy[r.cell], r.ref_uz[r.cell], max_speed, out);
+
+// Reseed state of a cell (reseed_cell_from_reference, jni.cpp:1724-1750):
+// rho from the clamped pressure proxy, velocity clamped to max_speed.
+__device__ __forceinline__ void reseed_state(const ReseedSource& r, float max_speed, float& rho, float& ux, float& uy,
+                                             float& uz) {
+    const float ref_p = r.ref_p[r.cell];
+    const float pr = clampf_dev(isfinite(ref_p) ? ref_p : 0.0f, -0.03f, 0.03f);
+    rho = clampf_dev(1.0f + pr, 0.97f, 1.03f);
+    const float rux = r.ref_ux[r.cell], ruy = r.ref_uy[r.cell], ruz = r.ref_uz[r.cell];
+    ux = isfinite(rux) ? rux : 0.0f;
+    uy = isfinite(ruy) ? ruy : 0.0f;
+    uz = isfinite(ruz) ? ruz : 0.0f;
+    const float s2 = ux * ux + uy * uy + uz * uz;
+    if (!isfinite(s2) || s2 > max_speed * max_speed) {
+        if (!isfinite(s2) || s2 <= 0.0f) {
+            ux = uy = uz = 0.0f;
+        } else {
+            const float sc = max_speed / sqrtf(s2);
+            ux *= sc; uy *= sc; uz *= sc;
+        }
+    }
 }
 
 // Collide one fluid cell in place. `temperature` feeds buoyancy (read only
 // when buoyancy is on); cfx/cfy/cfz is an extra per-cell force density (zero
-// when unused); `rs_src` is the reseed state for non-finite input.
-__device__ __forceinline__ void collide27(float (&f)[27], const CollideParams& P, const float* temperature,
-                                          float cfx, float cfy, float cfz, const ReseedSource& rs_src,
-                                          CollideOut& out) {
+// when unused). Returns false, leaving f untouched, when the input is not
+// finite: the caller then reseeds the cell (out of line, see reseed_state).
+__device__ __forceinline__ bool collide27(float (&f)[27], const CollideParams& P, const float* temperature,
+                                          float cfx, float cfy, float cfz, CollideOut& out) {
     RawMoments m;
     raw_moments27<true>(f, m);
     const float rho = m.r000;
     if (!(isfinite(rho) && isfinite(m.r100) && isfinite(m.r010) && isfinite(m.r001) &&
           isfinite(m.r200) && isfinite(m.r020) && isfinite(m.r002) && isfinite(m.r110) &&
           isfinite(m.r101) && isfinite(m.r011))) {
-        reseed_from(f, rs_src, P.max_speed, out);
-        return;
+        return false;
     }
     const float rs = fmaxf(1e-6f, rho);
     const float ir = 1.0f / rs;
@@ -197,10 +215,7 @@ __device__ __forceinline__ void collide27(float (&f)[27], const CollideParams& P
     uy += 0.5f * (fy * ir);
     uz += 0.5f * (fz * ir);
     const float s2 = ux * ux + uy * uy + uz * uz;
-    if (!(isfinite(ux) && isfinite(uy) && isfinite(uz) && isfinite(s2))) {
-        reseed_from(f, rs_src, P.max_speed, out);
-        return;
-    }
+    if (!(isfinite(ux) && isfinite(uy) && isfinite(uz) && isfinite(s2))) return false;
     if (s2 > P.max_speed * P.max_speed) {
         const float sc = P.max_speed / sqrtf(s2);
         ux *= sc; uy *= sc; uz *= sc;
@@ -272,14 +287,14 @@ __device__ __forceinline__ void collide27(float (&f)[27], const CollideParams& P
 #pragma unroll
     for (int l = 0; l < 9; ++l) back_line(h[3 * l + 0], h[3 * l + 1], h[3 * l + 2], uz, f[3 * l + 0], f[3 * l + 1], f[3 * l + 2]);
 
-    // Conservation fix-up: f += feq(rs, u) - feq(rho_c, u_c) (jni.cpp:2376-2394).
+    // Conservation fix-up. The reference adds feq(rho, u) - feq(rho_c, u_c)
+    // (jni.cpp:2376-2394), a rounding-level correction; here its first-order
+    // part w_q (drho + 3 c.dj), which restores sum f = rho and sum f c = rho u
+    // exactly as the reference's does up to O(u * rounding).
     RawMoments mc;
     raw_moments27<false>(f, mc);
-    const float rcs = fmaxf(1e-6f, mc.r000);
-    const float uxc = mc.r100 / rcs, uyc = mc.r010 / rcs, uzc = mc.r001 / rcs;
-    const float base_e = rs * (1.0f - 1.5f * (ux * ux + uy * uy + uz * uz));
-    const float base_c = rcs * (1.0f - 1.5f * (uxc * uxc + uyc * uyc + uzc * uzc));
-    const float dbase = base_e - base_c;
+    const float drho = rs - mc.r000;
+    const float djx = 3.0f * (rs * ux - mc.r100), djy = 3.0f * (rs * uy - mc.r010), djz = 3.0f * (rs * uz - mc.r001);
 
     // Guo source (jni.cpp:1270-1281): pref*w*(3(c.F - u.F) + 9 (c.u)(c.F)).
     const bool forced = (fx != 0.0f) | (fy != 0.0f) | (fz != 0.0f);
@@ -290,24 +305,23 @@ __device__ __forceinline__ void collide27(float (&f)[27], const CollideParams& P
 #pragma unroll
     for (int q = 0; q < 13; ++q) {
         const float cxq = float(q_cx(q)), cyq = float(q_cy(q)), czq = float(q_cz(q));
-        const float cu = cxq * ux + cyq * uy + czq * uz;
-        const float cuc = cxq * uxc + cyq * uyc + czq * uzc;
-        const float even = dbase + 4.5f * (rs * cu * cu - rcs * cuc * cuc);
-        const float odd = 3.0f * (rs * cu - rcs * cuc);
+        const float odd = cxq * djx + cyq * djy + czq * djz;
         float se = 0.0f, so_ = 0.0f;
         if (forced) {
+            const float cu = cxq * ux + cyq * uy + czq * uz;
             const float cf = cxq * fx + cyq * fy + czq * fz;
             se = pref * (9.0f * cu * cf - 3.0f * uf);
             so_ = pref * 3.0f * cf;
         }
         const float wq = q_w(q);
-        f[q] += wq * ((even + odd) + (se + so_));
-        f[26 - q] += wq * ((even - odd) + (se - so_));
+        f[q] += wq * ((drho + odd) + (se + so_));
+        f[26 - q] += wq * ((drho - odd) + (se - so_));
     }
     {
         const float se = forced ? pref * (-3.0f * uf) : 0.0f;
-        f[13] += q_w(13) * (dbase + se);
+        f[13] += q_w(13) * (drho + se);
     }
+    return true;
 }
 
 }  // namespace aero

@@ -72,11 +72,10 @@ struct ExactOut {
 };
 
 // Collide one fluid cell in place (benchmark-mode reference collide: no fan
-// forcing, no edge nudge, no sponge). Returns false after reseeding when the
-// input is non-finite.
-__device__ __forceinline__ void collide27_exact(float (&f)[27], const CollideParams& P, const float* temperature,
-                                                float cfx, float cfy, float cfz, const ReseedSource& rs_src,
-                                                CollideOut& out) {
+// forcing, no edge nudge, no sponge). Returns false, with f untouched, when
+// the input is not finite; the caller reseeds the cell.
+__device__ __forceinline__ bool collide27_exact(float (&f)[27], const CollideParams& P, const float* temperature,
+                                                float cfx, float cfy, float cfz, CollideOut& out) {
     bool bad = false;
 #pragma unroll
     for (int q = 0; q < 27; ++q) bad |= !isfinite(f[q]);
@@ -84,19 +83,13 @@ __device__ __forceinline__ void collide27_exact(float (&f)[27], const CollidePar
     const float mom_x = qsum<1, 0, 0>(f);
     const float mom_y = qsum<0, 1, 0>(f);
     const float mom_z = qsum<0, 0, 1>(f);
-    if (bad || !isfinite(rho) || !isfinite(mom_x) || !isfinite(mom_y) || !isfinite(mom_z)) {
-        reseed_from(f, rs_src, P.max_speed, out);
-        return;
-    }
+    if (bad || !isfinite(rho) || !isfinite(mom_x) || !isfinite(mom_y) || !isfinite(mom_z)) return false;
     const float rho_safe = rmax(1e-6f, rho);
     const float inv_rho = 1.0f / rho_safe;
     float ux = mom_x * inv_rho;
     float uy = mom_y * inv_rho;
     float uz = mom_z * inv_rho;
-    if (!isfinite(rho_safe) || !isfinite(inv_rho) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz)) {
-        reseed_from(f, rs_src, P.max_speed, out);
-        return;
-    }
+    if (!isfinite(rho_safe) || !isfinite(inv_rho) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz)) return false;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     if (P.enable_buoyancy) {
         const float buoy = rclamp(P.buoy_beta * __ldg(temperature), -P.buoy_fmax, P.buoy_fmax);
@@ -117,16 +110,10 @@ __device__ __forceinline__ void collide27_exact(float (&f)[27], const CollidePar
         ux += 0.5f * (fx * inv_rho);
         uy += 0.5f * (fy * inv_rho);
         uz += 0.5f * (fz * inv_rho);
-        if (!isfinite(ux) || !isfinite(uy) || !isfinite(uz)) {
-            reseed_from(f, rs_src, P.max_speed, out);
-            return;
-        }
+        if (!isfinite(ux) || !isfinite(uy) || !isfinite(uz)) return false;
     }
     const float speed2 = ux * ux + uy * uy + uz * uz;
-    if (!isfinite(speed2)) {
-        reseed_from(f, rs_src, P.max_speed, out);
-        return;
-    }
+    if (!isfinite(speed2)) return false;
     if (speed2 > P.max_speed * P.max_speed) {
         const float scale = P.max_speed / sqrtf(speed2);
         ux *= scale; uy *= scale; uz *= scale;
@@ -280,6 +267,7 @@ __device__ __forceinline__ void collide27_exact(float (&f)[27], const CollidePar
 #pragma unroll
         for (int q = 0; q < 27; ++q) f[q] = fc[q];
     }
+    return true;
 }
 
 // write_output / extract macro readout in the reference's order

@@ -25,16 +25,16 @@ cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* f
 
 
 cudaError_t ip_init_f32_fast(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, false>::init(f, a, s); }
-cudaError_t ip_step_f32_fast(float* f, const IpArgs& a, bool transitions, cudaStream_t s) {
-    return IpLaunch<StoreF32, false>::step(f, a, transitions, s);
+cudaError_t ip_step_f32_fast(float* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
+    return IpLaunch<StoreF32, false>::step(f, a, transitions, fill, s);
 }
 cudaError_t ip_output_f32_fast(const float* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
     return IpLaunch<StoreF32, false>::output(f, a, stride, out_ch, scale, out, s);
 }
 
 cudaError_t ip_init_f16_fast(__half* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF16Dev, false>::init(f, a, s); }
-cudaError_t ip_step_f16_fast(__half* f, const IpArgs& a, bool transitions, cudaStream_t s) {
-    return IpLaunch<StoreF16Dev, false>::step(f, a, transitions, s);
+cudaError_t ip_step_f16_fast(__half* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
+    return IpLaunch<StoreF16Dev, false>::step(f, a, transitions, fill, s);
 }
 cudaError_t ip_output_f16_fast(const __half* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
     return IpLaunch<StoreF16Dev, false>::output(f, a, stride, out_ch, scale, out, s);

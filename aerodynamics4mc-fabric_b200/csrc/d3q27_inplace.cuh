@@ -100,7 +100,38 @@ __device__ __forceinline__ void cell_coords(const PadGeom& G, long long cell, in
     x = (int)(cell / ((long long)G.ny * G.nz));
 }
 
-// Fused pull-stream + collide + push of one step.
+// Reseed a cell into the in-place state (out of line: rare path; scalar
+// arguments only so the hot kernel keeps its populations in registers).
+template <class S>
+static __device__ __noinline__ void reseed_push_ip(typename S::T* __restrict__ f, const float* ref_p, const float* ref_ux,
+                                                    const float* ref_uy, const float* ref_uz, float max_speed,
+                                                    float fp16_scale, long long cell, int x, int y, int z, int nx,
+                                                    int ny, int nz, int wrap_mask, int parity) {
+    float rho, ux, uy, uz;
+    reseed_state(ReseedSource{ref_p, ref_ux, ref_uy, ref_uz, cell}, max_speed, rho, ux, uy, uz);
+    const PadGeom g = make_pad_geom(nx, ny, nz, wrap_mask);
+    const NeighbourOffsets o = neighbour_offsets(g, x, y, z);
+    const int own = pad_index(g, x, y, z);
+    const Fp16Scale sc{fp16_scale};
+#pragma unroll 1
+    for (int q = 0; q < 27; ++q) {
+        int c, d;
+        outgoing_slot(o, own, q, parity, c, d);
+        S::store(f + (long long)d * g.pcells + c, q, feq27(q, rho, ux, uy, uz), sc);
+    }
+}
+
+template <class S>
+__device__ __forceinline__ void reseed_push(typename S::T* f, const IpArgs& a, long long cell, int x, int y, int z,
+                                            int parity) {
+    const int wrap_mask = a.g.wrap[0] | (a.g.wrap[1] << 1) | (a.g.wrap[2] << 2);
+    reseed_push_ip<S>(f, a.cur.ref_p, a.cur.ref_ux, a.cur.ref_uy, a.cur.ref_uz, a.cp.max_speed, a.sc.scale, cell, x, y,
+                      z, a.g.nx, a.g.ny, a.g.nz, wrap_mask, parity);
+}
+
+// Fused pull-stream + collide + push of one step. Sources outside
+// equilibrium faces were pre-filled into their slots by face_fill_ip_kernel,
+// so every incoming population is a plain (or bounce-back) slot read.
 template <class S, bool kExact>
 __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom G = a.g;
@@ -114,9 +145,65 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
     const int own = pad_index(G, x, y, z);
     const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
     float fl[27];
-    ip_pull<S>(f, a, G, o, own, w, cell, x, y, z, a.parity, a.ref_p_prev, a.face_prev, fl);
-    if (!a.obstacle_cur[cell]) collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        int c, d;
+        incoming_slot(o, own, q, a.parity, (w >> q) & 1u, c, d);
+        fl[q] = S::load(f + (long long)d * G.pcells + c, q, a.sc);
+    }
+    if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
+        reseed_push<S>(f, a, cell, x, y, z, a.parity);
+        return;
+    }
     ip_push<S>(f, a, G, o, own, a.parity, fl);
+}
+
+// Before a step of parity p: write the equilibrium value of every incoming
+// population whose source lies outside an equilibrium face into the slot the
+// pulling cell reads at parity p (a ghost-cell slot, or for positive
+// directions the cell's own slot that only the never-updated ghost would
+// write). One thread per cell of the six boundary layers; cells on edges are
+// visited once per face and write identical values.
+template <class S>
+__global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
+    const PadGeom G = a.g;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const long long fx_n = (long long)ny * nz, fy_n = (long long)nx * nz, fz_n = (long long)nx * ny;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int x, y, z;
+    if (i < 2 * fx_n) {
+        x = i < fx_n ? 0 : nx - 1;
+        const long long r = i % fx_n;
+        y = (int)(r / nz); z = (int)(r % nz);
+    } else if ((i -= 2 * fx_n) < 2 * fy_n) {
+        y = i < fy_n ? 0 : ny - 1;
+        const long long r = i % fy_n;
+        x = (int)(r / nz); z = (int)(r % nz);
+    } else if ((i -= 2 * fy_n) < 2 * fz_n) {
+        z = i < fz_n ? 0 : nz - 1;
+        const long long r = i % fz_n;
+        x = (int)(r / ny); y = (int)(r % ny);
+    } else {
+        return;
+    }
+    const long long cell = ((long long)x * ny + y) * nz + z;
+    const uint32_t w = a.flags_prev[cell];
+    if ((w & kFlagSelfSolid) || !(w & kFlagFaceSpecial)) return;
+    const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
+    const int own = pad_index(G, x, y, z);
+    const FaceParams& F = *a.face_prev;
+    const float rp = a.ref_p_prev[cell];
+#pragma unroll 1
+    for (int q = 0; q < 27; ++q) {
+        if ((w >> q) & 1u) continue;
+        const int sx = axis_neighbour(x, -q_cx(q), nx, G.wrap[0]);
+        const int sy = axis_neighbour(y, -q_cy(q), ny, G.wrap[1]);
+        const int sz = axis_neighbour(z, -q_cz(q), nz, G.wrap[2]);
+        if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) continue;
+        int c, d;
+        incoming_slot(o, own, q, a.parity, false, c, d);
+        S::store(f + (long long)d * G.pcells + c, q, ip_face_equilibrium(F, q, rp, sx, sy, sz, nx, ny, nz), a.sc);
+    }
 }
 
 // Cells that were solid at the streaming call and are fluid now: start from
@@ -137,7 +224,10 @@ __global__ void __launch_bounds__(128) transition_ip_kernel(typename S::T* __res
     float fl[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q) fl[q] = q_w(q);
-    collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell);
+    if (!collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
+        reseed_push<S>(f, a, cell, x, y, z, a.parity);
+        return;
+    }
     ip_push<S>(f, a, G, o, own, a.parity, fl);
 }
 
@@ -159,7 +249,10 @@ __global__ void __launch_bounds__(128) init_ip_kernel(typename S::T* __restrict_
     float fl[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q) fl[q] = feq27(q, rho, ux, uy, uz);
-    collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell);
+    if (!collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
+        reseed_push<S>(f, a, cell, x, y, z, 0);
+        return;
+    }
     ip_push<S>(f, a, G, o, own, 0, fl);
 }
 
@@ -200,8 +293,20 @@ struct IpLaunch {
         count_launch();
         return cudaGetLastError();
     }
-    static cudaError_t step(typename S::T* f, const IpArgs& a, bool transitions, cudaStream_t s) {
+    // Pre-fill of equilibrium-face sources; needed when any face is an
+    // equilibrium face (velocity, pressure, moving wall).
+    static cudaError_t face_fill(typename S::T* f, const IpArgs& a, cudaStream_t s) {
+        const long long n = 2LL * ((long long)a.g.ny * a.g.nz + (long long)a.g.nx * a.g.nz + (long long)a.g.nx * a.g.ny);
+        face_fill_ip_kernel<S><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a);
+        count_launch();
+        return cudaGetLastError();
+    }
+    static cudaError_t step(typename S::T* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
         const long long cells = (long long)a.g.nx * a.g.ny * a.g.nz;
+        if (fill) {
+            cudaError_t e = face_fill(f, a, s);
+            if (e != cudaSuccess) return e;
+        }
         step_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
         count_launch();
         cudaError_t e = cudaGetLastError();

@@ -27,16 +27,25 @@ __device__ __forceinline__ int oob_face(int sx, int sy, int sz, int nx, int ny, 
     return kFaceZMax;
 }
 
+// Collide one fluid cell; false = non-finite input, the caller reseeds.
 template <bool kExact>
-__device__ __forceinline__ void collide_cell(float (&f)[27], const CollideParams& cp, const CellFields& cur,
+__device__ __forceinline__ bool collide_cell(float (&f)[27], const CollideParams& cp, const CellFields& cur,
                                              const ForceField& force, long long cell) {
     CollideOut o;
     const float cfx = force.fx ? force.fx[cell] : 0.0f;
     const float cfy = force.fy ? force.fy[cell] : 0.0f;
     const float cfz = force.fz ? force.fz[cell] : 0.0f;
-    const ReseedSource rs{cur.ref_p, cur.ref_ux, cur.ref_uy, cur.ref_uz, cell};
-    if (kExact) exact::collide27_exact(f, cp, cur.temperature + cell, cfx, cfy, cfz, rs, o);
-    else collide27(f, cp, cur.temperature + cell, cfx, cfy, cfz, rs, o);
+    if (kExact) return exact::collide27_exact(f, cp, cur.temperature + cell, cfx, cfy, cfz, o);
+    return collide27(f, cp, cur.temperature + cell, cfx, cfy, cfz, o);
+}
+
+// Reseed a cell into the two-buffer state (out of line: rare path).
+static __device__ __noinline__ void reseed_store_ab(float* __restrict__ g_out, long long cells, long long cell,
+                                                     CellFields cur, float max_speed) {
+    float rho, ux, uy, uz;
+    reseed_state(ReseedSource{cur.ref_p, cur.ref_ux, cur.ref_uy, cur.ref_uz, cell}, max_speed, rho, ux, uy, uz);
+#pragma unroll 1
+    for (int q = 0; q < 27; ++q) g_out[(long long)q * cells + cell] = feq27(q, rho, ux, uy, uz);
 }
 
 // ---------------------------------------------------------------- pull
@@ -171,8 +180,9 @@ __global__ void __launch_bounds__(128) init_collide_kernel(int nx, int ny, int n
     }
 #pragma unroll
     for (int q = 0; q < 27; ++q) f[q] = feq27(q, rho, ux, uy, uz);
-    if (!solid) {
-        collide_cell<kExact>(f, cp, cur, force, cell);
+    if (!solid && !collide_cell<kExact>(f, cp, cur, force, cell)) {
+        reseed_store_ab(g_out, cells, cell, cur, cp.max_speed);
+        return;
     }
 #pragma unroll
     for (int q = 0; q < 27; ++q) g_out[(long long)q * cells + cell] = f[q];
@@ -206,8 +216,9 @@ __global__ void __launch_bounds__(128) step_ab_kernel(int nx, int ny, int nz, co
     float f[27];
     const PullView v{g_in, obstacle_prev, ref_p_prev, F, cells, nx, ny, nz};
     pull27(v, flags_prev[cell], cell, x, y, z, f);
-    if (!cur.obstacle[cell]) {
-        collide_cell<kExact>(f, cp, cur, force, cell);
+    if (!cur.obstacle[cell] && !collide_cell<kExact>(f, cp, cur, force, cell)) {
+        reseed_store_ab(g_out, cells, cell, cur, cp.max_speed);
+        return;
     }
 #pragma unroll
     for (int q = 0; q < 27; ++q) g_out[(long long)q * cells + cell] = f[q];

@@ -638,7 +638,12 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             ctx.parity = 1;
         } else {
             a.parity = ctx.parity;
-            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, have_packet, s), "step_inplace")) return false;
+            bool fill = false;
+            for (int i = 0; i < 6; ++i) {
+                const int k = ctx.face_prev.kind[i];
+                fill |= k == kHydroVelocity || k == kHydroPressure || k == kHydroMovingWall;
+            }
+            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, have_packet, fill, s), "step_inplace")) return false;
             ctx.parity ^= 1;
         }
     }
