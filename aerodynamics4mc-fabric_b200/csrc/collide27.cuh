@@ -192,11 +192,8 @@ __device__ __forceinline__ bool collide27(float (&f)[27], const CollideParams& P
     RawMoments m;
     raw_moments27<true>(f, m);
     const float rho = m.r000;
-    if (!(isfinite(rho) && isfinite(m.r100) && isfinite(m.r010) && isfinite(m.r001) &&
-          isfinite(m.r200) && isfinite(m.r020) && isfinite(m.r002) && isfinite(m.r110) &&
-          isfinite(m.r101) && isfinite(m.r011))) {
-        return false;
-    }
+    // Any non-finite population makes the plain sum rho non-finite.
+    if (!isfinite(rho)) return false;
     const float rs = fmaxf(1e-6f, rho);
     const float ir = 1.0f / rs;
     float ux = m.r100 * ir, uy = m.r010 * ir, uz = m.r001 * ir;

@@ -112,7 +112,7 @@ static __device__ __noinline__ void reseed_push_ip(typename S::T* __restrict__ f
     const PadGeom g = make_pad_geom(nx, ny, nz, wrap_mask);
     const NeighbourOffsets o = neighbour_offsets(g, x, y, z);
     const int own = pad_index(g, x, y, z);
-    const Fp16Scale sc{fp16_scale};
+    const Fp16Scale sc{fp16_scale, 1.0f / fp16_scale};
 #pragma unroll 1
     for (int q = 0; q < 27; ++q) {
         int c, d;
@@ -132,7 +132,7 @@ __device__ __forceinline__ void reseed_push(typename S::T* f, const IpArgs& a, l
 // Fused pull-stream + collide + push of one step. Sources outside
 // equilibrium faces were pre-filled into their slots by face_fill_ip_kernel,
 // so every incoming population is a plain (or bounce-back) slot read.
-template <class S, bool kExact>
+template <class S, bool kExact, int kParity>
 __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom G = a.g;
     const long long cells = (long long)G.nx * G.ny * G.nz;
@@ -148,14 +148,19 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         int c, d;
-        incoming_slot(o, own, q, a.parity, (w >> q) & 1u, c, d);
-        fl[q] = S::load(f + (long long)d * G.pcells + c, q, a.sc);
+        incoming_slot(o, own, q, kParity, (w >> q) & 1u, c, d);
+        fl[q] = S::load(f + (d * G.pcells + c), q, a.sc);
     }
     if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
-        reseed_push<S>(f, a, cell, x, y, z, a.parity);
+        reseed_push<S>(f, a, cell, x, y, z, kParity);
         return;
     }
-    ip_push<S>(f, a, G, o, own, a.parity, fl);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        int c, d;
+        outgoing_slot(o, own, q, kParity, c, d);
+        S::store(f + (d * G.pcells + c), q, fl[q], a.sc);
+    }
 }
 
 // Before a step of parity p: write the equilibrium value of every incoming
@@ -307,7 +312,8 @@ struct IpLaunch {
             cudaError_t e = face_fill(f, a, s);
             if (e != cudaSuccess) return e;
         }
-        step_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
+        if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
+        else step_ip_kernel<S, kExact, 1><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
         count_launch();
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess || !transitions) return e;

@@ -34,6 +34,7 @@ __host__ __device__ constexpr bool q_positive(int q) { return q > 13; }
 // Per-brick FP16 storage scale (deviation from the rest weights).
 struct Fp16Scale {
     float scale;      // S: stored half = (f - w_q) * S / w_q
+    float inv_scale;  // 1 / S
 };
 
 // Population storage policies.
@@ -49,17 +50,19 @@ struct StoreF32 {
     }
 };
 
-// FP16 deviation storage: h = (f - w_q) * (S / w_q), f = w_q + h * (w_q / S).
-// Stored values are clamped to the finite FP16 range before rounding.
+// FP16 deviation storage: h = (f - w_q) * (S / w_q) = f * (S / w_q) - S,
+// f = w_q + h * (w_q / S). The per-brick scale S keeps |h| far below the FP16
+// range for any admissible state (|u| <= the speed clamp); a state that
+// overflows anyway stores inf, and the next collision reseeds that cell (the
+// reference's rule for non-finite populations).
 struct StoreF16Dev {
     using T = __half;
     __device__ __forceinline__ static float load(const __half* __restrict__ a, int q, const Fp16Scale& s) {
         const float h = __half2float(__ldg(a));
-        return fmaf(h, q_w(q) / s.scale, q_w(q));
+        return fmaf(h, q_w(q) * s.inv_scale, q_w(q));
     }
     __device__ __forceinline__ static void store(__half* __restrict__ a, int q, float v, const Fp16Scale& s) {
-        const float d = (v - q_w(q)) * (s.scale / q_w(q));
-        *a = __float2half_rn(fminf(65504.0f, fmaxf(-65504.0f, d)));
+        *a = __float2half_rn(fmaf(v, s.scale * (1.0f / q_w(q)), -s.scale));
     }
 };
 

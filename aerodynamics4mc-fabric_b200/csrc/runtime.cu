@@ -490,7 +490,7 @@ static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const Collide
     a.cur = ctx.fields(cur_slot);
     a.force = ctx.force_field();
     a.cp = cp;
-    a.sc = Fp16Scale{ctx.fp16_scale};
+    a.sc = Fp16Scale{ctx.fp16_scale, ctx.fp16_scale > 0.0f ? 1.0f / ctx.fp16_scale : 0.0f};
     return a;
 }
 
