@@ -187,6 +187,7 @@ SIGNATURES = {
     "aero_lbm_b200_advance_rect": (_I, [_LL, _I]),
     "aero_lbm_b200_set_streaming_mode": (_I, [_I]),
     "aero_lbm_b200_set_collision_mode": (_I, [_I]),
+    "aero_lbm_b200_conservation_sums": (_I, [_LL, ctypes.POINTER(ctypes.c_double)]),
     "aero_lbm_b200_set_force_field": (_I, [_LL, _F32P, _I]),
     "aero_lbm_b200_set_physics_overrides": (None, [_F, _F, _I]),
     # wind-tunnel ABI
@@ -333,6 +334,13 @@ class LbmContext:
         soa = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float32).reshape(-1) for a in (fx, fy, fz)]))
         if not self.lib.aero_lbm_b200_set_force_field(self.key, fptr(soa), soa.size):
             raise RuntimeError(f"set_force_field failed: {last_error(self.lib)}")
+
+    def conservation_sums(self) -> np.ndarray:
+        """FP64 {sum rho, sum rho u} over fluid cells of the current state."""
+        out = np.zeros(4, dtype=np.float64)
+        if not self.lib.aero_lbm_b200_conservation_sums(self.key, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))):
+            raise RuntimeError(f"conservation_sums failed: {last_error(self.lib)}")
+        return out
 
     def release(self) -> None:
         self.lib.aero_lbm_release_context(self.key)

@@ -20,6 +20,7 @@
 #include "../../include/aero_lbm_b200.h"
 #include "d3q27_kernels.cuh"
 #include "ip_launch.h"
+#include "conservation.cuh"
 #include "runtime_internal.h"
 
 namespace aero {
@@ -393,6 +394,8 @@ void Context::release_device() {
     fr(reinterpret_cast<void*&>(out));
     fr(reinterpret_cast<void*&>(force));
     fr(ip);
+    fr(scratch);
+    scratch_cap = 0;
     packet_cap = out_cap = 0;
     layout = 0;
     parity = 0;
@@ -1028,6 +1031,40 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streaming_mode(int mode) {
     if (mode < 0 || mode > 2) return 0;
     g_stream_mode = mode;
     return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums(long long key, double* out4) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    Context* c = find_context(key);
+    if (!c || !c->initialized || !out4) {
+        set_error("conservation_sums: no initialized context or null output");
+        return 0;
+    }
+    cudaStream_t s = current_stream();
+    const int blocks = conservation_blocks(c->cells);
+    const size_t need = (size_t)blocks * 4 * sizeof(double) + 4 * sizeof(double);
+    if (c->scratch_cap < need) {
+        if (c->scratch) cudaFree(c->scratch);
+        c->scratch = nullptr;
+        c->scratch_cap = 0;
+        if (!cuda_ok(cudaMalloc(&c->scratch, need), "cudaMalloc(conservation scratch)")) return 0;
+        c->scratch_cap = need;
+    }
+    double* partials = static_cast<double*>(c->scratch);
+    double* dev_out = partials + (size_t)blocks * 4;
+    cudaError_t e;
+    if (c->layout == 0) {
+        e = launch_conservation_ab(c->nx, c->ny, c->nz, c->g[c->cur], c->flags[c->slot], c->obstacle[c->slot],
+                                   c->ref_p[c->slot], c->d_face[c->slot], partials, dev_out, s);
+    } else {
+        IpArgs a = ip_args(*c, c->slot, c->slot, current_collide_params());
+        a.parity = c->parity;
+        e = launch_conservation_ip(c->ip_variant, c->ip, a, partials, dev_out, s);
+    }
+    if (!cuda_ok(e, "conservation kernels")) return 0;
+    if (!cuda_ok(cudaMemcpyAsync(out4, dev_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy sums")) return 0;
+    return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
 }
 
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_collision_mode(int mode) {

@@ -45,6 +45,8 @@ struct Context {
     int periodic_mask = 0;   // axes wrapped by the in-place layout
     float fp16_scale = 0.0f; // per-brick FP16 deviation scale
     uint64_t bytes_per_step = 0;  // algorithmic population bytes per cell-step x cells
+    void* scratch = nullptr; // conservation-sum partials
+    size_t scratch_cap = 0;
     int cur = 0;
     int slot = 0;
     bool allocated = false;

@@ -212,6 +212,12 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_advance_rect(long long context_key, int s
 /* Select the streaming scheme of a context: 0 automatic (in-place when every
  * face is local), 1 two-buffer pull, 2 in-place esoteric pull. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streaming_mode(int mode);
+/* Global mass and momentum of a context's current streamed state (the
+ * populations the next step collides), summed in FP64 over fluid cells:
+ * out4 = {sum rho, sum rho ux, sum rho uy, sum rho uz}. Uses a per-context
+ * device scratch buffer (allocated on first use) for the block partial sums;
+ * synchronises the library stream. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums(long long context_key, double* out4);
 /* FP32 collision arithmetic: 0 = the reference's operation order, no
  * multiply-add contraction (bit-identical to the reference CPU step; default),
  * 1 = factorised moment transforms with contraction (same scheme, fewer flops,
