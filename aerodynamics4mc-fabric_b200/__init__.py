@@ -190,6 +190,19 @@ SIGNATURES = {
     "aero_lbm_b200_conservation_sums": (_I, [_LL, ctypes.POINTER(ctypes.c_double)]),
     "aero_lbm_b200_set_force_field": (_I, [_LL, _F32P, _I]),
     "aero_lbm_b200_set_physics_overrides": (None, [_F, _F, _I]),
+    # batched bricks
+    "aero_lbm_b200_batch_create": (_I, [ctypes.POINTER(_LL)]),
+    "aero_lbm_b200_batch_add_brick": (_I, [_LL, _I, _I, _I, _I, _U8P, _F32P, _F, _F32P, _I32P, _I32P]),
+    "aero_lbm_b200_batch_finalize": (_I, [_LL, _I, _F]),
+    "aero_lbm_b200_batch_set_options": (_I, [_LL, _I, _I]),
+    "aero_lbm_b200_batch_tick": (_I, [_LL, _I]),
+    "aero_lbm_b200_batch_autotune": (_I, [_LL, _I, _I32P, _I32P, _F32P]),
+    "aero_lbm_b200_batch_info": (_I, [_LL, ctypes.POINTER(_LL), ctypes.POINTER(ctypes.c_double), _I32P, _I32P,
+                                     ctypes.POINTER(_LL)]),
+    "aero_lbm_b200_batch_copy_atlas": (_I, [_LL, _I, _I16P, _I]),
+    "aero_lbm_b200_batch_copy_flow": (_I, [_LL, _I, _F32P, _I]),
+    "aero_lbm_b200_batch_destroy": (None, [_LL]),
+    "aero_lbm_b200_batch_last_error": (ctypes.c_char_p, []),
     # wind-tunnel ABI
     "aero_solver_default_grid": (None, [ctypes.POINTER(AeroGridDesc)]),
     "aero_solver_default_boundary": (None, [ctypes.POINTER(AeroBoundaryDesc)]),
@@ -344,3 +357,89 @@ class LbmContext:
 
     def release(self) -> None:
         self.lib.aero_lbm_release_context(self.key)
+
+
+class BrickBatch:
+    """Batched bricks advanced by one persistent launch per tick
+    (aero_lbm_b200_batch_*)."""
+
+    def __init__(self, lib: ctypes.CDLL | None = None):
+        self.lib = lib or load_library()
+        h = ctypes.c_longlong(0)
+        if not self.lib.aero_lbm_b200_batch_create(ctypes.byref(h)):
+            raise RuntimeError(self.error())
+        self.handle = h.value
+        self.dims: list[tuple] = []
+
+    def error(self) -> str:
+        m = self.lib.aero_lbm_b200_batch_last_error()
+        return m.decode() if m else ""
+
+    def add_brick(self, dims, obstacle=None, velocity=None, tau: float = 0.55, force=(0.0, 0.0, 0.0),
+                  faces=None, precision: int = 0) -> int:
+        nx, ny, nz = (int(d) for d in dims)
+        cells = nx * ny * nz
+        ob = None if obstacle is None else np.ascontiguousarray(np.asarray(obstacle, np.uint8).reshape(-1))
+        vel = None
+        if velocity is not None:
+            vel = np.ascontiguousarray(np.concatenate([np.asarray(v, np.float32).reshape(-1) for v in velocity]))
+            assert vel.size == 3 * cells
+        fo = np.ascontiguousarray(np.asarray(force, np.float32))
+        fk = None if faces is None else np.ascontiguousarray(np.asarray(faces, np.int32))
+        idx = ctypes.c_int(-1)
+        ok = self.lib.aero_lbm_b200_batch_add_brick(
+            self.handle, nx, ny, nz, int(precision), None if ob is None else u8ptr(ob),
+            None if vel is None else fptr(vel), float(tau), fptr(fo),
+            None if fk is None else fk.ctypes.data_as(_I32P), ctypes.byref(idx))
+        if not ok:
+            raise RuntimeError(self.error())
+        self.dims.append((nx, ny, nz))
+        return idx.value
+
+    def finalize(self, stride: int = 4, velocity_scale: float = 20.0) -> None:
+        if not self.lib.aero_lbm_b200_batch_finalize(self.handle, int(stride), float(velocity_scale)):
+            raise RuntimeError(self.error())
+        self.stride = stride
+
+    def set_options(self, use_graph: bool = True, publish: bool = True) -> None:
+        if not self.lib.aero_lbm_b200_batch_set_options(self.handle, int(use_graph), int(publish)):
+            raise RuntimeError(self.error())
+
+    def tick(self, n: int = 1) -> None:
+        if not self.lib.aero_lbm_b200_batch_tick(self.handle, int(n)):
+            raise RuntimeError(self.error())
+
+    def autotune(self, trial_ticks: int = 4) -> tuple[int, int, float]:
+        t, b, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
+        if not self.lib.aero_lbm_b200_batch_autotune(self.handle, int(trial_ticks), ctypes.byref(t), ctypes.byref(b),
+                                                      ctypes.byref(ms)):
+            raise RuntimeError(self.error())
+        return t.value, b.value, ms.value
+
+    def info(self) -> dict:
+        c, by, a, u, t = ctypes.c_longlong(0), ctypes.c_double(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_longlong(0)
+        self.lib.aero_lbm_b200_batch_info(self.handle, ctypes.byref(c), ctypes.byref(by), ctypes.byref(a), ctypes.byref(u),
+                                          ctypes.byref(t))
+        return {"cells": c.value, "bytes_per_tick": by.value, "atlas_records": a.value, "units": u.value,
+                "ticks": t.value}
+
+    def atlas(self, brick: int) -> np.ndarray:
+        nx, ny, nz = self.dims[brick]
+        s = self.stride
+        n = ((nx + s - 1) // s) * ((ny + s - 1) // s) * ((nz + s - 1) // s)
+        out = np.zeros(4 * n, np.int16)
+        if not self.lib.aero_lbm_b200_batch_copy_atlas(self.handle, brick, out.ctypes.data_as(_I16P), out.size):
+            raise RuntimeError(self.error())
+        return out.reshape(n, 4)
+
+    def flow(self, brick: int) -> np.ndarray:
+        cells = int(np.prod(self.dims[brick]))
+        out = np.zeros(4 * cells, np.float32)
+        if not self.lib.aero_lbm_b200_batch_copy_flow(self.handle, brick, fptr(out), out.size):
+            raise RuntimeError(self.error())
+        return out.reshape(cells, 4)
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.aero_lbm_b200_batch_destroy(self.handle)
+            self.handle = 0

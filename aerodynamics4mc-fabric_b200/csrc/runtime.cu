@@ -500,7 +500,7 @@ static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const Collide
 // Per-brick FP16 scale: a power of two S such that the normalised deviation
 // (f - w)/w of the largest expected state (reference speed u, |rho - 1| <= 0.03,
 // a non-equilibrium margin of 0.5) times S stays below 2^14.
-static float fp16_scale_for_speed(float umax) {
+float fp16_scale_for_speed(float umax) {
     umax = std::min(std::max(umax, 0.0f), 0.57735026919f * 0.6f);
     const float dev = 0.03f + 3.0f * 1.7320508f * umax + 15.0f * umax * umax + 0.5f;
     float s = 1.0f;

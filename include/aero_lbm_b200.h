@@ -231,6 +231,45 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_force_field(long long context_key, co
  * negative value keeps the reference default. */
 AERO_LBM_B200_EXPORT void aero_lbm_b200_set_physics_overrides(float smagorinsky_c, float buoyancy_beta, int gravity_axis);
 
+/* ---- batched bricks (no reference counterpart: the reference steps bricks one
+ * aero_lbm_step_rect call at a time, native/src/aero_lbm_simulation_bridge.cpp:1092-1166) ----
+ * Many independent bricks of uneven sizes, each with its own mask, relaxation
+ * time, body force and storage precision, advanced by one persistent launch
+ * per tick, with a stride-s packed int16 velocity publish per tick. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_create(long long* out_handle);
+/* precision 0 = fp32, 1 = fp16 deviation storage; obstacle: cells bytes (or
+ * null); init_velocity_soa: 3 x cells floats (or null = rest); tau in
+ * (0.5, 0.95]; body_force: 3 floats (force density) or null; face_kinds: 6
+ * AeroLbmHydrodynamicBoundaryKind values, periodic or bounce-back only (null =
+ * all periodic). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_add_brick(long long handle, int nx, int ny, int nz, int precision,
+                                                       const uint8_t* obstacle, const float* init_velocity_soa,
+                                                       float tau, const float* body_force, const int* face_kinds,
+                                                       int* out_index);
+/* Allocate device state and the work list; velocity_scale = dx/dt used to
+ * convert published velocities to m/s before quantisation. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_finalize(long long handle, int publish_stride, float velocity_scale);
+/* use_graph: replay ticks from a captured CUDA graph; publish: run the
+ * stride-s publish after every tick. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_set_options(long long handle, int use_graph, int publish);
+/* Queue `ticks` ticks on the library stream (no synchronisation). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_tick(long long handle, int ticks);
+/* Time launch shapes on the live bricks (trial ticks are real ticks) and keep
+ * the fastest; reports the choice and its time per tick. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_autotune(long long handle, int trial_ticks, int* out_threads,
+                                                      int* out_blocks_per_sm, float* out_ms_per_tick);
+/* Cells, algorithmic population bytes per tick, atlas records, work units and
+ * ticks done so far (autotuning trials included). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_info(long long handle, long long* out_cells, double* out_bytes_per_tick,
+                                                  int* out_atlas_records, int* out_units, long long* out_ticks);
+/* Packed int16 atlas of one brick from the last published tick (4 values per
+ * atlas cell, quantised like aero_lbm_simulation_copy_brick_world_packed_flow_atlas). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_copy_atlas(long long handle, int brick, int16_t* out, int value_count);
+/* Flow state of one brick (cells x 4 floats, write_output semantics, scale 1). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_copy_flow(long long handle, int brick, float* out, int value_count);
+AERO_LBM_B200_EXPORT void aero_lbm_b200_batch_destroy(long long handle);
+AERO_LBM_B200_EXPORT const char* aero_lbm_b200_batch_last_error(void);
+
 /* ---- wind-tunnel ABI (native/include/aero_solver_capi.h:1-115) ---- */
 enum {
     AERO_SOLVER_ABI_VERSION = 1,
