@@ -407,15 +407,24 @@ bool ensure_graph(Batch& B, cudaStream_t s) {
 }
 
 bool run_ticks(Batch& B, int n, cudaStream_t s) {
-    if (!B.initialized) {
+    int left = n;
+    if (!B.initialized && left > 0) {
+        // The first tick collides the initial equilibrium (no streaming), like
+        // the first aero_lbm_step_rect call of a context.
         const int grid = std::max(1, std::min(B.units, 8 * B.sms));
         batch_init_kernel<<<grid, B.shape.threads, 0, s>>>(B.d_descs, B.d_unit_brick, B.units);
         count_launch();
         if (!bok(cudaGetLastError(), "batch_init_kernel")) return false;
+        if (B.publish) {
+            batch_publish_kernel<<<(int)B.bricks.size(), 256, 0, s>>>(B.d_descs, 1, B.stride, B.velocity_scale, B.d_atlas);
+            count_launch();
+            if (!bok(cudaGetLastError(), "batch_publish_kernel")) return false;
+        }
         B.initialized = true;
         B.parity = 1;
+        --left;
+        ++B.ticks;
     }
-    int left = n;
     // Graph replays cover pairs of ticks starting at parity 0.
     if (B.use_graph && left >= 2) {
         if (B.parity == 1) {
@@ -632,7 +641,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_autotune(long long handle, int tria
     }
     cudaStream_t s = current_stream();
     trial_ticks = std::max(2, trial_ticks + (trial_ticks & 1));
-    if (!run_ticks(*B, 0, s)) return 0;  // initialise
+    if (!B->initialized && !run_ticks(*B, 1, s)) return 0;  // the first (initialising) tick
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
