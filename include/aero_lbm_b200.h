@@ -218,6 +218,15 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streaming_mode(int mode);
  * device scratch buffer (allocated on first use) for the block partial sums;
  * synchronises the library stream. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums(long long context_key, double* out4);
+/* Allocation-free form of aero_lbm_b200_conservation_sums, for callers that
+ * cannot call cudaMalloc (a real-time tick thread that must not stall on an
+ * allocation that synchronises the device; an embedding with a fixed device
+ * memory budget). No counterpart in the reference. Its scratch is a static
+ * 256 KiB device array, so contexts of at most 2,097,152 cells (128^3) are
+ * accepted; larger ones return 0 with an error. The first call on a device
+ * looks up the array's address; make it before any stream capture. Calls
+ * share the array: overlapping calls on the GPU race. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums_noalloc(long long context_key, double* out4);
 /* FP32 collision arithmetic: 0 = the reference's operation order, no
  * multiply-add contraction (bit-identical to the reference CPU step; default),
  * 1 = factorised moment transforms with contraction (same scheme, fewer flops,
