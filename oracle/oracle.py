@@ -367,3 +367,123 @@ def flow_errors(out: np.ndarray, ref: np.ndarray) -> dict:
     u = float(np.max(np.abs(out[:, :3] - ref[:, :3]))) / (speed if speed > 0 else 1.0)
     rho = float(np.max(np.abs(out[:, 3] - ref[:, 3]))) / float(np.max(1.0 + ref[:, 3]))
     return {"u": u, "rho": rho}
+
+
+# ---------------------------------------------------------------- D3Q19 mesoscale
+MESO_CHANNELS = 25
+MESO_OUT = 6
+
+
+class MesoConfig(ctypes.Structure):
+    """AeroLbmMesoscaleConfig (native/include/aero_lbm_capi.h:124-140)."""
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32), ("struct_size", ctypes.c_uint32),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx_m", ctypes.c_float), ("dt_s", ctypes.c_float), ("molecular_nu_m2_s", ctypes.c_float),
+        ("prandtl_air", ctypes.c_float), ("turbulent_prandtl", ctypes.c_float),
+        ("reference_density_kg_m3", ctypes.c_float), ("ambient_air_temperature_k", ctypes.c_float),
+        ("deep_ground_temperature_k", ctypes.c_float), ("background_wind_m_s", ctypes.c_float * 3),
+        ("reserved", ctypes.c_uint32 * 8),
+    ]
+
+
+class MesoTransport(ctypes.Structure):
+    _fields_ = [("velocity_scale", ctypes.c_double), ("tau_shear", ctypes.c_double), ("tau_thermal", ctypes.c_double)]
+
+
+class MesoOptions(ctypes.Structure):
+    _fields_ = [
+        ("periodic_sides", ctypes.c_int), ("free_slip_top", ctypes.c_int), ("fixed_tau", ctypes.c_int),
+        ("enable_sgs", ctypes.c_int), ("disable_edge_blend", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("tau_hydro", ctypes.c_double), ("smagorinsky_c", ctypes.c_double), ("body_force", ctypes.c_double * 3),
+    ]
+
+
+def meso_transport(dx: float, dt: float, nu: float, pr: float) -> MesoTransport:
+    """derive_transport in float32 (mesoscale.cpp:45-68, hydro_core.h:109-115,
+    thermal_core.cpp:5-15)."""
+    dx, dt, nu, pr = f32(dx), f32(dt), f32(nu), f32(pr)
+    t = MesoTransport()
+    t.velocity_scale = float(dx / dt)
+    nu_lat = f32(nu * dt) / f32(dx * dx)
+    t.tau_shear = float(f32(0.5) + f32(3.0) * nu_lat)
+    alpha = f32(nu / pr)
+    alpha_lat = f32(alpha * dt) / f32(dx * dx)
+    t.tau_thermal = float(f32(0.5) + alpha_lat / f32(0.25))
+    return t
+
+
+class MesoOracle:
+    """Restated D3Q19 mesoscale step; precision 'f32' or 'f64'."""
+
+    def __init__(self, dims, dx=64.0, dt=5.0, nu=1.5e-5, pr=0.71, precision="f32", options: MesoOptions | None = None):
+        lib = Oracle.lib()
+        lib.oracle_d3q19_create.restype = ctypes.c_void_p
+        lib.oracle_d3q19_create.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(MesoTransport), ctypes.POINTER(MesoOptions), ctypes.c_double]
+        lib.oracle_d3q19_step.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_d3q19_destroy.argtypes = [ctypes.c_void_p]
+        self.lib = lib
+        self.dims = tuple(int(d) for d in dims)
+        self.cells = int(np.prod(self.dims))
+        tr = meso_transport(dx, dt, nu, pr)
+        self.h = lib.oracle_d3q19_create(*self.dims, 0 if precision == "f32" else 1, ctypes.byref(tr),
+                                         ctypes.byref(options) if options else None, float(np.float32(dt)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_d3q19_destroy(self.h)
+            self.h = None
+
+    def step(self, forcing: np.ndarray) -> np.ndarray:
+        fo = np.ascontiguousarray(forcing, np.float32)
+        out = np.zeros(self.cells * MESO_OUT, np.float32)
+        if not self.lib.oracle_d3q19_step(self.h, fo.ctypes.data, out.ctypes.data):
+            raise RuntimeError("oracle d3q19 step failed")
+        return out.reshape(self.cells, MESO_OUT)
+
+
+def meso_ref_run(dims, forcing: np.ndarray, steps: int, dx=64.0, dt=5.0, nu=1.5e-5, pr=0.71, path: Path = REF_LIB):
+    """The reference library's aero_lbm_mesoscale_step_context, `steps` calls."""
+    lib = ctypes.CDLL(str(path))
+    lib.aero_lbm_mesoscale_default_config.argtypes = [ctypes.POINTER(MesoConfig)]
+    lib.aero_lbm_mesoscale_create_context.argtypes = [ctypes.POINTER(MesoConfig), ctypes.POINTER(ctypes.c_longlong)]
+    lib.aero_lbm_mesoscale_create_context.restype = ctypes.c_int
+    lib.aero_lbm_mesoscale_step_context.argtypes = [ctypes.c_longlong, ctypes.POINTER(MesoConfig), ctypes.c_void_p, ctypes.c_void_p]
+    lib.aero_lbm_mesoscale_step_context.restype = ctypes.c_int
+    lib.aero_lbm_mesoscale_release_context.argtypes = [ctypes.c_longlong]
+    cfg = MesoConfig()
+    lib.aero_lbm_mesoscale_default_config(ctypes.byref(cfg))
+    cfg.nx, cfg.ny, cfg.nz = dims
+    cfg.dx_m, cfg.dt_s, cfg.molecular_nu_m2_s, cfg.prandtl_air = dx, dt, nu, pr
+    key = ctypes.c_longlong(0)
+    if not lib.aero_lbm_mesoscale_create_context(ctypes.byref(cfg), ctypes.byref(key)):
+        raise RuntimeError("mesoscale create failed")
+    fo = np.ascontiguousarray(forcing, np.float32)
+    out = np.zeros(int(np.prod(dims)) * MESO_OUT, np.float32)
+    for _ in range(steps):
+        if not lib.aero_lbm_mesoscale_step_context(key.value, ctypes.byref(cfg), fo.ctypes.data, out.ctypes.data):
+            raise RuntimeError("mesoscale step failed")
+    lib.aero_lbm_mesoscale_release_context(key.value)
+    return out.reshape(-1, MESO_OUT)
+
+
+def meso_forcing(dims, seed: int = 0, terrain_max: float = 3.0, wind=(6.0, 0.0, 3.0)) -> np.ndarray:
+    """Seeded 25-channel forcing: heightmap terrain (cells below it solid, the
+    mesoscale grid is y-up), temperatures, roughness, humidity, background wind."""
+    nx, ny, nz = dims
+    rng = np.random.default_rng(seed)
+    F = np.zeros((nx, ny, nz, MESO_CHANNELS), np.float32)
+    h = rng.uniform(0.0, terrain_max, (nx, nz)).astype(np.float32)
+    y = np.arange(ny)[None, :, None]
+    F[..., 0] = h[:, None, :]
+    F[..., 1] = 288.0
+    F[..., 2] = 288.15 + rng.uniform(-2, 2, (nx, ny, nz))
+    F[..., 3] = 289.65
+    F[..., 4] = 290.0 + rng.uniform(-3, 3, (nx, 1, nz))
+    F[..., 5] = rng.uniform(0.0, 2.0, (nx, 1, nz))
+    F[..., 6] = wind[0]
+    F[..., 7] = wind[2]
+    F[..., 9] = rng.uniform(0.2, 0.8, (nx, ny, nz))
+    F[..., 19] = wind[1]
+    F[..., 24] = (y < np.floor(h)[:, None, :]).astype(np.float32)
+    return F.reshape(-1, MESO_CHANNELS)

@@ -14,6 +14,10 @@ Fixtures:
   c1_16_200.npz   the same set-up at 16^3, 200 steps.
   tunnel_16_60.npz wind-tunnel faces (velocity inlet x-, convective outflow
                   x+, symmetry y/z), sphere obstacle, SGS off; 60 steps.
+  meso_12x8x10_30.npz D3Q19 mesoscale step (aero_lbm_mesoscale_step_context),
+                  12 x 8 x 10 (y up), seeded 25-channel forcing (seed 5,
+                  terrain up to 3 cells, wind (6, 0, 3) m/s), dx 64 m,
+                  dt 5 s; the 6-channel state after 30 calls.
 """
 from __future__ import annotations
 
@@ -77,6 +81,12 @@ def main() -> int:
     out = ref.run((16, 16, 16), cfg, pk, 60)
     np.savez_compressed(OUT / "tunnel_16_60.npz", out=out, obstacle=obst, steps=60, input_sha256=digest(pk))
     print("tunnel_16_60 written")
+    dims, seed, steps = (12, 8, 10), 5, 30
+    forcing = O.meso_forcing(dims, seed=seed)
+    out = O.meso_ref_run(dims, forcing, steps)
+    np.savez_compressed(OUT / "meso_12x8x10_30.npz", out=out, seed=seed, dims=np.array(dims), steps=steps,
+                        input_sha256=digest(forcing))
+    print("meso_12x8x10_30 written")
     return 0
 
 
