@@ -140,6 +140,34 @@ class AeroStepInput(ctypes.Structure):
 class AeroStepOutput(ctypes.Structure):
     _fields_ = [("flow_out", ctypes.POINTER(ctypes.c_float)), ("max_velocity", ctypes.c_float), ("status", ctypes.c_int)]
 
+class AeroLbmMesoscaleConfig(ctypes.Structure):
+    """native/include/aero_lbm_capi.h:124-141"""
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32), ("struct_size", ctypes.c_uint32),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx_m", ctypes.c_float), ("dt_s", ctypes.c_float), ("molecular_nu_m2_s", ctypes.c_float),
+        ("prandtl_air", ctypes.c_float), ("turbulent_prandtl", ctypes.c_float),
+        ("reference_density_kg_m3", ctypes.c_float), ("ambient_air_temperature_k", ctypes.c_float),
+        ("deep_ground_temperature_k", ctypes.c_float), ("background_wind_m_s", ctypes.c_float * 3),
+        ("reserved", ctypes.c_uint32 * 8),
+    ]
+
+
+class AeroLbmMesoscaleTransport(ctypes.Structure):
+    """native/include/aero_lbm_capi.h:143-149"""
+    _fields_ = [(n, ctypes.c_float) for n in ("velocity_scale_m_s_per_lattice", "nu_molecular_lattice",
+                                               "alpha_molecular_lattice", "tau_shear_molecular",
+                                               "tau_thermal_molecular")]
+
+
+class AeroLbmB200MesoscaleOptions(ctypes.Structure):
+    _fields_ = [
+        ("periodic_sides", ctypes.c_int), ("free_slip_top", ctypes.c_int), ("fixed_tau", ctypes.c_int),
+        ("enable_sgs", ctypes.c_int), ("disable_edge_blend", ctypes.c_int), ("hydro_only", ctypes.c_int),
+        ("tau_hydro", ctypes.c_double), ("smagorinsky_c", ctypes.c_double), ("body_force", ctypes.c_double * 3),
+        ("storage", ctypes.c_int), ("threads", ctypes.c_int),
+    ]
+
 
 # ---------------------------------------------------------------- loading
 _P = ctypes.c_void_p
@@ -204,6 +232,18 @@ SIGNATURES = {
     "aero_lbm_b200_batch_copy_flow": (_I, [_LL, _I, _F32P, _I]),
     "aero_lbm_b200_batch_destroy": (None, [_LL]),
     "aero_lbm_b200_batch_last_error": (ctypes.c_char_p, []),
+    # D3Q19 mesoscale ABI
+    "aero_lbm_mesoscale_default_config": (None, [ctypes.POINTER(AeroLbmMesoscaleConfig)]),
+    "aero_lbm_mesoscale_derive_transport": (_I, [ctypes.POINTER(AeroLbmMesoscaleConfig),
+                                                 ctypes.POINTER(AeroLbmMesoscaleTransport)]),
+    "aero_lbm_mesoscale_create_context": (_I, [ctypes.POINTER(AeroLbmMesoscaleConfig), ctypes.POINTER(_LL)]),
+    "aero_lbm_mesoscale_step_context": (_I, [_LL, ctypes.POINTER(AeroLbmMesoscaleConfig), _F32P, _F32P]),
+    "aero_lbm_mesoscale_release_context": (None, [_LL]),
+    "aero_lbm_b200_mesoscale_default_options": (None, [ctypes.POINTER(AeroLbmB200MesoscaleOptions)]),
+    "aero_lbm_b200_mesoscale_set_options": (_I, [_LL, ctypes.POINTER(AeroLbmB200MesoscaleOptions)]),
+    "aero_lbm_b200_mesoscale_advance": (_I, [_LL, _I]),
+    "aero_lbm_b200_mesoscale_read_state": (_I, [_LL, _F32P]),
+    "aero_lbm_b200_mesoscale_info": (_I, [_LL, ctypes.POINTER(_LL), ctypes.POINTER(ctypes.c_double)]),
     # wind-tunnel ABI
     "aero_solver_default_grid": (None, [ctypes.POINTER(AeroGridDesc)]),
     "aero_solver_default_boundary": (None, [ctypes.POINTER(AeroBoundaryDesc)]),
@@ -444,3 +484,66 @@ class BrickBatch:
         if self.handle:
             self.lib.aero_lbm_b200_batch_destroy(self.handle)
             self.handle = 0
+
+
+class MesoscaleContext:
+    """A D3Q19 mesoscale grid (aero_lbm_mesoscale_* plus the B200 options).
+
+    ``dims`` = (nx, ny, nz) with y up; forcing arrays are (cells, 25) float32,
+    outputs (cells, 6)."""
+
+    def __init__(self, dims, dx_m: float = 64.0, dt_s: float = 5.0, nu: float = 1.5e-5, prandtl: float = 0.71,
+                 options: dict | None = None, lib: ctypes.CDLL | None = None):
+        self.lib = lib or load_library()
+        self.cfg = AeroLbmMesoscaleConfig()
+        self.lib.aero_lbm_mesoscale_default_config(ctypes.byref(self.cfg))
+        self.cfg.nx, self.cfg.ny, self.cfg.nz = (int(d) for d in dims)
+        self.cfg.dx_m, self.cfg.dt_s, self.cfg.molecular_nu_m2_s, self.cfg.prandtl_air = dx_m, dt_s, nu, prandtl
+        self.dims = tuple(int(d) for d in dims)
+        self.cells = int(np.prod(self.dims))
+        key = ctypes.c_longlong(0)
+        if not self.lib.aero_lbm_mesoscale_create_context(ctypes.byref(self.cfg), ctypes.byref(key)):
+            raise RuntimeError("mesoscale_create_context failed: " + last_error(self.lib))
+        self.key = key.value
+        if options:
+            self.set_options(**options)
+
+    def set_options(self, **kw) -> None:
+        o = AeroLbmB200MesoscaleOptions()
+        self.lib.aero_lbm_b200_mesoscale_default_options(ctypes.byref(o))
+        for k, v in kw.items():
+            if k == "body_force":
+                for a in range(3):
+                    o.body_force[a] = float(v[a])
+            else:
+                setattr(o, k, v)
+        if not self.lib.aero_lbm_b200_mesoscale_set_options(self.key, ctypes.byref(o)):
+            raise RuntimeError("mesoscale_set_options failed: " + last_error(self.lib))
+
+    def step(self, forcing: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        fo = np.ascontiguousarray(forcing, np.float32)
+        if out is None:
+            out = np.zeros((self.cells, 6), np.float32)
+        if not self.lib.aero_lbm_mesoscale_step_context(self.key, ctypes.byref(self.cfg), fptr(fo), fptr(out)):
+            raise RuntimeError("mesoscale_step_context failed: " + last_error(self.lib))
+        return out
+
+    def advance(self, steps: int) -> None:
+        if not self.lib.aero_lbm_b200_mesoscale_advance(self.key, int(steps)):
+            raise RuntimeError("mesoscale_advance failed: " + last_error(self.lib))
+
+    def state(self) -> np.ndarray:
+        out = np.zeros((self.cells, 6), np.float32)
+        if not self.lib.aero_lbm_b200_mesoscale_read_state(self.key, fptr(out)):
+            raise RuntimeError("mesoscale_read_state failed: " + last_error(self.lib))
+        return out
+
+    def info(self) -> dict:
+        c, b = ctypes.c_longlong(0), ctypes.c_double(0)
+        self.lib.aero_lbm_b200_mesoscale_info(self.key, ctypes.byref(c), ctypes.byref(b))
+        return {"cells": c.value, "bytes_per_step": b.value}
+
+    def release(self) -> None:
+        if self.key:
+            self.lib.aero_lbm_mesoscale_release_context(self.key)
+            self.key = 0

@@ -123,3 +123,53 @@ def c2_terrain_boussinesq(n: int = 128, seed: int = 2024, tau: float = 0.55, ste
     faces = [far, far, {"kind": PERIODIC}, {"kind": PERIODIC}, {"kind": BOUNCE_BACK}, far]
     return BrickCase("c2-terrain-boussinesq", (n, n, n), obstacle, u, temp, faces, tau, u_in, sgs=True,
                      smagorinsky_c=0.1, buoyancy=True, buoyancy_beta=1e-4, gravity_axis=2, steps=steps)
+
+
+MESO_CHANNELS = 25
+
+
+@dataclass
+class MesoCase:
+    """A D3Q19 mesoscale grid (y up, cell = (x*ny + y)*nz + z): the 25-channel
+    forcing of aero_lbm_mesoscale_step_context plus the step options."""
+    name: str
+    dims: tuple                     # (nx, ny, nz), ny vertical
+    forcing: np.ndarray             # float32 (cells, 25)
+    dx_m: float
+    dt_s: float
+    options: dict                   # periodic_sides, free_slip_top, fixed_tau, tau_hydro, enable_sgs,
+                                    # smagorinsky_c, body_force, hydro_only, disable_edge_blend
+    steps: int = 2000
+
+    @property
+    def cells(self) -> int:
+        return int(np.prod(self.dims))
+
+    @property
+    def velocity_scale(self) -> float:
+        return float(np.float32(self.dx_m) / np.float32(self.dt_s))
+
+
+def c3_meso_terrain(nx: int = 256, nz: int = 256, ny: int = 64, seed: int = 77, steps: int = 2000,
+                    dx_m: float = 64.0, dt_s: float = 5.0) -> MesoCase:
+    """Mesoscale boundary layer: seeded smooth terrain (3-octave value noise up
+    to 12 cells at ny=64, scaled with ny) as the bounce-back ground, a free-slip
+    lid, periodic sides, a body force (1e-6, 0, 0), tau 0.52 with Smagorinsky
+    (C = 0.1), initial u_x(y) = 0.06 ln(1+y) / ln(ny+1) (as the background
+    wind channel, which seeds the state). The hydrodynamic distribution runs
+    alone (no thermal distribution, no target relaxation)."""
+    h = value_noise_heightmap(nx, nz, 3, 12.0 * ny / 64.0, seed)
+    y = np.arange(ny, dtype=np.float64)[None, :, None]
+    F = np.zeros((nx, ny, nz, MESO_CHANNELS), np.float32)
+    solid = (y < h[:, None, :])
+    vs = float(np.float32(dx_m) / np.float32(dt_s))
+    ux = 0.06 * np.log1p(y) / np.log(ny + 1.0)
+    F[..., 0] = h[:, None, :]
+    F[..., 2] = 288.15
+    F[..., 3] = 289.65
+    F[..., 4] = 290.0
+    F[..., 6] = np.broadcast_to(ux * vs, (nx, ny, nz))
+    F[..., 24] = solid.astype(np.float32)
+    opts = {"periodic_sides": 1, "free_slip_top": 1, "fixed_tau": 1, "tau_hydro": 0.52, "enable_sgs": 1,
+            "smagorinsky_c": 0.1, "body_force": (1e-6, 0.0, 0.0), "hydro_only": 1, "disable_edge_blend": 1}
+    return MesoCase("c3-meso-terrain", (nx, ny, nz), F.reshape(-1, MESO_CHANNELS), dx_m, dt_s, opts, steps)

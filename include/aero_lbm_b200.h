@@ -279,6 +279,83 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_copy_flow(long long handle, int bri
 AERO_LBM_B200_EXPORT void aero_lbm_b200_batch_destroy(long long handle);
 AERO_LBM_B200_EXPORT const char* aero_lbm_b200_batch_last_error(void);
 
+/* ---- D3Q19 mesoscale ABI (native/include/aero_lbm_capi.h:124-150, 286-301;
+ *      native/src/aero_lbm_mesoscale.cpp:1397-1510) ---- */
+
+/* native/include/aero_lbm_capi.h:124 — mesoscale grid (y up). */
+typedef struct AeroLbmMesoscaleConfig {
+    uint32_t abi_version;
+    uint32_t struct_size;
+    int nx;
+    int ny;
+    int nz;
+    float dx_m;
+    float dt_s;
+    float molecular_nu_m2_s;
+    float prandtl_air;
+    float turbulent_prandtl;
+    float reference_density_kg_m3;
+    float ambient_air_temperature_k;
+    float deep_ground_temperature_k;
+    float background_wind_m_s[3];
+    uint32_t reserved[8];
+} AeroLbmMesoscaleConfig;
+
+/* native/include/aero_lbm_capi.h:143 */
+typedef struct AeroLbmMesoscaleTransport {
+    float velocity_scale_m_s_per_lattice;
+    float nu_molecular_lattice;
+    float alpha_molecular_lattice;
+    float tau_shear_molecular;
+    float tau_thermal_molecular;
+} AeroLbmMesoscaleTransport;
+
+/* native/include/aero_lbm_capi.h:286 (mesoscale.cpp:1399) — 32 x 4 x 32, dx 64 m, dt 5 s, ... */
+AERO_LBM_B200_EXPORT void aero_lbm_mesoscale_default_config(AeroLbmMesoscaleConfig* out_config);
+/* native/include/aero_lbm_capi.h:287 (mesoscale.cpp:1420) — lattice transport of a config. */
+AERO_LBM_B200_EXPORT int aero_lbm_mesoscale_derive_transport(const AeroLbmMesoscaleConfig* config,
+                                                             AeroLbmMesoscaleTransport* out_transport);
+/* native/include/aero_lbm_capi.h:291 (mesoscale.cpp:1436) — keys count up from 1. */
+AERO_LBM_B200_EXPORT int aero_lbm_mesoscale_create_context(const AeroLbmMesoscaleConfig* config, long long* out_context_key);
+/* native/include/aero_lbm_capi.h:295 (mesoscale.cpp:1452) — one step: forcing is cells x 25
+ * floats, out_state cells x 6 (ambient K, deep ground K, surface K, wind x, y, z m/s). The
+ * first call (and the first after a shape change) seeds from the forcing. Synchronous. */
+AERO_LBM_B200_EXPORT int aero_lbm_mesoscale_step_context(long long context_key, const AeroLbmMesoscaleConfig* config,
+                                                         const float* forcing, float* out_state);
+/* native/include/aero_lbm_capi.h:301 (mesoscale.cpp:1500) */
+AERO_LBM_B200_EXPORT void aero_lbm_mesoscale_release_context(long long context_key);
+
+/* B200 extension: options of the mesoscale step the reference does not have.
+ * All zero = the reference step. hydro_only runs the hydrodynamic
+ * distribution alone (relaxation toward the cell's own rho, u; no thermal
+ * distribution, no forcing targets; output channels rho, 0, 0, wind) in one
+ * fused pull + collide launch per call, with FP32 populations (storage 0,
+ * bit-identical to the restatement) or FP16 deviations (storage 1). */
+typedef struct AeroLbmB200MesoscaleOptions {
+    int periodic_sides;      /* x and z wrap */
+    int free_slip_top;       /* specular lid at y = ny */
+    int fixed_tau;           /* use tau_hydro instead of the derived, clamped tau */
+    int enable_sgs;          /* Smagorinsky on the even hydrodynamic rate */
+    int disable_edge_blend;  /* no 2-cell equilibrium blend at open sides / top */
+    int hydro_only;
+    double tau_hydro;
+    double smagorinsky_c;
+    double body_force[3];    /* lattice force density (Guo source), y up */
+    int storage;             /* hydro_only: 0 FP32, 1 FP16 deviations */
+    int threads;             /* hydro_only: block size 64, 128 or 256 (0 = 256) */
+} AeroLbmB200MesoscaleOptions;
+
+AERO_LBM_B200_EXPORT void aero_lbm_b200_mesoscale_default_options(AeroLbmB200MesoscaleOptions* out_options);
+/* Set a context's options; the context re-seeds at its next step. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_mesoscale_set_options(long long context_key, const AeroLbmB200MesoscaleOptions* options);
+/* `steps` more steps with the forcing of the last step call, on the library
+ * stream, without output or synchronisation (device-resident stepping). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_mesoscale_advance(long long context_key, int steps);
+/* The output state of the current step (cells x 6); synchronises. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_mesoscale_read_state(long long context_key, float* out_state);
+/* Cells and algorithmic population bytes per step of a context (after its first step). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_mesoscale_info(long long context_key, long long* out_cells, double* out_bytes_per_step);
+
 /* ---- wind-tunnel ABI (native/include/aero_solver_capi.h:1-115) ---- */
 enum {
     AERO_SOLVER_ABI_VERSION = 1,

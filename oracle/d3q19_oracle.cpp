@@ -52,7 +52,8 @@ typedef struct OracleD3Q19Options {
     int fixed_tau;          // use tau_hydro below instead of the derived, clamped tau
     int enable_sgs;         // Smagorinsky on the even hydrodynamic rate
     int disable_edge_blend; // no 2-cell equilibrium blend at the sides / top
-    int reserved;
+    int hydro_only;         // hydrodynamic distribution alone: relax toward the cell's own
+                            // rho, u (no forcing targets); output (rho, 0, 0, wind)
     double tau_hydro;
     double smagorinsky_c;
     double body_force[3];   // lattice force density (x, y, z; y is up)
@@ -154,6 +155,20 @@ struct Meso {
 
     struct Targets { T rho, ux, uy, uz, teq, nsurf, ndeep; };
 
+    // hydro_only: the cell's own moments, no target relaxation.
+    Targets own_moments(const float* F, int i) const {
+        if (solid(F, i)) return Targets{T(1), T(0), T(0), T(0), T(0), surface[i], deep[i]};
+        T r = T(0), ux = T(0), uy = T(0), uz = T(0);
+        for (int q = 0; q < Q; ++q) {
+            const T fq = f[di(i, q)];
+            r += fq;
+            ux += fq * T(kCx[q]); uy += fq * T(kCy[q]); uz += fq * T(kCz[q]);
+        }
+        r = std::max(T(1.0e-6), r);
+        ux /= r; uy /= r; uz /= r;
+        return Targets{r, ux, uy, uz, T(0), surface[i], deep[i]};
+    }
+
     Targets targets(const float* F, T dt_s, int x, int y, int z) const {
         const int i = idx(x, y, z);
         const T dt = std::max(T(1.0e-3), dt_s);
@@ -229,7 +244,7 @@ struct Meso {
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     const int i = idx(x, y, z);
-                    const Targets t = targets(F, dt_s, x, y, z);
+                    const Targets t = opt.hydro_only ? own_moments(F, i) : targets(F, dt_s, x, y, z);
                     ndeep[i] = t.ndeep;
                     nsurf[i] = t.nsurf;
                     T om_h_even = T(1.0) / tau_h;
@@ -335,7 +350,7 @@ struct Meso {
                             fv = pf[di(i, kOpp[q])];
                             gv = geq(q, wall_temp(F, i), T(0), T(0), T(0));
                             bounced = true;
-                        } else if (opt.free_slip_top && sy >= ny) {
+                        } else if (opt.free_slip_top && sy >= ny && sx >= 0 && sx < nx && sz >= 0 && sz < nz) {
                             // specular reflection at the lid: the population that left the cell
                             // (sx, ny-1, sz) upward with the mirrored velocity
                             int mq = 0;
@@ -392,7 +407,11 @@ struct Meso {
         if (out)
             for (int i = 0; i < cells; ++i) {
                 float* o = out + (size_t)i * kOut;
-                o[0] = float(ambient[i]); o[1] = float(deep[i]); o[2] = float(surface[i]);
+                if (opt.hydro_only) {
+                    o[0] = float(rho[i]); o[1] = 0.0f; o[2] = 0.0f;
+                } else {
+                    o[0] = float(ambient[i]); o[1] = float(deep[i]); o[2] = float(surface[i]);
+                }
                 o[3] = float(wx[i]); o[4] = float(wy[i]); o[5] = float(wz[i]);
             }
     }

@@ -394,7 +394,7 @@ class MesoTransport(ctypes.Structure):
 class MesoOptions(ctypes.Structure):
     _fields_ = [
         ("periodic_sides", ctypes.c_int), ("free_slip_top", ctypes.c_int), ("fixed_tau", ctypes.c_int),
-        ("enable_sgs", ctypes.c_int), ("disable_edge_blend", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("enable_sgs", ctypes.c_int), ("disable_edge_blend", ctypes.c_int), ("hydro_only", ctypes.c_int),
         ("tau_hydro", ctypes.c_double), ("smagorinsky_c", ctypes.c_double), ("body_force", ctypes.c_double * 3),
     ]
 

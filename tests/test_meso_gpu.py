@@ -1,0 +1,196 @@
+"""D3Q19 mesoscale step on the GPU through the C ABI.
+
+The reference model (hydrodynamic + thermal distributions relaxed toward
+forcing targets) and the hydrodynamic-only fused step with FP32 populations
+are compared bit-for-bit with the oracle (and with the reference's golden
+fixture). FP16 deviation storage is compared with the oracle's FP64 run of the
+same scheme: after 400 steps of the C3 set-up at 48 x 32 x 48, wind error
+relative to the largest wind <= 2.5e-3 (measured 1.7e-3) and density error
+<= 1e-4."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import aero_b200
+import oracle as O
+from test_inplace_gpu import load_cases
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+cases = load_cases()
+
+
+def bits(a) -> np.ndarray:
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def assert_bits(got, want, what=""):
+    g, w = bits(got), bits(want)
+    bad = np.flatnonzero(g.reshape(-1) != w.reshape(-1))
+    assert bad.size == 0, f"{what}: {bad.size} values differ, first at {bad[:5]}: " \
+                          f"{np.asarray(got).reshape(-1)[bad[:5]]} vs {np.asarray(want).reshape(-1)[bad[:5]]}"
+
+
+def oracle_options(opts: dict | None) -> O.MesoOptions | None:
+    if not opts:
+        return None
+    o = O.MesoOptions()
+    o.tau_hydro, o.smagorinsky_c = 0.58, 0.1
+    for k, v in opts.items():
+        if k == "body_force":
+            for a in range(3):
+                o.body_force[a] = float(v[a])
+        elif k in ("storage", "threads"):
+            continue
+        else:
+            setattr(o, k, v)
+    return o
+
+
+def run_both(dims, forcing_seq, opts=None, dx=64.0, dt=5.0, precision="f32"):
+    """Step the GPU context and the oracle through the same forcing sequence;
+    yield (gpu_out, oracle_out) after every call."""
+    ctx = aero_b200.MesoscaleContext(dims, dx_m=dx, dt_s=dt, options=opts)
+    orc = O.MesoOracle(dims, dx=dx, dt=dt, precision=precision, options=oracle_options(opts))
+    try:
+        for F in forcing_seq:
+            yield ctx.step(F), orc.step(F)
+    finally:
+        ctx.release()
+
+
+def test_reference_model_matches_golden(gpu):
+    g = np.load(GOLDEN / "meso_12x8x10_30.npz")
+    dims = tuple(int(d) for d in g["dims"])
+    F = O.meso_forcing(dims, seed=int(g["seed"]))
+    ctx = aero_b200.MesoscaleContext(dims)
+    for _ in range(int(g["steps"])):
+        out = ctx.step(F)
+    ctx.release()
+    assert_bits(out, g["out"], "golden")
+
+
+@pytest.mark.parametrize("dims,dt,seed,wind", [
+    ((9, 5, 7), 5.0, 11, (6.0, 0.0, 3.0)),
+    ((8, 1, 8), 5.0, 12, (2.0, 0.5, -4.0)),
+    ((33, 7, 20), 0.5, 13, (20.0, 1.0, 0.0)),
+])
+def test_reference_model_bit_exact(gpu, dims, dt, seed, wind):
+    F = O.meso_forcing(dims, seed=seed, wind=wind)
+    for k, (a, b) in enumerate(run_both(dims, [F] * 25, dt=dt)):
+        if k in (0, 1, 24):
+            assert_bits(a, b, f"call {k}")
+
+
+def test_reference_model_forcing_changes(gpu):
+    """The forcing (solid mask, winds, temperatures) changes between calls."""
+    dims = (14, 6, 11)
+    seq = [O.meso_forcing(dims, seed=40 + (k // 4), wind=(5.0 + k, 0.0, -2.0)) for k in range(16)]
+    for k, (a, b) in enumerate(run_both(dims, seq)):
+        assert_bits(a, b, f"call {k}")
+
+
+def test_reference_model_with_options(gpu):
+    dims = (12, 9, 10)
+    F = O.meso_forcing(dims, seed=5)
+    opts = {"periodic_sides": 1, "free_slip_top": 1, "fixed_tau": 1, "tau_hydro": 0.6, "enable_sgs": 1,
+            "smagorinsky_c": 0.1, "body_force": (2e-5, 0.0, -1e-5)}
+    for k, (a, b) in enumerate(run_both(dims, [F] * 20, opts)):
+        if k in (0, 19):
+            assert_bits(a, b, f"call {k}")
+
+
+def c3_small(nx=24, ny=16, nz=20, seed=3):
+    return cases.c3_meso_terrain(nx=nx, nz=nz, ny=ny, seed=seed)
+
+
+def test_hydro_fp32_bit_exact_c3_small(gpu):
+    c = c3_small()
+    for k, (a, b) in enumerate(run_both(c.dims, [c.forcing] * 120, c.options, c.dx_m, c.dt_s)):
+        if k in (0, 1, 2, 119):
+            assert_bits(a, b, f"call {k}")
+
+
+def test_hydro_fp32_open_boundaries_and_mask_change(gpu):
+    """Open sides and top with the edge blend, a mask that changes between
+    calls, SGS, and a body force."""
+    dims = (13, 7, 9)
+    seq = [O.meso_forcing(dims, seed=60 + (k // 5), terrain_max=3.0, wind=(8.0, 0.5, 2.0)) for k in range(15)]
+    opts = {"hydro_only": 1, "enable_sgs": 1, "body_force": (1e-5, 0.0, 0.0), "fixed_tau": 1, "tau_hydro": 0.55}
+    for k, (a, b) in enumerate(run_both(dims, seq, opts)):
+        assert_bits(a, b, f"call {k}")
+
+
+@pytest.mark.parametrize("hydro", [0, 1])
+def test_advance_matches_step_calls(gpu, hydro):
+    dims = (10, 8, 12)
+    F = O.meso_forcing(dims, seed=9)
+    opts = {"hydro_only": hydro, "periodic_sides": 1, "free_slip_top": 1}
+    a = aero_b200.MesoscaleContext(dims, options=opts)
+    b = aero_b200.MesoscaleContext(dims, options=opts)
+    a.step(F)
+    a.advance(9)
+    got = a.state()
+    for _ in range(10):
+        want = b.step(F)
+    a.release()
+    b.release()
+    assert_bits(got, want, "advance")
+
+
+@pytest.mark.parametrize("threads", [64, 128])
+def test_hydro_block_sizes_agree(gpu, threads):
+    c = c3_small(20, 12, 16)
+    outs = []
+    for t in (256, threads):
+        ctx = aero_b200.MesoscaleContext(c.dims, options={**c.options, "threads": t})
+        for _ in range(30):
+            out = ctx.step(c.forcing)
+        outs.append(out)
+        ctx.release()
+    assert_bits(outs[0], outs[1], "threads")
+
+
+def test_hydro_fp16_vs_fp64_c3(gpu):
+    c = c3_small(48, 32, 48, seed=8)
+    steps = 400
+    ctx = aero_b200.MesoscaleContext(c.dims, options={**c.options, "storage": 1})
+    ref = O.MesoOracle(c.dims, dx=c.dx_m, dt=c.dt_s, precision="f64", options=oracle_options(c.options))
+    for _ in range(steps):
+        got = ctx.step(c.forcing)
+        want = ref.step(c.forcing)
+    ctx.release()
+    vs = c.velocity_scale
+    umax = np.abs(want[:, 3:]).max()
+    err_u = np.abs(got[:, 3:] - want[:, 3:]).max() / umax
+    err_rho = np.abs(got[:, 0] - want[:, 0]).max()
+    assert umax > 0.03 * vs
+    assert err_u <= 2.5e-3, err_u
+    assert err_rho <= 1e-4, err_rho
+
+
+def test_hydro_full_size_c3_bit_exact_first_steps(gpu):
+    """The full 256 x 64 x 256 grid: three calls bit-for-bit against the oracle."""
+    c = cases.c3_meso_terrain()
+    for k, (a, b) in enumerate(run_both(c.dims, [c.forcing] * 3, c.options, c.dx_m, c.dt_s)):
+        assert_bits(a, b, f"call {k}")
+
+
+def test_shape_change_reseeds(gpu):
+    d1, d2 = (8, 5, 8), (10, 6, 7)
+    F1, F2 = O.meso_forcing(d1, seed=1), O.meso_forcing(d2, seed=2)
+    ctx = aero_b200.MesoscaleContext(d1)
+    for _ in range(3):
+        ctx.step(F1)
+    ctx.cfg.nx, ctx.cfg.ny, ctx.cfg.nz = d2
+    ctx.cells = int(np.prod(d2))
+    got = [ctx.step(F2) for _ in range(4)][-1]
+    ctx.release()
+    orc = O.MesoOracle(d2)
+    for _ in range(4):
+        want = orc.step(F2)
+    assert_bits(got, want, "reseed")
