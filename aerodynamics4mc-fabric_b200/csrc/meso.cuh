@@ -76,6 +76,7 @@ struct HydroArgs {
     float scale, inv_scale;        // FP16 deviation scale (FP16 storage only)
     HydroRates h;
     const uint8_t* solid_prev;     // mask the pull streams with (the previous call's)
+    const uint32_t* flags_prev;    // pull classification of solid_prev (meso_hydro_flags)
     const uint8_t* solid_cur;      // mask of this call's collision
     const float* forcing_prev;     // previous call's forcing (open-boundary winds)
     const void* src;               // 19 x cells, float or __half
@@ -93,6 +94,12 @@ enum MesoHydroMode { kHydroInit = 0, kHydroStep = 1, kHydroOutput = 2 };
 cudaError_t meso_hydro_seed(const float* forcing, int nx, int ny, int nz, float velocity_scale, bool fp16, float scale,
                             void* dst, uint8_t* solid, cudaStream_t s);
 cudaError_t meso_hydro_mask(const float* forcing, long long cells, uint8_t* solid, cudaStream_t s);
+// Pull classification word per cell: bit q (0..18) = direction q bounces back,
+// kHydroSlow = the cell pulls through an open side or the lid, or is blended,
+// kHydroSelfSolid = the cell is solid.
+constexpr uint32_t kHydroSelfSolid = 1u << 31;
+constexpr uint32_t kHydroSlow = 1u << 30;
+cudaError_t meso_hydro_flags(const meso::HydroArgs& a, const uint8_t* solid, uint32_t* flags, cudaStream_t s);
 cudaError_t meso_hydro_launch(const meso::HydroArgs& a, int mode, bool fp16, int threads, cudaStream_t s);
 
 }  // namespace aero

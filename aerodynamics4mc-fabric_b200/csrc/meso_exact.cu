@@ -450,9 +450,25 @@ __global__ void __launch_bounds__(256) meso_hydro_kernel(HydroArgs A) {
     if (kMode == kHydroInit) {
 #pragma unroll
         for (int q = 0; q < 19; ++q) f[q] = S::load(src + q * cells + i, q, A.inv_scale);
-    } else if (A.solid_prev[i]) {
+    } else if (A.flags_prev[i] & kHydroSelfSolid) {
 #pragma unroll
         for (int q = 0; q < 19; ++q) f[q] = hfeq(q, 1.0f, 0.0f, 0.0f, 0.0f);
+    } else if (!(A.flags_prev[i] & kHydroSlow)) {
+        // interior (or periodic / ground) cell: every source is known from the
+        // classification word, so the 19 loads are independent of each other
+        const uint32_t w = A.flags_prev[i];
+        long long idx[19];
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            int sx = x - mcx(q), sz = z - mcz(q);
+            if (A.periodic_sides) {
+                sx = sx < 0 ? sx + nx : (sx >= nx ? sx - nx : sx);
+                sz = sz < 0 ? sz + nz : (sz >= nz ? sz - nz : sz);
+            }
+            idx[q] = ((w >> q) & 1u) ? (long long)mopp(q) * cells + i : (long long)q * cells + midx(A, sx, y - mcy(q), sz);
+        }
+#pragma unroll
+        for (int q = 0; q < 19; ++q) f[q] = S::load(src + idx[q], q, A.inv_scale);
     } else {
         int edge = min(min(x, z), min(nx - 1 - x, nz - 1 - z));
         int top = ny - 1 - y;
@@ -513,7 +529,7 @@ __global__ void __launch_bounds__(256) meso_hydro_kernel(HydroArgs A) {
     }
     if (kMode == kHydroOutput) {
         float* o = A.out_state + i * kMesoStateChannels;
-        if (A.solid_prev[i]) {
+        if (A.flags_prev[i] & kHydroSelfSolid) {
             o[0] = 1.0f;
             o[1] = o[2] = o[3] = o[4] = o[5] = 0.0f;
             return;
@@ -583,6 +599,41 @@ __global__ void meso_hydro_seed_kernel(const float* __restrict__ F, int nx, int 
     for (int q = 0; q < 19; ++q) S::store(dst + q * cells + i, q, hfeq(q, 1.0f, lx, ly, lz), scale);
 }
 
+// Pull classification of a mask (see meso_hydro_flags).
+__global__ void meso_hydro_flags_kernel(HydroArgs A, const uint8_t* __restrict__ solid, uint32_t* __restrict__ flags) {
+    const int nx = A.nx, ny = A.ny, nz = A.nz;
+    const long long cells = (long long)nx * ny * nz;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cells) return;
+    if (solid[i]) {
+        flags[i] = kHydroSelfSolid;
+        return;
+    }
+    const int z = (int)(i % nz), y = (int)((i / nz) % ny), x = (int)(i / ((long long)ny * nz));
+    int edge = min(min(x, z), min(nx - 1 - x, nz - 1 - z));
+    int top = ny - 1 - y;
+    if (A.periodic_sides) edge = 1 << 20;
+    if (A.free_slip_top) top = 1 << 20;
+    const int sponge = min(edge, top);
+    bool slow = A.edge_blend && sponge < 2;
+    uint32_t w = 0;
+    for (int q = 0; q < 19; ++q) {
+        int sx = x - mcx(q), sy = y - mcy(q), sz = z - mcz(q);
+        if (A.periodic_sides) {
+            sx = sx < 0 ? sx + nx : (sx >= nx ? sx - nx : sx);
+            sz = sz < 0 ? sz + nz : (sz >= nz ? sz - nz : sz);
+        }
+        if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) {
+            if (solid[midx(A, sx, sy, sz)]) w |= 1u << q;
+        } else if (sy < 0) {
+            w |= 1u << q;
+        } else {
+            slow = true;
+        }
+    }
+    flags[i] = w | (slow ? kHydroSlow : 0u);
+}
+
 __global__ void meso_mask_kernel(const float* __restrict__ F, long long cells, uint8_t* __restrict__ solid) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < cells) solid[i] = solid_at(F, i) ? 1 : 0;
@@ -619,6 +670,13 @@ cudaError_t meso_hydro_seed(const float* forcing, int nx, int ny, int nz, float 
     else
         meso::meso_hydro_seed_kernel<meso::MesoF32><<<blocks, 256, 0, s>>>(forcing, nx, ny, nz, velocity_scale, scale,
                                                                            static_cast<float*>(dst), solid);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t meso_hydro_flags(const meso::HydroArgs& a, const uint8_t* solid, uint32_t* flags, cudaStream_t s) {
+    const long long cells = (long long)a.nx * a.ny * a.nz;
+    meso::meso_hydro_flags_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(a, solid, flags);
     count_launch();
     return cudaGetLastError();
 }

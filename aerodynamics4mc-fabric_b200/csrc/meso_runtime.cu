@@ -66,6 +66,7 @@ struct MesoContext {
     float fp16_scale = 1.0f;
     float* forcing[2] = {nullptr, nullptr};
     uint8_t* solid[2] = {nullptr, nullptr};
+    uint32_t* flags[2] = {nullptr, nullptr};  // hydro: pull classification of solid[k]
     int fslot = 0;          // forcing / mask of the last step call
     // reference model
     float *f = nullptr, *g = nullptr, *pf = nullptr, *pg = nullptr;
@@ -78,12 +79,14 @@ struct MesoContext {
 
     ~MesoContext() { release(); }
     void release() {
-        for (void* p : {(void*)forcing[0], (void*)forcing[1], (void*)solid[0], (void*)solid[1], (void*)f, (void*)g,
+        for (void* p : {(void*)forcing[0], (void*)forcing[1], (void*)solid[0], (void*)solid[1], (void*)flags[0],
+                        (void*)flags[1], (void*)f, (void*)g,
                         (void*)pf, (void*)pg, (void*)ambient, (void*)deep, (void*)surface, (void*)ndeep, (void*)nsurf,
                         pop[0], pop[1], (void*)out})
             if (p) cudaFree(p);
         forcing[0] = forcing[1] = nullptr;
         solid[0] = solid[1] = nullptr;
+        flags[0] = flags[1] = nullptr;
         f = g = pf = pg = ambient = deep = surface = ndeep = nsurf = out = nullptr;
         pop[0] = pop[1] = nullptr;
         cells = 0;
@@ -121,7 +124,8 @@ bool allocate(MesoContext& c) {
     if (!ok) return false;
     if (c.hydro) {
         const size_t bytes = n * 19 * (c.fp16 ? 2 : 4);
-        ok = cuda_ok(cudaMalloc(&c.pop[0], bytes), "meso populations") && cuda_ok(cudaMalloc(&c.pop[1], bytes), "meso populations");
+        ok = cuda_ok(cudaMalloc(&c.pop[0], bytes), "meso populations") && cuda_ok(cudaMalloc(&c.pop[1], bytes), "meso populations") &&
+             dev_alloc(&c.flags[0], n, "meso flags") && dev_alloc(&c.flags[1], n, "meso flags");
     } else {
         ok = dev_alloc(&c.f, n * 19, "meso f") && dev_alloc(&c.g, n * 19, "meso g") && dev_alloc(&c.pf, n * 19, "meso post f") &&
              dev_alloc(&c.pg, n * 19, "meso post g") && dev_alloc(&c.ambient, n, "meso ambient") &&
@@ -189,6 +193,7 @@ meso::HydroArgs hydro_args(const MesoContext& c, const Transport& t, int prev_sl
     a.inv_scale = c.fp16 ? 1.0f / c.fp16_scale : 1.0f;
     a.h = rates(c, t);
     a.solid_prev = c.solid[prev_slot];
+    a.flags_prev = c.flags[prev_slot];
     a.solid_cur = c.solid[cur_slot];
     a.forcing_prev = c.forcing[prev_slot];
     a.src = c.pop[c.cur];
@@ -319,14 +324,17 @@ AERO_LBM_B200_EXPORT int aero_lbm_mesoscale_step_context(long long key, const Ae
             c->fp16_scale = c->fp16 ? fp16_scale_for_speed(seed_speed(forcing, c->cells, t.velocity_scale)) : 1.0f;
             c->cur = 0;
             if (!cuda_ok(meso_hydro_seed(c->forcing[slot], c->nx, c->ny, c->nz, t.velocity_scale, c->fp16, c->fp16_scale,
-                                         c->pop[0], c->solid[slot], s), "mesoscale hydro seed"))
+                                         c->pop[0], c->solid[slot], s), "mesoscale hydro seed") ||
+                !cuda_ok(meso_hydro_flags(hydro_args(*c, t, slot, slot), c->solid[slot], c->flags[slot], s), "mesoscale flags"))
                 return 0;
             const meso::HydroArgs a = hydro_args(*c, t, slot, slot);
             if (!cuda_ok(meso_hydro_launch(a, kHydroInit, c->fp16, hydro_threads(*c), s), "mesoscale hydro init")) return 0;
             c->cur = 1;
             c->initialized = true;
         } else {
-            if (!cuda_ok(meso_hydro_mask(c->forcing[slot], c->cells, c->solid[slot], s), "mesoscale mask")) return 0;
+            if (!cuda_ok(meso_hydro_mask(c->forcing[slot], c->cells, c->solid[slot], s), "mesoscale mask") ||
+                !cuda_ok(meso_hydro_flags(hydro_args(*c, t, slot, slot), c->solid[slot], c->flags[slot], s), "mesoscale flags"))
+                return 0;
             if (!hydro_step(*c, t, c->fslot, slot, s)) return 0;
         }
         c->fslot = slot;
