@@ -300,6 +300,44 @@ def run_batch_leg(aero, lib, torch, stream, ticks: int, warmup: int) -> dict:
             "graph": True, "publish_stride": 4, "launches_in_timed_region": int(launches)}
 
 
+def run_meso_leg(aero, lib, torch, stream, steps: int, warmup: int) -> dict:
+    """C3: D3Q19 mesoscale grid 256 x 64 x 256 (y up): seeded terrain up to 12
+    cells as the bounce-back ground, free-slip lid, periodic sides, body force
+    (1e-6, 0, 0), log-profile initial wind, tau 0.52 + Smagorinsky, the
+    hydrodynamic distribution in one fused launch per step; FP32 and FP16
+    storage, `steps` steps each from the seeded state, and the FP16-vs-FP32
+    wind difference at the end."""
+    cases = load_cases()
+    c = cases.c3_meso_terrain(steps=steps)
+    res, states = {}, {}
+    for name, storage in (("fp32", 0), ("fp16", 1)):
+        ctx = aero.MesoscaleContext(c.dims, dx_m=c.dx_m, dt_s=c.dt_s, options={**c.options, "storage": storage})
+        ctx.step(c.forcing)
+        ctx.advance(warmup)
+        torch.cuda.synchronize()
+        launches0 = lib.aero_lbm_b200_launch_count()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        ctx.advance(steps)
+        end.record(stream)
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(end)
+        info = ctx.info()
+        states[name] = ctx.state()
+        ctx.release()
+        res[name] = {"mlups": c.cells * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps,
+                     "achieved_gbs": info["bytes_per_step"] / (ms / steps * 1e-3) / 1e9,
+                     "bytes_per_cell": info["bytes_per_step"] / c.cells,
+                     "launches": int(lib.aero_lbm_b200_launch_count() - launches0)}
+    a, b = states["fp16"][:, 3:].astype(np.float64), states["fp32"][:, 3:].astype(np.float64)
+    wmax = float(np.max(np.abs(b)))
+    return {"workload": "d3q19 256x64x256 (y up) terrain <= 12 cells, free-slip lid, periodic sides, "
+                        "force (1e-6,0,0), tau 0.52 + SGS C=0.1, hydrodynamic distribution",
+            "steps": steps + warmup + 1, "timed_steps": steps, **{f"{k}_{m}": v[m] for k, v in res.items() for m in v},
+            "fp16_over_fp32": res["fp16"]["mlups"] / res["fp32"]["mlups"],
+            "fp16_vs_fp32_wind_rel": float(np.max(np.abs(a - b))) / wmax if wmax > 0 else None}
+
+
 def run_ours(args) -> dict | None:
     import torch
     import torch.distributed as dist
@@ -414,6 +452,9 @@ def run_ours(args) -> dict | None:
     batch = None
     if args.batch_ticks > 0:
         batch = run_batch_leg(aero, lib, torch, stream, args.batch_ticks, args.warmup)
+    meso = None
+    if args.meso_steps > 0:
+        meso = run_meso_leg(aero, lib, torch, stream, args.meso_steps, args.warmup)
 
     if world > 1:
         dist.barrier()
@@ -424,6 +465,9 @@ def run_ours(args) -> dict | None:
     peak, peak_kind = measured_peaks()
     if batch is not None:
         batch["frac_of_peak"] = batch["achieved_gbs"] / peak
+    if meso is not None:
+        for k in ("fp32", "fp16"):
+            meso[f"{k}_frac_of_peak"] = meso[f"{k}_achieved_gbs"] / peak
     h = results["fp16"]
     achieved = h["achieved_gbs"]
     out = {
@@ -447,7 +491,8 @@ def run_ours(args) -> dict | None:
                    **{f"fp16_over_{v}": h["mlups"] / results[v]["mlups"] for v in results if v != "fp16"},
                    **{f"{v}_frac_of_peak": results[v]["achieved_gbs"] / peak for v in results if v != "fp16"},
                    "accuracy": acc,
-                   "batch": batch},
+                   "batch": batch,
+                   "meso_d3q19": meso},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic_record(f"step_ip_fp16@{n}"), "peak_source": peak_kind,
                      "bytes_per_cell": VARIANTS["fp16"][2], "kernel": "step_ip_kernel<StoreF16Dev, fast>"},
@@ -474,6 +519,7 @@ def main() -> int:
     ap.add_argument("--batch-ticks", type=int, default=500, help="ticks of the 512-brick batch leg (0 skips it)")
     ap.add_argument("--variants", default="fp32_exact,fp32_fast",
                     help="FP32 variants measured beside the FP16 headline (comma list, may be empty)")
+    ap.add_argument("--meso-steps", type=int, default=2000, help="steps of the D3Q19 mesoscale leg (0 skips it)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the FP16-vs-FP32 accuracy leg (0 skips it)")
     args = ap.parse_args()
