@@ -169,6 +169,14 @@ class AeroLbmB200MesoscaleOptions(ctypes.Structure):
     ]
 
 
+class AeroLbmB200AdjointConfig(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("face_kind", ctypes.c_int * 6),
+        ("tau", ctypes.c_float), ("smagorinsky_c", ctypes.c_float), ("buoyancy_beta", ctypes.c_float),
+        ("steps", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("reserved", ctypes.c_int),
+    ]
+
+
 # ---------------------------------------------------------------- loading
 _P = ctypes.c_void_p
 _F32P = ctypes.POINTER(ctypes.c_float)
@@ -244,6 +252,17 @@ SIGNATURES = {
     "aero_lbm_b200_mesoscale_advance": (_I, [_LL, _I]),
     "aero_lbm_b200_mesoscale_read_state": (_I, [_LL, _F32P]),
     "aero_lbm_b200_mesoscale_info": (_I, [_LL, ctypes.POINTER(_LL), ctypes.POINTER(ctypes.c_double)]),
+    # discrete adjoint
+    "aero_lbm_b200_adjoint_default_config": (None, [ctypes.POINTER(AeroLbmB200AdjointConfig)]),
+    "aero_lbm_b200_adjoint_create": (_I, [ctypes.POINTER(AeroLbmB200AdjointConfig), _U8P, _F32P, ctypes.POINTER(_LL)]),
+    "aero_lbm_b200_adjoint_set_probes": (_I, [_LL, _I, _I32P, _F32P]),
+    "aero_lbm_b200_adjoint_forward": (_I, [_LL, _F32P, _F32P, _I, ctypes.POINTER(ctypes.c_double), _F32P]),
+    "aero_lbm_b200_adjoint_gradient": (_I, [_LL, _F32P, _F32P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "aero_lbm_b200_adjoint_timing": (_I, [_LL, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "aero_lbm_b200_adjoint_destroy": (None, [_LL]),
+    "aero_lbm_b200_adjoint_last_error": (ctypes.c_char_p, []),
+    "aero_lbm_b200_adjoint_collide_vjp_host": (_I, [_I, ctypes.POINTER(AeroLbmB200AdjointConfig), ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     # wind-tunnel ABI
     "aero_solver_default_grid": (None, [ctypes.POINTER(AeroGridDesc)]),
     "aero_solver_default_boundary": (None, [ctypes.POINTER(AeroBoundaryDesc)]),
@@ -547,3 +566,80 @@ class MesoscaleContext:
         if self.key:
             self.lib.aero_lbm_mesoscale_release_context(self.key)
             self.key = 0
+
+
+def _dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class AdjointBrick:
+    """Differentiable brick (aero_lbm_b200_adjoint_*): loss = sum over probes of
+    |u - target|^2 after `steps` calls; gradients with respect to the body-force
+    field (3, nx, ny, nz) and the inflow vector."""
+
+    def __init__(self, obstacle: np.ndarray, temperature: np.ndarray | None = None, lib: ctypes.CDLL | None = None,
+                 **config):
+        self.lib = lib or load_library()
+        cfg = AeroLbmB200AdjointConfig()
+        self.lib.aero_lbm_b200_adjoint_default_config(ctypes.byref(cfg))
+        cfg.nx, cfg.ny, cfg.nz = obstacle.shape
+        for k, v in config.items():
+            if k == "face_kind":
+                for i in range(6):
+                    cfg.face_kind[i] = int(v[i])
+            else:
+                setattr(cfg, k, v)
+        self.cfg = cfg
+        self.dims = tuple(obstacle.shape)
+        self.cells = int(np.prod(self.dims))
+        ob = np.ascontiguousarray(obstacle, np.uint8)
+        tp = None if temperature is None else np.ascontiguousarray(temperature, np.float32)
+        h = ctypes.c_longlong(0)
+        if not self.lib.aero_lbm_b200_adjoint_create(ctypes.byref(cfg), u8ptr(ob), fptr(tp) if tp is not None else None,
+                                                     ctypes.byref(h)):
+            raise RuntimeError("adjoint_create failed: " + self.error())
+        self.handle = h.value
+
+    def error(self) -> str:
+        m = self.lib.aero_lbm_b200_adjoint_last_error()
+        return m.decode() if m else ""
+
+    def set_probes(self, cells: np.ndarray, targets: np.ndarray) -> None:
+        c = np.ascontiguousarray(cells, np.int32)
+        t = np.ascontiguousarray(targets, np.float32).reshape(-1)
+        if not self.lib.aero_lbm_b200_adjoint_set_probes(self.handle, c.size, c.ctypes.data_as(_I32P), fptr(t)):
+            raise RuntimeError("adjoint_set_probes failed: " + self.error())
+        self.nprobe = c.size
+
+    def forward(self, force: np.ndarray | None, inflow, precision: int = 0):
+        fo = None if force is None else np.ascontiguousarray(force, np.float32).reshape(-1)
+        ui = np.ascontiguousarray(inflow, np.float32)
+        loss = np.zeros(1, np.float64)
+        u = np.zeros(3 * self.nprobe, np.float32)
+        if not self.lib.aero_lbm_b200_adjoint_forward(self.handle, fptr(fo) if fo is not None else None, fptr(ui),
+                                                      precision, _dptr(loss), fptr(u)):
+            raise RuntimeError("adjoint_forward failed: " + self.error())
+        return float(loss[0]), u.reshape(-1, 3)
+
+    def gradient(self, force: np.ndarray | None, inflow):
+        fo = None if force is None else np.ascontiguousarray(force, np.float32).reshape(-1)
+        ui = np.ascontiguousarray(inflow, np.float32)
+        loss = np.zeros(1, np.float64)
+        gf = np.zeros(3 * self.cells, np.float64)
+        gu = np.zeros(3, np.float64)
+        if not self.lib.aero_lbm_b200_adjoint_gradient(self.handle, fptr(fo) if fo is not None else None, fptr(ui),
+                                                       _dptr(loss), _dptr(gf), _dptr(gu)):
+            raise RuntimeError("adjoint_gradient failed: " + self.error())
+        return float(loss[0]), gf.reshape((3,) + self.dims), gu
+
+    def timing(self) -> dict:
+        v = [ctypes.c_double(0) for _ in range(4)]
+        self.lib.aero_lbm_b200_adjoint_timing(self.handle, *[ctypes.byref(x) for x in v])
+        return {"forward_ms_per_step": v[0].value, "recompute_ms_per_step": v[1].value,
+                "reverse_ms_per_step": v[2].value, "total_ms": v[3].value}
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.aero_lbm_b200_adjoint_destroy(self.handle)
+            self.handle = 0

@@ -173,3 +173,56 @@ def c3_meso_terrain(nx: int = 256, nz: int = 256, ny: int = 64, seed: int = 77, 
     opts = {"periodic_sides": 1, "free_slip_top": 1, "fixed_tau": 1, "tau_hydro": 0.52, "enable_sgs": 1,
             "smagorinsky_c": 0.1, "body_force": (1e-6, 0.0, 0.0), "hydro_only": 1, "disable_edge_blend": 1}
     return MesoCase("c3-meso-terrain", (nx, ny, nz), F.reshape(-1, MESO_CHANNELS), dx_m, dt_s, opts, steps)
+
+
+@dataclass
+class AdjointCase:
+    """Inverse problem on one brick: probes, their targets from a hidden run,
+    and the point (force field, inflow) the gradient is taken at."""
+    name: str
+    dims: tuple
+    obstacle: np.ndarray          # uint8 (nx, ny, nz)
+    temperature: np.ndarray       # float32 (nx, ny, nz)
+    config: dict                  # AeroLbmB200AdjointConfig fields
+    force_true: np.ndarray        # float32 (3, nx, ny, nz), the hidden run's body force
+    inflow_true: tuple
+    probes: np.ndarray            # int32 cell indices
+    force0: np.ndarray            # gradient point
+    inflow0: tuple
+
+
+def smooth_force_field(dims, amplitude: float, sigma: float, seed: int) -> np.ndarray:
+    """3 x dims Gaussian-filtered (periodic) white noise, each component scaled
+    to a maximum magnitude of `amplitude`."""
+    from scipy.ndimage import gaussian_filter
+
+    rng = np.random.default_rng(seed)
+    out = np.zeros((3,) + tuple(dims), np.float32)
+    for a in range(3):
+        g = gaussian_filter(rng.normal(size=dims), sigma, mode="wrap")
+        out[a] = (amplitude * g / np.max(np.abs(g))).astype(np.float32)
+    return out
+
+
+def c5_adjoint(n: int = 64, steps: int = 200, checkpoint_every: int = 20, seed: int = 55, nprobe: int = 64) -> AdjointCase:
+    """n^3 brick with SGS (C = 0.1), Boussinesq (g*beta = 1e-4, temperature
+    -1e-3 z plus a warm bubble), a seeded 5% obstacle mask, inflow faces at x-,
+    x+ and z+ (equilibrium at the inflow vector), periodic y, bounce-back
+    ground; hidden body force: smooth random field (amplitude 1e-5, Gaussian
+    sigma 6 at n = 64) with inflow (0.05, 0.01, 0); 64 interior fluid probes.
+    The gradient is taken at half the hidden force and a perturbed inflow."""
+    rng = np.random.default_rng(seed)
+    obstacle = (rng.random((n, n, n)) < 0.05).astype(np.uint8)
+    s = n / 64.0
+    g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1).astype(np.float64)
+    centre = np.array([n / 2, n / 2, 16.0 * s])
+    temp = (-1e-3 * g[..., 2] + 0.01 * np.exp(-np.sum((g - centre) ** 2, -1) / (2 * (6.0 * s) ** 2))).astype(np.float32)
+    force = smooth_force_field((n, n, n), 1e-5, 6.0 * s, seed + 1)
+    lo, hi = max(2, n // 8), n - max(2, n // 8)
+    cand = [(x, y, z) for x, y, z in rng.integers(lo, hi, (nprobe * 4, 3)) if obstacle[x, y, z] == 0]
+    cells = sorted({(x * n + y) * n + z for x, y, z in cand})
+    probes = np.array(rng.permutation(cells)[:nprobe], np.int32)
+    config = {"face_kind": (4, 4, 1, 1, 2, 4), "tau": 0.55, "smagorinsky_c": 0.1, "buoyancy_beta": 1e-4,
+              "steps": steps, "checkpoint_every": checkpoint_every}
+    return AdjointCase("c5-adjoint", (n, n, n), obstacle, temp, config, force, (0.05, 0.01, 0.0), probes,
+                       (0.5 * force).astype(np.float32), (0.045, 0.012, 0.002))

@@ -356,6 +356,51 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_mesoscale_read_state(long long context_ke
 /* Cells and algorithmic population bytes per step of a context (after its first step). */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_mesoscale_info(long long context_key, long long* out_cells, double* out_bytes_per_step);
 
+/* ---- B200 extension: discrete adjoint of the brick step (no counterpart in
+ *      the reference). A brick with a static mask and temperature field is run
+ *      forward `steps` calls from the equilibrium at the inflow vector; the loss
+ *      is the squared velocity mismatch at probe cells after the last call, and
+ *      its gradient with respect to the per-cell body-force field and the inflow
+ *      vector comes from the reverse sweep, with states checkpointed every
+ *      `checkpoint_every` calls and recomputed per segment. ---- */
+typedef struct AeroLbmB200AdjointConfig {
+    int nx;
+    int ny;
+    int nz;
+    int face_kind[6];      /* x-, x+, y-, y+, z-, z+: 1 periodic, 2 bounce-back, 4 velocity (feq at the inflow) */
+    float tau;             /* shear (and normal) relaxation time */
+    float smagorinsky_c;   /* 0 = no SGS */
+    float buoyancy_beta;   /* g*beta along +z from the temperature field; 0 = off */
+    int steps;             /* forward calls */
+    int checkpoint_every;  /* K (1 = keep every state) */
+    int reserved;
+} AeroLbmB200AdjointConfig;
+
+AERO_LBM_B200_EXPORT void aero_lbm_b200_adjoint_default_config(AeroLbmB200AdjointConfig* out_config);
+/* obstacle: cells bytes (1 = solid); temperature: cells floats or null. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_create(const AeroLbmB200AdjointConfig* config, const uint8_t* obstacle,
+                                                      const float* temperature, long long* out_handle);
+/* Probe cell indices ((x*ny+y)*nz+z, fluid cells) and their target velocities (count x 3, lattice units). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_set_probes(long long handle, int count, const int* cells, const float* targets);
+/* Forward run: loss and probe velocities (count x 3). force_soa: 3 x cells or null; inflow: 3.
+ * precision 0 = the FP32 model the gradient is taken of, 1 = the same model in FP64. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_forward(long long handle, const float* force_soa, const float* inflow,
+                                                       int precision, double* out_loss, float* out_probe_u);
+/* Loss and gradients (FP64): out_grad_force 3 x cells (SoA) or null, out_grad_inflow 3. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_gradient(long long handle, const float* force_soa, const float* inflow,
+                                                        double* out_loss, double* out_grad_force, double* out_grad_inflow);
+/* Device ms per call of the last gradient run: forward, segment recomputation, reverse; and its wall ms. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_timing(long long handle, double* out_forward_ms_per_step,
+                                                      double* out_recompute_ms_per_step, double* out_reverse_ms_per_step,
+                                                      double* out_total_ms);
+AERO_LBM_B200_EXPORT void aero_lbm_b200_adjoint_destroy(long long handle);
+AERO_LBM_B200_EXPORT const char* aero_lbm_b200_adjoint_last_error(void);
+/* One cell's collision and its vector-Jacobian product, on the host CPU (precision 0 float, 1 double). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_collide_vjp_host(int precision, const AeroLbmB200AdjointConfig* config,
+                                                                const double* f_in, double temperature,
+                                                                const double* cell_force, const double* lam_out,
+                                                                double* f_out, double* lam_in, double* lam_force);
+
 /* ---- wind-tunnel ABI (native/include/aero_solver_capi.h:1-115) ---- */
 enum {
     AERO_SOLVER_ABI_VERSION = 1,
