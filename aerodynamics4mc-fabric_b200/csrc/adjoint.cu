@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(128) adj_reverse_kernel(StepArgs<float> A, con
         cell_force(A, i, t, fx, fy, fz);
         float fo[27];
         CollideTape<float> tape;
-        collide_fwd<float>(p, A.cp, t, fx, fy, fz, fo, tape);
+        collide_fwd<float, false>(p, A.cp, t, fx, fy, fz, fo, tape);
         float lo[27], li[27], lf[3];
 #pragma unroll
         for (int q = 0; q < 27; ++q) lo[q] = lam_n[(long long)q * A.G.cells + i];

@@ -127,7 +127,9 @@ __host__ __device__ __forceinline__ bool inside(T v, T lo, T hi) { return v > lo
 
 // Forward collision of one fluid cell. `temp` is the cell's temperature
 // (buoyancy), (cfx, cfy, cfz) its extra force density.
-template <class T>
+// kOutput = false fills the tape only (what the reverse sweep needs) and
+// leaves fo unset.
+template <class T, bool kOutput = true>
 __host__ __device__ void collide_fwd(const T (&f)[27], const CollideParams& P, T temp, T cfx, T cfy, T cfz, T (&fo)[27],
                                      CollideTape<T>& s) {
     T r000 = 0, r100 = 0, r010 = 0, r001 = 0, r200 = 0, r020 = 0, r002 = 0, r110 = 0, r101 = 0, r011 = 0;
@@ -232,6 +234,12 @@ __host__ __device__ void collide_fwd(const T (&f)[27], const CollideParams& P, T
     K[K222] = (K[K200] * K[K020] * K[K002] + T(2) * K[K110] * K[K110] * K[K002] + T(2) * K[K101] * K[K101] * K[K020] +
                T(2) * K[K011] * K[K011] * K[K200] + T(8) * K[K110] * K[K101] * K[K011]) * irs * irs;
 
+    s.forced = (F[0] != T(0)) || (F[1] != T(0)) || (F[2] != T(0));
+    const T omc = clamp_t(s.om_o, T(0), T(1.999));
+    s.pref_free = inside(s.om_o, T(0), T(1.999)) && (T(1) - T(0.5) * omc) > T(0);
+    s.pref = max_t(T(0), T(1) - T(0.5) * omc);
+    if (!kOutput) return;
+
     T g[3][9], h[27];
     back_transform<T>(s.K, s.u, g, h, fo);
 
@@ -245,10 +253,6 @@ __host__ __device__ void collide_fwd(const T (&f)[27], const CollideParams& P, T
     }
     const T drho = s.rs - m0;
     const T djx = T(3) * (s.rs * ux - m1x), djy = T(3) * (s.rs * uy - m1y), djz = T(3) * (s.rs * uz - m1z);
-    s.forced = (F[0] != T(0)) || (F[1] != T(0)) || (F[2] != T(0));
-    const T omc = clamp_t(s.om_o, T(0), T(1.999));
-    s.pref_free = inside(s.om_o, T(0), T(1.999)) && (T(1) - T(0.5) * omc) > T(0);
-    s.pref = max_t(T(0), T(1) - T(0.5) * omc);
     const T uf = ux * F[0] + uy * F[1] + uz * F[2];
 #pragma unroll
     for (int q = 0; q < 27; ++q) {

@@ -338,6 +338,30 @@ def run_meso_leg(aero, lib, torch, stream, steps: int, warmup: int) -> dict:
             "fp16_vs_fp32_wind_rel": float(np.max(np.abs(a - b))) / wmax if wmax > 0 else None}
 
 
+def run_adjoint_leg(aero, lib, torch) -> dict:
+    """C5: 64^3 FP32 brick (SGS, Boussinesq, 5% obstacles), 200 calls with a
+    checkpoint every 20; loss = squared velocity mismatch at 64 probes against
+    a hidden run with a smooth random body-force field; gradient with respect
+    to the force field and the inflow vector. Reports the device time per call
+    of the forward, of the segment recomputation and of the reverse launch."""
+    cases = load_cases()
+    c = cases.c5_adjoint()
+    b = aero.AdjointBrick(c.obstacle, c.temperature, lib=lib, **c.config)
+    b.set_probes(c.probes, np.zeros((len(c.probes), 3), np.float32))
+    _, t = b.forward(c.force_true, c.inflow_true, precision=1)
+    b.set_probes(c.probes, t)
+    b.gradient(c.force0, c.inflow0)  # warm-up
+    loss, gf, gu = b.gradient(c.force0, c.inflow0)
+    tm = b.timing()
+    b.close()
+    fwd = tm["forward_ms_per_step"]
+    per_step = tm["recompute_ms_per_step"] + tm["reverse_ms_per_step"]
+    return {"workload": "d3q27 64^3 fp32, SGS + Boussinesq + 5% obstacles, 200 calls, checkpoint every 20, 64 probes",
+            "loss": loss, "grad_inflow": [float(v) for v in gu], "grad_force_max": float(np.max(np.abs(gf))),
+            **tm, "adjoint_over_forward": per_step / fwd if fwd > 0 else None,
+            "reverse_only_over_forward": tm["reverse_ms_per_step"] / fwd if fwd > 0 else None}
+
+
 def run_ours(args) -> dict | None:
     import torch
     import torch.distributed as dist
@@ -455,6 +479,7 @@ def run_ours(args) -> dict | None:
     meso = None
     if args.meso_steps > 0:
         meso = run_meso_leg(aero, lib, torch, stream, args.meso_steps, args.warmup)
+    adjoint = run_adjoint_leg(aero, lib, torch) if args.adjoint else None
 
     if world > 1:
         dist.barrier()
@@ -492,7 +517,8 @@ def run_ours(args) -> dict | None:
                    **{f"{v}_frac_of_peak": results[v]["achieved_gbs"] / peak for v in results if v != "fp16"},
                    "accuracy": acc,
                    "batch": batch,
-                   "meso_d3q19": meso},
+                   "meso_d3q19": meso,
+                   "adjoint": adjoint},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic_record(f"step_ip_fp16@{n}"), "peak_source": peak_kind,
                      "bytes_per_cell": VARIANTS["fp16"][2], "kernel": "step_ip_kernel<StoreF16Dev, fast>"},
@@ -520,6 +546,7 @@ def main() -> int:
     ap.add_argument("--variants", default="fp32_exact,fp32_fast",
                     help="FP32 variants measured beside the FP16 headline (comma list, may be empty)")
     ap.add_argument("--meso-steps", type=int, default=2000, help="steps of the D3Q19 mesoscale leg (0 skips it)")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false", help="skip the adjoint (gradient) leg")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the FP16-vs-FP32 accuracy leg (0 skips it)")
     args = ap.parse_args()
