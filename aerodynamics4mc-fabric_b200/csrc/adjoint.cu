@@ -71,9 +71,7 @@ __host__ __device__ __forceinline__ int pull_source(const Geo& G, int x, int y, 
 }
 
 __device__ __forceinline__ void cell_xyz(const Geo& G, long long i, int& x, int& y, int& z) {
-    z = (int)(i % G.nz);
-    y = (int)((i / G.nz) % G.ny);
-    x = (int)(i / ((long long)G.ny * G.nz));
+    cell_xyz32(i, G.ny, G.nz, x, y, z);
 }
 
 template <class T>

@@ -95,9 +95,7 @@ __device__ __forceinline__ void ip_push(typename S::T* __restrict__ f, const IpA
 }
 
 __device__ __forceinline__ void cell_coords(const PadGeom& G, long long cell, int& x, int& y, int& z) {
-    z = (int)(cell % G.nz);
-    y = (int)((cell / G.nz) % G.ny);
-    x = (int)(cell / ((long long)G.ny * G.nz));
+    cell_xyz32(cell, G.ny, G.nz, x, y, z);
 }
 
 // Reseed a cell into the in-place state (out of line: rare path; scalar
@@ -132,16 +130,33 @@ __device__ __forceinline__ void reseed_push(typename S::T* f, const IpArgs& a, l
 // Fused pull-stream + collide + push of one step. Sources outside
 // equilibrium faces were pre-filled into their slots by face_fill_ip_kernel,
 // so every incoming population is a plain (or bounce-back) slot read.
+// Launch geometry of the step: one block row per (x, y) line, z along the
+// block (grid = (ceil(nz / block), ny, nx)), so the cell coordinates need no
+// division.
+__device__ __forceinline__ bool line_cell(const PadGeom& G, int& x, int& y, int& z, long long& cell) {
+    z = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y;
+    x = blockIdx.z;
+    cell = ((long long)x * G.ny + y) * G.nz + z;
+    return z < G.nz;
+}
+
+inline dim3 line_grid(const PadGeom& g, int block, int cells_per_thread = 1) {
+    const int n = (g.nz + cells_per_thread - 1) / cells_per_thread;
+    return dim3((unsigned)((n + block - 1) / block), (unsigned)g.ny, (unsigned)g.nx);
+}
+
+// Threads per block of the line launch: a multiple of 32 covering n, at most 128.
+inline int line_block(int n) { return n >= 128 ? 128 : ((n + 31) / 32) * 32; }
+
 template <class S, bool kExact, int kParity>
 __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom G = a.g;
-    const long long cells = (long long)G.nx * G.ny * G.nz;
-    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= cells) return;
+    int x, y, z;
+    long long cell;
+    if (!line_cell(G, x, y, z, cell)) return;
     const uint32_t w = a.flags_prev[cell];
     if (w & kFlagSelfSolid) return;  // memory of a solid cell is link storage; transitions run separately
-    int x, y, z;
-    cell_coords(G, cell, x, y, z);
     const int own = pad_index(G, x, y, z);
     const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
     float fl[27];
@@ -312,8 +327,9 @@ struct IpLaunch {
             cudaError_t e = face_fill(f, a, s);
             if (e != cudaSuccess) return e;
         }
-        if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
-        else step_ip_kernel<S, kExact, 1><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
+        const int lb = line_block(a.g.nz);
+        if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
+        else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
         count_launch();
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess || !transitions) return e;

@@ -210,9 +210,8 @@ __global__ void __launch_bounds__(128) step_ab_kernel(int nx, int ny, int nz, co
     const long long cells = (long long)nx * ny * nz;
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= cells) return;
-    const int z = (int)(cell % nz);
-    const int y = (int)((cell / nz) % ny);
-    const int x = (int)(cell / ((long long)ny * nz));
+    int x, y, z;
+    cell_xyz32(cell, ny, nz, x, y, z);
     float f[27];
     const PullView v{g_in, obstacle_prev, ref_p_prev, F, cells, nx, ny, nz};
     pull27(v, flags_prev[cell], cell, x, y, z, f);

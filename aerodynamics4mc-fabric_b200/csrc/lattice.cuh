@@ -54,4 +54,16 @@ constexpr uint32_t kFlagSelfSolid = 1u << 27;
 constexpr uint32_t kFlagFaceSpecial = 1u << 28;
 constexpr uint32_t kFlagBounceMask = (1u << 27) - 1u;
 
+// Coordinates of cell (x*ny + y)*nz + z. Grids hold fewer than 2^31 cells, so
+// 32-bit unsigned division suffices (a 64-bit division costs several times the
+// instructions).
+__host__ __device__ __forceinline__ void cell_xyz32(long long cell, int ny, int nz, int& x, int& y, int& z) {
+    const unsigned c = (unsigned)cell, unz = (unsigned)nz, uny = (unsigned)ny;
+    const unsigned line = c / unz;
+    z = (int)(c - line * unz);
+    const unsigned xx = line / uny;
+    y = (int)(line - xx * uny);
+    x = (int)xx;
+}
+
 }  // namespace aero

@@ -23,6 +23,7 @@
 #include <cuda_fp16.h>
 
 #include "d3q27_kernels.cuh"
+#include "lattice.cuh"
 #include "meso.cuh"
 
 namespace aero {
@@ -233,7 +234,8 @@ __global__ void __launch_bounds__(128) meso_collide_kernel(MesoArgs A) {
     const long long cells = (long long)A.nx * A.ny * A.nz;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cells) return;
-    const int z = (int)(i % A.nz), y = (int)((i / A.nz) % A.ny), x = (int)(i / ((long long)A.ny * A.nz));
+    int x, y, z;
+    cell_xyz32(i, A.ny, A.nz, x, y, z);
     float f[19], g[19];
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
@@ -273,7 +275,8 @@ __global__ void __launch_bounds__(128) meso_stream_kernel(MesoArgs A) {
     const long long cells = (long long)nx * ny * nz;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cells) return;
-    const int z = (int)(i % nz), y = (int)((i / nz) % ny), x = (int)(i / ((long long)ny * nz));
+    int x, y, z;
+    cell_xyz32(i, ny, nz, x, y, z);
     const float* F = A.forcing;
     float* out = A.out_state ? A.out_state + i * kMesoStateChannels : nullptr;
     if (solid_at(F, i)) {
@@ -444,7 +447,8 @@ __global__ void __launch_bounds__(256) meso_hydro_kernel(HydroArgs A) {
     const long long cells = (long long)nx * ny * nz;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= cells) return;
-    const int z = (int)(i % nz), y = (int)((i / nz) % ny), x = (int)(i / ((long long)ny * nz));
+    int x, y, z;
+    cell_xyz32(i, ny, nz, x, y, z);
     const T* __restrict__ src = static_cast<const T*>(A.src);
     float f[19];
     if (kMode == kHydroInit) {
@@ -609,7 +613,8 @@ __global__ void meso_hydro_flags_kernel(HydroArgs A, const uint8_t* __restrict__
         flags[i] = kHydroSelfSolid;
         return;
     }
-    const int z = (int)(i % nz), y = (int)((i / nz) % ny), x = (int)(i / ((long long)ny * nz));
+    int x, y, z;
+    cell_xyz32(i, ny, nz, x, y, z);
     int edge = min(min(x, z), min(nx - 1 - x, nz - 1 - z));
     int top = ny - 1 - y;
     if (A.periodic_sides) edge = 1 << 20;
