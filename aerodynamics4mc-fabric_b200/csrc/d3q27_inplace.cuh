@@ -10,6 +10,7 @@
 #pragma once
 
 #include "d3q27_step.cuh"
+#include "collide27_x2.cuh"
 #include "inplace27.cuh"
 
 namespace aero {
@@ -25,6 +26,7 @@ struct IpArgs {
     ForceField force;
     CollideParams cp;
     Fp16Scale sc;
+    int cells_per_thread;            // factorised step: 1 scalar kernel, 2 packed pair kernel
 };
 
 // Equilibrium value of a face (velocity / pressure / moving wall), the only
@@ -178,6 +180,129 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
     }
 }
 
+// Loads and stores of two cells' populations of one direction.
+template <class S>
+struct PairIO;
+template <>
+struct PairIO<StoreF32> {
+    __device__ __forceinline__ static F2 load(const float* p0, const float* p1, int, const Fp16Scale&) {
+        return f2(__ldg(p0), __ldg(p1));
+    }
+    __device__ __forceinline__ static void store(float* p0, float* p1, bool s0, bool s1, int, F2 v, const Fp16Scale&) {
+        if (s0) *p0 = v.v.x;
+        if (s1) *p1 = v.v.y;
+    }
+};
+template <>
+struct PairIO<StoreF16Dev> {
+    __device__ __forceinline__ static F2 load(const __half* p0, const __half* p1, int q, const Fp16Scale& s) {
+        const float2 h = make_float2(__half2float(__ldg(p0)), __half2float(__ldg(p1)));
+        const float w = q_w(q), k = w * s.inv_scale;
+        return F2{__ffma2_rn(h, make_float2(k, k), make_float2(w, w))};
+    }
+    __device__ __forceinline__ static void store(__half* p0, __half* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
+        const float k = s.scale * (1.0f / q_w(q));
+        const float2 h = __ffma2_rn(v.v, make_float2(k, k), make_float2(-s.scale, -s.scale));
+        if (s0) *p0 = __float2half_rn(h.x);
+        if (s1) *p1 = __float2half_rn(h.y);
+    }
+};
+
+// Factorised-collision step with two z-adjacent cells per thread and the
+// collision in packed FP32 (collide27_x2.cuh); line grid over cell pairs.
+// Pairs without periodic wraps address every slot at a launch-uniform offset
+// (one of two per direction, by the bounce-back bit; the second cell's slots
+// one element after the first's).
+// A cell that is fluid at the streaming call and solid now is not collided:
+// its streamed populations pass through (reloaded from its incoming slots,
+// which only this cell writes, before any store). A lane whose input is not
+// finite is reseeded.
+#ifndef AERO_IP2_MIN_BLOCKS
+#define AERO_IP2_MIN_BLOCKS 5
+#endif
+template <class S, int kParity>
+__global__ void __launch_bounds__(128, AERO_IP2_MIN_BLOCKS) step_ip2_kernel(typename S::T* __restrict__ f, IpArgs a) {
+    const PadGeom& G = a.g;
+    const int z0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (z0 >= G.nz) return;
+    const int y = blockIdx.y, x = blockIdx.z;
+    const long long cell0 = ((long long)x * G.ny + y) * G.nz + z0;
+    const bool has1 = z0 + 1 < G.nz;
+    const uint32_t w0 = a.flags_prev[cell0];
+    const uint32_t w1 = has1 ? a.flags_prev[cell0 + 1] : kFlagSelfSolid;
+    const bool live0 = !(w0 & kFlagSelfSolid), live1 = !(w1 & kFlagSelfSolid);
+    if (!live0 && !live1) return;
+    const bool pass0 = live0 && a.obstacle_cur[cell0] != 0;
+    const bool pass1 = live1 && a.obstacle_cur[cell0 + 1] != 0;
+    const int own0 = pad_index(G, x, y, z0);
+    const int own1 = own0 + 1;  // z0 + 1 (the ghost cell when z0 + 1 == nz: inside the padded array)
+    const bool flat = no_wrap(G, x, y, z0) && (!has1 || no_wrap(G, x, y, z0 + 1));
+    typename S::T* __restrict__ base0 = f + own0;
+    F2 fl[27];
+    if (flat) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q)
+            fl[q] = PairIO<S>::load(base0 + in_offset(G, q, kParity, (w0 >> q) & 1u),
+                                    base0 + 1 + in_offset(G, q, kParity, (w1 >> q) & 1u), q, a.sc);
+    } else {
+        const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
+        const NeighbourOffsets o1 = neighbour_offsets(G, x, y, has1 ? z0 + 1 : z0);
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            int c0, d0, c1, d1;
+            incoming_slot(o0, own0, q, kParity, (w0 >> q) & 1u, c0, d0);
+            incoming_slot(o1, own1, q, kParity, (w1 >> q) & 1u, c1, d1);
+            fl[q] = PairIO<S>::load(f + (d0 * G.pcells + c0), f + (d1 * G.pcells + c1), q, a.sc);
+        }
+    }
+    const float* temp = a.cur.temperature;
+    const F2 t = a.cp.enable_buoyancy ? f2(temp[cell0], has1 ? temp[cell0 + 1] : 0.0f) : f2(0.0f);
+    F2 cfx = f2(0.0f), cfy = f2(0.0f), cfz = f2(0.0f);
+    if (a.force.fx) {
+        cfx = f2(a.force.fx[cell0], has1 ? a.force.fx[cell0 + 1] : 0.0f);
+        cfy = f2(a.force.fy[cell0], has1 ? a.force.fy[cell0 + 1] : 0.0f);
+        cfz = f2(a.force.fz[cell0], has1 ? a.force.fz[cell0 + 1] : 0.0f);
+    }
+    bool ok[2];
+    collide27_x2(fl, a.cp, t, cfx, cfy, cfz, ok);
+    if (pass0 || pass1) {
+        const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
+        const NeighbourOffsets o1 = neighbour_offsets(G, x, y, has1 ? z0 + 1 : z0);
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            int c, d;
+            if (pass0) {
+                incoming_slot(o0, own0, q, kParity, (w0 >> q) & 1u, c, d);
+                fl[q].v.x = S::load(f + (d * G.pcells + c), q, a.sc);
+            }
+            if (pass1) {
+                incoming_slot(o1, own1, q, kParity, (w1 >> q) & 1u, c, d);
+                fl[q].v.y = S::load(f + (d * G.pcells + c), q, a.sc);
+            }
+        }
+    }
+    const bool st0 = live0 && (ok[0] || pass0), st1 = live1 && (ok[1] || pass1);
+    if (live0 && !ok[0] && !pass0) reseed_push<S>(f, a, cell0, x, y, z0, kParity);
+    if (live1 && !ok[1] && !pass1) reseed_push<S>(f, a, cell0 + 1, x, y, z0 + 1, kParity);
+    if (flat) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            const int off = out_offset(G, q, kParity);
+            PairIO<S>::store(base0 + off, base0 + off + 1, st0, st1, q, fl[q], a.sc);
+        }
+        return;
+    }
+    const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
+    const NeighbourOffsets o1 = neighbour_offsets(G, x, y, has1 ? z0 + 1 : z0);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        int c0, d0, c1, d1;
+        outgoing_slot(o0, own0, q, kParity, c0, d0);
+        outgoing_slot(o1, own1, q, kParity, c1, d1);
+        PairIO<S>::store(f + (d0 * G.pcells + c0), f + (d1 * G.pcells + c1), st0, st1, q, fl[q], a.sc);
+    }
+}
+
 // Before a step of parity p: write the equilibrium value of every incoming
 // population whose source lies outside an equilibrium face into the slot the
 // pulling cell reads at parity p (a ghost-cell slot, or for positive
@@ -327,9 +452,15 @@ struct IpLaunch {
             cudaError_t e = face_fill(f, a, s);
             if (e != cudaSuccess) return e;
         }
-        const int lb = line_block(a.g.nz);
-        if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
-        else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
+        if (!kExact && a.cells_per_thread == 2) {
+            const int lb = line_block((a.g.nz + 1) / 2);
+            if (a.parity == 0) step_ip2_kernel<S, 0><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
+            else step_ip2_kernel<S, 1><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
+        } else {
+            const int lb = line_block(a.g.nz);
+            if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
+            else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
+        }
         count_launch();
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess || !transitions) return e;

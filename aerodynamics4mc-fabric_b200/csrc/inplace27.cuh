@@ -129,6 +129,28 @@ __device__ __forceinline__ void incoming_slot(const NeighbourOffsets& o, int own
     cell = (q == kRest27 || q_positive(q)) ? own : link_cell(o, q, -1);
 }
 
+// Slot offsets relative to a cell's own padded index, for a cell none of
+// whose neighbours wraps around a periodic axis (the neighbour along c is
+// then own + link_offset(c)); launch-uniform apart from the bounce choice.
+__device__ __forceinline__ int link_offset(const PadGeom& g, int q) { return (q_cx(q) * g.py + q_cy(q)) * g.pz + q_cz(q); }
+// bounce: the parity-flipped slot of the same memory cell
+__device__ __forceinline__ int in_offset(const PadGeom& g, int q, int p, bool bounce = false) {
+    const bool even = (p == 0) != bounce;
+    const int dir = q == kRest27 ? kRest27 : (even ? q_opp(q) : q);
+    const int cell = (q == kRest27 || q_positive(q)) ? 0 : -link_offset(g, q);
+    return dir * g.pcells + cell;
+}
+__device__ __forceinline__ int out_offset(const PadGeom& g, int q, int p) {
+    const int dir = q == kRest27 ? kRest27 : (p == 0 ? q : q_opp(q));
+    const int cell = (q == kRest27 || !q_positive(q)) ? 0 : link_offset(g, q);
+    return dir * g.pcells + cell;
+}
+// True when no neighbour of (x, y, z) wraps around a periodic axis.
+__device__ __forceinline__ bool no_wrap(const PadGeom& g, int x, int y, int z) {
+    return !((g.wrap[0] && (x == 0 || x == g.nx - 1)) || (g.wrap[1] && (y == 0 || y == g.ny - 1)) ||
+             (g.wrap[2] && (z == 0 || z == g.nz - 1)));
+}
+
 // Memory cell and slot direction of outgoing population q at parity p.
 __device__ __forceinline__ void outgoing_slot(const NeighbourOffsets& o, int own, int q, int p, int& cell, int& dir) {
     dir = q == kRest27 ? kRest27 : (p == 0 ? q : q_opp(q));

@@ -44,6 +44,7 @@ struct TimingStats {
 
 RuntimeConfig g_cfg;
 std::recursive_mutex g_mutex;  // guards every entry point (the caller is one worker thread)
+int g_cells_per_thread = 2;    // in-place factorised step: 1 scalar kernel, 2 packed pair kernel
 std::unordered_map<long long, std::unique_ptr<Context>> g_contexts;
 std::string g_last_error;
 std::string g_timing_text;
@@ -494,6 +495,7 @@ static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const Collide
     a.force = ctx.force_field();
     a.cp = cp;
     a.sc = Fp16Scale{ctx.fp16_scale, ctx.fp16_scale > 0.0f ? 1.0f / ctx.fp16_scale : 0.0f};
+    a.cells_per_thread = g_cells_per_thread;
     return a;
 }
 
@@ -1071,6 +1073,16 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_collision_mode(int mode) {
     std::lock_guard<std::recursive_mutex> lk(g_mutex);
     if (mode < 0 || mode > 1) return 0;
     g_collision_mode = mode;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_cells_per_thread(int n) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (n != 1 && n != 2) {
+        set_error("set_cells_per_thread: 1 or 2");
+        return 0;
+    }
+    g_cells_per_thread = n;
     return 1;
 }
 

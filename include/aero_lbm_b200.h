@@ -232,6 +232,11 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums_noalloc(long long conte
  * 1 = factorised moment transforms with contraction (same scheme, fewer flops,
  * agrees to FP32 rounding per step). */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_collision_mode(int mode);
+/* Launch shape of the in-place step with the factorised collision (FP16
+ * storage, FP32 collision mode 1): 2 = two z-adjacent cells per thread with the
+ * collision in sm_100 packed FP32 (default), 1 = one cell per thread. Same
+ * scheme; results agree to FP32 rounding. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_cells_per_thread(int cells_per_thread);
 /* Per-cell force density field for a context (3 x cells floats, SoA order
  * fx[cells], fy[cells], fz[cells]; host pointer; null clears). */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_force_field(long long context_key, const float* force_soa, int value_count);

@@ -141,3 +141,64 @@ def test_fp16_storage_bytes_and_scale(gpu):
         gpu.aero_lbm_set_realtime_solver_mode(0)
     assert np.max(np.abs(out[:, :3])) < 1e-6
     assert np.max(np.abs(out[:, 3])) < 1e-6
+
+
+def _porous_case(dims, seed):
+    rng = np.random.default_rng(seed)
+    obst = (rng.random(dims) < 0.06).astype(np.uint8)
+    obst[:, :, 0] = 1
+    u = [np.float32(0.05) + rng.uniform(-0.005, 0.005, dims).astype(np.float32),
+         rng.uniform(-0.005, 0.005, dims).astype(np.float32), rng.uniform(-0.005, 0.005, dims).astype(np.float32)]
+    return obst, u
+
+
+@pytest.mark.parametrize("cells_per_thread", [1, 2])
+@pytest.mark.parametrize("dims", [(20, 18, 24), (10, 9, 13)])
+def test_fast_collision_launch_shapes(gpu, dims, cells_per_thread):
+    """The factorised FP32 in-place step, one cell per thread or two z-adjacent
+    cells per thread with the packed FP32 collision (odd nz leaves a lone last
+    cell), against the oracle's FP64 run: velocity within 1e-4 of the max
+    speed, density within 1e-5 after 60 steps."""
+    obst, u = _porous_case(dims, seed=sum(dims))
+    cfg = O.c1_config()
+    assert gpu.aero_lbm_b200_set_cells_per_thread(cells_per_thread) == 1
+    try:
+        out, _ = lbm_cases.run_product(gpu, dims, cfg, O.packet_from(obst, *u), 60, key=51, streaming_mode=2,
+                                       collision_mode=1)
+    finally:
+        gpu.aero_lbm_b200_set_collision_mode(0)
+        gpu.aero_lbm_b200_set_cells_per_thread(2)
+    o = O.Oracle(dims, O.derive_params(cfg), "f64")
+    o.set_fields(obst, *u)
+    o.step(60)
+    e = O.flow_errors(out, o.output())
+    assert e["u"] <= 1e-4 and e["rho"] <= 1e-5, e
+
+
+def test_fast_collision_mask_change(gpu):
+    """Mask changes between calls with the two-cell kernel: cells turning
+    solid pass their streamed populations through, cells opening up go
+    through the transition kernel."""
+    n = 12
+    obst, u, p, cfg = local_faces_case(n, seed=6)
+    obst2 = obst.copy()
+    rng = np.random.default_rng(98)
+    obst2[(rng.random(obst.shape) < 0.04) & (obst == 0)] = 1
+    obst2[(rng.random(obst.shape) < 0.5) & (obst == 1)] = 0
+    pk1, pk2 = O.packet_from(obst, *u, pressure=p), O.packet_from(obst2, *u, pressure=p)
+    gpu.aero_lbm_b200_set_streaming_mode(2)
+    gpu.aero_lbm_b200_set_collision_mode(1)
+    try:
+        ctx = aero_b200.LbmContext((n, n, n), key=53, lib=gpu)
+        ctx.configure(lbm_cases.product_config(gpu, cfg))
+        o = O.Oracle((n, n, n), O.derive_params(cfg), "f64")
+        out = None
+        for s in range(24):
+            pk, ob = (pk1, obst) if s < 10 else (pk2, obst2)
+            out = ctx.step(pk, output=(s + 1 == 24))
+            o.set_fields(ob, *u, pressure=p)
+            o.step(1)
+    finally:
+        gpu.aero_lbm_b200_set_collision_mode(0)
+    e = O.flow_errors(out, o.output())
+    assert e["u"] <= 1e-4 and e["rho"] <= 1e-5, e
