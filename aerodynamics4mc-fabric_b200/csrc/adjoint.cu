@@ -455,12 +455,6 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_create(const AeroLbmB200AdjointCo
         ok = adj_ok(cudaMalloc(&b->temperature, n * sizeof(float)), "adjoint alloc") &&
              adj_ok(cudaMemcpy(b->temperature, temperature, n * sizeof(float), cudaMemcpyHostToDevice), "temperature upload");
     if (ok) ok = adj_ok(cudaMemcpy(b->solid, obstacle, n, cudaMemcpyHostToDevice), "mask upload");
-    const int K = cfg->checkpoint_every;
-    const int segments = (cfg->steps + K - 1) / K;
-    b->ckpt.assign(segments, nullptr);
-    for (int j = 1; ok && j < segments; ++j) ok = adj_ok(cudaMalloc(&b->ckpt[j], b->state_elems * sizeof(float)), "checkpoint alloc");
-    b->seg.assign(std::max(0, K - 1), nullptr);
-    for (int j = 0; ok && j < K - 1; ++j) ok = adj_ok(cudaMalloc(&b->seg[j], b->state_elems * sizeof(float)), "segment alloc");
     if (!ok) {
         delete b;
         return 0;
@@ -582,6 +576,25 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_gradient(long long handle, const 
     const int N = b->cfg.steps, K = b->cfg.checkpoint_every;
     const Geo G = b->geo;
     const size_t bytes = b->state_elems * sizeof(float);
+    // checkpoint and segment states, allocated at the first gradient call
+    // (forward-only use needs neither)
+    if (b->ckpt.empty()) {
+        const int segments = (N + K - 1) / K;
+        b->ckpt.assign(segments, nullptr);
+        b->seg.assign(std::max(0, K - 1), nullptr);
+        bool got = true;
+        for (int j = 1; got && j < segments; ++j) got = adj_ok(cudaMalloc(&b->ckpt[j], bytes), "checkpoint alloc");
+        for (int j = 0; got && j < K - 1; ++j) got = adj_ok(cudaMalloc(&b->seg[j], bytes), "segment alloc");
+        if (!got) {
+            for (float* p : b->ckpt)
+                if (p) cudaFree(p);
+            for (float* p : b->seg)
+                if (p) cudaFree(p);
+            b->ckpt.clear();
+            b->seg.clear();
+            return 0;
+        }
+    }
     cudaEvent_t ev[6];
     for (auto& e : ev) cudaEventCreate(&e);
     const size_t du_bytes = 3 * ((size_t)b->rev_blocks + 1) * sizeof(double);

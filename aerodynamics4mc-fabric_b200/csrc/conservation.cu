@@ -131,6 +131,8 @@ cudaError_t launch_conservation_ip(int variant, const void* f, const IpArgs& a, 
     const int blocks = conservation_blocks((long long)a.g.nx * a.g.ny * a.g.nz);
     if (variant == kIpF16Fast) {
         conservation_ip_kernel<StoreF16Dev><<<blocks, kConservationThreads, 0, s>>>(static_cast<const __half*>(f), a, partials);
+    } else if (variant == kIpI16Fast) {
+        conservation_ip_kernel<StoreI16Dev><<<blocks, kConservationThreads, 0, s>>>(static_cast<const short*>(f), a, partials);
     } else {
         conservation_ip_kernel<StoreF32><<<blocks, kConservationThreads, 0, s>>>(static_cast<const float*>(f), a, partials);
     }

@@ -209,6 +209,8 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums_noalloc(long long conte
         a.sc = Fp16Scale{c->fp16_scale, c->fp16_scale > 0.0f ? 1.0f / c->fp16_scale : 0.0f};
         if (c->ip_variant == kIpF16Fast)
             static_sums_ip_kernel<StoreF16Dev><<<blocks, kStaticThreads, 0, s>>>(static_cast<const __half*>(c->ip), a, scratch);
+        else if (c->ip_variant == kIpI16Fast)
+            static_sums_ip_kernel<StoreI16Dev><<<blocks, kStaticThreads, 0, s>>>(static_cast<const short*>(c->ip), a, scratch);
         else
             static_sums_ip_kernel<StoreF32><<<blocks, kStaticThreads, 0, s>>>(static_cast<const float*>(c->ip), a, scratch);
     }

@@ -40,4 +40,12 @@ cudaError_t ip_output_f16_fast(const __half* f, const IpArgs& a, int stride, int
     return IpLaunch<StoreF16Dev, false>::output(f, a, stride, out_ch, scale, out, s);
 }
 
+cudaError_t ip_init_i16_fast(short* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreI16Dev, false>::init(f, a, s); }
+cudaError_t ip_step_i16_fast(short* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
+    return IpLaunch<StoreI16Dev, false>::step(f, a, transitions, fill, s);
+}
+cudaError_t ip_output_i16_fast(const short* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
+    return IpLaunch<StoreI16Dev, false>::output(f, a, stride, out_ch, scale, out, s);
+}
+
 }  // namespace aero

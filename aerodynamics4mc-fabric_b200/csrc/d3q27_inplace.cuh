@@ -208,6 +208,21 @@ struct PairIO<StoreF16Dev> {
     }
 };
 
+template <>
+struct PairIO<StoreI16Dev> {
+    __device__ __forceinline__ static F2 load(const short* p0, const short* p1, int q, const Fp16Scale& s) {
+        const float2 h = make_float2((float)__ldg(p0), (float)__ldg(p1));
+        const float w = q_w(q), k = w * s.inv_scale;
+        return F2{__ffma2_rn(h, make_float2(k, k), make_float2(w, w))};
+    }
+    __device__ __forceinline__ static void store(short* p0, short* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
+        const float k = s.scale * (1.0f / q_w(q));
+        const float2 h = __ffma2_rn(v.v, make_float2(k, k), make_float2(-s.scale, -s.scale));
+        if (s0) *p0 = sat_round_s16(h.x);
+        if (s1) *p1 = sat_round_s16(h.y);
+    }
+};
+
 // Factorised-collision step with two z-adjacent cells per thread and the
 // collision in packed FP32 (collide27_x2.cuh); line grid over cell pairs.
 // Pairs without periodic wraps address every slot at a launch-uniform offset

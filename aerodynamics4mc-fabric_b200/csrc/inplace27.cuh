@@ -66,6 +66,28 @@ struct StoreF16Dev {
     }
 };
 
+// 16-bit fixed-point deviation storage: h = round((f - w_q) * S / w_q),
+// saturated to [-32767, 32767], f = w_q + h * w_q / S, with a per-brick
+// scale S = 32767 / d_max (d_max bounds |f - w_q| / w_q for the brick's
+// speeds). Same bytes as IEEE half, but a uniform resolution d_max / 32767
+// over the whole range instead of 11 significant bits: the deviations that
+// carry the flow (|f - w| / w ~ 0.1-1) are stored 5-10x more precisely. A
+// non-finite value stores 0 (the rest weight).
+__device__ __forceinline__ short sat_round_s16(float x) {
+    short r;
+    asm("cvt.rni.sat.s16.f32 %0, %1;" : "=h"(r) : "f"(x));
+    return r < -32767 ? (short)-32767 : r;
+}
+struct StoreI16Dev {
+    using T = short;
+    __device__ __forceinline__ static float load(const short* __restrict__ a, int q, const Fp16Scale& s) {
+        return fmaf((float)__ldg(a), q_w(q) * s.inv_scale, q_w(q));
+    }
+    __device__ __forceinline__ static void store(short* __restrict__ a, int q, float v, const Fp16Scale& s) {
+        *a = sat_round_s16(fmaf(v, s.scale * (1.0f / q_w(q)), -s.scale));
+    }
+};
+
 // Geometry of one padded brick and the per-axis wrap rule.
 struct PadGeom {
     int nx, ny, nz;

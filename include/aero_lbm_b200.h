@@ -237,6 +237,12 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_collision_mode(int mode);
  * collision in sm_100 packed FP32 (default), 1 = one cell per thread. Same
  * scheme; results agree to FP32 rounding. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_cells_per_thread(int cells_per_thread);
+/* Format of the 16-bit deviation storage chosen by
+ * aero_lbm_set_realtime_solver_mode(3), for contexts created afterwards:
+ * 0 = IEEE half of (f - w) * S / w with a power-of-two per-brick S (default),
+ * 1 = 16-bit fixed point of the same deviation with S = 32767 / d_max (uniform
+ * resolution; several times more precise for flowing states). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_fp16_format(int format);
 /* Per-cell force density field for a context (3 x cells floats, SoA order
  * fx[cells], fy[cells], fz[cells]; host pointer; null clears). */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_force_field(long long context_key, const float* force_soa, int value_count);

@@ -46,11 +46,12 @@ def test_sums_match_oracle(gpu, streaming):
     assert np.max(np.abs(sums[1:] - ref[1:])) / ref[0] < 1e-9
 
 
-@pytest.mark.parametrize("solver_mode,tol", [(0, 2e-6), (3, 5e-5)])
-def test_periodic_brick_conserves_mass(gpu, solver_mode, tol):
+@pytest.mark.parametrize("solver_mode,fmt,tol", [(0, 0, 2e-6), (3, 0, 5e-5), (3, 1, 5e-5)])
+def test_periodic_brick_conserves_mass(gpu, solver_mode, fmt, tol):
     obst, u, p, cfg = periodic_case(n=24, seed=8)
     n = obst.shape[0]
     gpu.aero_lbm_set_realtime_solver_mode(solver_mode)
+    gpu.aero_lbm_b200_set_fp16_format(fmt)
     try:
         out, ctx = lbm_cases.run_product(gpu, (n, n, n), cfg, O.packet_from(obst, *u, pressure=p), 1, key=61)
         m0 = ctx.conservation_sums()[0]
@@ -58,4 +59,5 @@ def test_periodic_brick_conserves_mass(gpu, solver_mode, tol):
         m1 = ctx.conservation_sums()[0]
     finally:
         gpu.aero_lbm_set_realtime_solver_mode(0)
+        gpu.aero_lbm_b200_set_fp16_format(0)
     assert abs(m1 - m0) / m0 < tol, (m0, m1)

@@ -202,3 +202,19 @@ def test_fast_collision_mask_change(gpu):
         gpu.aero_lbm_b200_set_collision_mode(0)
     e = O.flow_errors(out, o.output())
     assert e["u"] <= 1e-4 and e["rho"] <= 1e-5, e
+
+
+@pytest.mark.parametrize("fmt", [0, 1])
+def test_sixteen_bit_formats_against_fp64(gpu, fmt):
+    """16-bit deviation storage, IEEE half (0) and fixed point (1), on the
+    32^3 terrain brick against the oracle's FP64 run after 200 steps: velocity
+    within 1e-3 of the max speed (fixed point: within 3e-4), density 1e-4."""
+    cases = load_cases()
+    case = cases.c2_terrain_boussinesq(n=32, seed=7)
+    assert gpu.aero_lbm_b200_set_fp16_format(fmt) == 1
+    try:
+        out16, _ = _fp16_run(gpu, case, 200, key=45 + fmt)
+    finally:
+        gpu.aero_lbm_b200_set_fp16_format(0)
+    e = O.flow_errors(out16, _oracle_run(case, 200, "f64"))
+    assert e["u"] <= (3e-4 if fmt else 1e-3) and e["rho"] <= 1e-4, e
