@@ -43,7 +43,7 @@ struct BrickDesc {
     int precision;            // 0 fp32, 1 fp16
     int unit_begin;           // first work unit of this brick
     int atlas_offset;         // first atlas record (4 x int16) of this brick
-    int pad;
+    int pairs;                // 1: two z-adjacent cells per thread (nz even), packed FP32 collision
 };
 
 namespace {
@@ -83,6 +83,77 @@ __device__ __forceinline__ void batch_cell(const BrickDesc& b, int cell) {
     }
 }
 
+// Two z-adjacent cells (cell0 even, nz even) with the collision in packed FP32
+// (collide27_x2.cuh): the batch form of step_ip2_kernel. Cells without
+// periodic wraps address their slots at offsets uniform over the brick.
+template <class S, int kParity>
+__device__ __forceinline__ void batch_pair(const BrickDesc& b, int cell0) {
+    const PadGeom& G = b.g;
+    typename S::T* f = static_cast<typename S::T*>(b.f);
+    const uint32_t w0 = b.flags[cell0], w1 = b.flags[cell0 + 1];
+    const bool live0 = !(w0 & kFlagSelfSolid), live1 = !(w1 & kFlagSelfSolid);
+    if (!live0 && !live1) return;
+    if ((live0 && b.obstacle[cell0]) || (live1 && b.obstacle[cell0 + 1])) {
+        // fluid at streaming, solid now: the one-cell path passes it through
+        batch_cell<S, kParity>(b, cell0);
+        batch_cell<S, kParity>(b, cell0 + 1);
+        return;
+    }
+    int x, y, z0;
+    cell_coords(G, cell0, x, y, z0);
+    const int own0 = pad_index(G, x, y, z0);
+    const bool flat = no_wrap(G, x, y, z0) && no_wrap(G, x, y, z0 + 1);
+    typename S::T* __restrict__ base0 = f + own0;
+    F2 fl[27];
+    if (flat) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q)
+            fl[q] = PairIO<S>::load(base0 + in_offset(G, q, kParity, (w0 >> q) & 1u),
+                                    base0 + 1 + in_offset(G, q, kParity, (w1 >> q) & 1u), q, b.sc);
+    } else {
+        const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
+        const NeighbourOffsets o1 = neighbour_offsets(G, x, y, z0 + 1);
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            int c0, d0, c1, d1;
+            incoming_slot(o0, own0, q, kParity, (w0 >> q) & 1u, c0, d0);
+            incoming_slot(o1, own0 + 1, q, kParity, (w1 >> q) & 1u, c1, d1);
+            fl[q] = PairIO<S>::load(f + (d0 * G.pcells + c0), f + (d1 * G.pcells + c1), q, b.sc);
+        }
+    }
+    bool ok[2];
+    collide27_x2(fl, b.cp, f2(0.0f), f2(0.0f), f2(0.0f), f2(0.0f), ok);
+    const bool st0 = live0 && ok[0], st1 = live1 && ok[1];
+    if (live0 && !ok[0] || live1 && !ok[1]) {
+        const long long cells = (long long)G.nx * G.ny * G.nz;
+        const int wrap_mask = G.wrap[0] | (G.wrap[1] << 1) | (G.wrap[2] << 2);
+        for (int k = 0; k < 2; ++k)
+            if ((k == 0 ? live0 && !ok[0] : live1 && !ok[1]))
+                reseed_push_ip<S>(f, b.ref, b.ref + cells, b.ref + 2 * cells, b.ref + 3 * cells, b.cp.max_speed, b.sc.scale,
+                                  cell0 + k, x, y, z0 + k, G.nx, G.ny, G.nz, wrap_mask, kParity);
+    }
+    if (flat) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            const int off = out_offset(G, q, kParity);
+            PairIO<S>::store(base0 + off, base0 + off + 1, st0, st1, q, fl[q], b.sc);
+        }
+        return;
+    }
+    const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
+    const NeighbourOffsets o1 = neighbour_offsets(G, x, y, z0 + 1);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        int c0, d0, c1, d1;
+        outgoing_slot(o0, own0, q, kParity, c0, d0);
+        outgoing_slot(o1, own0 + 1, q, kParity, c1, d1);
+        PairIO<S>::store(f + (d0 * G.pcells + c0), f + (d1 * G.pcells + c1), st0, st1, q, fl[q], b.sc);
+    }
+}
+
+// Cells per thread of a brick's work units.
+__device__ __forceinline__ int unit_span(const BrickDesc& b) { return b.pairs ? 2 : 1; }
+
 // Copy one brick descriptor into shared memory (one 32-bit word per thread).
 __device__ __forceinline__ void stage_desc(BrickDesc& dst, const BrickDesc* src) {
     constexpr int kWords = (int)(sizeof(BrickDesc) / 4);
@@ -93,9 +164,10 @@ __device__ __forceinline__ void stage_desc(BrickDesc& dst, const BrickDesc* src)
 }
 
 // One persistent launch per tick: each resident tile walks the work list with
-// a fixed stride; a unit is `blockDim.x` consecutive cells of one brick. The
-// unit's brick descriptor is staged in shared memory, so its fields are read
-// where they are used instead of occupying registers.
+// a fixed stride; a unit is `blockDim.x` consecutive cells of one brick, or
+// `2 * blockDim.x` (two z-adjacent cells per thread) for bricks with even nz.
+// The unit's brick descriptor is staged in shared memory, so its fields are
+// read where they are used instead of occupying registers.
 template <int kParity>
 __global__ void batch_step_kernel(const BrickDesc* __restrict__ descs, const int* __restrict__ unit_brick, int units) {
     __shared__ BrickDesc sd;
@@ -104,10 +176,16 @@ __global__ void batch_step_kernel(const BrickDesc* __restrict__ descs, const int
         stage_desc(sd, descs + unit_brick[u]);
         __syncthreads();
         const int cells = sd.g.nx * sd.g.ny * sd.g.nz;
-        const int cell = (u - sd.unit_begin) * blockDim.x + threadIdx.x;
+        const int span = unit_span(sd);
+        const int cell = ((u - sd.unit_begin) * blockDim.x + threadIdx.x) * span;
         if (cell >= cells) continue;
-        if (sd.precision == 1) batch_cell<StoreF16Dev, kParity>(sd, cell);
-        else batch_cell<StoreF32, kParity>(sd, cell);
+        if (span == 2) {
+            if (sd.precision == 1) batch_pair<StoreF16Dev, kParity>(sd, cell);
+            else batch_pair<StoreF32, kParity>(sd, cell);
+        } else {
+            if (sd.precision == 1) batch_cell<StoreF16Dev, kParity>(sd, cell);
+            else batch_cell<StoreF32, kParity>(sd, cell);
+        }
     }
 }
 
@@ -162,7 +240,9 @@ __global__ void batch_init_kernel(const BrickDesc* __restrict__ descs, const int
     for (int u = blockIdx.x; u < units; u += gridDim.x) {
         const BrickDesc& b = descs[unit_brick[u]];
         const int cells = b.g.nx * b.g.ny * b.g.nz;
-        const int cell = (u - b.unit_begin) * blockDim.x + threadIdx.x;
+        const int span = unit_span(b);
+        for (int k = 0; k < span; ++k) {
+        const int cell = ((u - b.unit_begin) * blockDim.x + threadIdx.x) * span + k;
         if (cell >= cells || b.obstacle[cell]) continue;
         const PadGeom& G = b.g;
         int x, y, z;
@@ -182,6 +262,7 @@ __global__ void batch_init_kernel(const BrickDesc* __restrict__ descs, const int
             outgoing_slot(o, own, q, 0, c, d);
             if (b.precision == 1) StoreF16Dev::store(static_cast<__half*>(b.f) + (d * G.pcells + c), q, fl[q], b.sc);
             else StoreF32::store(static_cast<float*>(b.f) + (d * G.pcells + c), q, fl[q], b.sc);
+        }
         }
     }
 }
@@ -347,8 +428,10 @@ bool build_units(Batch& B, int threads) {
         d.precision = hb.precision;
         d.sc = Fp16Scale{hb.fp16_scale, 1.0f / hb.fp16_scale};
         d.unit_begin = (int)unit_brick.size();
+        d.pairs = (hb.nz % 2 == 0) ? 1 : 0;
         const int cells = hb.nx * hb.ny * hb.nz;
-        const int nunits = (cells + threads - 1) / threads;
+        const int span = threads * (d.pairs ? 2 : 1);
+        const int nunits = (cells + span - 1) / span;
         for (int u = 0; u < nunits; ++u) unit_brick.push_back((int)i);
         d.atlas_offset = atlas;
         atlas += hb.atlas_cells;

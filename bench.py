@@ -222,7 +222,9 @@ def cpu_baseline_single(seconds: float = 15.0) -> dict | None:
 # ---------------------------------------------------------------- our arm
 VARIANTS = {
     # name: (realtime solver mode, collision mode, bytes per cell-step, storage note)
-    "fp16": (3, 1, 27 * 2 * 2 + 1, "fp16 deviation storage, in-place esoteric pull, factorised collision"),
+    "fp16": (3, 1, 27 * 2 * 2 + 1, "fp16 deviation storage, in-place esoteric pull, factorised collision, "
+                                   "two cells per thread in packed FP32"),
+    "i16": (3, 1, 27 * 2 * 2 + 1, "16-bit fixed-point deviation storage, in-place esoteric pull, factorised collision"),
     "fp32_exact": (0, 0, 27 * 4 * 2 + 1, "fp32, in-place esoteric pull, reference-order collision (bit-exact)"),
     "fp32_fast": (0, 1, 27 * 4 * 2 + 1, "fp32, in-place esoteric pull, factorised collision"),
 }
@@ -233,6 +235,7 @@ def setup_context(aero, lib, case, variant: str, key: int, streaming: int):
 
     solver_mode, collision, _, _ = VARIANTS[variant]
     lib.aero_lbm_set_realtime_solver_mode(solver_mode)
+    lib.aero_lbm_b200_set_fp16_format(1 if variant == "i16" else 0)
     lib.aero_lbm_b200_set_collision_mode(collision)
     lib.aero_lbm_b200_set_physics_overrides(case.smagorinsky_c, case.buoyancy_beta, case.gravity_axis)
     lib.aero_lbm_b200_set_streaming_mode(streaming)
@@ -257,6 +260,7 @@ def setup_context(aero, lib, case, variant: str, key: int, streaming: int):
         raise RuntimeError(aero.last_error(lib))
     lib.aero_lbm_set_realtime_solver_mode(0)
     lib.aero_lbm_b200_set_collision_mode(0)
+    lib.aero_lbm_b200_set_fp16_format(0)
     return ctx, packet, pk_ptr
 
 
@@ -421,7 +425,7 @@ def run_ours(args) -> dict | None:
 
     results = {}
     head_ctx = None
-    for variant in ("fp16", "fp32_exact", "fp32_fast"):
+    for variant in ("fp16", "fp32_exact", "fp32_fast", "i16"):
         if variant != "fp16" and variant not in args.variants:
             continue
         steps = args.steps if variant == "fp16" else max(10, args.steps // 2)
@@ -457,21 +461,33 @@ def run_ours(args) -> dict | None:
     e2e_value = cells * world * e2e_steps / e2e_s / 1e6
     ctx.release()
 
-    # Accuracy leg: FP16 storage against the bit-exact FP32 step after the
-    # same number of steps from the same inputs.
+    # Accuracy leg: every variant after `accuracy_steps` calls from the same
+    # inputs against the FP64 run of the same scheme (the adjoint module's
+    # forward in double precision, every fluid cell probed), and FP16
+    # against the bit-exact FP32 step.
     acc = None
     if args.accuracy_steps > 0:
         outs = {}
-        for variant, key in (("fp16", 90 + rank), ("fp32_exact", 95 + rank)):
-            c, _, _ = setup_context(aero, lib, case, variant, key, args.streaming)
+        for k, variant in enumerate(("fp16", "i16", "fp32_fast", "fp32_exact")):
+            c, _, _ = setup_context(aero, lib, case, variant, 90 + 8 * rank + k, args.streaming)
             c.advance(args.accuracy_steps - 1)
             outs[variant] = c.flow_state()
             c.release()
+        fluid = np.flatnonzero(case.obstacle.reshape(-1) == 0).astype(np.int32)
+        ab = aero.AdjointBrick(case.obstacle, case.temperature, lib=lib, face_kind=[f["kind"] for f in case.faces],
+                               tau=case.tau, smagorinsky_c=case.smagorinsky_c, buoyancy_beta=case.buoyancy_beta,
+                               steps=args.accuracy_steps, checkpoint_every=20)
+        ab.set_probes(fluid, np.zeros((fluid.size, 3), np.float32))
+        _, u64 = ab.forward(None, case.u_ref, precision=1)
+        ab.close()
+        speed64 = float(np.max(np.linalg.norm(u64.astype(np.float64), axis=1)))
         ref = outs["fp32_exact"].astype(np.float64)
         speed = float(np.max(np.linalg.norm(ref[:, :3], axis=1)))
         acc = {"steps": args.accuracy_steps,
+               **{f"{v}_vs_fp64_u": float(np.max(np.abs(outs[v][fluid, :3] - u64))) / speed64 for v in outs},
                "fp16_vs_fp32_u": float(np.max(np.abs(outs["fp16"][:, :3] - ref[:, :3]))) / speed,
-               "fp16_vs_fp32_rho": float(np.max(np.abs(outs["fp16"][:, 3] - ref[:, 3]))) / float(np.max(1 + ref[:, 3]))}
+               "fp16_vs_fp32_rho": float(np.max(np.abs(outs["fp16"][:, 3] - ref[:, 3]))) / float(np.max(1 + ref[:, 3])),
+               "metric": "max |u - u64| / max |u64| over fluid cells"}
 
     batch = None
     if args.batch_ticks > 0:
@@ -520,8 +536,8 @@ def run_ours(args) -> dict | None:
                    "meso_d3q19": meso,
                    "adjoint": adjoint},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic_record(f"step_ip_fp16@{n}"), "peak_source": peak_kind,
-                     "bytes_per_cell": VARIANTS["fp16"][2], "kernel": "step_ip_kernel<StoreF16Dev, fast>"},
+                     "traffic": traffic_record(f"step_ip2_fp16@{n}"), "peak_source": peak_kind,
+                     "bytes_per_cell": VARIANTS["fp16"][2], "kernel": "step_ip2_kernel<StoreF16Dev>"},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": int(packet.numel() * 4),
                 "d2h_bytes_per_step": int(atlas.nbytes), "steps": e2e_steps,
                 "api": "aero_lbm_step_rect (pinned packet) + aero_lbm_extract_flow_atlas_rect(stride 4)"},
@@ -543,7 +559,7 @@ def main() -> int:
     ap.add_argument("--streaming", type=int, default=0, help="0 auto, 1 two-buffer, 2 in-place")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-ticks", type=int, default=500, help="ticks of the 512-brick batch leg (0 skips it)")
-    ap.add_argument("--variants", default="fp32_exact,fp32_fast",
+    ap.add_argument("--variants", default="fp32_exact,fp32_fast,i16",
                     help="FP32 variants measured beside the FP16 headline (comma list, may be empty)")
     ap.add_argument("--meso-steps", type=int, default=2000, help="steps of the D3Q19 mesoscale leg (0 skips it)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false", help="skip the adjoint (gradient) leg")
