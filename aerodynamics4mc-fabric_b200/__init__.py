@@ -165,7 +165,7 @@ class AeroLbmB200MesoscaleOptions(ctypes.Structure):
         ("periodic_sides", ctypes.c_int), ("free_slip_top", ctypes.c_int), ("fixed_tau", ctypes.c_int),
         ("enable_sgs", ctypes.c_int), ("disable_edge_blend", ctypes.c_int), ("hydro_only", ctypes.c_int),
         ("tau_hydro", ctypes.c_double), ("smagorinsky_c", ctypes.c_double), ("body_force", ctypes.c_double * 3),
-        ("storage", ctypes.c_int), ("threads", ctypes.c_int),
+        ("storage", ctypes.c_int), ("threads", ctypes.c_int), ("collision", ctypes.c_int), ("reserved", ctypes.c_int),
     ]
 
 

@@ -91,7 +91,9 @@ cudaError_t meso_launch_step(const meso::MesoArgs& a, cudaStream_t s);
 
 // Hydrodynamic-only step. `fp16` selects __half deviation storage.
 enum MesoHydroMode { kHydroInit = 0, kHydroStep = 1, kHydroOutput = 2 };
-cudaError_t meso_hydro_seed(const float* forcing, int nx, int ny, int nz, float velocity_scale, bool fp16, float scale,
+// Population storage of the hydrodynamic-only step.
+enum MesoStorage { kMesoStoreF32 = 0, kMesoStoreF16 = 1, kMesoStoreI16 = 2 };
+cudaError_t meso_hydro_seed(const float* forcing, int nx, int ny, int nz, float velocity_scale, int storage, float scale,
                             void* dst, uint8_t* solid, cudaStream_t s);
 cudaError_t meso_hydro_mask(const float* forcing, long long cells, uint8_t* solid, cudaStream_t s);
 // Pull classification word per cell: bit q (0..18) = direction q bounces back,
@@ -100,6 +102,9 @@ cudaError_t meso_hydro_mask(const float* forcing, long long cells, uint8_t* soli
 constexpr uint32_t kHydroSelfSolid = 1u << 31;
 constexpr uint32_t kHydroSlow = 1u << 30;
 cudaError_t meso_hydro_flags(const meso::HydroArgs& a, const uint8_t* solid, uint32_t* flags, cudaStream_t s);
-cudaError_t meso_hydro_launch(const meso::HydroArgs& a, int mode, bool fp16, int threads, cudaStream_t s);
+cudaError_t meso_hydro_launch(const meso::HydroArgs& a, int mode, int storage, int threads, cudaStream_t s);
+// Fused step with two z-adjacent cells per thread and the TRT collision in
+// packed FP32 (meso_fast.cu); nz must be even.
+cudaError_t meso_hydro_fast_step(const meso::HydroArgs& a, int storage, cudaStream_t s);
 
 }  // namespace aero

@@ -25,29 +25,11 @@
 #include "d3q27_kernels.cuh"
 #include "lattice.cuh"
 #include "meso.cuh"
+#include "meso_lattice.cuh"
 
 namespace aero {
 namespace meso {
 
-// lattice (native/src/aero_lbm_mesoscale.cpp:146-174): rest, 6 faces, 12 edges
-__host__ __device__ constexpr int mcx(int q) {
-    return (q == 1 || q == 7 || q == 9 || q == 11 || q == 13) ? 1 : ((q == 2 || q == 8 || q == 10 || q == 12 || q == 14) ? -1 : 0);
-}
-__host__ __device__ constexpr int mcy(int q) {
-    return (q == 3 || q == 7 || q == 10 || q == 15 || q == 17) ? 1 : ((q == 4 || q == 8 || q == 9 || q == 16 || q == 18) ? -1 : 0);
-}
-__host__ __device__ constexpr int mcz(int q) {
-    return (q == 5 || q == 11 || q == 14 || q == 15 || q == 18) ? 1 : ((q == 6 || q == 12 || q == 13 || q == 16 || q == 17) ? -1 : 0);
-}
-__host__ __device__ constexpr int mopp(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
-// same x and z component, opposite y component (specular reflection at the lid)
-__host__ __device__ constexpr int mmirror(int q) {
-    return q == 3 ? 4 : q == 4 ? 3 : q == 7 ? 9 : q == 9 ? 7 : q == 8 ? 10 : q == 10 ? 8
-         : q == 15 ? 18 : q == 18 ? 15 : q == 16 ? 17 : q == 17 ? 16 : q;
-}
-static_assert(mcx(mmirror(7)) == 1 && mcy(mmirror(7)) == -1 && mcz(mmirror(16)) == -1 && mcy(mmirror(16)) == 1, "mirror");
-
-__device__ __forceinline__ float mw(int q) { return q == 0 ? 1.0f / 3.0f : (q < 7 ? 1.0f / 18.0f : 1.0f / 36.0f); }
 __device__ __forceinline__ float fx_(int q) { return (float)mcx(q); }
 __device__ __forceinline__ float fy_(int q) { return (float)mcy(q); }
 __device__ __forceinline__ float fz_(int q) { return (float)mcz(q); }
@@ -423,23 +405,6 @@ __global__ void meso_seed_kernel(MesoArgs A) {
 // seeded state; outputs stream the current post-collision state once more.
 // Two population buffers; each holds post-collision values.
 
-// Storage of one population: FP32 as is, or FP16 deviations
-// h = (f - w_q) * S / w_q with a per-grid power-of-two scale S.
-struct MesoF32 {
-    using T = float;
-    __device__ __forceinline__ static float load(const float* __restrict__ p, int, float) { return __ldg(p); }
-    __device__ __forceinline__ static void store(float* __restrict__ p, int, float v, float) { *p = v; }
-};
-struct MesoF16 {
-    using T = __half;
-    __device__ __forceinline__ static float load(const __half* __restrict__ p, int q, float inv_scale) {
-        return fmaf(__half2float(__ldg(p)), mw(q) * inv_scale, mw(q));
-    }
-    __device__ __forceinline__ static void store(__half* __restrict__ p, int q, float v, float scale) {
-        *p = __float2half_rn(fmaf(v, scale * (1.0f / mw(q)), -scale));
-    }
-};
-
 template <class S, int kMode>
 __global__ void __launch_bounds__(256) meso_hydro_kernel(HydroArgs A) {
     using T = typename S::T;
@@ -665,13 +630,16 @@ cudaError_t meso_launch_step(const meso::MesoArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t meso_hydro_seed(const float* forcing, int nx, int ny, int nz, float velocity_scale, bool fp16, float scale,
+cudaError_t meso_hydro_seed(const float* forcing, int nx, int ny, int nz, float velocity_scale, int storage, float scale,
                             void* dst, uint8_t* solid, cudaStream_t s) {
     const long long cells = (long long)nx * ny * nz;
     const unsigned blocks = (unsigned)((cells + 255) / 256);
-    if (fp16)
+    if (storage == kMesoStoreF16)
         meso::meso_hydro_seed_kernel<meso::MesoF16><<<blocks, 256, 0, s>>>(forcing, nx, ny, nz, velocity_scale, scale,
                                                                            static_cast<__half*>(dst), solid);
+    else if (storage == kMesoStoreI16)
+        meso::meso_hydro_seed_kernel<meso::MesoI16><<<blocks, 256, 0, s>>>(forcing, nx, ny, nz, velocity_scale, scale,
+                                                                           static_cast<short*>(dst), solid);
     else
         meso::meso_hydro_seed_kernel<meso::MesoF32><<<blocks, 256, 0, s>>>(forcing, nx, ny, nz, velocity_scale, scale,
                                                                            static_cast<float*>(dst), solid);
@@ -702,12 +670,14 @@ static void hydro_dispatch(const meso::HydroArgs& a, int mode, unsigned blocks, 
         meso::meso_hydro_kernel<S, kHydroOutput><<<blocks, threads, 0, s>>>(a);
 }
 
-cudaError_t meso_hydro_launch(const meso::HydroArgs& a, int mode, bool fp16, int threads, cudaStream_t s) {
+cudaError_t meso_hydro_launch(const meso::HydroArgs& a, int mode, int storage, int threads, cudaStream_t s) {
     if (threads != 64 && threads != 128 && threads != 256) return cudaErrorInvalidValue;
     const long long cells = (long long)a.nx * a.ny * a.nz;
     const unsigned blocks = (unsigned)((cells + threads - 1) / threads);
-    if (fp16)
+    if (storage == kMesoStoreF16)
         hydro_dispatch<meso::MesoF16>(a, mode, blocks, threads, s);
+    else if (storage == kMesoStoreI16)
+        hydro_dispatch<meso::MesoI16>(a, mode, blocks, threads, s);
     else
         hydro_dispatch<meso::MesoF32>(a, mode, blocks, threads, s);
     count_launch();

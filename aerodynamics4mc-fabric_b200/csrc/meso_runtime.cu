@@ -62,7 +62,7 @@ struct MesoContext {
     long long cells = 0;
     bool initialized = false;
     bool hydro = false;     // layout of the allocated state
-    bool fp16 = false;
+    int storage = 0;        // kMesoStore* of the allocated state (hydro only)
     float fp16_scale = 1.0f;
     float* forcing[2] = {nullptr, nullptr};
     uint8_t* solid[2] = {nullptr, nullptr};
@@ -94,7 +94,7 @@ struct MesoContext {
         out_valid = false;
     }
     double bytes_per_step() const {
-        if (hydro) return (double)cells * (19.0 * 2.0 * (fp16 ? 2.0 : 4.0) + 1.0);
+        if (hydro) return (double)cells * (19.0 * 2.0 * (storage ? 2.0 : 4.0) + 1.0);
         // collide: f, g read + written; stream: post f, g read, f, g written; forcing 2 x 100 B; fields; output
         return (double)cells * (19.0 * 4.0 * 8.0 + 2.0 * 100.0 + 10.0 * 4.0 + 24.0);
     }
@@ -115,7 +115,7 @@ bool allocate(MesoContext& c) {
     c.nz = c.config.nz;
     c.cells = (long long)c.nx * c.ny * c.nz;
     c.hydro = c.opt.hydro_only != 0;
-    c.fp16 = c.hydro && c.opt.storage == 1;
+    c.storage = c.hydro ? c.opt.storage : 0;
     const size_t n = (size_t)c.cells;
     bool ok = dev_alloc(&c.forcing[0], n * kMesoForcingChannels, "meso forcing") &&
               dev_alloc(&c.forcing[1], n * kMesoForcingChannels, "meso forcing") &&
@@ -123,7 +123,7 @@ bool allocate(MesoContext& c) {
               dev_alloc(&c.out, n * kMesoStateChannels, "meso output");
     if (!ok) return false;
     if (c.hydro) {
-        const size_t bytes = n * 19 * (c.fp16 ? 2 : 4);
+        const size_t bytes = n * 19 * (c.storage ? 2 : 4);
         ok = cuda_ok(cudaMalloc(&c.pop[0], bytes), "meso populations") && cuda_ok(cudaMalloc(&c.pop[1], bytes), "meso populations") &&
              dev_alloc(&c.flags[0], n, "meso flags") && dev_alloc(&c.flags[1], n, "meso flags");
     } else {
@@ -189,8 +189,8 @@ meso::HydroArgs hydro_args(const MesoContext& c, const Transport& t, int prev_sl
     a.edge_blend = c.opt.disable_edge_blend ? 0 : 1;
     a.velocity_scale = t.velocity_scale;
     a.max_speed = 0.35f * t.velocity_scale;
-    a.scale = c.fp16 ? c.fp16_scale : 1.0f;
-    a.inv_scale = c.fp16 ? 1.0f / c.fp16_scale : 1.0f;
+    a.scale = c.storage ? c.fp16_scale : 1.0f;
+    a.inv_scale = c.storage ? 1.0f / c.fp16_scale : 1.0f;
     a.h = rates(c, t);
     a.solid_prev = c.solid[prev_slot];
     a.flags_prev = c.flags[prev_slot];
@@ -216,14 +216,17 @@ bool model_step(MesoContext& c, const Transport& t, int slot, cudaStream_t s) {
 // One hydrodynamic-only call: fused pull (prev_slot) + collision (cur_slot).
 bool hydro_step(MesoContext& c, const Transport& t, int prev_slot, int cur_slot, cudaStream_t s) {
     const meso::HydroArgs a = hydro_args(c, t, prev_slot, cur_slot);
-    if (!cuda_ok(meso_hydro_launch(a, kHydroStep, c.fp16, hydro_threads(c), s), "mesoscale hydro step")) return false;
+    const bool packed = c.opt.collision == 1 && c.nz % 2 == 0;
+    if (!cuda_ok(packed ? meso_hydro_fast_step(a, c.storage, s) : meso_hydro_launch(a, kHydroStep, c.storage, hydro_threads(c), s),
+                 "mesoscale hydro step"))
+        return false;
     c.cur ^= 1;
     return true;
 }
 
 bool hydro_output(MesoContext& c, const Transport& t, cudaStream_t s) {
     const meso::HydroArgs a = hydro_args(c, t, c.fslot, c.fslot);
-    return cuda_ok(meso_hydro_launch(a, kHydroOutput, c.fp16, hydro_threads(c), s), "mesoscale hydro output");
+    return cuda_ok(meso_hydro_launch(a, kHydroOutput, c.storage, hydro_threads(c), s), "mesoscale hydro output");
 }
 
 // Largest |lattice wind| of the seeding forcing (host copy), for the FP16 scale.
@@ -310,7 +313,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_mesoscale_step_context(long long key, const Ae
     const bool shape_changed = c->nx != config->nx || c->ny != config->ny || c->nz != config->nz;
     c->config = *config;
     if (shape_changed || !c->cells || c->hydro != (c->opt.hydro_only != 0) ||
-        c->fp16 != (c->opt.hydro_only != 0 && c->opt.storage == 1)) {
+        c->storage != (c->opt.hydro_only != 0 ? c->opt.storage : 0)) {
         if (!allocate(*c)) return 0;
     }
     const Transport t = derive(*config);
@@ -321,14 +324,16 @@ AERO_LBM_B200_EXPORT int aero_lbm_mesoscale_step_context(long long key, const Ae
         return 0;
     if (c->hydro) {
         if (!c->initialized) {
-            c->fp16_scale = c->fp16 ? fp16_scale_for_speed(seed_speed(forcing, c->cells, t.velocity_scale)) : 1.0f;
+            const float us = seed_speed(forcing, c->cells, t.velocity_scale);
+            c->fp16_scale = c->storage == kMesoStoreF16 ? fp16_scale_for_speed(us)
+                          : c->storage == kMesoStoreI16 ? i16_scale_for_speed(us) : 1.0f;
             c->cur = 0;
-            if (!cuda_ok(meso_hydro_seed(c->forcing[slot], c->nx, c->ny, c->nz, t.velocity_scale, c->fp16, c->fp16_scale,
+            if (!cuda_ok(meso_hydro_seed(c->forcing[slot], c->nx, c->ny, c->nz, t.velocity_scale, c->storage, c->fp16_scale,
                                          c->pop[0], c->solid[slot], s), "mesoscale hydro seed") ||
                 !cuda_ok(meso_hydro_flags(hydro_args(*c, t, slot, slot), c->solid[slot], c->flags[slot], s), "mesoscale flags"))
                 return 0;
             const meso::HydroArgs a = hydro_args(*c, t, slot, slot);
-            if (!cuda_ok(meso_hydro_launch(a, kHydroInit, c->fp16, hydro_threads(*c), s), "mesoscale hydro init")) return 0;
+            if (!cuda_ok(meso_hydro_launch(a, kHydroInit, c->storage, hydro_threads(*c), s), "mesoscale hydro init")) return 0;
             c->cur = 1;
             c->initialized = true;
         } else {
@@ -373,8 +378,12 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_mesoscale_set_options(long long key, cons
         set_error("mesoscale_set_options: unknown context or null options");
         return 0;
     }
-    if (o->storage != 0 && !(o->storage == 1 && o->hydro_only)) {
-        set_error("mesoscale_set_options: FP16 storage needs hydro_only");
+    if (o->storage < 0 || o->storage > 2 || (o->storage != 0 && !o->hydro_only)) {
+        set_error("mesoscale_set_options: storage 0 (FP32), 1 (FP16) or 2 (16-bit fixed point); 16-bit storage needs hydro_only");
+        return 0;
+    }
+    if (o->collision != 0 && o->collision != 1) {
+        set_error("mesoscale_set_options: collision 0 (reference order) or 1 (packed two-cell)");
         return 0;
     }
     if (o->threads != 0 && o->threads != 64 && o->threads != 128 && o->threads != 256) {

@@ -89,6 +89,7 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
 bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out);
 // Per-brick FP16 deviation scale for a brick whose speed stays below umax.
 float fp16_scale_for_speed(float umax);
+float i16_scale_for_speed(float umax);
 // Device-side output into `dev_out` (no copy, no synchronisation).
 bool output_device(Context& ctx, int stride, int out_ch, float scale, float* dev_out);
 

@@ -352,8 +352,11 @@ typedef struct AeroLbmB200MesoscaleOptions {
     double tau_hydro;
     double smagorinsky_c;
     double body_force[3];    /* lattice force density (Guo source), y up */
-    int storage;             /* hydro_only: 0 FP32, 1 FP16 deviations */
+    int storage;             /* hydro_only: 0 FP32, 1 FP16 deviations, 2 16-bit fixed-point deviations */
     int threads;             /* hydro_only: block size 64, 128 or 256 (0 = 256) */
+    int collision;           /* hydro_only: 0 reference order (FP32 bit-identical to the restatement),
+                                1 two cells per thread in packed FP32 (nz even; agrees to FP32 rounding) */
+    int reserved;
 } AeroLbmB200MesoscaleOptions;
 
 AERO_LBM_B200_EXPORT void aero_lbm_b200_mesoscale_default_options(AeroLbmB200MesoscaleOptions* out_options);

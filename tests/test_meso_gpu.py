@@ -44,7 +44,7 @@ def oracle_options(opts: dict | None) -> O.MesoOptions | None:
         if k == "body_force":
             for a in range(3):
                 o.body_force[a] = float(v[a])
-        elif k in ("storage", "threads"):
+        elif k in ("storage", "threads", "collision"):
             continue
         else:
             setattr(o, k, v)
@@ -194,3 +194,38 @@ def test_shape_change_reseeds(gpu):
     for _ in range(4):
         want = orc.step(F2)
     assert_bits(got, want, "reseed")
+
+
+def _errors(got, want):
+    wmax = float(np.abs(want[:, 3:]).max())
+    return float(np.abs(got[:, 3:] - want[:, 3:]).max()) / wmax, float(np.abs(got[:, 0] - want[:, 0]).max())
+
+
+@pytest.mark.parametrize("storage,bound", [(0, 2e-5), (1, 2.5e-3), (2, 1e-3)])
+def test_hydro_packed_two_cell_step(gpu, storage, bound):
+    """The packed two-cell step (collision 1) with FP32, FP16 and 16-bit
+    fixed-point storage against the oracle's FP64 run of the C3 set-up at
+    48 x 32 x 48 after 200 steps: wind error relative to the largest wind
+    within the stated bound, density within 1e-4."""
+    c = c3_small(48, 32, 48, seed=8)
+    opts = {**c.options, "storage": storage, "collision": 1}
+    last = None
+    for last in run_both(c.dims, [c.forcing] * 200, opts, c.dx_m, c.dt_s, precision="f64"):
+        pass
+    e_u, e_rho = _errors(*last)
+    assert e_u <= bound and e_rho <= 1e-4, (e_u, e_rho)
+
+
+def test_hydro_packed_open_boundaries_mask_change_odd_nz(gpu):
+    """Open sides and lid with the edge blend, a changing mask, force and SGS
+    through the packed step; an odd nz falls back to the reference-order
+    kernel. Against the oracle's FP64 run: wind within 1e-4 of the largest."""
+    for dims in ((14, 7, 10), (12, 6, 9)):
+        seq = [O.meso_forcing(dims, seed=70 + (k // 5), terrain_max=3.0, wind=(8.0, 0.5, 2.0)) for k in range(15)]
+        opts = {"hydro_only": 1, "enable_sgs": 1, "body_force": (1e-5, 0.0, 0.0), "fixed_tau": 1, "tau_hydro": 0.55,
+                "collision": 1}
+        last = None
+        for last in run_both(dims, seq, opts, precision="f64"):
+            pass
+        e_u, e_rho = _errors(*last)
+        assert e_u <= 1e-4 and e_rho <= 1e-5, (dims, e_u, e_rho)
