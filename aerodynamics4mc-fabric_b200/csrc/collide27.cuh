@@ -37,7 +37,7 @@ struct CollideParams {
     int enable_sgs;
     int enable_buoyancy;
     int gravity_axis;       // axis the buoyant force points along (+): 0 x, 1 y, 2 z
-    int pad;
+    int zero_bits;          // always 0 (value-initialised): a run-time zero for collide27_exact_x2.cuh
 };
 
 // Reference clamp constants (jni.cpp:118-132).

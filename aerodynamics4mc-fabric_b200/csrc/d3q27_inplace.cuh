@@ -11,6 +11,7 @@
 
 #include "d3q27_step.cuh"
 #include "collide27_x2.cuh"
+#include "collide27_exact_x2.cuh"
 #include "inplace27.cuh"
 
 namespace aero {
@@ -223,8 +224,10 @@ struct PairIO<StoreI16Dev> {
     }
 };
 
-// Factorised-collision step with two z-adjacent cells per thread and the
-// collision in packed FP32 (collide27_x2.cuh); line grid over cell pairs.
+// Step with two z-adjacent cells per thread and the collision in packed FP32:
+// the factorised collision (collide27_x2.cuh), or with kExact the
+// reference-order one (collide27_exact_x2.cuh, bit-identical per lane to the
+// one-cell kernel); line grid over cell pairs.
 // Pairs without periodic wraps address every slot at a launch-uniform offset
 // (one of two per direction, by the bounce-back bit; the second cell's slots
 // one element after the first's).
@@ -235,8 +238,11 @@ struct PairIO<StoreI16Dev> {
 #ifndef AERO_IP2_MIN_BLOCKS
 #define AERO_IP2_MIN_BLOCKS 5
 #endif
-template <class S, int kParity>
-__global__ void __launch_bounds__(128, AERO_IP2_MIN_BLOCKS) step_ip2_kernel(typename S::T* __restrict__ f, IpArgs a) {
+#ifndef AERO_IP2X_MIN_BLOCKS
+#define AERO_IP2X_MIN_BLOCKS 4
+#endif
+template <class S, bool kExact, int kParity>
+__global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_MIN_BLOCKS) step_ip2_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom& G = a.g;
     const int z0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (z0 >= G.nz) return;
@@ -279,7 +285,8 @@ __global__ void __launch_bounds__(128, AERO_IP2_MIN_BLOCKS) step_ip2_kernel(type
         cfz = f2(a.force.fz[cell0], has1 ? a.force.fz[cell0 + 1] : 0.0f);
     }
     bool ok[2];
-    collide27_x2(fl, a.cp, t, cfx, cfy, cfz, ok);
+    if (kExact) exact::collide27_exact_x2(fl, a.cp, t, cfx, cfy, cfz, ok);
+    else collide27_x2(fl, a.cp, t, cfx, cfy, cfz, ok);
     if (pass0 || pass1) {
         const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
         const NeighbourOffsets o1 = neighbour_offsets(G, x, y, has1 ? z0 + 1 : z0);
@@ -467,10 +474,10 @@ struct IpLaunch {
             cudaError_t e = face_fill(f, a, s);
             if (e != cudaSuccess) return e;
         }
-        if (!kExact && a.cells_per_thread == 2) {
+        if (a.cells_per_thread == 2) {
             const int lb = line_block((a.g.nz + 1) / 2);
-            if (a.parity == 0) step_ip2_kernel<S, 0><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
-            else step_ip2_kernel<S, 1><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
+            if (a.parity == 0) step_ip2_kernel<S, kExact, 0><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
+            else step_ip2_kernel<S, kExact, 1><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
         } else {
             const int lb = line_block(a.g.nz);
             if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);

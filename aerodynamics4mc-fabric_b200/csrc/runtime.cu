@@ -44,7 +44,7 @@ struct TimingStats {
 
 RuntimeConfig g_cfg;
 std::recursive_mutex g_mutex;  // guards every entry point (the caller is one worker thread)
-int g_cells_per_thread = 2;    // in-place factorised step: 1 scalar kernel, 2 packed pair kernel
+int g_cells_per_thread = 2;    // in-place step: 1 one cell per thread, 2 two cells per thread (packed collision)
 int g_fp16_format = 0;         // 16-bit storage: 0 IEEE half deviations, 1 fixed-point deviations
 std::unordered_map<long long, std::unique_ptr<Context>> g_contexts;
 std::string g_last_error;

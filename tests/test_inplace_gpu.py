@@ -119,12 +119,22 @@ def test_fp16_terrain_against_fp64(gpu):
     assert np.all(out16[solid] == 0)
 
 
-def test_fp32_terrain_bit_identical(gpu):
+@pytest.mark.parametrize("cells_per_thread", [1, 2])
+@pytest.mark.parametrize("n", [24, 23])
+def test_fp32_terrain_bit_identical(gpu, n, cells_per_thread):
+    """Reference-order FP32 step, one cell per thread or two z-adjacent cells
+    per thread with the collision in packed FP32 (odd n leaves a lone last
+    cell in every line): bit-identical to the oracle's FP32 run."""
     cases = load_cases()
-    case = cases.c2_terrain_boussinesq(n=24, seed=8)
+    case = cases.c2_terrain_boussinesq(n=n, seed=8)
     steps = 60
-    out, ctx = lbm_cases.run_product(gpu, case.dims, case.config_dict(), case.packet(), steps, key=43,
-                                     smagorinsky_c=case.smagorinsky_c, beta=case.buoyancy_beta, axis=case.gravity_axis)
+    assert gpu.aero_lbm_b200_set_cells_per_thread(cells_per_thread) == 1
+    try:
+        out, ctx = lbm_cases.run_product(gpu, case.dims, case.config_dict(), case.packet(), steps, key=43,
+                                         smagorinsky_c=case.smagorinsky_c, beta=case.buoyancy_beta,
+                                         axis=case.gravity_axis)
+    finally:
+        gpu.aero_lbm_b200_set_cells_per_thread(2)
     assert_bits(out, _oracle_run(case, steps, "f32"))
 
 
