@@ -27,7 +27,9 @@ struct IpArgs {
     ForceField force;
     CollideParams cp;
     Fp16Scale sc;
-    int cells_per_thread;            // factorised step: 1 scalar kernel, 2 packed pair kernel
+    int cells_per_thread;            // 1 one cell per thread, 2 two cells per thread (packed collision)
+    int streamed;                    // factorised two-cell step: populations streamed by bulk async copies
+    int* fault;                      // device word set to 1 by a streamed step whose copies never landed
 };
 
 // Equilibrium value of a face (velocity / pressure / moving wall), the only
@@ -451,53 +453,5 @@ __global__ void output_ip_kernel(const typename S::T* __restrict__ f, IpArgs a, 
     dst[0] = o4[0]; dst[1] = o4[1]; dst[2] = o4[2]; dst[3] = o4[3];
     for (int c = 4; c < out_ch; ++c) dst[c] = 0.0f;
 }
-
-template <class S, bool kExact>
-struct IpLaunch {
-    static cudaError_t init(typename S::T* f, const IpArgs& a, cudaStream_t s) {
-        const long long cells = (long long)a.g.nx * a.g.ny * a.g.nz;
-        init_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
-        count_launch();
-        return cudaGetLastError();
-    }
-    // Pre-fill of equilibrium-face sources; needed when any face is an
-    // equilibrium face (velocity, pressure, moving wall).
-    static cudaError_t face_fill(typename S::T* f, const IpArgs& a, cudaStream_t s) {
-        const long long n = 2LL * ((long long)a.g.ny * a.g.nz + (long long)a.g.nx * a.g.nz + (long long)a.g.nx * a.g.ny);
-        face_fill_ip_kernel<S><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a);
-        count_launch();
-        return cudaGetLastError();
-    }
-    static cudaError_t step(typename S::T* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
-        const long long cells = (long long)a.g.nx * a.g.ny * a.g.nz;
-        if (fill) {
-            cudaError_t e = face_fill(f, a, s);
-            if (e != cudaSuccess) return e;
-        }
-        if (a.cells_per_thread == 2) {
-            const int lb = line_block((a.g.nz + 1) / 2);
-            if (a.parity == 0) step_ip2_kernel<S, kExact, 0><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
-            else step_ip2_kernel<S, kExact, 1><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
-        } else {
-            const int lb = line_block(a.g.nz);
-            if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
-            else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
-        }
-        count_launch();
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess || !transitions) return e;
-        transition_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
-        count_launch();
-        return cudaGetLastError();
-    }
-    static cudaError_t output(const typename S::T* f, const IpArgs& a, int stride, int out_ch, float scale, float* out,
-                              cudaStream_t s) {
-        const int sx = (a.g.nx + stride - 1) / stride, sy = (a.g.ny + stride - 1) / stride, sz = (a.g.nz + stride - 1) / stride;
-        const long long n = (long long)sx * sy * sz;
-        output_ip_kernel<S, kExact><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a, stride, sx, sy, sz, out_ch, scale, out);
-        count_launch();
-        return cudaGetLastError();
-    }
-};
 
 }  // namespace aero

@@ -2,7 +2,7 @@
 // collision variant; defined in d3q27_exact.cu and d3q27_fast.cu.
 #pragma once
 
-#include "d3q27_inplace.cuh"
+#include "ip_launch_t.cuh"
 
 namespace aero {
 

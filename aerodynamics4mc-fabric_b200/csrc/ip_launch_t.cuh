@@ -1,0 +1,61 @@
+// Host-side launchers of the in-place (esoteric pull) brick kernels, one
+// instantiation per storage / collision variant (d3q27_exact.cu,
+// d3q27_fast.cu).
+#pragma once
+
+#include "d3q27_async.cuh"
+
+namespace aero {
+
+template <class S, bool kExact>
+struct IpLaunch {
+    static cudaError_t init(typename S::T* f, const IpArgs& a, cudaStream_t s) {
+        const long long cells = (long long)a.g.nx * a.g.ny * a.g.nz;
+        init_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
+        count_launch();
+        return cudaGetLastError();
+    }
+    // Pre-fill of equilibrium-face sources; needed when any face is an
+    // equilibrium face (velocity, pressure, moving wall).
+    static cudaError_t face_fill(typename S::T* f, const IpArgs& a, cudaStream_t s) {
+        const long long n = 2LL * ((long long)a.g.ny * a.g.nz + (long long)a.g.nx * a.g.nz + (long long)a.g.nx * a.g.ny);
+        face_fill_ip_kernel<S><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a);
+        count_launch();
+        return cudaGetLastError();
+    }
+    static cudaError_t step(typename S::T* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
+        const long long cells = (long long)a.g.nx * a.g.ny * a.g.nz;
+        if (fill) {
+            cudaError_t e = face_fill(f, a, s);
+            if (e != cudaSuccess) return e;
+        }
+        if (!kExact && a.cells_per_thread == 2 && a.streamed && IpaLaunch<S>::eligible(a)) {
+            cudaError_t e = IpaLaunch<S>::step(f, a, s);
+            if (e != cudaSuccess) return e;
+        } else if (a.cells_per_thread == 2) {
+            const int lb = line_block((a.g.nz + 1) / 2);
+            if (a.parity == 0) step_ip2_kernel<S, kExact, 0><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
+            else step_ip2_kernel<S, kExact, 1><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
+        } else {
+            const int lb = line_block(a.g.nz);
+            if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
+            else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
+        }
+        count_launch();
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess || !transitions) return e;
+        transition_ip_kernel<S, kExact><<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(f, a);
+        count_launch();
+        return cudaGetLastError();
+    }
+    static cudaError_t output(const typename S::T* f, const IpArgs& a, int stride, int out_ch, float scale, float* out,
+                              cudaStream_t s) {
+        const int sx = (a.g.nx + stride - 1) / stride, sy = (a.g.ny + stride - 1) / stride, sz = (a.g.nz + stride - 1) / stride;
+        const long long n = (long long)sx * sy * sz;
+        output_ip_kernel<S, kExact><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a, stride, sx, sy, sz, out_ch, scale, out);
+        count_launch();
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace aero

@@ -44,6 +44,7 @@ struct TimingStats {
 
 RuntimeConfig g_cfg;
 std::recursive_mutex g_mutex;  // guards every entry point (the caller is one worker thread)
+int g_streamed_step = 0;      // factorised two-cell in-place step: bulk-copy streamed kernel where eligible (opt-in)
 int g_cells_per_thread = 2;    // in-place step: 1 one cell per thread, 2 two cells per thread (packed collision)
 int g_fp16_format = 0;         // 16-bit storage: 0 IEEE half deviations, 1 fixed-point deviations
 std::unordered_map<long long, std::unique_ptr<Context>> g_contexts;
@@ -395,6 +396,7 @@ void Context::release_device() {
     fr(reinterpret_cast<void*&>(packet));
     fr(reinterpret_cast<void*&>(out));
     fr(reinterpret_cast<void*&>(force));
+    fr(reinterpret_cast<void*&>(fault));
     fr(ip);
     fr(scratch);
     scratch_cap = 0;
@@ -410,7 +412,7 @@ bool Context::allocate(int nx_, int ny_, int nz_) {
     nx = nx_; ny = ny_; nz = nz_;
     cells = (long long)nx * ny * nz;
     const size_t c = (size_t)cells;
-    auto al = [&](void** p, size_t bytes) { return cuda_ok(cudaMalloc(p, bytes), "cudaMalloc"); };
+    auto al = [&](void** p, size_t bytes) { return cuda_ok(cudaMalloc(p, bytes + kCopySlack), "cudaMalloc"); };
     bool ok = true;
     for (int i = 0; i < 2 && ok; ++i) {
         ok = ok && al(reinterpret_cast<void**>(&obstacle[i]), c);
@@ -422,6 +424,8 @@ bool Context::allocate(int nx_, int ny_, int nz_) {
     ok = ok && al(reinterpret_cast<void**>(&ref_uy), c * sizeof(float));
     ok = ok && al(reinterpret_cast<void**>(&ref_uz), c * sizeof(float));
     ok = ok && al(reinterpret_cast<void**>(&temperature), c * sizeof(float));
+    ok = ok && al(reinterpret_cast<void**>(&fault), sizeof(int));
+    ok = ok && cuda_ok(cudaMemset(fault, 0, sizeof(int)), "cudaMemset(fault)");
     if (!ok) {
         release_device();
         return false;
@@ -497,6 +501,8 @@ static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const Collide
     a.cp = cp;
     a.sc = Fp16Scale{ctx.fp16_scale, ctx.fp16_scale > 0.0f ? 1.0f / ctx.fp16_scale : 0.0f};
     a.cells_per_thread = g_cells_per_thread;
+    a.streamed = g_streamed_step;
+    a.fault = ctx.fault;
     return a;
 }
 
@@ -556,7 +562,7 @@ static bool choose_layout(Context& ctx, const FaceParams& face, const float* pac
         set_error("in-place layout: brick too large for 32-bit slot indexing");
         return false;
     }
-    if (!cuda_ok(cudaMalloc(&ctx.ip, bytes), "cudaMalloc(in-place populations)")) return false;
+    if (!cuda_ok(cudaMalloc(&ctx.ip, bytes + kCopySlack), "cudaMalloc(in-place populations)")) return false;
     if (!cuda_ok(cudaMemsetAsync(ctx.ip, 0, bytes, current_stream()), "cudaMemset(in-place)")) return false;
     ctx.bytes_per_step = (uint64_t)c * (27ull * elem * 2 + 1);
     if (half) {
@@ -701,7 +707,14 @@ bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_
     }
     if (!output_device(ctx, stride, out_ch, scale, ctx.out)) return false;
     if (!cuda_ok(cudaMemcpyAsync(host_out, ctx.out, bytes, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(output)")) return false;
-    return cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize(output)");
+    int fault = 0;
+    if (!cuda_ok(cudaMemcpyAsync(&fault, ctx.fault, sizeof(int), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(fault)")) return false;
+    if (!cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize(output)")) return false;
+    if (fault) {
+        set_error("in-place step: a tile's bulk copies did not complete within the wait limit; the state is invalid");
+        return false;
+    }
+    return true;
 }
 
 void record_timing(double copy_ms, double solver_ms, double readback_ms, double total_ms, bool cached) {
@@ -1099,6 +1112,16 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_cells_per_thread(int n) {
     return 1;
 }
 
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streamed_step(int on) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (on != 0 && on != 1) {
+        set_error("set_streamed_step: 0 or 1");
+        return 0;
+    }
+    g_streamed_step = on;
+    return 1;
+}
+
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_fp16_format(int format) {
     std::lock_guard<std::recursive_mutex> lk(g_mutex);
     if (format != 0 && format != 1) {
@@ -1126,7 +1149,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_force_field(long long key, const floa
         set_error("set_force_field: value_count must be 3 * cells");
         return 0;
     }
-    if (!c->force && !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&c->force), (size_t)c->cells * 3 * sizeof(float)), "cudaMalloc(force)")) return 0;
+    if (!c->force && !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&c->force), (size_t)c->cells * 3 * sizeof(float) + kCopySlack), "cudaMalloc(force)")) return 0;
     cudaStream_t s = current_stream();
     if (!cuda_ok(cudaMemcpyAsync(c->force, force_soa, (size_t)c->cells * 3 * sizeof(float), cudaMemcpyHostToDevice, s), "copy force")) return 0;
     return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;

@@ -17,6 +17,11 @@ namespace aero {
 // ref_p and flags are double-buffered: index `slot` holds the inputs and pull
 // classification of the last call, which the next call's fused kernel streams
 // with (the reference streams at the end of each call with that call's mask).
+// Bytes added after every per-cell array that the streamed in-place step
+// reads with 16-byte-granular bulk copies (a run's last granule may extend
+// up to 15 bytes past the array's last element).
+constexpr size_t kCopySlack = 256;
+
 struct Context {
     int nx = 0, ny = 0, nz = 0;
     long long cells = 0;
@@ -34,6 +39,7 @@ struct Context {
     float* out = nullptr;
     size_t out_cap = 0;
     float* force = nullptr;  // optional per-cell force density, SoA (3 * cells)
+    int* fault = nullptr;    // device word: a streamed in-place step lost a tile's copies
     FaceParams face_prev{};
     FaceParams h_face[2]{};  // host copies (source of the async uploads; must outlive them)
     // Layout chosen at the first step: 0 two-buffer pull (g[0], g[1]),

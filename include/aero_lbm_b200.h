@@ -232,11 +232,17 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums_noalloc(long long conte
  * 1 = factorised moment transforms with contraction (same scheme, fewer flops,
  * agrees to FP32 rounding per step). */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_collision_mode(int mode);
-/* Launch shape of the in-place step with the factorised collision (FP16
- * storage, FP32 collision mode 1): 2 = two z-adjacent cells per thread with the
- * collision in sm_100 packed FP32 (default), 1 = one cell per thread. Same
- * scheme; results agree to FP32 rounding. */
+/* Launch shape of the in-place step: 2 = two z-adjacent cells per thread with
+ * the collision in sm_100 packed FP32 (default), 1 = one cell per thread. With
+ * the reference-order collision both shapes are bit-identical; with the
+ * factorised one they agree to FP32 rounding. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_cells_per_thread(int cells_per_thread);
+/* In-place step with the factorised collision, two cells per thread, on a
+ * brick whose z axis is not periodic: 1 = each warp streams its next 64-cell
+ * tile into shared memory with bulk asynchronous copies while it collides the
+ * current one, 0 = per-thread loads (default; faster on B200). Same
+ * arithmetic, bit-identical results. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streamed_step(int on);
 /* Format of the 16-bit deviation storage chosen by
  * aero_lbm_set_realtime_solver_mode(3), for contexts created afterwards:
  * 0 = IEEE half of (f - w) * S / w with a power-of-two per-brick S (default),
