@@ -18,11 +18,17 @@
 //   stream_and_bounce       native/src/aero_lbm_jni.cpp:2415-2452
 //   write_output            native/src/aero_lbm_jni.cpp:2535-2581
 //   strided atlas extract   native/src/aero_lbm_jni.cpp:9246-9450
+//   temperature transport   native/src/aero_lbm_jni.cpp:2049-2143 (benchmark
+//                           branch), helpers 738-769, 1783-1950; per-call order
+//                           and state rules 1752-1781, 8028-8064, 8480-8507
 //
 // Knobs the reference hard-codes are parameters here (Smagorinsky constant,
 // buoyancy coefficient and axis, a uniform or per-cell body force); with the
-// reference's values they reduce to the reference step. Temperature is a
-// static per-cell field (the reference's scalar transport is not restated).
+// reference's values they reduce to the reference step. Temperature: with
+// thermal_transport = 1 the reference's benchmark-mode scalar transport
+// (first-order semi-Lagrangian advection by the previous collision's velocity,
+// explicit diffusion, optional source, thermal faces) runs before every
+// collision; with 0 the temperature is the packet's field of each call.
 //
 // Driven from Python with ctypes (tests/ and bench.py's CPU baseline only).
 
@@ -32,6 +38,7 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -71,7 +78,14 @@ typedef struct OracleD3Q27Params {
     int enable_buoyancy;
     int gravity_axis;          // 0,1,2: axis the buoyancy force acts along (+)
     int disable_convective_outflow;  // flag for INHERIT_GAME faces
-    int reserved;
+    int thermal_transport;     // 0: temperature = the packet field; 1: reference scalar transport
+    int thermal_kind[6];       // reference thermal face kinds (0 inherit .. 5 Neumann)
+    double face_temperature[6];
+    double face_heat_flux[6];
+    double thermal_diffusivity;    // reference benchmark value 0.035
+    double initial_temperature;    // benchmark config initial_temperature
+    int internal_thermal_source;   // 1: the packet's source channel feeds the transport
+    int packet_has_temperature;    // 1: the packet carries the temperature channel (>= 11 channels)
 } OracleD3Q27Params;
 
 }  // extern "C"
@@ -119,6 +133,7 @@ struct D3Q27Oracle {
 
     std::vector<T> f, f_post, rho, ux, uy, uz;
     std::vector<T> ref_ux, ref_uy, ref_uz, ref_p, temperature;
+    std::vector<T> temperature_next, ref_temperature, thermal_source;
     std::vector<T> force_x, force_y, force_z;  // optional per-cell force density
     std::vector<uint8_t> obstacle;
     bool initialized = false;
@@ -137,6 +152,9 @@ struct D3Q27Oracle {
         ref_ux.assign(cells, T(0)); ref_uy.assign(cells, T(0)); ref_uz.assign(cells, T(0));
         ref_p.assign(cells, T(0));
         temperature.assign(cells, T(0));
+        temperature_next.assign(cells, T(0));
+        ref_temperature.assign(cells, T(0));
+        thermal_source.assign(cells, T(0));
         obstacle.assign(cells, 0);
         force_x.clear(); force_y.clear(); force_z.clear();
     }
@@ -265,8 +283,96 @@ struct D3Q27Oracle {
                 f[di(cell, q)] = eq;
                 f_post[di(cell, q)] = eq;
             }
+            if (p.thermal_transport) {
+                // benchmark mode: a zero state takes initial_temperature, a
+                // non-zero fluid state the packet's reference temperature
+                if (std::fabs(temperature[cell]) < T(1e-8f)) temperature[cell] = clampv(T(float(p.initial_temperature)), t_min, t_max);
+                else if (!obstacle[cell]) temperature[cell] = clampv(ref_temperature[cell], t_min, t_max);
+                temperature[cell] = clampv(temperature[cell], t_min, t_max);
+                temperature_next[cell] = temperature[cell];
+            }
         }
         initialized = true;
+    }
+
+    // ---- temperature transport (native/src/aero_lbm_jni.cpp:738-769, 1783-1950, 2049-2143, 8037-8064)
+    T t_min = T(-1.0), t_max = T(1.0);
+    T thermal_neighbour(const std::vector<T>& field, int x, int y, int z, T self) const {
+        const int dims[3] = {nx, ny, nz};
+        int* c[3] = {&x, &y, &z};
+        for (int a = 0; a < 3; ++a) {
+            int& v = *c[a];
+            if (v >= 0 && v < dims[a]) continue;
+            const int face = v < 0 ? 2 * a : 2 * a + 1;
+            if (p.thermal_kind[face] != 2) continue;  // PERIODIC
+            v %= dims[a];
+            if (v < 0) v += dims[a];
+        }
+        const int face = oob_face(x, y, z);
+        if (face >= 0) {
+            switch (p.thermal_kind[face]) {
+                case 4: return clampv(T(float(p.face_temperature[face])), t_min, t_max);          // TEMPERATURE_DIRICHLET
+                case 5: return clampv(T(self + T(float(p.face_heat_flux[face]))), t_min, t_max);  // HEAT_FLUX_NEUMANN
+                default: return self;
+            }
+        }
+        const size_t cell = cell_index(x, y, z);
+        if (obstacle[cell]) return self;
+        return field[cell];
+    }
+    T sample_trilinear(const std::vector<T>& field, T x, T y, T z, T fallback) const {
+        const int x0 = int(std::floor(x)), y0 = int(std::floor(y)), z0 = int(std::floor(z));
+        const int x1 = x0 + 1, y1 = y0 + 1, z1 = z0 + 1;
+        const T fx = x - T(x0), fy = y - T(y0), fz = z - T(z0);
+        const T c000 = thermal_neighbour(field, x0, y0, z0, fallback);
+        const T c100 = thermal_neighbour(field, x1, y0, z0, fallback);
+        const T c010 = thermal_neighbour(field, x0, y1, z0, fallback);
+        const T c110 = thermal_neighbour(field, x1, y1, z0, fallback);
+        const T c001 = thermal_neighbour(field, x0, y0, z1, fallback);
+        const T c101 = thermal_neighbour(field, x1, y0, z1, fallback);
+        const T c011 = thermal_neighbour(field, x0, y1, z1, fallback);
+        const T c111 = thermal_neighbour(field, x1, y1, z1, fallback);
+        const T c00 = c000 + (c100 - c000) * fx;
+        const T c10 = c010 + (c110 - c010) * fx;
+        const T c01 = c001 + (c101 - c001) * fx;
+        const T c11 = c011 + (c111 - c011) * fx;
+        const T c0 = c00 + (c10 - c00) * fy;
+        const T c1 = c01 + (c11 - c01) * fy;
+        return c0 + (c1 - c0) * fz;
+    }
+    // Calls after the first: solid cells of this call hold no temperature
+    // (the runtime nudge toward the packet is zero in benchmark mode).
+    void apply_temperature_reference() {
+        if (!p.packet_has_temperature) return;
+        for (size_t cell = 0; cell < cells; ++cell)
+            if (obstacle[cell]) temperature[cell] = temperature_next[cell] = T(0);
+    }
+    // First-order semi-Lagrangian advection by the previous collision's
+    // velocity + explicit diffusion + source (benchmark branch, dt = 1).
+    void update_temperature() {
+        const T dt = T(1.0f), cooling = T(0.0f);
+        const T alpha = T(float(p.thermal_diffusivity));
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    const size_t cell = cell_index(x, y, z);
+                    if (obstacle[cell]) {
+                        temperature_next[cell] = T(0);
+                        continue;
+                    }
+                    const T tc = temperature[cell];
+                    const T adv = sample_trilinear(temperature, T(float(x)) - dt * ux[cell], T(float(y)) - dt * uy[cell],
+                                                   T(float(z)) - dt * uz[cell], tc);
+                    const T t_sum = thermal_neighbour(temperature, x + 1, y, z, tc) + thermal_neighbour(temperature, x - 1, y, z, tc) +
+                                    thermal_neighbour(temperature, x, y + 1, z, tc) + thermal_neighbour(temperature, x, y - 1, z, tc) +
+                                    thermal_neighbour(temperature, x, y, z + 1, tc) + thermal_neighbour(temperature, x, y, z - 1, tc);
+                    const T lap = t_sum - T(6.0f) * tc;
+                    const T src = p.internal_thermal_source ? clampv(thermal_source[cell], T(-0.006f), T(0.006f)) : T(0);
+                    const T t_next = adv + dt * (alpha * lap + src - cooling * adv);
+                    temperature_next[cell] = clampv(t_next, t_min, t_max);
+                }
+        temperature.swap(temperature_next);
+        temperature_next = temperature;
     }
 
     void reseed(size_t cell) {
@@ -538,6 +644,8 @@ struct D3Q27Oracle {
 
     void step() {
         if (!initialized) initialize();
+        else if (p.thermal_transport) apply_temperature_reference();
+        if (p.thermal_transport) update_temperature();
         collide();
         stream();
         ++steps_done;
@@ -561,7 +669,8 @@ void load_fields(D3Q27Oracle<T>& o, const uint8_t* obstacle, const float* ux, co
         const float pv = pressure ? pressure[c] : 0.0f;
         o.ref_p[c] = T(std::min(0.03f, std::max(-0.03f, pv)));
         const float tv = temperature ? temperature[c] : 0.0f;
-        o.temperature[c] = T(std::min(1.0f, std::max(-1.0f, tv)));
+        if (o.p.thermal_transport) o.ref_temperature[c] = T(std::min(1.0f, std::max(-1.0f, tv)));
+        else o.temperature[c] = T(std::min(1.0f, std::max(-1.0f, tv)));
     }
 }
 
@@ -603,6 +712,43 @@ int oracle_d3q27_set_fields(void* handle, const uint8_t* obstacle, const float* 
     if (!h) return 0;
     if (h->f32) load_fields(*h->f32, obstacle, ux, uy, uz, pressure, temperature);
     else load_fields(*h->f64, obstacle, ux, uy, uz, pressure, temperature);
+    return 1;
+}
+
+// Thermal source per cell (packet channel 9, clamped to +-0.006 like the
+// reference's ingest); null = zeros.
+int oracle_d3q27_set_thermal_source(void* handle, const float* src) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h) return 0;
+    auto run = [&](auto& o) {
+        using TT = typename std::decay_t<decltype(o.f)>::value_type;
+        for (size_t c = 0; c < o.cells; ++c)
+            o.thermal_source[c] = TT(src ? std::min(0.006f, std::max(-0.006f, src[c])) : 0.0f);
+    };
+    if (h->f32) run(*h->f32);
+    else run(*h->f64);
+    return 1;
+}
+
+// Temperature state (cells floats) with aero_lbm_{get,set}_temperature_state_rect
+// semantics (set clamps with min(1, max(-1, v)), native/src/aero_lbm_jni.cpp:8028-8035).
+int oracle_d3q27_get_temperature(void* handle, float* out) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !out) return 0;
+    if (h->f32) for (size_t c = 0; c < h->f32->cells; ++c) out[c] = h->f32->temperature[c];
+    else for (size_t c = 0; c < h->f64->cells; ++c) out[c] = float(h->f64->temperature[c]);
+    return 1;
+}
+int oracle_d3q27_set_temperature(void* handle, const float* in) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !in) return 0;
+    auto run = [&](auto& o) {
+        using TT = typename std::decay_t<decltype(o.f)>::value_type;
+        for (size_t c = 0; c < o.cells; ++c)
+            o.temperature[c] = o.temperature_next[c] = TT(std::min(1.0f, std::max(-1.0f, in[c])));
+    };
+    if (h->f32) run(*h->f32);
+    else run(*h->f64);
     return 1;
 }
 

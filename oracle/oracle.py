@@ -32,6 +32,8 @@ f32 = np.float32
 # Face kinds / flags (same numbering as the C ABI).
 PERIODIC, BOUNCE_BACK, MOVING_WALL, VELOCITY, PRESSURE, CONVECTIVE, SYMMETRY = 1, 2, 3, 4, 5, 6, 7
 INHERIT_GAME = 0
+# thermal face kinds (native/include/aero_lbm_capi.h:57-62)
+THERMAL_INHERIT, THERMAL_DISABLED, THERMAL_PERIODIC, THERMAL_ADIABATIC, THERMAL_DIRICHLET, THERMAL_NEUMANN = 0, 1, 2, 3, 4, 5
 FLAG_DISABLE_CONVECTIVE_OUTFLOW = 1 << 3
 FLAG_DISABLE_SGS = 1 << 5
 FLAG_DISABLE_BUOYANCY = 1 << 7
@@ -67,7 +69,14 @@ class OracleParams(ctypes.Structure):
         ("enable_buoyancy", ctypes.c_int),
         ("gravity_axis", ctypes.c_int),
         ("disable_convective_outflow", ctypes.c_int),
-        ("reserved", ctypes.c_int),
+        ("thermal_transport", ctypes.c_int),
+        ("thermal_kind", ctypes.c_int * 6),
+        ("face_temperature", ctypes.c_double * 6),
+        ("face_heat_flux", ctypes.c_double * 6),
+        ("thermal_diffusivity", ctypes.c_double),
+        ("initial_temperature", ctypes.c_double),
+        ("internal_thermal_source", ctypes.c_int),
+        ("packet_has_temperature", ctypes.c_int),
     ]
 
 
@@ -96,7 +105,10 @@ def derive_params(cfg: dict) -> OracleParams:
     1023-1031 (beta). ``cfg`` keys: reynolds, reference_length,
     initial_velocity, faces (list of 6 dicts: kind, velocity, pressure),
     sgs (bool), buoyancy (bool), smagorinsky_c, buoyancy_beta, gravity_axis,
-    body_force, disable_convective."""
+    body_force, disable_convective; temperature transport: thermal_transport
+    (bool, the reference's benchmark-mode scalar transport), initial_temperature,
+    thermal_source (bool), packet_channels; per face thermal (kind),
+    temperature, heat_flux."""
     faces = cfg["faces"]
     speed = _norm(cfg.get("initial_velocity", (0, 0, 0)))
     for fc in faces:
@@ -131,6 +143,15 @@ def derive_params(cfg: dict) -> OracleParams:
     p.enable_buoyancy = 1 if cfg.get("buoyancy", False) else 0
     p.gravity_axis = int(cfg.get("gravity_axis", 1))
     p.disable_convective_outflow = 1 if cfg.get("disable_convective", False) else 0
+    p.thermal_transport = 1 if cfg.get("thermal_transport", False) else 0
+    for i, fc in enumerate(faces):
+        p.thermal_kind[i] = int(fc.get("thermal", THERMAL_DISABLED))
+        p.face_temperature[i] = float(f32(fc.get("temperature", 0.0)))
+        p.face_heat_flux[i] = float(f32(fc.get("heat_flux", 0.0)))
+    p.thermal_diffusivity = float(f32(0.035))
+    p.initial_temperature = float(f32(cfg.get("initial_temperature", 0.0)))
+    p.internal_thermal_source = 1 if cfg.get("thermal_source", False) else 0
+    p.packet_has_temperature = 1 if int(cfg.get("packet_channels", 11)) > 10 else 0
     return p
 
 
@@ -157,6 +178,9 @@ class Oracle:
             lib.oracle_d3q27_extract_atlas.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
             lib.oracle_d3q27_macro.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.oracle_d3q27_get_f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.oracle_d3q27_set_thermal_source.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.oracle_d3q27_get_temperature.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.oracle_d3q27_set_temperature.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             cls._lib = lib
         return cls._lib
 
@@ -184,6 +208,20 @@ class Oracle:
         arrs = [self._p(obstacle, np.uint8)] + [self._p(v, np.float32) for v in (ux, uy, uz, pressure, temperature)]
         self._keep = [a for a, _ in arrs]
         self.lib().oracle_d3q27_set_fields(self.h, *[p for _, p in arrs])
+
+    def set_thermal_source(self, src):
+        arr, ptr = self._p(src, np.float32)
+        self._keep_src = arr
+        self.lib().oracle_d3q27_set_thermal_source(self.h, ptr)
+
+    def temperature(self) -> np.ndarray:
+        out = np.zeros(self.cells, dtype=np.float32)
+        self.lib().oracle_d3q27_get_temperature(self.h, out.ctypes.data)
+        return out
+
+    def set_temperature(self, t):
+        arr = np.ascontiguousarray(np.asarray(t, np.float32).reshape(-1))
+        self.lib().oracle_d3q27_set_temperature(self.h, arr.ctypes.data)
 
     def set_force_field(self, fx, fy, fz):
         arrs = [self._p(v, np.float32) for v in (fx, fy, fz)]
@@ -248,11 +286,15 @@ def config_struct(struct_type, cfg: dict, default_fn):
     flags = c.flags
     flags = (flags & ~FLAG_DISABLE_SGS) if cfg.get("sgs", False) else (flags | FLAG_DISABLE_SGS)
     flags = (flags & ~FLAG_DISABLE_BUOYANCY) if cfg.get("buoyancy", False) else (flags | FLAG_DISABLE_BUOYANCY)
-    flags |= 1 << 6  # DISABLE_INTERNAL_THERMAL_SOURCE
+    if not cfg.get("thermal_source", False):
+        flags |= 1 << 6  # DISABLE_INTERNAL_THERMAL_SOURCE
+    else:
+        flags &= ~(1 << 6)
     if cfg.get("disable_convective", False):
         flags |= FLAG_DISABLE_CONVECTIVE_OUTFLOW
     c.flags = flags
     c.reynolds_number = cfg.get("reynolds", 100.0)
+    c.initial_temperature = cfg.get("initial_temperature", 0.0)
     c.reference_length = cfg.get("reference_length", 1.0)
     for i, v in enumerate(cfg.get("initial_velocity", (0, 0, 0))):
         c.initial_velocity[i] = v
@@ -261,7 +303,9 @@ def config_struct(struct_type, cfg: dict, default_fn):
     for name, fc in zip(("x_min", "x_max", "y_min", "y_max", "z_min", "z_max"), cfg["faces"]):
         face = getattr(c, name)
         face.hydrodynamic_kind = int(fc.get("kind", INHERIT_GAME))
-        face.thermal_kind = 1
+        face.thermal_kind = int(fc.get("thermal", THERMAL_DISABLED))
+        face.temperature = fc.get("temperature", 0.0)
+        face.heat_flux = fc.get("heat_flux", 0.0)
         for a, v in enumerate(fc.get("velocity", (0, 0, 0))):
             face.velocity[a] = v
         face.pressure = fc.get("pressure", 0.0)
@@ -285,12 +329,19 @@ class RefLib:
         lib.aero_lbm_benchmark_set_config.argtypes = [ctypes.c_void_p]
         lib.aero_lbm_benchmark_set_config.restype = ctypes.c_int
         lib.aero_lbm_last_error.restype = ctypes.c_char_p
+        lib.aero_lbm_set_temperature_state_rect.argtypes = [ctypes.c_int] * 3 + [ctypes.c_longlong, ctypes.c_void_p]
+        lib.aero_lbm_set_temperature_state_rect.restype = ctypes.c_int
+        lib.aero_lbm_get_temperature_state_rect.argtypes = [ctypes.c_int] * 3 + [ctypes.c_longlong, ctypes.c_void_p]
+        lib.aero_lbm_get_temperature_state_rect.restype = ctypes.c_int
         lib.aero_lbm_runtime_info.restype = ctypes.c_char_p
         self.lib = lib
 
-    def run(self, dims, cfg: dict, packet: np.ndarray, steps: int, out_every: int | None = None, key: int = 1):
+    def run(self, dims, cfg: dict, packet: np.ndarray, steps: int, out_every: int | None = None, key: int = 1,
+            temperature_state: np.ndarray | None = None):
         """Initialise, configure and step; returns the final write_output
-        (cells x 4) from the last step."""
+        (cells x 4) from the last step. ``temperature_state``: loaded with
+        aero_lbm_set_temperature_state_rect before the first step. The
+        temperature state after the last step is left in ``self.temperature``."""
         nx, ny, nz = dims
         lib = self.lib
         if not lib.aero_lbm_init_rect(nx, ny, nz, packet.shape[1], 4):
@@ -298,12 +349,20 @@ class RefLib:
         c = config_struct(RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
         if not lib.aero_lbm_benchmark_set_config(ctypes.byref(c)):
             raise RuntimeError("set_config failed")
+        cells = nx * ny * nz
+        if temperature_state is not None:
+            t = np.ascontiguousarray(np.asarray(temperature_state, np.float32).reshape(-1))
+            if not lib.aero_lbm_set_temperature_state_rect(nx, ny, nz, key, t.ctypes.data):
+                raise RuntimeError(lib.aero_lbm_last_error())
         out = np.zeros(nx * ny * nz * 4, dtype=np.float32)
         pk = np.ascontiguousarray(packet, dtype=np.float32)
         for s in range(steps):
             want = (s + 1 == steps) or (out_every and (s + 1) % out_every == 0)
             if not lib.aero_lbm_step_rect(pk.ctypes.data, nx, ny, nz, key, out.ctypes.data if want else None):
                 raise RuntimeError(lib.aero_lbm_last_error())
+        self.temperature = np.zeros(cells, dtype=np.float32)
+        if not lib.aero_lbm_get_temperature_state_rect(nx, ny, nz, key, self.temperature.ctypes.data):
+            raise RuntimeError(lib.aero_lbm_last_error())
         return out.reshape(-1, 4)
 
 
@@ -331,7 +390,7 @@ def c1_config(tau: float = 0.55, u0: float = 0.05, sgs: bool = True) -> dict:
     }
 
 
-def packet_from(obstacle, ux, uy, uz, pressure=None, temperature=None, channels: int = 11) -> np.ndarray:
+def packet_from(obstacle, ux, uy, uz, pressure=None, temperature=None, channels: int = 11, source=None) -> np.ndarray:
     cells = obstacle.size
     pk = np.zeros((cells, channels), dtype=np.float32)
     pk[:, 0] = (obstacle.reshape(-1) != 0)
@@ -342,7 +401,35 @@ def packet_from(obstacle, ux, uy, uz, pressure=None, temperature=None, channels:
         pk[:, 8] = np.asarray(pressure, np.float32).reshape(-1)
     if temperature is not None and channels > 10:
         pk[:, 10] = np.asarray(temperature, np.float32).reshape(-1)
+    if source is not None and channels > 9:
+        pk[:, 9] = np.asarray(source, np.float32).reshape(-1)
     return pk
+
+
+def thermal_case(n: int = 12, seed: int = 11):
+    """Buoyancy with the reference's temperature transport on an n^3 brick:
+    8% random solids, u = (0.04,0,0) + U(-0.01,0.01), packet temperature
+    U(-0.3,0.3) and source U(-0.01,0.01), every thermal face kind (Dirichlet
+    0.2 / -0.4, Neumann 0.05, periodic y, adiabatic ground), initial
+    temperature 0.1, temperature state preloaded with 0.5 (so that fluid cells
+    start from the packet's temperature). Returns obstacle, (ux, uy, uz),
+    temperature, source, the config dict and the preload."""
+    rng = np.random.default_rng(seed)
+    dims = (n, n, n)
+    obst = (rng.random(dims) < 0.08).astype(np.uint8)
+    u = (np.float32(0.04) + rng.uniform(-0.01, 0.01, dims).astype(np.float32),
+         rng.uniform(-0.01, 0.01, dims).astype(np.float32), rng.uniform(-0.01, 0.01, dims).astype(np.float32))
+    temp = rng.uniform(-0.3, 0.3, dims).astype(np.float32)
+    src = rng.uniform(-0.01, 0.01, dims).astype(np.float32)
+    faces = [{"kind": VELOCITY, "velocity": (0.04, 0, 0), "thermal": THERMAL_DIRICHLET, "temperature": 0.2},
+             {"kind": PRESSURE, "pressure": 0.001, "thermal": THERMAL_NEUMANN, "heat_flux": 0.05},
+             {"kind": PERIODIC, "thermal": THERMAL_PERIODIC}, {"kind": PERIODIC, "thermal": THERMAL_PERIODIC},
+             {"kind": BOUNCE_BACK, "thermal": THERMAL_ADIABATIC},
+             {"kind": MOVING_WALL, "velocity": (0.03, 0, 0), "thermal": THERMAL_DIRICHLET, "temperature": -0.4}]
+    cfg = {"reynolds": 60.0, "initial_velocity": (0.04, 0.0, 0.0), "faces": faces, "sgs": True, "buoyancy": True,
+           "thermal_transport": True, "initial_temperature": 0.1, "thermal_source": True}
+    preload = np.full(n ** 3, 0.5, np.float32)
+    return obst, u, temp, src, cfg, preload
 
 
 def rel_err(a: np.ndarray, b: np.ndarray) -> float:

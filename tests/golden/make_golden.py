@@ -18,6 +18,13 @@ Fixtures:
                   12 x 8 x 10 (y up), seeded 25-channel forcing (seed 5,
                   terrain up to 3 cells, wind (6, 0, 3) m/s), dx 64 m,
                   dt 5 s; the 6-channel state after 30 calls.
+  thermal_12_20.npz buoyancy on with the reference's temperature transport:
+                  oracle.thermal_case(12, seed 11) (every thermal face kind,
+                  packet source channel, state preloaded), 20 steps; the
+                  write_output result and the temperature state.
+
+`python tests/golden/make_golden.py thermal` regenerates only the fixtures
+whose name contains "thermal" (any substring filter works).
 """
 from __future__ import annotations
 
@@ -63,9 +70,24 @@ def tunnel_case(n: int = 16):
     return obst, (ux, zero, zero.copy()), cfg
 
 
+def thermal_fixture(ref) -> None:
+    n, seed, steps = 12, 11, 20
+    obst, u, temp, src, cfg, preload = O.thermal_case(n, seed)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+    out = ref.run((n, n, n), cfg, pk, steps, temperature_state=preload)
+    np.savez_compressed(OUT / "thermal_12_20.npz", out=out, temperature=ref.temperature, seed=seed, n=n, steps=steps,
+                        input_sha256=digest(pk, preload))
+    print("thermal_12_20 written")
+
+
 def main() -> int:
     O.build(ref=True)
     ref = O.RefLib()
+    only = sys.argv[1] if len(sys.argv) > 1 else ""
+    if only:
+        if only in "thermal_12_20":
+            thermal_fixture(ref)
+        return 0
     for name, n, steps in (("c1_16_200", 16, 200), ("c1_32_1000", 32, 1000)):
         seed = 1234
         obst, u = O.c1_inputs(seed=seed, n=n)
@@ -87,6 +109,7 @@ def main() -> int:
     np.savez_compressed(OUT / "meso_12x8x10_30.npz", out=out, seed=seed, dims=np.array(dims), steps=steps,
                         input_sha256=digest(forcing))
     print("meso_12x8x10_30 written")
+    thermal_fixture(ref)
     return 0
 
 

@@ -84,3 +84,43 @@ def test_oracle_f64_is_the_same_scheme():
         o.set_fields(obst, *u)
         o.step(50)
     assert O.rel_err(a.macro()[:, 1:], b.macro()[:, 1:]) < 1e-5
+
+
+def _thermal_oracle(n, seed, steps, precision="f32"):
+    obst, u, temp, src, cfg, preload = O.thermal_case(n, seed)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), precision)
+    o.set_temperature(preload)
+    o.set_fields(obst, *u, temperature=temp)
+    o.set_thermal_source(src)
+    o.step(steps)
+    return o
+
+
+def test_oracle_thermal_transport_matches_golden():
+    """Buoyancy driven by the reference's benchmark-mode temperature transport
+    (advection by the previous collision's velocity, diffusion, packet source,
+    Dirichlet / Neumann / periodic / adiabatic thermal faces): flow output and
+    temperature state bit-identical to the reference library's fixture."""
+    g = np.load(GOLDEN / "thermal_12_20.npz")
+    o = _thermal_oracle(int(g["n"]), int(g["seed"]), int(g["steps"]))
+    assert _bits_equal(o.output(), g["out"])
+    assert _bits_equal(o.temperature(), g["temperature"])
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("preload,source", [(False, False), (True, True)])
+def test_oracle_thermal_transport_matches_reference_live(preload, source):
+    n, steps = 10, 15
+    obst, u, temp, src, cfg, pre = O.thermal_case(n, seed=23)
+    cfg = dict(cfg, thermal_source=source)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+    ref = O.RefLib()
+    out = ref.run((n, n, n), cfg, pk, steps, temperature_state=pre if preload else None)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+    if preload:
+        o.set_temperature(pre)
+    o.set_fields(obst, *u, temperature=temp)
+    o.set_thermal_source(src)
+    o.step(steps)
+    assert _bits_equal(o.output(), out)
+    assert _bits_equal(o.temperature(), ref.temperature)
