@@ -225,6 +225,7 @@ SIGNATURES = {
     "aero_lbm_b200_set_collision_mode": (_I, [_I]),
     "aero_lbm_b200_set_cells_per_thread": (_I, [_I]),
     "aero_lbm_b200_set_streamed_step": (_I, [_I]),
+    "aero_lbm_b200_set_thermal_transport": (_I, [_I]),
     "aero_lbm_b200_set_fp16_format": (_I, [_I]),
     "aero_lbm_b200_conservation_sums": (_I, [_LL, ctypes.POINTER(ctypes.c_double)]),
     "aero_lbm_b200_conservation_sums_noalloc": (_I, [_LL, ctypes.POINTER(ctypes.c_double)]),
@@ -405,6 +406,18 @@ class LbmContext:
         if not self.lib.aero_lbm_get_flow_state_rect(*self.dims, self.key, fptr(out)):
             raise RuntimeError(f"get_flow_state failed: {last_error(self.lib)}")
         return out.reshape(self.cells, 4)
+
+    def temperature_state(self) -> np.ndarray:
+        """The context's temperature state (cells floats)."""
+        out = np.zeros(self.cells, dtype=np.float32)
+        if not self.lib.aero_lbm_get_temperature_state_rect(*self.dims, self.key, fptr(out)):
+            raise RuntimeError(f"get_temperature_state failed: {last_error(self.lib)}")
+        return out
+
+    def set_temperature_state(self, t) -> None:
+        arr = np.ascontiguousarray(np.asarray(t, np.float32).reshape(-1))
+        if not self.lib.aero_lbm_set_temperature_state_rect(*self.dims, self.key, fptr(arr)):
+            raise RuntimeError(f"set_temperature_state failed: {last_error(self.lib)}")
 
     def set_force_field(self, fx, fy, fz) -> None:
         soa = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float32).reshape(-1) for a in (fx, fy, fz)]))

@@ -54,6 +54,16 @@ class BrickCase:
             "gravity_axis": self.gravity_axis,
         }
 
+    def temperature_state(self) -> np.ndarray | None:
+        """Temperature state to load (aero_lbm_set_temperature_state_rect)
+        before the first step. With the temperature transport, the first call
+        keeps a non-zero state's fluid cells at the packet's temperature
+        (otherwise every cell starts at the configured initial temperature),
+        so loading the case's field makes the run start from it."""
+        if self.temperature is None:
+            return None
+        return np.ascontiguousarray(self.temperature.reshape(-1), dtype=np.float32)
+
     def packet(self, channels: int = 11) -> np.ndarray:
         pk = np.zeros((self.cells, channels), dtype=np.float32)
         pk[:, 0] = (self.obstacle.reshape(-1) != 0)

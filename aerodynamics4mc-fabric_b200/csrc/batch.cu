@@ -71,7 +71,7 @@ __device__ __forceinline__ void batch_cell(const BrickDesc& b, int cell) {
             const long long cells = (long long)G.nx * G.ny * G.nz;
             const int wrap_mask = G.wrap[0] | (G.wrap[1] << 1) | (G.wrap[2] << 2);
             reseed_push_ip<S>(f, b.ref, b.ref + cells, b.ref + 2 * cells, b.ref + 3 * cells, b.cp.max_speed,
-                              b.sc.scale, cell, x, y, z, G.nx, G.ny, G.nz, wrap_mask, kParity);
+                              b.sc.scale, cell, x, y, z, G.nx, G.ny, G.nz, wrap_mask, kParity, nullptr);
             return;
         }
     }
@@ -122,7 +122,8 @@ __device__ __forceinline__ void batch_pair(const BrickDesc& b, int cell0) {
         }
     }
     bool ok[2];
-    collide27_x2(fl, b.cp, f2(0.0f), f2(0.0f), f2(0.0f), f2(0.0f), ok);
+    F2 uc[3];
+    collide27_x2(fl, b.cp, f2(0.0f), f2(0.0f), f2(0.0f), f2(0.0f), ok, uc);
     const bool st0 = live0 && ok[0], st1 = live1 && ok[1];
     if (live0 && !ok[0] || live1 && !ok[1]) {
         const long long cells = (long long)G.nx * G.ny * G.nz;
@@ -130,7 +131,7 @@ __device__ __forceinline__ void batch_pair(const BrickDesc& b, int cell0) {
         for (int k = 0; k < 2; ++k)
             if ((k == 0 ? live0 && !ok[0] : live1 && !ok[1]))
                 reseed_push_ip<S>(f, b.ref, b.ref + cells, b.ref + 2 * cells, b.ref + 3 * cells, b.cp.max_speed, b.sc.scale,
-                                  cell0 + k, x, y, z0 + k, G.nx, G.ny, G.nz, wrap_mask, kParity);
+                                  cell0 + k, x, y, z0 + k, G.nx, G.ny, G.nz, wrap_mask, kParity, nullptr);
     }
     if (flat) {
 #pragma unroll

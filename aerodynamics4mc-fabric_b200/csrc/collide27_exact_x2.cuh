@@ -105,7 +105,7 @@ __device__ __forceinline__ X2 feq2x(const Mul2& M, int q, X2 rho, X2 ux, X2 uy, 
 // Collide two fluid cells in place; ok[k] = false: lane k's input was not
 // finite (its result is meaningless; the caller reseeds that cell).
 __device__ __forceinline__ void collide27_exact_x2_impl(X2 (&f)[27], const CollideParams& P, X2 temp, X2 cfx, X2 cfy,
-                                                        X2 cfz, bool (&ok)[2]) {
+                                                        X2 cfz, bool (&ok)[2], X2 (&u)[3]) {
     const Mul2 M = make_mul2(P.zero_bits);
     bool bad0 = false, bad1 = false;
 #pragma unroll
@@ -171,6 +171,9 @@ __device__ __forceinline__ void collide27_exact_x2_impl(X2 (&f)[27], const Colli
         }
     }
 
+    u[0] = ux;
+    u[1] = uy;
+    u[2] = uz;
     const X2 r200 = qsum2<2, 0, 0>(f), r020 = qsum2<0, 2, 0>(f), r002 = qsum2<0, 0, 2>(f);
     const X2 r110 = qsum2<1, 1, 0>(f), r101 = qsum2<1, 0, 1>(f), r011 = qsum2<0, 1, 1>(f);
 
@@ -335,15 +338,19 @@ __device__ __forceinline__ void collide27_exact_x2_impl(X2 (&f)[27], const Colli
     }
 }
 
-// Entry point on the step kernels' packed type.
+// Entry point on the step kernels' packed type; u: the velocity each lane's
+// collision used (post-clamp midpoint velocity).
 __device__ __forceinline__ void collide27_exact_x2(F2 (&f)[27], const CollideParams& P, F2 temp, F2 cfx, F2 cfy, F2 cfz,
-                                                   bool (&ok)[2]) {
-    X2 g[27];
+                                                   bool (&ok)[2], F2 (&u)[3]) {
+    X2 g[27], v[3];
 #pragma unroll
     for (int q = 0; q < 27; ++q) g[q] = X2{f[q].v};
-    collide27_exact_x2_impl(g, P, X2{temp.v}, X2{cfx.v}, X2{cfy.v}, X2{cfz.v}, ok);
+    collide27_exact_x2_impl(g, P, X2{temp.v}, X2{cfx.v}, X2{cfy.v}, X2{cfz.v}, ok, v);
 #pragma unroll
     for (int q = 0; q < 27; ++q) f[q] = F2{g[q].v};
+    u[0] = F2{v[0].v};
+    u[1] = F2{v[1].v};
+    u[2] = F2{v[2].v};
 }
 
 }  // namespace exact

@@ -116,9 +116,10 @@ __device__ __forceinline__ void back_line_odd_x2(F2 m1, F2 u, F2& fm, F2& f0, F2
 // Collide two fluid cells (lanes x and y of every F2) in place. temp: the
 // cells' temperatures (read when buoyancy is on); cf*: extra force densities.
 // ok[k] = false: lane k's input was not finite; its populations are then
-// meaningless and the caller reseeds that cell.
+// meaningless and the caller reseeds that cell. u: the velocity the
+// collision used (midpoint velocity after the speed clamp), per lane.
 __device__ __forceinline__ void collide27_x2(F2 (&f)[27], const CollideParams& P, F2 temp, F2 cfx, F2 cfy, F2 cfz,
-                                             bool (&ok)[2]) {
+                                             bool (&ok)[2], F2 (&u)[3]) {
     F2 r000, r100, r010, r001, r200, r020, r002, r110, r101, r011;
     raw_moments27_x2(f, r000, r100, r010, r001, r200, r020, r002, r110, r101, r011);
     const F2 rho = r000;
@@ -150,6 +151,9 @@ __device__ __forceinline__ void collide27_x2(F2 (&f)[27], const CollideParams& P
         uy = uy * sc;
         uz = uz * sc;
     }
+    u[0] = ux;
+    u[1] = uy;
+    u[2] = uz;
 
     // second-order central moments about u (binomial shift of the raw moments)
     const F2 c200 = fma2(ux * ux, rho, fma2(f2(-2.0f) * ux, r100, r200));

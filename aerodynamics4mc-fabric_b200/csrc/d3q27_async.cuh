@@ -295,7 +295,14 @@ __global__ void __launch_bounds__(kIpaWarps * 32, AERO_IPA_MIN_BLOCKS)
         if (t + nw < tiles)
             ipa_post<S, kParity, AERO_IPA_BULK>(f, G, a.flags_prev, a.obstacle_cur, temp_src, a.force.fx, a.force.fy,
                                                 a.force.fz, wbuf, bar, t + nw, tiles_per_line, lane);
-        if (!live0 && !live1) continue;
+        if (!live0 && !live1) {
+            if (a.cur.u_last) {
+                const long long c0 = ((long long)p.x * G.ny + p.y) * G.nz + z0;
+                if (in0) record_u(a.cur, c0, 0.0f, 0.0f, 0.0f);
+                if (in1) record_u(a.cur, c0 + 1, 0.0f, 0.0f, 0.0f);
+            }
+            continue;
+        }
 
         const int x = p.x, y = p.y;
         const long long cell0 = ((long long)x * G.ny + y) * G.nz + z0;
@@ -330,7 +337,10 @@ __global__ void __launch_bounds__(kIpaWarps * 32, AERO_IPA_MIN_BLOCKS)
             }
         }
         bool ok[2];
-        collide27_x2(fl, a.cp, t2, cfx, cfy, cfz, ok);
+        F2 uc[3];
+        collide27_x2(fl, a.cp, t2, cfx, cfy, cfz, ok, uc);
+        record_u2(a.cur, cell0, in1, live0 && !pass0 && ok[0], live1 && !pass1 && ok[1], live0 && !ok[0] && !pass0,
+                  live1 && !ok[1] && !pass1, uc);
         if (pass0 || pass1) {
             const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
             const NeighbourOffsets o1 = neighbour_offsets(G, x, y, in1 ? z0 + 1 : z0);

@@ -109,9 +109,15 @@ template <class S>
 static __device__ __noinline__ void reseed_push_ip(typename S::T* __restrict__ f, const float* ref_p, const float* ref_ux,
                                                     const float* ref_uy, const float* ref_uz, float max_speed,
                                                     float fp16_scale, long long cell, int x, int y, int z, int nx,
-                                                    int ny, int nz, int wrap_mask, int parity) {
+                                                    int ny, int nz, int wrap_mask, int parity, float* u_last) {
     float rho, ux, uy, uz;
     reseed_state(ReseedSource{ref_p, ref_ux, ref_uy, ref_uz, cell}, max_speed, rho, ux, uy, uz);
+    if (u_last) {
+        const long long cells = (long long)nx * ny * nz;
+        u_last[cell] = ux;
+        u_last[cells + cell] = uy;
+        u_last[2 * cells + cell] = uz;
+    }
     const PadGeom g = make_pad_geom(nx, ny, nz, wrap_mask);
     const NeighbourOffsets o = neighbour_offsets(g, x, y, z);
     const int own = pad_index(g, x, y, z);
@@ -129,7 +135,19 @@ __device__ __forceinline__ void reseed_push(typename S::T* f, const IpArgs& a, l
                                             int parity) {
     const int wrap_mask = a.g.wrap[0] | (a.g.wrap[1] << 1) | (a.g.wrap[2] << 2);
     reseed_push_ip<S>(f, a.cur.ref_p, a.cur.ref_ux, a.cur.ref_uy, a.cur.ref_uz, a.cp.max_speed, a.sc.scale, cell, x, y,
-                      z, a.g.nx, a.g.ny, a.g.nz, wrap_mask, parity);
+                      z, a.g.nx, a.g.ny, a.g.nz, wrap_mask, parity, a.cur.u_last);
+}
+
+// Velocities a two-cell step leaves for the temperature transport: the
+// collision's on collided lanes, 0 on lanes that are solid now or were at
+// the streaming call (a reseeded lane records its own in reseed_push; a
+// cell that opened up is recorded by the transition kernel).
+__device__ __forceinline__ void record_u2(const CellFields& c, long long cell0, bool has1, bool col0, bool col1,
+                                          bool reseed0, bool reseed1, const F2 (&u)[3]) {
+    if (!c.u_last) return;
+    if (!reseed0) record_u(c, cell0, col0 ? u[0].v.x : 0.0f, col0 ? u[1].v.x : 0.0f, col0 ? u[2].v.x : 0.0f);
+    if (has1 && !reseed1)
+        record_u(c, cell0 + 1, col1 ? u[0].v.y : 0.0f, col1 ? u[1].v.y : 0.0f, col1 ? u[2].v.y : 0.0f);
 }
 
 // Fused pull-stream + collide + push of one step. Sources outside
@@ -161,7 +179,10 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
     long long cell;
     if (!line_cell(G, x, y, z, cell)) return;
     const uint32_t w = a.flags_prev[cell];
-    if (w & kFlagSelfSolid) return;  // memory of a solid cell is link storage; transitions run separately
+    if (w & kFlagSelfSolid) {  // memory of a solid cell is link storage; transitions run separately
+        record_u(a.cur, cell, 0.0f, 0.0f, 0.0f);
+        return;
+    }
     const int own = pad_index(G, x, y, z);
     const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
     float fl[27];
@@ -171,6 +192,7 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
         incoming_slot(o, own, q, kParity, (w >> q) & 1u, c, d);
         fl[q] = S::load(f + (d * G.pcells + c), q, a.sc);
     }
+    if (a.obstacle_cur[cell]) record_u(a.cur, cell, 0.0f, 0.0f, 0.0f);
     if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
         reseed_push<S>(f, a, cell, x, y, z, kParity);
         return;
@@ -254,7 +276,13 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
     const uint32_t w0 = a.flags_prev[cell0];
     const uint32_t w1 = has1 ? a.flags_prev[cell0 + 1] : kFlagSelfSolid;
     const bool live0 = !(w0 & kFlagSelfSolid), live1 = !(w1 & kFlagSelfSolid);
-    if (!live0 && !live1) return;
+    if (!live0 && !live1) {
+        if (a.cur.u_last) {
+            record_u(a.cur, cell0, 0.0f, 0.0f, 0.0f);
+            if (has1) record_u(a.cur, cell0 + 1, 0.0f, 0.0f, 0.0f);
+        }
+        return;
+    }
     const bool pass0 = live0 && a.obstacle_cur[cell0] != 0;
     const bool pass1 = live1 && a.obstacle_cur[cell0 + 1] != 0;
     const int own0 = pad_index(G, x, y, z0);
@@ -287,8 +315,11 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
         cfz = f2(a.force.fz[cell0], has1 ? a.force.fz[cell0 + 1] : 0.0f);
     }
     bool ok[2];
-    if (kExact) exact::collide27_exact_x2(fl, a.cp, t, cfx, cfy, cfz, ok);
-    else collide27_x2(fl, a.cp, t, cfx, cfy, cfz, ok);
+    F2 uc[3];
+    if (kExact) exact::collide27_exact_x2(fl, a.cp, t, cfx, cfy, cfz, ok, uc);
+    else collide27_x2(fl, a.cp, t, cfx, cfy, cfz, ok, uc);
+    record_u2(a.cur, cell0, has1, live0 && !pass0 && ok[0], live1 && !pass1 && ok[1], live0 && !ok[0] && !pass0,
+              live1 && !ok[1] && !pass1, uc);
     if (pass0 || pass1) {
         const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
         const NeighbourOffsets o1 = neighbour_offsets(G, x, y, has1 ? z0 + 1 : z0);
@@ -408,7 +439,10 @@ __global__ void __launch_bounds__(128) init_ip_kernel(typename S::T* __restrict_
     const long long cells = (long long)G.nx * G.ny * G.nz;
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= cells) return;
-    if (a.cur.obstacle[cell]) return;
+    if (a.cur.obstacle[cell]) {
+        record_u(a.cur, cell, 0.0f, 0.0f, 0.0f);
+        return;
+    }
     int x, y, z;
     cell_coords(G, cell, x, y, z);
     const int own = pad_index(G, x, y, z);

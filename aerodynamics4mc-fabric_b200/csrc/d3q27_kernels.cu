@@ -33,7 +33,15 @@ __global__ void ingest_packet_kernel(const float* __restrict__ packet, int in_ch
     out.ref_uz[cell] = isfinite(vz) ? vz : 0.0f;
     out.ref_p[cell] = clampf_dev(p[kChStateP], -0.03f, 0.03f);
     const float t = in_ch > kChStateTemp ? p[kChStateTemp] : 0.0f;
-    out.temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
+    if (out.ref_temperature) {
+        // transported temperature: the packet's field is the reference
+        // temperature, channel 9 the source (ingest_payload, jni.cpp:1683-1693)
+        out.ref_temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
+        const float src = in_ch > kChThermalSource ? p[kChThermalSource] : 0.0f;
+        out.thermal_source[cell] = clampf_dev(src, -0.006f, 0.006f);
+    } else {
+        out.temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
+    }
 }
 
 cudaError_t launch_ingest_packet(const float* packet, int in_channels, BrickDims d, CellFields out, cudaStream_t stream) {

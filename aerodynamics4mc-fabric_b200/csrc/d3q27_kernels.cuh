@@ -45,8 +45,23 @@ struct CellFields {
     float* ref_uy;
     float* ref_uz;
     float* ref_p;         // clamped pressure proxy
-    float* temperature;   // clamped reference temperature (static buoyancy field)
+    float* temperature;   // temperature the collision's buoyancy reads (the transported state, or the packet's field)
+    // Temperature transport (null when it is off): the packet's temperature
+    // and source channels, and the velocity every collision leaves per cell
+    // (SoA ux, uy, uz; 0 on solid cells) for the next call's advection.
+    float* ref_temperature = nullptr;
+    float* thermal_source = nullptr;
+    float* u_last = nullptr;
+    long long cells = 0;  // SoA stride of u_last
 };
+
+// Velocity a collision leaves for the next call's temperature advection.
+__device__ __forceinline__ void record_u(const CellFields& c, long long cell, float ux, float uy, float uz) {
+    if (!c.u_last) return;
+    c.u_last[cell] = ux;
+    c.u_last[c.cells + cell] = uy;
+    c.u_last[2 * c.cells + cell] = uz;
+}
 
 struct ForceField {
     const float* fx;      // optional per-cell force density (SoA); null = none

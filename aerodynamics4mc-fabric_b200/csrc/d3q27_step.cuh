@@ -35,8 +35,10 @@ __device__ __forceinline__ bool collide_cell(float (&f)[27], const CollideParams
     const float cfx = force.fx ? force.fx[cell] : 0.0f;
     const float cfy = force.fy ? force.fy[cell] : 0.0f;
     const float cfz = force.fz ? force.fz[cell] : 0.0f;
-    if (kExact) return exact::collide27_exact(f, cp, cur.temperature + cell, cfx, cfy, cfz, o);
-    return collide27(f, cp, cur.temperature + cell, cfx, cfy, cfz, o);
+    const bool ok = kExact ? exact::collide27_exact(f, cp, cur.temperature + cell, cfx, cfy, cfz, o)
+                           : collide27(f, cp, cur.temperature + cell, cfx, cfy, cfz, o);
+    if (ok) record_u(cur, cell, o.ux, o.uy, o.uz);
+    return ok;
 }
 
 // Reseed a cell into the two-buffer state (out of line: rare path).
@@ -44,6 +46,7 @@ static __device__ __noinline__ void reseed_store_ab(float* __restrict__ g_out, l
                                                      CellFields cur, float max_speed) {
     float rho, ux, uy, uz;
     reseed_state(ReseedSource{cur.ref_p, cur.ref_ux, cur.ref_uy, cur.ref_uz, cell}, max_speed, rho, ux, uy, uz);
+    record_u(cur, cell, ux, uy, uz);
 #pragma unroll 1
     for (int q = 0; q < 27; ++q) g_out[(long long)q * cells + cell] = feq27(q, rho, ux, uy, uz);
 }
@@ -180,6 +183,7 @@ __global__ void __launch_bounds__(128) init_collide_kernel(int nx, int ny, int n
     }
 #pragma unroll
     for (int q = 0; q < 27; ++q) f[q] = feq27(q, rho, ux, uy, uz);
+    if (solid) record_u(cur, cell, 0.0f, 0.0f, 0.0f);
     if (!solid && !collide_cell<kExact>(f, cp, cur, force, cell)) {
         reseed_store_ab(g_out, cells, cell, cur, cp.max_speed);
         return;
@@ -215,6 +219,7 @@ __global__ void __launch_bounds__(128) step_ab_kernel(int nx, int ny, int nz, co
     float f[27];
     const PullView v{g_in, obstacle_prev, ref_p_prev, F, cells, nx, ny, nz};
     pull27(v, flags_prev[cell], cell, x, y, z, f);
+    if (cur.obstacle[cell]) record_u(cur, cell, 0.0f, 0.0f, 0.0f);
     if (!cur.obstacle[cell] && !collide_cell<kExact>(f, cp, cur, force, cell)) {
         reseed_store_ab(g_out, cells, cell, cur, cp.max_speed);
         return;

@@ -22,6 +22,7 @@
 #include "ip_launch.h"
 #include "conservation.cuh"
 #include "runtime_internal.h"
+#include "thermal.cuh"
 
 namespace aero {
 
@@ -44,6 +45,7 @@ struct TimingStats {
 
 RuntimeConfig g_cfg;
 std::recursive_mutex g_mutex;  // guards every entry point (the caller is one worker thread)
+int g_thermal_mode = -1;      // temperature transport: -1 with buoyancy, 0 never (packet field), 1 always
 int g_streamed_step = 0;      // factorised two-cell in-place step: bulk-copy streamed kernel where eligible (opt-in)
 int g_cells_per_thread = 2;    // in-place step: 1 one cell per thread, 2 two cells per thread (packed collision)
 int g_fp16_format = 0;         // 16-bit storage: 0 IEEE half deviations, 1 fixed-point deviations
@@ -84,6 +86,7 @@ constexpr float kSgsNutToNu0Max = 5.0f;
 constexpr float kSgsBulkCoupling = 0.30f;
 constexpr float kBoussinesqBeta = 9.81f * (1.0f / 300.0f) * 20.0f * ((1.0f / 20.0f) * (1.0f / 20.0f) / 1.0f);
 constexpr float kBoussinesqForceMax = 0.02f;
+constexpr float kThermalDiffusivity = 0.035f;  // benchmark-mode scalar diffusivity (jni.cpp:154)
 constexpr float kMaxSpeed = 0.57735026919f * 0.60f;
 constexpr uint32_t kKnownFlags = 0xffu;
 
@@ -393,6 +396,11 @@ void Context::release_device() {
     fr(reinterpret_cast<void*&>(ref_uy));
     fr(reinterpret_cast<void*&>(ref_uz));
     fr(reinterpret_cast<void*&>(temperature));
+    fr(reinterpret_cast<void*&>(temperature_next));
+    fr(reinterpret_cast<void*&>(ref_temperature));
+    fr(reinterpret_cast<void*&>(thermal_source));
+    fr(reinterpret_cast<void*&>(u_last));
+    thermal = false;
     fr(reinterpret_cast<void*&>(packet));
     fr(reinterpret_cast<void*&>(out));
     fr(reinterpret_cast<void*&>(force));
@@ -424,8 +432,9 @@ bool Context::allocate(int nx_, int ny_, int nz_) {
     ok = ok && al(reinterpret_cast<void**>(&ref_uy), c * sizeof(float));
     ok = ok && al(reinterpret_cast<void**>(&ref_uz), c * sizeof(float));
     ok = ok && al(reinterpret_cast<void**>(&temperature), c * sizeof(float));
+    ok = ok && cuda_ok(cudaMemsetAsync(temperature, 0, c * sizeof(float), current_stream()), "cudaMemset(temperature)");
     ok = ok && al(reinterpret_cast<void**>(&fault), sizeof(int));
-    ok = ok && cuda_ok(cudaMemset(fault, 0, sizeof(int)), "cudaMemset(fault)");
+    ok = ok && cuda_ok(cudaMemsetAsync(fault, 0, sizeof(int), current_stream()), "cudaMemset(fault)");
     if (!ok) {
         release_device();
         return false;
@@ -439,7 +448,14 @@ bool Context::allocate(int nx_, int ny_, int nz_) {
 }
 
 CellFields Context::fields(int s) const {
-    return CellFields{obstacle[s], ref_ux, ref_uy, ref_uz, ref_p[s], temperature};
+    CellFields c{obstacle[s], ref_ux, ref_uy, ref_uz, ref_p[s], temperature};
+    if (thermal) {
+        c.ref_temperature = ref_temperature;
+        c.thermal_source = thermal_source;
+        c.u_last = u_last;
+        c.cells = cells;
+    }
+    return c;
 }
 
 ForceField Context::force_field() const {
@@ -593,12 +609,47 @@ static bool classify(Context& ctx, int slot, const FaceParams& face, const Brick
     return cuda_ok(launch_build_flags(ctx.obstacle[slot], d, face, ctx.flags[slot], s), "build_flags");
 }
 
+// Temperature transport arrays of a context (allocated on first use).
+static bool ensure_thermal(Context& ctx) {
+    if (ctx.u_last) return true;
+    const size_t c = (size_t)ctx.cells;
+    auto al = [&](float** p, size_t n) {
+        return cuda_ok(cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(float) + kCopySlack), "cudaMalloc(thermal)") &&
+               cuda_ok(cudaMemsetAsync(*p, 0, n * sizeof(float), current_stream()), "cudaMemset(thermal)");
+    };
+    return al(&ctx.temperature_next, c) && al(&ctx.ref_temperature, c) && al(&ctx.thermal_source, c) &&
+           al(&ctx.u_last, 3 * c);
+}
+
+// Thermal faces and diffusivity of the benchmark configuration
+// (effective_thermal_diffusivity, jni.cpp:966-972).
+static ThermalFaces current_thermal_faces() {
+    ThermalFaces t{};
+    for (int i = 0; i < 6; ++i) {
+        const auto& c = face_cfg(i);
+        t.kind[i] = c.thermal_kind;
+        t.temperature[i] = c.temperature;
+        t.heat_flux[i] = c.heat_flux;
+    }
+    return t;
+}
+static float thermal_diffusivity() {
+    if (!heated_cavity()) return kThermalDiffusivity;
+    const float pr = std::max(1.0e-6f, finite_or(g_bench.prandtl_number, 0.71f));
+    return base_nu_shear() / pr;
+}
+
 // One step of a context. packet may be null (cached step); out may be null.
 bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet) {
     cudaStream_t s = current_stream();
     const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
     const FaceParams face_now = current_face_params();
     const CollideParams cp = current_collide_params();
+    // The reference updates the temperature before every collision
+    // (run_cpu_step, jni.cpp:8480-8507); it reaches the flow through the
+    // buoyancy force.
+    ctx.thermal = g_thermal_mode == 1 || (g_thermal_mode == -1 && cp.enable_buoyancy);
+    if (ctx.thermal && !ensure_thermal(ctx)) return false;
     const int in_ch = g_cfg.input_channels;
     const bool have_packet = packet != nullptr;
     if (!have_packet && !ctx.has_inputs) {
@@ -637,6 +688,24 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     }
 
     if (!ctx.initialized && !choose_layout(ctx, face_now, packet, host_packet)) return false;
+    if (ctx.thermal) {
+        if (!ctx.initialized) {
+            const ThermalInitArgs ti{ctx.cells, ctx.temperature, ctx.u_last, ctx.obstacle[new_slot], ctx.ref_temperature,
+                                     ctx.ref_ux, ctx.ref_uy, ctx.ref_uz, g_bench.initial_temperature, bench_active() ? 1 : 0};
+            if (!cuda_ok(launch_thermal_init(ti, s), "thermal_init")) return false;
+        }
+        ThermalArgs ta{};
+        ta.nx = ctx.nx; ta.ny = ctx.ny; ta.nz = ctx.nz; ta.cells = ctx.cells;
+        ta.t = ctx.temperature;
+        ta.t_next = ctx.temperature_next;
+        ta.u = ctx.u_last;
+        ta.obstacle = ctx.obstacle[new_slot];
+        ta.source = bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_INTERNAL_THERMAL_SOURCE) ? nullptr : ctx.thermal_source;
+        ta.alpha = thermal_diffusivity();
+        ta.faces = current_thermal_faces();
+        if (!cuda_ok(launch_thermal_update(ta, s), "thermal_update")) return false;
+        std::swap(ctx.temperature, ctx.temperature_next);
+    }
     if (ctx.layout == 0) {
         float* g_next = ctx.g[1 - ctx.cur];
         if (!ctx.initialized) {
@@ -882,7 +951,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_get_temperature_state_rect(int nx, int ny, int
     std::lock_guard<std::recursive_mutex> lk(g_mutex);
     clear_error();
     Context* c = find_context(key);
-    if (!c || !out || !c->has_inputs || c->nx != nx || c->ny != ny || c->nz != nz) {
+    if (!g_cfg.initialized || !c || !out || c->nx != nx || c->ny != ny || c->nz != nz) {
         set_error("get_temperature_state: no context of these dimensions");
         return 0;
     }
@@ -891,14 +960,17 @@ AERO_LBM_B200_EXPORT int aero_lbm_get_temperature_state_rect(int nx, int ny, int
     return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
 }
 
+// assign_temperature_state (jni.cpp:8028-8035): creates the context when it
+// does not exist yet; values clamped with min(1, max(-1, v)).
 AERO_LBM_B200_EXPORT int aero_lbm_set_temperature_state_rect(int nx, int ny, int nz, long long key, const float* t) {
     std::lock_guard<std::recursive_mutex> lk(g_mutex);
     clear_error();
-    Context* c = find_context(key);
-    if (!c || !t || c->nx != nx || c->ny != ny || c->nz != nz) {
-        set_error("set_temperature_state: no context of these dimensions");
+    if (!g_cfg.initialized || !t || nx <= 0 || ny <= 0 || nz <= 0) {
+        set_error("set_temperature_state: runtime not initialised or bad arguments");
         return 0;
     }
+    Context* c = get_or_create_context(key, nx, ny, nz);
+    if (!c) return 0;
     std::unique_ptr<float[]> tmp(new float[(size_t)c->cells]);
     for (long long i = 0; i < c->cells; ++i) tmp[i] = clampf_h(t[i], -1.0f, 1.0f);
     cudaStream_t s = current_stream();
@@ -1109,6 +1181,16 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_cells_per_thread(int n) {
         return 0;
     }
     g_cells_per_thread = n;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_thermal_transport(int mode) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (mode < -1 || mode > 1) {
+        set_error("set_thermal_transport: -1, 0 or 1");
+        return 0;
+    }
+    g_thermal_mode = mode;
     return 1;
 }
 

@@ -33,7 +33,12 @@ struct Context {
     float* ref_ux = nullptr;
     float* ref_uy = nullptr;
     float* ref_uz = nullptr;
-    float* temperature = nullptr;
+    float* temperature = nullptr;       // temperature the collision reads (transported state, or the packet field)
+    float* temperature_next = nullptr;  // transport: the other state buffer
+    float* ref_temperature = nullptr;   // transport: packet temperature channel
+    float* thermal_source = nullptr;    // transport: packet source channel
+    float* u_last = nullptr;            // transport: velocity of the last collision, SoA 3 x cells
+    bool thermal = false;               // the current call runs the temperature transport
     float* packet = nullptr;
     size_t packet_cap = 0;
     float* out = nullptr;

@@ -1,0 +1,69 @@
+// Temperature transport of the brick step: the reference's benchmark-mode
+// scalar update (update_temperature_field, native/src/aero_lbm_jni.cpp:2049-2143,
+// first-order branch; helpers 738-769 and 1783-1950), run before every
+// collision so that the Boussinesq force sees the transported field:
+//
+//   T'(x) = clamp(A + dt (alpha lap T(x) + s(x)), -1, 1),   dt = 1,
+//   A     = trilinear sample of T at x - dt u(x), u = the previous collision's
+//           velocity (post-clamp midpoint velocity; 0 on solid cells),
+//   lap   = sum of the six face neighbours - 6 T(x),
+//
+// where a neighbour or sample corner that is solid, or outside a face that is
+// not thermally periodic, takes the face rule (Dirichlet: the face temperature,
+// Neumann: T(x) + heat flux, otherwise T(x); for the sample the centre's T(x)
+// stands in). Solid cells hold 0. Built with --fmad=false and the reference's
+// operation order: bit-identical to the reference CPU step.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "d3q27_kernels.cuh"
+
+namespace aero {
+
+// Thermal face kinds (native/include/aero_lbm_capi.h:57-62).
+enum ThermalKind { kThermalInherit = 0, kThermalDisabled = 1, kThermalPeriodic = 2, kThermalAdiabatic = 3,
+                   kThermalDirichlet = 4, kThermalNeumann = 5 };
+
+struct ThermalFaces {
+    int kind[6];            // x-, x+, y-, y+, z-, z+
+    float temperature[6];   // Dirichlet value (clamped to +-1 when used)
+    float heat_flux[6];     // Neumann increment
+};
+
+struct ThermalArgs {
+    int nx, ny, nz;
+    long long cells;
+    const float* t;             // state before the update
+    float* t_next;              // state after the update
+    const float* u;             // previous collision velocity, SoA (ux, uy, uz), 3 x cells
+    const uint8_t* obstacle;    // mask of this call
+    const float* source;        // per-cell source (clamped to +-0.006) or null
+    float alpha;                // thermal diffusivity
+    ThermalFaces faces;
+};
+
+// First call of a context: the state and the velocity the first update
+// advects with (initialize_distributions, jni.cpp:1752-1781). benchmark: a
+// state of magnitude < 1e-8 takes initial_temperature, any other fluid cell
+// the packet's reference temperature; otherwise fluid cells take the
+// reference temperature. u = the packet velocity on fluid cells, 0 on solids.
+struct ThermalInitArgs {
+    long long cells;
+    float* t;
+    float* u;                   // SoA 3 x cells
+    const uint8_t* obstacle;
+    const float* ref_t;
+    const float* ref_ux;
+    const float* ref_uy;
+    const float* ref_uz;
+    float initial_temperature;
+    int benchmark;
+};
+
+cudaError_t launch_thermal_init(const ThermalInitArgs& a, cudaStream_t s);
+cudaError_t launch_thermal_update(const ThermalArgs& a, cudaStream_t s);
+
+}  // namespace aero

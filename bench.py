@@ -154,6 +154,8 @@ def _ref_worker(args):
     lib.aero_lbm_init_rect(w, w, w, 11, 4)
     c = O.config_struct(O.RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
     lib.aero_lbm_benchmark_set_config(ctypes.byref(c))
+    # the window's temperature field as the starting state (as our arm loads it)
+    lib.aero_lbm_set_temperature_state_rect(w, w, w, 1, np.ascontiguousarray(temp.reshape(-1)).ctypes.data)
     pk = O.packet_from(obst, *u, temperature=temp)
     for _ in range(warmup):
         lib.aero_lbm_step_rect(pk.ctypes.data, w, w, w, 1, None)
@@ -230,7 +232,11 @@ VARIANTS = {
 }
 
 
-def setup_context(aero, lib, case, variant: str, key: int, streaming: int):
+def setup_context(aero, lib, case, variant: str, key: int, streaming: int, thermal: int = -1):
+    """A context of the case stepped once (with a pinned host packet). thermal:
+    the temperature-transport mode (aero_lbm_b200_set_thermal_transport) left
+    set for the context's later steps; with the transport the case's
+    temperature field is loaded as the starting state."""
     import torch
 
     solver_mode, collision, _, _ = VARIANTS[variant]
@@ -254,6 +260,9 @@ def setup_context(aero, lib, case, variant: str, key: int, streaming: int):
         for a, v in enumerate(fc.get("velocity", (0, 0, 0))):
             face.velocity[a] = v
     ctx.configure(cfg)
+    lib.aero_lbm_b200_set_thermal_transport(thermal)
+    if thermal != 0 and case.temperature_state() is not None:
+        ctx.set_temperature_state(case.temperature_state())
     packet = torch.from_numpy(case.packet()).pin_memory()
     pk_ptr = ctypes.cast(packet.data_ptr(), ctypes.POINTER(ctypes.c_float))
     if not lib.aero_lbm_step_rect(pk_ptr, n, n, n, key, None):
@@ -474,11 +483,15 @@ def run_ours(args) -> dict | None:
     acc = None
     if args.accuracy_steps > 0:
         outs = {}
+        # The FP64 reference run (the adjoint module's forward) takes the
+        # temperature as a fixed field, so the variants run without the
+        # temperature transport here: the leg measures storage precision.
         for k, variant in enumerate(("fp16", "i16", "fp32_fast", "fp32_exact")):
-            c, _, _ = setup_context(aero, lib, case, variant, 90 + 8 * rank + k, args.streaming)
+            c, _, _ = setup_context(aero, lib, case, variant, 90 + 8 * rank + k, args.streaming, thermal=0)
             c.advance(args.accuracy_steps - 1)
             outs[variant] = c.flow_state()
             c.release()
+        lib.aero_lbm_b200_set_thermal_transport(-1)
         fluid = np.flatnonzero(case.obstacle.reshape(-1) == 0).astype(np.int32)
         ab = aero.AdjointBrick(case.obstacle, case.temperature, lib=lib, face_kind=[f["kind"] for f in case.faces],
                                tau=case.tau, smagorinsky_c=case.smagorinsky_c, buoyancy_beta=case.buoyancy_beta,

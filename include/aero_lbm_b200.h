@@ -237,6 +237,15 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_collision_mode(int mode);
  * the reference-order collision both shapes are bit-identical; with the
  * factorised one they agree to FP32 rounding. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_cells_per_thread(int cells_per_thread);
+/* Temperature transport before every collision (the reference's
+ * benchmark-mode update: first-order semi-Lagrangian advection by the
+ * previous collision's velocity, diffusion, the packet's source channel,
+ * thermal faces; native/src/aero_lbm_jni.cpp:2049-2143): -1 = whenever
+ * buoyancy is enabled (default; the only case where it changes the flow),
+ * 1 = always (the temperature state then evolves exactly like the
+ * reference's also without buoyancy), 0 = never (the packet's temperature
+ * channel is the buoyancy field of each call). */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_thermal_transport(int mode);
 /* In-place step with the factorised collision, two cells per thread, on a
  * brick whose z axis is not periodic: 1 = each warp streams its next 64-cell
  * tile into shared memory with bulk asynchronous copies while it collides the

@@ -143,7 +143,8 @@ def derive_params(cfg: dict) -> OracleParams:
     p.enable_buoyancy = 1 if cfg.get("buoyancy", False) else 0
     p.gravity_axis = int(cfg.get("gravity_axis", 1))
     p.disable_convective_outflow = 1 if cfg.get("disable_convective", False) else 0
-    p.thermal_transport = 1 if cfg.get("thermal_transport", False) else 0
+    # the product's default: transport whenever buoyancy is on
+    p.thermal_transport = 1 if cfg.get("thermal_transport", cfg.get("buoyancy", False)) else 0
     for i, fc in enumerate(faces):
         p.thermal_kind[i] = int(fc.get("thermal", THERMAL_DISABLED))
         p.face_temperature[i] = float(f32(fc.get("temperature", 0.0)))

@@ -16,12 +16,15 @@ def product_config(lib, cfg: dict) -> aero_b200.AeroLbmBenchmarkConfig:
 
 def run_product(lib, dims, cfg: dict, packet: np.ndarray, steps: int, key: int = 7,
                 smagorinsky_c: float = -1.0, beta: float = -1.0, axis: int = -1,
-                streaming_mode: int = 0, collision_mode: int = 0) -> tuple[np.ndarray, aero_b200.LbmContext]:
+                streaming_mode: int = 0, collision_mode: int = 0,
+                temperature_state: np.ndarray | None = None) -> tuple[np.ndarray, aero_b200.LbmContext]:
     lib.aero_lbm_b200_set_physics_overrides(smagorinsky_c, beta, axis)
     lib.aero_lbm_b200_set_streaming_mode(streaming_mode)
     lib.aero_lbm_b200_set_collision_mode(collision_mode)
     ctx = aero_b200.LbmContext(dims, input_channels=packet.shape[1], key=key, lib=lib)
     ctx.configure(product_config(lib, cfg))
+    if temperature_state is not None:
+        ctx.set_temperature_state(temperature_state)
     out = None
     for s in range(steps):
         out = ctx.step(packet if s == 0 else None, output=(s + 1 == steps))

@@ -93,7 +93,8 @@ def _fp16_run(gpu, case, steps, key):
     try:
         out, ctx = lbm_cases.run_product(gpu, case.dims, case.config_dict(), case.packet(), steps, key=key,
                                          smagorinsky_c=case.smagorinsky_c, beta=case.buoyancy_beta,
-                                         axis=case.gravity_axis, streaming_mode=0)
+                                         axis=case.gravity_axis, streaming_mode=0,
+                                         temperature_state=case.temperature_state())
     finally:
         gpu.aero_lbm_set_realtime_solver_mode(0)
     return out, ctx
@@ -102,6 +103,8 @@ def _fp16_run(gpu, case, steps, key):
 def _oracle_run(case, steps, precision):
     cfg = case.config_dict()
     o = O.Oracle(case.dims, O.derive_params(cfg), precision)
+    if case.temperature_state() is not None:
+        o.set_temperature(case.temperature_state())
     o.set_fields(case.obstacle, *case.u, temperature=case.temperature)
     o.step(steps)
     return o.output()
@@ -132,7 +135,7 @@ def test_fp32_terrain_bit_identical(gpu, n, cells_per_thread):
     try:
         out, ctx = lbm_cases.run_product(gpu, case.dims, case.config_dict(), case.packet(), steps, key=43,
                                          smagorinsky_c=case.smagorinsky_c, beta=case.buoyancy_beta,
-                                         axis=case.gravity_axis)
+                                         axis=case.gravity_axis, temperature_state=case.temperature_state())
     finally:
         gpu.aero_lbm_b200_set_cells_per_thread(2)
     assert_bits(out, _oracle_run(case, steps, "f32"))
