@@ -63,27 +63,188 @@ __device__ __forceinline__ float th_sample(const ThermalArgs& a, float x, float 
     return c0 + (c1 - c0) * fz;
 }
 
-// One thread per cell on a line grid (z along the block).
-__global__ void __launch_bounds__(128) thermal_update_kernel(ThermalArgs a) {
-    const int z = blockIdx.x * blockDim.x + threadIdx.x;
-    if (z >= a.nz) return;
-    const int y = blockIdx.y, x = blockIdx.z;
-    const long long cell = ((long long)x * a.ny + y) * a.nz + z;
-    if (a.obstacle[cell]) {
-        a.t_next[cell] = 0.0f;
+// The update reads the 3x3x3 neighbourhood of each cell (|u| < 1 keeps every
+// trilinear corner inside it). A block stages its tile plus a one-cell halo
+// in shared memory, each entry already resolved by th_neighbour's rules:
+// code 0 = use the value (a fluid cell's temperature, or a Dirichlet face's
+// clamped temperature), 1 = the querying cell's own value (solid cell,
+// adiabatic / disabled / inherit face), 2 = own value + the stored Neumann
+// flux, clamped. Periodic faces are resolved by staging the wrapped cell.
+// Lookups specialise on what the tile holds (block-uniform): only code 0
+// (most of the air above a terrain), codes 0 and 1, or any code.
+constexpr int kTZ = 32, kTY = 8, kTX = 4;  // cells per block: z x y x x
+constexpr int kSY = kTZ + 2, kSX = (kTY + 2) * (kTZ + 2), kTile = (kTX + 2) * kSX;
+
+enum TileKind { kTileClean = 0, kTileSolid = 1, kTileAny = 2 };
+
+template <int kKind>
+__device__ __forceinline__ float tile_at(const float* sv, const unsigned char* sc, int i, float self) {
+    const float v = sv[i];
+    if (kKind == kTileClean) return v;
+    const int c = sc[i];
+    if (kKind == kTileSolid) return c ? self : v;
+    return c == 0 ? v : (c == 1 ? self : exact::rclamp(self + v, -1.0f, 1.0f));
+}
+
+// One staged entry outside the brick: th_neighbour's rules without the
+// querying cell's value (rare path).
+__device__ __noinline__ void stage_outside(const ThermalFaces* F, const float* t, const uint8_t* obstacle, int nx, int ny,
+                                           int nz, int x, int y, int z, float* v, unsigned char* code) {
+    if ((x < 0 || x >= nx) && F->kind[x < 0 ? 0 : 1] == kThermalPeriodic) {
+        x %= nx;
+        if (x < 0) x += nx;
+    }
+    if ((y < 0 || y >= ny) && F->kind[y < 0 ? 2 : 3] == kThermalPeriodic) {
+        y %= ny;
+        if (y < 0) y += ny;
+    }
+    if ((z < 0 || z >= nz) && F->kind[z < 0 ? 4 : 5] == kThermalPeriodic) {
+        z %= nz;
+        if (z < 0) z += nz;
+    }
+    int face = -1;
+    if (x < 0) face = 0;
+    else if (x >= nx) face = 1;
+    else if (y < 0) face = 2;
+    else if (y >= ny) face = 3;
+    else if (z < 0) face = 4;
+    else if (z >= nz) face = 5;
+    *v = 0.0f;
+    if (face >= 0) {
+        const int kind = F->kind[face];
+        if (kind == kThermalDirichlet) {
+            *code = 0;
+            *v = exact::rclamp(F->temperature[face], -1.0f, 1.0f);
+        } else if (kind == kThermalNeumann) {
+            *code = 2;
+            *v = F->heat_flux[face];
+        } else {
+            *code = 1;
+        }
         return;
     }
+    const int cell = (x * ny + y) * nz + z;
+    *code = obstacle[cell] ? 1 : 0;
+    if (!*code) *v = __ldg(t + cell);
+}
+
+// th_sample for a cell moving a full cell or more per step (never after a
+// collision: the speed clamp keeps |u| < 1; only a first call's packet
+// velocity can); out of line.
+__device__ __noinline__ float th_sample_far(const ThermalArgs& a, float px, float py, float pz, float fallback) {
+    return th_sample(a, px, py, pz, fallback);
+}
+
+template <int kKind>
+__device__ __forceinline__ void update_cell(const ThermalArgs& a, const float* sv, const unsigned char* sc, int c, int x,
+                                            int y, int z, int cell, const float (&uv)[3], float src) {
     const float dt = 1.0f, cooling = 0.0f;
-    const float tc = a.t[cell];
-    const float ux = a.u[cell], uy = a.u[a.cells + cell], uz = a.u[2 * a.cells + cell];
-    const float adv = th_sample(a, (float)x - dt * ux, (float)y - dt * uy, (float)z - dt * uz, tc);
-    const float t_sum = th_neighbour(a, x + 1, y, z, tc) + th_neighbour(a, x - 1, y, z, tc) +
-                        th_neighbour(a, x, y + 1, z, tc) + th_neighbour(a, x, y - 1, z, tc) +
-                        th_neighbour(a, x, y, z + 1, tc) + th_neighbour(a, x, y, z - 1, tc);
+    const float tc = sv[c];
+    const float ux = uv[0], uy = uv[1], uz = uv[2];
+    const float px = (float)x - dt * ux, py = (float)y - dt * uy, pz = (float)z - dt * uz;
+    float adv;
+    if (fabsf(ux) < 1.0f && fabsf(uy) < 1.0f && fabsf(uz) < 1.0f) {
+        const int x0 = (int)floorf(px), y0 = (int)floorf(py), z0 = (int)floorf(pz);
+        const float fx = px - (float)x0, fy = py - (float)y0, fz = pz - (float)z0;
+        const int b = c + (x0 - x) * kSX + (y0 - y) * kSY + (z0 - z);  // corner (x0, y0, z0)
+        const float c000 = tile_at<kKind>(sv, sc, b, tc);
+        const float c100 = tile_at<kKind>(sv, sc, b + kSX, tc);
+        const float c010 = tile_at<kKind>(sv, sc, b + kSY, tc);
+        const float c110 = tile_at<kKind>(sv, sc, b + kSX + kSY, tc);
+        const float c001 = tile_at<kKind>(sv, sc, b + 1, tc);
+        const float c101 = tile_at<kKind>(sv, sc, b + kSX + 1, tc);
+        const float c011 = tile_at<kKind>(sv, sc, b + kSY + 1, tc);
+        const float c111 = tile_at<kKind>(sv, sc, b + kSX + kSY + 1, tc);
+        const float c00 = c000 + (c100 - c000) * fx;
+        const float c10 = c010 + (c110 - c010) * fx;
+        const float c01 = c001 + (c101 - c001) * fx;
+        const float c11 = c011 + (c111 - c011) * fx;
+        const float c0 = c00 + (c10 - c00) * fy;
+        const float c1 = c01 + (c11 - c01) * fy;
+        adv = c0 + (c1 - c0) * fz;
+    } else {
+        adv = th_sample_far(a, px, py, pz, tc);
+    }
+    const float t_sum = tile_at<kKind>(sv, sc, c + kSX, tc) + tile_at<kKind>(sv, sc, c - kSX, tc) +
+                        tile_at<kKind>(sv, sc, c + kSY, tc) + tile_at<kKind>(sv, sc, c - kSY, tc) +
+                        tile_at<kKind>(sv, sc, c + 1, tc) + tile_at<kKind>(sv, sc, c - 1, tc);
     const float lap = t_sum - 6.0f * tc;
-    const float src = a.source ? exact::rclamp(a.source[cell], -0.006f, 0.006f) : 0.0f;
     const float t_next = adv + dt * (a.alpha * lap + src - cooling * adv);
     a.t_next[cell] = exact::rclamp(t_next, -1.0f, 1.0f);
+}
+
+// Block = (32 z) x (8 y) threads over a kTX x kTY x kTZ tile: each thread
+// updates the kTX cells of its (y, z) column. Loads are grouped so that many
+// are in flight at once (the kernel is latency-bound). Bricks stay below 2^31
+// cells (32-bit cell indices).
+__global__ void __launch_bounds__(kTZ * kTY, 5) thermal_update_kernel(ThermalArgs a) {
+    __shared__ float sv[kTile];
+    __shared__ unsigned char sc[kTile];
+    const int zb = blockIdx.x * kTZ, yb = blockIdx.y * kTY, xb = blockIdx.z * kTX;
+    const int tid = threadIdx.y * kTZ + threadIdx.x;
+    int seen = 0;  // bit c: some entry has code c
+    // columns (iy, iz) of the halo tile, all kTX + 2 x-planes each
+    for (int col = tid; col < kSX; col += kTZ * kTY) {
+        const int iy = col / kSY, iz = col - iy * kSY;
+        const int gy = yb + iy - 1, gz = zb + iz - 1;
+        const bool yz_in = (unsigned)gy < (unsigned)a.ny && (unsigned)gz < (unsigned)a.nz;
+        float tv[kTX + 2];
+        unsigned char ob[kTX + 2];
+#pragma unroll
+        for (int ix = 0; ix < kTX + 2; ++ix) {
+            const int gx = xb + ix - 1;
+            tv[ix] = 0.0f;
+            ob[ix] = 0;
+            if (yz_in && (unsigned)gx < (unsigned)a.nx) {
+                const int cell = (gx * a.ny + gy) * a.nz + gz;
+                ob[ix] = __ldg(a.obstacle + cell);
+                tv[ix] = __ldg(a.t + cell);
+            }
+        }
+#pragma unroll
+        for (int ix = 0; ix < kTX + 2; ++ix) {
+            const int gx = xb + ix - 1;
+            const int i = ix * kSX + col;
+            if (yz_in && (unsigned)gx < (unsigned)a.nx) {
+                const unsigned char code = ob[ix] ? 1 : 0;
+                sv[i] = code ? 0.0f : tv[ix];
+                sc[i] = code;
+                seen |= 1 << code;
+            } else {
+                stage_outside(&a.faces, a.t, a.obstacle, a.nx, a.ny, a.nz, gx, gy, gz, &sv[i], &sc[i]);
+                seen |= 1 << sc[i];
+            }
+        }
+    }
+    const int any_neumann = __syncthreads_or(seen & 4);
+    const int any_self = __syncthreads_or(seen & 2);
+    const int z = zb + threadIdx.x, y = yb + threadIdx.y;
+    if (y >= a.ny || z >= a.nz) return;
+    float u[kTX][3], src[kTX];
+#pragma unroll
+    for (int k = 0; k < kTX; ++k) {
+        const int x = xb + k;
+        const int cell = (x * a.ny + y) * a.nz + z;
+        const bool in = x < a.nx;
+        u[k][0] = in ? __ldg(a.u + cell) : 0.0f;
+        u[k][1] = in ? __ldg(a.u + a.cells + cell) : 0.0f;
+        u[k][2] = in ? __ldg(a.u + 2 * a.cells + cell) : 0.0f;
+        src[k] = (in && a.source) ? exact::rclamp(__ldg(a.source + cell), -0.006f, 0.006f) : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < kTX; ++k) {
+        const int x = xb + k;
+        if (x >= a.nx) break;
+        const int cell = (x * a.ny + y) * a.nz + z;
+        const int c = (k + 1) * kSX + (threadIdx.y + 1) * kSY + threadIdx.x + 1;
+        if (sc[c] != 0) {  // solid now
+            a.t_next[cell] = 0.0f;
+            continue;
+        }
+        if (!any_neumann && !any_self) update_cell<kTileClean>(a, sv, sc, c, x, y, z, cell, u[k], src[k]);
+        else if (!any_neumann) update_cell<kTileSolid>(a, sv, sc, c, x, y, z, cell, u[k], src[k]);
+        else update_cell<kTileAny>(a, sv, sc, c, x, y, z, cell, u[k], src[k]);
+    }
 }
 
 __global__ void thermal_init_kernel(ThermalInitArgs a) {
@@ -110,9 +271,9 @@ cudaError_t launch_thermal_init(const ThermalInitArgs& a, cudaStream_t s) {
 
 cudaError_t launch_thermal_update(const ThermalArgs& a, cudaStream_t s) {
     if (a.cells <= 0) return cudaSuccess;
-    const int block = a.nz >= 128 ? 128 : ((a.nz + 31) / 32) * 32;
-    const dim3 grid((unsigned)((a.nz + block - 1) / block), (unsigned)a.ny, (unsigned)a.nx);
-    thermal_update_kernel<<<grid, block, 0, s>>>(a);
+    if (a.cells >= (1LL << 31)) return cudaErrorInvalidValue;  // 32-bit cell indices
+    const dim3 grid((unsigned)((a.nz + kTZ - 1) / kTZ), (unsigned)((a.ny + kTY - 1) / kTY), (unsigned)((a.nx + kTX - 1) / kTX));
+    thermal_update_kernel<<<grid, dim3(kTZ, kTY), 0, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }
