@@ -8,6 +8,7 @@
 // mask and faces) and then collide (with this call's inputs), so every call is
 // one fused pass and the output pass reads S(g) with this call's faces.
 #include <atomic>
+#include <vector>
 
 #include "d3q27_step.cuh"
 
@@ -18,6 +19,50 @@ std::atomic<uint64_t> g_launches{0};
 }
 uint64_t kernel_launch_count() { return g_launches.load(); }
 void count_launch() { g_launches.fetch_add(1); }
+
+namespace {
+struct StepTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;  // begin/end pairs, reused across resets
+    size_t used = 0;
+};
+StepTimer g_timer;
+cudaEvent_t timer_event() {
+    if (g_timer.used == g_timer.pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        g_timer.pool.push_back(e);
+    }
+    return g_timer.pool[g_timer.used++];
+}
+}  // namespace
+
+void step_timer_begin(cudaStream_t s) {
+    if (!g_timer.on) return;
+    if (cudaEvent_t e = timer_event()) cudaEventRecord(e, s);
+}
+void step_timer_end(cudaStream_t s) {
+    if (!g_timer.on) return;
+    if (cudaEvent_t e = timer_event()) cudaEventRecord(e, s);
+}
+void step_timer_reset(bool on) {
+    g_timer.on = on;
+    g_timer.used = 0;
+}
+// Sum of the recorded begin/end intervals (waits for the last event).
+bool step_timer_read(double* total_ms, int* launches) {
+    double t = 0.0;
+    const size_t pairs = g_timer.used / 2;
+    if (pairs && cudaEventSynchronize(g_timer.pool[2 * pairs - 1]) != cudaSuccess) return false;
+    for (size_t i = 0; i < pairs; ++i) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, g_timer.pool[2 * i], g_timer.pool[2 * i + 1]) != cudaSuccess) return false;
+        t += ms;
+    }
+    *total_ms = t;
+    *launches = (int)pairs;
+    return true;
+}
 
 // ---------------------------------------------------------------- ingest
 // Packet semantics of ingest_payload (native/src/aero_lbm_jni.cpp:1671-1694).

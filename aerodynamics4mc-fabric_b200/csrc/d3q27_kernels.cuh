@@ -96,5 +96,11 @@ cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* f
 
 uint64_t kernel_launch_count();
 void count_launch();
+// Optional CUDA-event timing of the brick step kernel launches (off unless
+// aero_lbm_b200_kernel_timer enabled it): brackets one launch on stream s.
+void step_timer_begin(cudaStream_t s);
+void step_timer_end(cudaStream_t s);
+void step_timer_reset(bool on);
+bool step_timer_read(double* total_ms, int* launches);
 
 }  // namespace aero

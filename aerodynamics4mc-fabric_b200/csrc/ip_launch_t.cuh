@@ -29,6 +29,7 @@ struct IpLaunch {
             cudaError_t e = face_fill(f, a, s);
             if (e != cudaSuccess) return e;
         }
+        step_timer_begin(s);
         if (!kExact && a.cells_per_thread == 2 && a.streamed && IpaLaunch<S>::eligible(a)) {
             cudaError_t e = IpaLaunch<S>::step(f, a, s);
             if (e != cudaSuccess) return e;
@@ -41,6 +42,7 @@ struct IpLaunch {
             if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
             else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
         }
+        step_timer_end(s);
         count_launch();
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess || !transitions) return e;

@@ -1109,6 +1109,18 @@ AERO_LBM_B200_EXPORT void aero_lbm_b200_set_stream(void* stream) {
 
 AERO_LBM_B200_EXPORT unsigned long long aero_lbm_b200_launch_count(void) { return kernel_launch_count(); }
 
+AERO_LBM_B200_EXPORT int aero_lbm_b200_kernel_timer(int on) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    step_timer_reset(on != 0);
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_kernel_time(double* total_ms, int* launches) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (!total_ms || !launches) return 0;
+    return step_timer_read(total_ms, launches) ? 1 : 0;
+}
+
 AERO_LBM_B200_EXPORT int aero_lbm_b200_advance_rect(long long key, int steps) {
     std::lock_guard<std::recursive_mutex> lk(g_mutex);
     clear_error();

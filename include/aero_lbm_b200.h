@@ -206,6 +206,13 @@ AERO_LBM_B200_EXPORT const char* aero_lbm_benchmark_info(void);
 AERO_LBM_B200_EXPORT void aero_lbm_b200_set_stream(void* stream);
 /* Number of kernels this library has launched since load. */
 AERO_LBM_B200_EXPORT unsigned long long aero_lbm_b200_launch_count(void);
+/* CUDA-event timing of the in-place step kernel launches alone (the
+ * population stream-collide kernel, without the face pre-fill, temperature
+ * transport or transition kernels): on != 0 starts a new record, 0 stops.
+ * kernel_time waits for the last recorded launch and returns the summed
+ * device time and the number of launches timed. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_kernel_timer(int on);
+AERO_LBM_B200_EXPORT int aero_lbm_b200_kernel_time(double* total_ms, int* launches);
 /* Advance a context `steps` times with its resident inputs, no host copies and
  * no synchronisation (the device-resident form of step_rect_cached). */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_advance_rect(long long context_key, int steps);
