@@ -379,10 +379,24 @@ def run_adjoint_leg(aero, lib, torch) -> dict:
     b.close()
     fwd = tm["forward_ms_per_step"]
     per_step = tm["recompute_ms_per_step"] + tm["reverse_ms_per_step"]
+    # Every state kept (checkpoint every call: 200 x 28 MB of FP32 state, well
+    # within one GPU's memory): no segment recomputation.
+    cfg1 = dict(c.config, checkpoint_every=1)
+    b1 = aero.AdjointBrick(c.obstacle, c.temperature, lib=lib, **cfg1)
+    b1.set_probes(c.probes, t)
+    b1.gradient(c.force0, c.inflow0)  # warm-up
+    loss1, gf1, gu1 = b1.gradient(c.force0, c.inflow0)
+    tm1 = b1.timing()
+    b1.close()
+    fwd1 = tm1["forward_ms_per_step"]
+    per_step1 = tm1["recompute_ms_per_step"] + tm1["reverse_ms_per_step"]
     return {"workload": "d3q27 64^3 fp32, SGS + Boussinesq + 5% obstacles, 200 calls, checkpoint every 20, 64 probes",
             "loss": loss, "grad_inflow": [float(v) for v in gu], "grad_force_max": float(np.max(np.abs(gf))),
             **tm, "adjoint_over_forward": per_step / fwd if fwd > 0 else None,
-            "reverse_only_over_forward": tm["reverse_ms_per_step"] / fwd if fwd > 0 else None}
+            "reverse_only_over_forward": tm["reverse_ms_per_step"] / fwd if fwd > 0 else None,
+            "store_all": {"checkpoint_every": 1, "adjoint_over_forward": per_step1 / fwd1 if fwd1 > 0 else None,
+                          "forward_ms_per_step": fwd1, "reverse_ms_per_step": tm1["reverse_ms_per_step"],
+                          "gradient_equal_to_checkpointed": bool(np.array_equal(gf1, gf) and np.array_equal(gu1, gu))}}
 
 
 def run_ours(args) -> dict | None:

@@ -18,8 +18,8 @@
 //   stream_and_bounce       native/src/aero_lbm_jni.cpp:2415-2452
 //   write_output            native/src/aero_lbm_jni.cpp:2535-2581
 //   strided atlas extract   native/src/aero_lbm_jni.cpp:9246-9450
-//   temperature transport   native/src/aero_lbm_jni.cpp:2049-2143 (benchmark
-//                           branch), helpers 738-769, 1783-1950; per-call order
+//   temperature transport   native/src/aero_lbm_jni.cpp:2049-2143 (first-order
+//                           and BFECC branches), helpers 738-769, 1783-1950; per-call order
 //                           and state rules 1752-1781, 8028-8064, 8480-8507
 //
 // Knobs the reference hard-codes are parameters here (Smagorinsky constant,
@@ -86,6 +86,7 @@ typedef struct OracleD3Q27Params {
     double initial_temperature;    // benchmark config initial_temperature
     int internal_thermal_source;   // 1: the packet's source channel feeds the transport
     int packet_has_temperature;    // 1: the packet carries the temperature channel (>= 11 channels)
+    int thermal_bfecc;             // 1: the BFECC branch (heated-cavity presets), 0: first-order
 } OracleD3Q27Params;
 
 }  // extern "C"
@@ -133,7 +134,7 @@ struct D3Q27Oracle {
 
     std::vector<T> f, f_post, rho, ux, uy, uz;
     std::vector<T> ref_ux, ref_uy, ref_uz, ref_p, temperature;
-    std::vector<T> temperature_next, ref_temperature, thermal_source;
+    std::vector<T> temperature_next, ref_temperature, thermal_source, temperature_scratch;
     std::vector<T> force_x, force_y, force_z;  // optional per-cell force density
     std::vector<uint8_t> obstacle;
     bool initialized = false;
@@ -153,6 +154,7 @@ struct D3Q27Oracle {
         ref_p.assign(cells, T(0));
         temperature.assign(cells, T(0));
         temperature_next.assign(cells, T(0));
+        temperature_scratch.assign(cells, T(0));
         ref_temperature.assign(cells, T(0));
         thermal_source.assign(cells, T(0));
         obstacle.assign(cells, 0);
@@ -347,9 +349,70 @@ struct D3Q27Oracle {
         for (size_t cell = 0; cell < cells; ++cell)
             if (obstacle[cell]) temperature[cell] = temperature_next[cell] = T(0);
     }
+    void local_bounds(int x, int y, int z, T& lo, T& hi) const {
+        const T c = temperature[cell_index(x, y, z)];
+        lo = hi = c;
+        const T nb[6] = {thermal_neighbour(temperature, x + 1, y, z, c), thermal_neighbour(temperature, x - 1, y, z, c),
+                         thermal_neighbour(temperature, x, y + 1, z, c), thermal_neighbour(temperature, x, y - 1, z, c),
+                         thermal_neighbour(temperature, x, y, z + 1, c), thermal_neighbour(temperature, x, y, z - 1, c)};
+        for (T v : nb) {
+            lo = std::min(lo, v);
+            hi = std::max(hi, v);
+        }
+    }
+    // BFECC branch (jni.cpp:2050-2135): forward advection, backward advection
+    // of that, the error-corrected field advected again and limited to the
+    // local min/max of the state, then diffusion + source (dt = 1).
+    void update_temperature_bfecc() {
+        const T dt = T(1.0f), cooling = T(0.0f);
+        const T alpha = T(float(p.thermal_diffusivity));
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    const size_t cell = cell_index(x, y, z);
+                    if (obstacle[cell]) { temperature_scratch[cell] = T(0); continue; }
+                    const T tc = temperature[cell];
+                    temperature_scratch[cell] = sample_trilinear(temperature, T(float(x)) - dt * ux[cell],
+                                                                 T(float(y)) - dt * uy[cell], T(float(z)) - dt * uz[cell], tc);
+                }
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    const size_t cell = cell_index(x, y, z);
+                    if (obstacle[cell]) { temperature_next[cell] = T(0); continue; }
+                    const T tc = temperature[cell];
+                    const T back = sample_trilinear(temperature_scratch, T(float(x)) + dt * ux[cell], T(float(y)) + dt * uy[cell],
+                                                    T(float(z)) + dt * uz[cell], temperature_scratch[cell]);
+                    temperature_next[cell] = clampv(T(tc + T(0.5f) * (tc - back)), t_min, t_max);
+                }
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    const size_t cell = cell_index(x, y, z);
+                    if (obstacle[cell]) { temperature_scratch[cell] = T(0); continue; }
+                    const T tc = temperature[cell];
+                    T adv = sample_trilinear(temperature_next, T(float(x)) - dt * ux[cell], T(float(y)) - dt * uy[cell],
+                                             T(float(z)) - dt * uz[cell], temperature_next[cell]);
+                    T lo, hi;
+                    local_bounds(x, y, z, lo, hi);
+                    adv = clampv(adv, lo, hi);
+                    const T t_sum = thermal_neighbour(temperature, x + 1, y, z, tc) + thermal_neighbour(temperature, x - 1, y, z, tc) +
+                                    thermal_neighbour(temperature, x, y + 1, z, tc) + thermal_neighbour(temperature, x, y - 1, z, tc) +
+                                    thermal_neighbour(temperature, x, y, z + 1, tc) + thermal_neighbour(temperature, x, y, z - 1, tc);
+                    const T lap = t_sum - T(6.0f) * tc;
+                    const T src = p.internal_thermal_source ? clampv(thermal_source[cell], T(-0.006f), T(0.006f)) : T(0);
+                    temperature_scratch[cell] = clampv(T(adv + dt * (alpha * lap + src - cooling * adv)), t_min, t_max);
+                }
+        temperature.swap(temperature_scratch);
+        temperature_next = temperature;
+    }
     // First-order semi-Lagrangian advection by the previous collision's
     // velocity + explicit diffusion + source (benchmark branch, dt = 1).
     void update_temperature() {
+        if (p.thermal_bfecc) {
+            update_temperature_bfecc();
+            return;
+        }
         const T dt = T(1.0f), cooling = T(0.0f);
         const T alpha = T(float(p.thermal_diffusivity));
         for (int x = 0; x < nx; ++x)

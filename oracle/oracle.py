@@ -34,6 +34,7 @@ PERIODIC, BOUNCE_BACK, MOVING_WALL, VELOCITY, PRESSURE, CONVECTIVE, SYMMETRY = 1
 INHERIT_GAME = 0
 # thermal face kinds (native/include/aero_lbm_capi.h:57-62)
 THERMAL_INHERIT, THERMAL_DISABLED, THERMAL_PERIODIC, THERMAL_ADIABATIC, THERMAL_DIRICHLET, THERMAL_NEUMANN = 0, 1, 2, 3, 4, 5
+PRESET_HEATED_CAVITY_2D, PRESET_HEATED_CAVITY_3D = 5, 6  # native/include/aero_lbm_capi.h:41-42
 FLAG_DISABLE_CONVECTIVE_OUTFLOW = 1 << 3
 FLAG_DISABLE_SGS = 1 << 5
 FLAG_DISABLE_BUOYANCY = 1 << 7
@@ -77,6 +78,7 @@ class OracleParams(ctypes.Structure):
         ("initial_temperature", ctypes.c_double),
         ("internal_thermal_source", ctypes.c_int),
         ("packet_has_temperature", ctypes.c_int),
+        ("thermal_bfecc", ctypes.c_int),
     ]
 
 
@@ -110,15 +112,23 @@ def derive_params(cfg: dict) -> OracleParams:
     thermal_source (bool), packet_channels; per face thermal (kind),
     temperature, heat_flux."""
     faces = cfg["faces"]
-    speed = _norm(cfg.get("initial_velocity", (0, 0, 0)))
-    for fc in faces:
-        speed = max(speed, _norm(fc.get("velocity", (0, 0, 0))))
-    re = f32(cfg.get("reynolds", 100.0))
     length = max(f32(1.0e-6), f32(cfg.get("reference_length", 1.0)))
-    if re <= f32(1.0e-6) or speed <= f32(1.0e-8):
-        nu = _clamp(RUNTIME_NU0, NU_MIN, NU_MAX)
+    cavity = int(cfg.get("preset", 0)) in (PRESET_HEATED_CAVITY_2D, PRESET_HEATED_CAVITY_3D)
+    if cavity:
+        # heated-cavity presets (jni.cpp:824-829, 947-954, 966-970, 1023-1031)
+        speed = _clamp(cfg.get("mach", 0.15), 1.0e-4, 0.30) * f32(np.sqrt(f32(1.0) / f32(3.0)))
+        ra = max(f32(1.0e-6), f32(cfg.get("rayleigh", 1.0e5)))
+        pr = max(f32(1.0e-6), f32(cfg.get("prandtl", 0.71)))
+        nu = _clamp(f32(speed * length) * f32(np.sqrt(f32(pr / ra))), NU_MIN, NU_MAX)
     else:
-        nu = _clamp(f32(speed * length) / re, NU_MIN, NU_MAX)
+        speed = _norm(cfg.get("initial_velocity", (0, 0, 0)))
+        for fc in faces:
+            speed = max(speed, _norm(fc.get("velocity", (0, 0, 0))))
+        re = f32(cfg.get("reynolds", 100.0))
+        if re <= f32(1.0e-6) or speed <= f32(1.0e-8):
+            nu = _clamp(RUNTIME_NU0, NU_MIN, NU_MAX)
+        else:
+            nu = _clamp(f32(speed * length) / re, NU_MIN, NU_MAX)
     tau_s = _clamp(f32(0.5) + f32(3.0) * _clamp(nu, NU_MIN, NU_MAX), TAU_MIN, TAU_MAX)
     tau_n = _clamp(f32(0.5) + f32(3.0) * _clamp(_clamp(nu, NU_MIN, NU_MAX), NU_MIN, NU_MAX), TAU_MIN, TAU_MAX)
     p = OracleParams()
@@ -129,7 +139,12 @@ def derive_params(cfg: dict) -> OracleParams:
     p.sgs_c2 = float(f32(c * c))
     p.sgs_nut_max_ratio = 5.0
     p.sgs_bulk_coupling = float(f32(0.30))
-    p.buoyancy_beta = float(f32(cfg.get("buoyancy_beta", BOUSSINESQ_BETA)))
+    beta = BOUSSINESQ_BETA
+    if cavity:
+        temps = [f32(fc.get("temperature", 0.0)) for fc in faces if fc.get("thermal") == THERMAL_DIRICHLET]
+        span = max(f32(1.0e-6), f32(max(temps) - min(temps))) if temps else f32(1.0)
+        beta = f32(speed * speed) / max(f32(1.0e-6), f32(length * span))
+    p.buoyancy_beta = float(f32(cfg.get("buoyancy_beta", beta)))
     p.buoyancy_force_max = float(f32(0.02))
     for i, v in enumerate(cfg.get("body_force", (0.0, 0.0, 0.0))):
         p.body_force[i] = float(f32(v))
@@ -149,7 +164,8 @@ def derive_params(cfg: dict) -> OracleParams:
         p.thermal_kind[i] = int(fc.get("thermal", THERMAL_DISABLED))
         p.face_temperature[i] = float(f32(fc.get("temperature", 0.0)))
         p.face_heat_flux[i] = float(f32(fc.get("heat_flux", 0.0)))
-    p.thermal_diffusivity = float(f32(0.035))
+    p.thermal_diffusivity = float(f32(nu / pr) if cavity else f32(0.035))
+    p.thermal_bfecc = 1 if cavity else 0
     p.initial_temperature = float(f32(cfg.get("initial_temperature", 0.0)))
     p.internal_thermal_source = 1 if cfg.get("thermal_source", False) else 0
     p.packet_has_temperature = 1 if int(cfg.get("packet_channels", 11)) > 10 else 0
@@ -283,7 +299,11 @@ def config_struct(struct_type, cfg: dict, default_fn):
     c = struct_type()
     default_fn(ctypes.byref(c))
     c.enabled = 1
-    c.preset = 0
+    c.preset = int(cfg.get("preset", 0))
+    if c.preset:
+        c.rayleigh_number = cfg.get("rayleigh", 1.0e5)
+        c.prandtl_number = cfg.get("prandtl", 0.71)
+        c.mach_number = cfg.get("mach", 0.15)
     flags = c.flags
     flags = (flags & ~FLAG_DISABLE_SGS) if cfg.get("sgs", False) else (flags | FLAG_DISABLE_SGS)
     flags = (flags & ~FLAG_DISABLE_BUOYANCY) if cfg.get("buoyancy", False) else (flags | FLAG_DISABLE_BUOYANCY)
@@ -431,6 +451,31 @@ def thermal_case(n: int = 12, seed: int = 11):
            "thermal_transport": True, "initial_temperature": 0.1, "thermal_source": True}
     preload = np.full(n ** 3, 0.5, np.float32)
     return obst, u, temp, src, cfg, preload
+
+
+def heated_cavity_case(n: int = 12, seed: int = 3, preset: int = PRESET_HEATED_CAVITY_3D):
+    """The reference's differentially heated cavity preset (Ra 1e5, Pr 0.71,
+    Mach 0.15; hot x- face 0.5, cold x+ face -0.5, bounce-back walls; 2-D:
+    periodic z) on an n^3 brick with 4% random solids, u = U(-0.01, 0.01),
+    packet temperature U(-0.2, 0.2), state preloaded with 0.3; the 3-D case
+    makes z- a Neumann face (flux 0.02). Its temperature transport is the
+    BFECC branch. Returns obstacle, (ux, uy, uz), temperature, config, preload."""
+    rng = np.random.default_rng(seed)
+    dims = (n, n, n)
+    obst = (rng.random(dims) < 0.04).astype(np.uint8)
+    u = tuple(rng.uniform(-0.01, 0.01, dims).astype(np.float32) for _ in range(3))
+    temp = rng.uniform(-0.2, 0.2, dims).astype(np.float32)
+    faces = [{"kind": BOUNCE_BACK, "thermal": THERMAL_DIRICHLET, "temperature": 0.5},
+             {"kind": BOUNCE_BACK, "thermal": THERMAL_DIRICHLET, "temperature": -0.5},
+             {"kind": BOUNCE_BACK, "thermal": THERMAL_ADIABATIC}, {"kind": BOUNCE_BACK, "thermal": THERMAL_ADIABATIC}]
+    if preset == PRESET_HEATED_CAVITY_2D:
+        faces += [{"kind": PERIODIC, "thermal": THERMAL_PERIODIC}] * 2
+    else:
+        faces += [{"kind": BOUNCE_BACK, "thermal": THERMAL_NEUMANN, "heat_flux": 0.02},
+                  {"kind": BOUNCE_BACK, "thermal": THERMAL_ADIABATIC}]
+    cfg = {"preset": preset, "rayleigh": 1e5, "prandtl": 0.71, "mach": 0.15, "faces": faces, "sgs": True,
+           "buoyancy": True, "thermal_transport": True, "initial_temperature": 0.0}
+    return obst, u, temp, cfg, np.full(n ** 3, 0.3, np.float32)
 
 
 def rel_err(a: np.ndarray, b: np.ndarray) -> float:

@@ -18,6 +18,9 @@ Fixtures:
                   12 x 8 x 10 (y up), seeded 25-channel forcing (seed 5,
                   terrain up to 3 cells, wind (6, 0, 3) m/s), dx 64 m,
                   dt 5 s; the 6-channel state after 30 calls.
+  cavity_12_25.npz the differentially heated cavity preset (3-D) with the
+                  BFECC temperature transport: oracle.heated_cavity_case(12,
+                  seed 3), 25 steps; write_output and the temperature state.
   thermal_12_20.npz buoyancy on with the reference's temperature transport:
                   oracle.thermal_case(12, seed 11) (every thermal face kind,
                   packet source channel, state preloaded), 20 steps; the
@@ -80,6 +83,16 @@ def thermal_fixture(ref) -> None:
     print("thermal_12_20 written")
 
 
+def cavity_fixture(ref) -> None:
+    n, seed, steps = 12, 3, 25
+    obst, u, temp, cfg, preload = O.heated_cavity_case(n, seed)
+    pk = O.packet_from(obst, *u, temperature=temp)
+    out = ref.run((n, n, n), cfg, pk, steps, temperature_state=preload)
+    np.savez_compressed(OUT / "cavity_12_25.npz", out=out, temperature=ref.temperature, seed=seed, n=n, steps=steps,
+                        input_sha256=digest(pk, preload))
+    print("cavity_12_25 written")
+
+
 def main() -> int:
     O.build(ref=True)
     ref = O.RefLib()
@@ -87,6 +100,8 @@ def main() -> int:
     if only:
         if only in "thermal_12_20":
             thermal_fixture(ref)
+        if only in "cavity_12_25":
+            cavity_fixture(ref)
         return 0
     for name, n, steps in (("c1_16_200", 16, 200), ("c1_32_1000", 32, 1000)):
         seed = 1234
@@ -110,6 +125,7 @@ def main() -> int:
                         input_sha256=digest(forcing))
     print("meso_12x8x10_30 written")
     thermal_fixture(ref)
+    cavity_fixture(ref)
     return 0
 
 

@@ -124,3 +124,35 @@ def test_oracle_thermal_transport_matches_reference_live(preload, source):
     o.step(steps)
     assert _bits_equal(o.output(), out)
     assert _bits_equal(o.temperature(), ref.temperature)
+
+
+def test_oracle_bfecc_transport_matches_golden():
+    """Heated-cavity preset: its BFECC temperature transport (forward and
+    backward advection, error correction, local limiter, diffusion) and the
+    preset's derived Rayleigh/Prandtl/Mach parameters, bit-identical to the
+    reference library's fixture."""
+    g = np.load(GOLDEN / "cavity_12_25.npz")
+    n = int(g["n"])
+    obst, u, temp, cfg, preload = O.heated_cavity_case(n, int(g["seed"]))
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+    o.set_temperature(preload)
+    o.set_fields(obst, *u, temperature=temp)
+    o.step(int(g["steps"]))
+    assert _bits_equal(o.output(), g["out"])
+    assert _bits_equal(o.temperature(), g["temperature"])
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("preset", [O.PRESET_HEATED_CAVITY_2D, O.PRESET_HEATED_CAVITY_3D])
+def test_oracle_bfecc_transport_matches_reference_live(preset):
+    n, steps = 10, 15
+    obst, u, temp, cfg, pre = O.heated_cavity_case(n, seed=9, preset=preset)
+    pk = O.packet_from(obst, *u, temperature=temp)
+    ref = O.RefLib()
+    out = ref.run((n, n, n), cfg, pk, steps, temperature_state=pre)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    o.set_fields(obst, *u, temperature=temp)
+    o.step(steps)
+    assert _bits_equal(o.output(), out)
+    assert _bits_equal(o.temperature(), ref.temperature)
