@@ -397,6 +397,7 @@ void Context::release_device() {
     fr(reinterpret_cast<void*&>(ref_uz));
     fr(reinterpret_cast<void*&>(temperature));
     fr(reinterpret_cast<void*&>(temperature_next));
+    fr(reinterpret_cast<void*&>(temperature_scratch));
     fr(reinterpret_cast<void*&>(ref_temperature));
     fr(reinterpret_cast<void*&>(thermal_source));
     fr(reinterpret_cast<void*&>(u_last));
@@ -617,8 +618,8 @@ static bool ensure_thermal(Context& ctx) {
         return cuda_ok(cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(float) + kCopySlack), "cudaMalloc(thermal)") &&
                cuda_ok(cudaMemsetAsync(*p, 0, n * sizeof(float), current_stream()), "cudaMemset(thermal)");
     };
-    return al(&ctx.temperature_next, c) && al(&ctx.ref_temperature, c) && al(&ctx.thermal_source, c) &&
-           al(&ctx.u_last, 3 * c);
+    return al(&ctx.temperature_next, c) && al(&ctx.temperature_scratch, c) && al(&ctx.ref_temperature, c) &&
+           al(&ctx.thermal_source, c) && al(&ctx.u_last, 3 * c);
 }
 
 // Thermal faces and diffusivity of the benchmark configuration
@@ -703,8 +704,14 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         ta.source = bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_INTERNAL_THERMAL_SOURCE) ? nullptr : ctx.thermal_source;
         ta.alpha = thermal_diffusivity();
         ta.faces = current_thermal_faces();
+        // thermal_bfecc_active (jni.cpp:871-873); outside benchmark mode the
+        // reference also strides the update and uses a turbulent local
+        // diffusivity, which this runtime does not model (no runtime-mode
+        // nudges or fans either)
+        ta.bfecc = (!bench_active() || heated_cavity()) ? 1 : 0;
+        ta.scratch = ctx.temperature_scratch;
         if (!cuda_ok(launch_thermal_update(ta, s), "thermal_update")) return false;
-        std::swap(ctx.temperature, ctx.temperature_next);
+        std::swap(ctx.temperature, ta.bfecc ? ctx.temperature_scratch : ctx.temperature_next);
     }
     if (ctx.layout == 0) {
         float* g_next = ctx.g[1 - ctx.cur];

@@ -35,6 +35,7 @@ struct Context {
     float* ref_uz = nullptr;
     float* temperature = nullptr;       // temperature the collision reads (transported state, or the packet field)
     float* temperature_next = nullptr;  // transport: the other state buffer
+    float* temperature_scratch = nullptr;  // transport (BFECC): third state buffer
     float* ref_temperature = nullptr;   // transport: packet temperature channel
     float* thermal_source = nullptr;    // transport: packet source channel
     float* u_last = nullptr;            // transport: velocity of the last collision, SoA 3 x cells

@@ -13,6 +13,12 @@
 // Neumann: T(x) + heat flux, otherwise T(x); for the sample the centre's T(x)
 // stands in). Solid cells hold 0. Built with --fmad=false and the reference's
 // operation order: bit-identical to the reference CPU step.
+//
+// The heated-cavity presets (and the reference outside benchmark mode) take
+// the BFECC branch instead (jni.cpp:2050-2135): S = A_-(T), N = clamp(T +
+// (T - A_+(S)) / 2), T' = clamp(clamp(A_-(N), local min/max of T) + dt (alpha
+// lap T + s)), with A_-/A_+ the trilinear samples at x -/+ dt u (their
+// fallback the sampled field's own value at x), three launches.
 #pragma once
 
 #include <cstdint>
@@ -43,6 +49,8 @@ struct ThermalArgs {
     const float* source;        // per-cell source (clamped to +-0.006) or null
     float alpha;                // thermal diffusivity
     ThermalFaces faces;
+    int bfecc;                  // 1: the BFECC branch (heated-cavity presets); the result lands in scratch
+    float* scratch;             // BFECC: third state buffer
 };
 
 // First call of a context: the state and the velocity the first update

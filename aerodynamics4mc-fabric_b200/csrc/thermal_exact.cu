@@ -9,7 +9,7 @@ namespace {
 
 // thermal_field_neighbor_or_self (jni.cpp:1800-1825) with remap_thermal_coords
 // (jni.cpp:738-749, 779-785) and thermal_face_for_oob (jni.cpp:761-769).
-__device__ __forceinline__ float th_neighbour(const ThermalArgs& a, int x, int y, int z, float self) {
+__device__ __forceinline__ float th_neighbour(const ThermalArgs& a, const float* field, int x, int y, int z, float self) {
     const ThermalFaces& F = a.faces;
     if ((x < 0 || x >= a.nx) && F.kind[x < 0 ? 0 : 1] == kThermalPeriodic) {
         x %= a.nx;
@@ -38,22 +38,26 @@ __device__ __forceinline__ float th_neighbour(const ThermalArgs& a, int x, int y
     }
     const long long cell = ((long long)x * a.ny + y) * a.nz + z;
     if (a.obstacle[cell]) return self;
-    return a.t[cell];
+    return field[cell];
+}
+__device__ __forceinline__ float th_neighbour(const ThermalArgs& a, int x, int y, int z, float self) {
+    return th_neighbour(a, a.t, x, y, z, self);
 }
 
 // sample_temperature_trilinear_field (jni.cpp:1910-1945).
-__device__ __forceinline__ float th_sample(const ThermalArgs& a, float x, float y, float z, float fallback) {
+__device__ __forceinline__ float th_sample(const ThermalArgs& a, const float* field, float x, float y, float z,
+                                           float fallback) {
     const int x0 = (int)floorf(x), y0 = (int)floorf(y), z0 = (int)floorf(z);
     const int x1 = x0 + 1, y1 = y0 + 1, z1 = z0 + 1;
     const float fx = x - (float)x0, fy = y - (float)y0, fz = z - (float)z0;
-    const float c000 = th_neighbour(a, x0, y0, z0, fallback);
-    const float c100 = th_neighbour(a, x1, y0, z0, fallback);
-    const float c010 = th_neighbour(a, x0, y1, z0, fallback);
-    const float c110 = th_neighbour(a, x1, y1, z0, fallback);
-    const float c001 = th_neighbour(a, x0, y0, z1, fallback);
-    const float c101 = th_neighbour(a, x1, y0, z1, fallback);
-    const float c011 = th_neighbour(a, x0, y1, z1, fallback);
-    const float c111 = th_neighbour(a, x1, y1, z1, fallback);
+    const float c000 = th_neighbour(a, field, x0, y0, z0, fallback);
+    const float c100 = th_neighbour(a, field, x1, y0, z0, fallback);
+    const float c010 = th_neighbour(a, field, x0, y1, z0, fallback);
+    const float c110 = th_neighbour(a, field, x1, y1, z0, fallback);
+    const float c001 = th_neighbour(a, field, x0, y0, z1, fallback);
+    const float c101 = th_neighbour(a, field, x1, y0, z1, fallback);
+    const float c011 = th_neighbour(a, field, x0, y1, z1, fallback);
+    const float c111 = th_neighbour(a, field, x1, y1, z1, fallback);
     const float c00 = c000 + (c100 - c000) * fx;
     const float c10 = c010 + (c110 - c010) * fx;
     const float c01 = c001 + (c101 - c001) * fx;
@@ -132,7 +136,74 @@ __device__ __noinline__ void stage_outside(const ThermalFaces* F, const float* t
 // collision: the speed clamp keeps |u| < 1; only a first call's packet
 // velocity can); out of line.
 __device__ __noinline__ float th_sample_far(const ThermalArgs& a, float px, float py, float pz, float fallback) {
-    return th_sample(a, px, py, pz, fallback);
+    return th_sample(a, a.t, px, py, pz, fallback);
+}
+
+// ---- BFECC branch (jni.cpp:2050-2135): one thread per cell, line grid.
+__device__ __forceinline__ bool th_line_cell(const ThermalArgs& a, int& x, int& y, int& z, int& cell) {
+    z = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y;
+    x = blockIdx.z;
+    cell = (x * a.ny + y) * a.nz + z;
+    return z < a.nz;
+}
+
+// scratch = A_-(T)
+__global__ void __launch_bounds__(128) bfecc_forward_kernel(ThermalArgs a) {
+    int x, y, z, cell;
+    if (!th_line_cell(a, x, y, z, cell)) return;
+    if (a.obstacle[cell]) {
+        a.scratch[cell] = 0.0f;
+        return;
+    }
+    const float dt = 1.0f;
+    const float ux = a.u[cell], uy = a.u[a.cells + cell], uz = a.u[2 * a.cells + cell];
+    a.scratch[cell] = th_sample(a, a.t, (float)x - dt * ux, (float)y - dt * uy, (float)z - dt * uz, a.t[cell]);
+}
+
+// next = clamp(T + (T - A_+(scratch)) / 2)
+__global__ void __launch_bounds__(128) bfecc_correct_kernel(ThermalArgs a) {
+    int x, y, z, cell;
+    if (!th_line_cell(a, x, y, z, cell)) return;
+    if (a.obstacle[cell]) {
+        a.t_next[cell] = 0.0f;
+        return;
+    }
+    const float dt = 1.0f;
+    const float tc = a.t[cell];
+    const float ux = a.u[cell], uy = a.u[a.cells + cell], uz = a.u[2 * a.cells + cell];
+    const float back = th_sample(a, a.scratch, (float)x + dt * ux, (float)y + dt * uy, (float)z + dt * uz, a.scratch[cell]);
+    a.t_next[cell] = exact::rclamp(tc + 0.5f * (tc - back), -1.0f, 1.0f);
+}
+
+// scratch = clamp(clamp(A_-(next), local bounds of T) + dt (alpha lap T + s))
+__global__ void __launch_bounds__(128) bfecc_final_kernel(ThermalArgs a) {
+    int x, y, z, cell;
+    if (!th_line_cell(a, x, y, z, cell)) return;
+    if (a.obstacle[cell]) {
+        a.scratch[cell] = 0.0f;
+        return;
+    }
+    const float dt = 1.0f, cooling = 0.0f;
+    const float tc = a.t[cell];
+    const float ux = a.u[cell], uy = a.u[a.cells + cell], uz = a.u[2 * a.cells + cell];
+    float adv = th_sample(a, a.t_next, (float)x - dt * ux, (float)y - dt * uy, (float)z - dt * uz, a.t_next[cell]);
+    const float n0 = th_neighbour(a, x + 1, y, z, tc), n1 = th_neighbour(a, x - 1, y, z, tc);
+    const float n2 = th_neighbour(a, x, y + 1, z, tc), n3 = th_neighbour(a, x, y - 1, z, tc);
+    const float n4 = th_neighbour(a, x, y, z + 1, tc), n5 = th_neighbour(a, x, y, z - 1, tc);
+    // local_temperature_bounds (jni.cpp:1883-1908): std::min / std::max in neighbour order
+    float lo = tc, hi = tc;
+    const float nb[6] = {n0, n1, n2, n3, n4, n5};
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        lo = exact::rmin(lo, nb[i]);
+        hi = exact::rmax(hi, nb[i]);
+    }
+    adv = exact::rclamp(adv, lo, hi);
+    const float t_sum = n0 + n1 + n2 + n3 + n4 + n5;
+    const float lap = t_sum - 6.0f * tc;
+    const float src = a.source ? exact::rclamp(a.source[cell], -0.006f, 0.006f) : 0.0f;
+    a.scratch[cell] = exact::rclamp(adv + dt * (a.alpha * lap + src - cooling * adv), -1.0f, 1.0f);
 }
 
 template <int kKind>
@@ -272,6 +343,17 @@ cudaError_t launch_thermal_init(const ThermalInitArgs& a, cudaStream_t s) {
 cudaError_t launch_thermal_update(const ThermalArgs& a, cudaStream_t s) {
     if (a.cells <= 0) return cudaSuccess;
     if (a.cells >= (1LL << 31)) return cudaErrorInvalidValue;  // 32-bit cell indices
+    if (a.bfecc) {
+        const int block = a.nz >= 128 ? 128 : ((a.nz + 31) / 32) * 32;
+        const dim3 grid((unsigned)((a.nz + block - 1) / block), (unsigned)a.ny, (unsigned)a.nx);
+        bfecc_forward_kernel<<<grid, block, 0, s>>>(a);
+        count_launch();
+        bfecc_correct_kernel<<<grid, block, 0, s>>>(a);
+        count_launch();
+        bfecc_final_kernel<<<grid, block, 0, s>>>(a);
+        count_launch();
+        return cudaGetLastError();
+    }
     const dim3 grid((unsigned)((a.nz + kTZ - 1) / kTZ), (unsigned)((a.ny + kTY - 1) / kTY), (unsigned)((a.nx + kTX - 1) / kTX));
     thermal_update_kernel<<<grid, dim3(kTZ, kTY), 0, s>>>(a);
     count_launch();

@@ -139,3 +139,18 @@ def test_thermal_modes(gpu):
     o.step(steps)
     assert_bits(out1, o.output())
     assert np.array_equal(t1.view(np.uint32), o.temperature().view(np.uint32))
+
+
+@pytest.mark.parametrize("streaming,cpt", [(1, 1), (2, 2)])
+def test_bfecc_transport_matches_reference_golden(gpu, streaming, cpt):
+    """Differentially heated cavity preset (3-D): the BFECC temperature
+    transport (three launches) and the preset's derived parameters,
+    bit-identical to the reference library's fixture (flow output and
+    temperature state)."""
+    g = np.load(GOLDEN / "cavity_12_25.npz")
+    n, steps = int(g["n"]), int(g["steps"])
+    obst, u, temp, cfg, preload = O.heated_cavity_case(n, int(g["seed"]))
+    pk = O.packet_from(obst, *u, temperature=temp)
+    out, t = _run(gpu, n, cfg, [(0, pk)], steps, streaming, preload, key=680 + streaming, cpt=cpt)
+    assert_bits(out, g["out"])
+    assert np.array_equal(t.view(np.uint32), np.asarray(g["temperature"], np.float32).view(np.uint32))
