@@ -18,6 +18,8 @@
 //   stream_and_bounce       native/src/aero_lbm_jni.cpp:2415-2452
 //   write_output            native/src/aero_lbm_jni.cpp:2535-2581
 //   strided atlas extract   native/src/aero_lbm_jni.cpp:9246-9450
+//   halo exchange           native/src/aero_lbm_jni.cpp:8136-8265 (slab bounds,
+//                           slab copies), 9692-9780 (layers entry point)
 //   temperature transport   native/src/aero_lbm_jni.cpp:2049-2143 (first-order
 //                           and BFECC branches), helpers 738-769, 1783-1950; per-call order
 //                           and state rules 1752-1781, 8028-8064, 8480-8507
@@ -721,6 +723,58 @@ struct Handle {
     std::unique_ptr<D3Q27Oracle<double>> f64;
 };
 
+// halo_exchange_slab_bounds (jni.cpp:8201-8264), one axis: the first
+// context's source start, the second's destination start, the second's
+// source start, the first's destination start and the slab size.
+bool halo_axis(int offset, int extent, int halo, int core, int& first_src, int& second_dst, int& second_src,
+               int& first_dst, int& size) {
+    switch (offset) {
+        case -1: first_src = halo; second_dst = extent - halo; second_src = core; first_dst = 0; size = halo; return true;
+        case 0: first_src = halo; second_dst = halo; second_src = halo; first_dst = halo; size = core; return true;
+        case 1: first_src = core; second_dst = 0; second_src = halo; first_dst = extent - halo; size = halo; return true;
+        default: return false;
+    }
+}
+
+// exchange_context_halo_cpu_layers (jni.cpp:8266-8426): the populations (27
+// per cell, the streamed state) and the temperature of one slab copied from
+// each context into the other's halo.
+template <typename T>
+int exchange_halo(D3Q27Oracle<T>& a, D3Q27Oracle<T>& b, int ox, int oy, int oz, int halo_layers) {
+    if (a.nx != b.nx || a.ny != b.ny || a.nz != b.nz || a.nx != a.ny || a.ny != a.nz) return 0;
+    const int n = a.nx;
+    const int halo = std::max(1, std::min(halo_layers, n / 2 - 1));
+    const int core = n - 2 * halo;
+    if (core <= 0) return 0;
+    int s1[3], d2[3], s2[3], d1[3], sz[3];
+    const int off[3] = {ox, oy, oz};
+    for (int k = 0; k < 3; ++k)
+        if (!halo_axis(off[k], n, halo, core, s1[k], d2[k], s2[k], d1[k], sz[k])) return 0;
+    auto copy = [&](const D3Q27Oracle<T>& src, D3Q27Oracle<T>& dst, const int* so, const int* doff) {
+        for (int x = 0; x < sz[0]; ++x)
+            for (int y = 0; y < sz[1]; ++y)
+                for (int z = 0; z < sz[2]; ++z) {
+                    const size_t sc = src.cell_index(so[0] + x, so[1] + y, so[2] + z);
+                    const size_t dc = dst.cell_index(doff[0] + x, doff[1] + y, doff[2] + z);
+                    for (int q = 0; q < 27; ++q) dst.f[dst.di(dc, q)] = src.f[src.di(sc, q)];
+                }
+    };
+    auto copy_t = [&](const D3Q27Oracle<T>& src, D3Q27Oracle<T>& dst, const int* so, const int* doff) {
+        for (int x = 0; x < sz[0]; ++x)
+            for (int y = 0; y < sz[1]; ++y)
+                for (int z = 0; z < sz[2]; ++z)
+                    dst.temperature[dst.cell_index(doff[0] + x, doff[1] + y, doff[2] + z)] =
+                        src.temperature[src.cell_index(so[0] + x, so[1] + y, so[2] + z)];
+    };
+    copy(a, b, s1, d2);
+    copy(b, a, s2, d1);
+    copy_t(a, b, s1, d2);
+    copy_t(b, a, s2, d1);
+    a.temperature_next = a.temperature;
+    b.temperature_next = b.temperature;
+    return 1;
+}
+
 template <typename T>
 void load_fields(D3Q27Oracle<T>& o, const uint8_t* obstacle, const float* ux, const float* uy, const float* uz,
                  const float* pressure, const float* temperature) {
@@ -852,6 +906,18 @@ int oracle_d3q27_output(void* handle, float scale, float* out) {
         for (size_t c = 0; c < h->f64->cells; ++c) h->f64->cell_output(c, double(scale), out + 4 * c);
     }
     return 1;
+}
+
+// aero_lbm_exchange_halo_layers_rect between two contexts of the same
+// precision and shape (the second one lies at offset (ox, oy, oz) in
+// {-1, 0, 1}^3 without 0 from the first).
+int oracle_d3q27_exchange_halo(void* first, void* second, int ox, int oy, int oz, int halo_layers) {
+    auto* a = static_cast<Handle*>(first);
+    auto* b = static_cast<Handle*>(second);
+    if (!a || !b || a->precision != b->precision || halo_layers <= 0) return 0;
+    if (ox < -1 || ox > 1 || oy < -1 || oy > 1 || oz < -1 || oz > 1 || (ox == 0 && oy == 0 && oz == 0)) return 0;
+    return a->f32 ? exchange_halo(*a->f32, *b->f32, ox, oy, oz, halo_layers)
+                  : exchange_halo(*a->f64, *b->f64, ox, oy, oz, halo_layers);
 }
 
 // Strided atlas (aero_lbm_extract_flow_atlas_rect semantics, scale 1).

@@ -198,6 +198,7 @@ class Oracle:
             lib.oracle_d3q27_set_thermal_source.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.oracle_d3q27_get_temperature.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.oracle_d3q27_set_temperature.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.oracle_d3q27_exchange_halo.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 4
             cls._lib = lib
         return cls._lib
 
@@ -235,6 +236,10 @@ class Oracle:
         out = np.zeros(self.cells, dtype=np.float32)
         self.lib().oracle_d3q27_get_temperature(self.h, out.ctypes.data)
         return out
+
+    def exchange_halo(self, other: "Oracle", offset, halo_layers: int):
+        if not self.lib().oracle_d3q27_exchange_halo(self.h, other.h, *[int(v) for v in offset], int(halo_layers)):
+            raise RuntimeError("oracle halo exchange failed")
 
     def set_temperature(self, t):
         arr = np.ascontiguousarray(np.asarray(t, np.float32).reshape(-1))
@@ -387,6 +392,44 @@ class RefLib:
         return out.reshape(-1, 4)
 
 
+    def run_pair(self, dims, cfg: dict, packets, steps: int, offset, halo_layers: int, exchange_every: int = 1,
+                 keys=(1, 2), temperature_states=(None, None)):
+        """Two contexts stepped call for call, aero_lbm_exchange_halo_layers_rect
+        between them after every ``exchange_every`` calls (not after the
+        last); returns both write_output results of the last call and leaves
+        both temperature states in ``self.temperatures``."""
+        nx, ny, nz = dims
+        lib = self.lib
+        lib.aero_lbm_exchange_halo_layers_rect.argtypes = [ctypes.c_int] * 4 + [ctypes.c_longlong] * 2 + [ctypes.c_int] * 3
+        lib.aero_lbm_exchange_halo_layers_rect.restype = ctypes.c_int
+        if not lib.aero_lbm_init_rect(nx, ny, nz, packets[0].shape[1], 4):
+            raise RuntimeError(lib.aero_lbm_last_error())
+        c = config_struct(RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
+        if not lib.aero_lbm_benchmark_set_config(ctypes.byref(c)):
+            raise RuntimeError("set_config failed")
+        for key, ts in zip(keys, temperature_states):
+            if ts is not None:
+                t = np.ascontiguousarray(np.asarray(ts, np.float32).reshape(-1))
+                if not lib.aero_lbm_set_temperature_state_rect(nx, ny, nz, key, t.ctypes.data):
+                    raise RuntimeError(lib.aero_lbm_last_error())
+        outs = [np.zeros(nx * ny * nz * 4, dtype=np.float32) for _ in keys]
+        pks = [np.ascontiguousarray(p, dtype=np.float32) for p in packets]
+        for s in range(steps):
+            last = s + 1 == steps
+            for key, pk, out in zip(keys, pks, outs):
+                if not lib.aero_lbm_step_rect(pk.ctypes.data, nx, ny, nz, key, out.ctypes.data if last else None):
+                    raise RuntimeError(lib.aero_lbm_last_error())
+            if not last and (s + 1) % exchange_every == 0:
+                if not lib.aero_lbm_exchange_halo_layers_rect(nx, ny, nz, halo_layers, keys[0], keys[1], *offset):
+                    raise RuntimeError(lib.aero_lbm_last_error())
+        self.temperatures = []
+        for key in keys:
+            t = np.zeros(nx * ny * nz, dtype=np.float32)
+            lib.aero_lbm_get_temperature_state_rect(nx, ny, nz, key, t.ctypes.data)
+            self.temperatures.append(t)
+        return [o.reshape(-1, 4) for o in outs]
+
+
 # ---------------------------------------------------------------- configs
 def c1_inputs(seed: int = 1234, n: int = 32, solid_p: float = 0.05, u0=(0.05, 0.0, 0.0), noise: float = 0.005):
     """Plain FP32 brick (32^3): solid floor z=0 + Bernoulli(p) interior,
@@ -451,6 +494,21 @@ def thermal_case(n: int = 12, seed: int = 11):
            "thermal_transport": True, "initial_temperature": 0.1, "thermal_source": True}
     preload = np.full(n ** 3, 0.5, np.float32)
     return obst, u, temp, src, cfg, preload
+
+
+def halo_case(n: int = 12, buoyancy: bool = True):
+    """Two bricks for the halo exchange: thermal_case(n, 11) (source off) and
+    a second brick with 8% solids (seed 5), u = (0.03,0,0) + U(-0.01,0.01),
+    temperature U(-0.3,0.3). Returns the config, both packets and the
+    temperature state both start from."""
+    obst, u, temp, src, cfg, pre = thermal_case(n, 11)
+    cfg = dict(cfg, thermal_source=False, buoyancy=buoyancy)
+    rng = np.random.default_rng(5)
+    dims = (n, n, n)
+    obst2 = (rng.random(dims) < 0.08).astype(np.uint8)
+    u2 = [np.float32(0.03) + rng.uniform(-0.01, 0.01, dims).astype(np.float32) for _ in range(3)]
+    temp2 = rng.uniform(-0.3, 0.3, dims).astype(np.float32)
+    return cfg, [packet_from(obst, *u, temperature=temp), packet_from(obst2, *u2, temperature=temp2)], pre
 
 
 def heated_cavity_case(n: int = 12, seed: int = 3, preset: int = PRESET_HEATED_CAVITY_3D):

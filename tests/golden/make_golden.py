@@ -21,6 +21,11 @@ Fixtures:
   cavity_12_25.npz the differentially heated cavity preset (3-D) with the
                   BFECC temperature transport: oracle.heated_cavity_case(12,
                   seed 3), 25 steps; write_output and the temperature state.
+  halo_12_12.npz  two overlapping 12^3 bricks (oracle.halo_case: the thermal
+                  case and a second seeded brick, buoyancy on), halo 2 at
+                  offset (1, -1, 0), aero_lbm_exchange_halo_layers_rect after
+                  every third of 12 calls; both write_output results and
+                  temperature states.
   thermal_12_20.npz buoyancy on with the reference's temperature transport:
                   oracle.thermal_case(12, seed 11) (every thermal face kind,
                   packet source channel, state preloaded), 20 steps; the
@@ -93,6 +98,16 @@ def cavity_fixture(ref) -> None:
     print("cavity_12_25 written")
 
 
+def halo_fixture(ref) -> None:
+    n, steps, offset, halo, every = 12, 12, (1, -1, 0), 2, 3
+    cfg, pks, pre = O.halo_case(n)
+    outs = ref.run_pair((n, n, n), cfg, pks, steps, offset, halo, exchange_every=every, temperature_states=(pre, pre))
+    np.savez_compressed(OUT / "halo_12_12.npz", out1=outs[0], out2=outs[1], t1=ref.temperatures[0], t2=ref.temperatures[1],
+                        n=n, steps=steps, offset=np.array(offset), halo=halo, every=every,
+                        input_sha256=digest(pks[0], pks[1], pre))
+    print("halo_12_12 written")
+
+
 def main() -> int:
     O.build(ref=True)
     ref = O.RefLib()
@@ -102,6 +117,8 @@ def main() -> int:
             thermal_fixture(ref)
         if only in "cavity_12_25":
             cavity_fixture(ref)
+        if only in "halo_12_12":
+            halo_fixture(ref)
         return 0
     for name, n, steps in (("c1_16_200", 16, 200), ("c1_32_1000", 32, 1000)):
         seed = 1234
@@ -126,6 +143,7 @@ def main() -> int:
     print("meso_12x8x10_30 written")
     thermal_fixture(ref)
     cavity_fixture(ref)
+    halo_fixture(ref)
     return 0
 
 

@@ -156,3 +156,42 @@ def test_oracle_bfecc_transport_matches_reference_live(preset):
     o.step(steps)
     assert _bits_equal(o.output(), out)
     assert _bits_equal(o.temperature(), ref.temperature)
+
+
+def _halo_oracles(cfg, pks, pre, steps, offset, halo, every, precision="f32"):
+    n = int(round(pks[0].shape[0] ** (1 / 3)))
+    os_ = [O.Oracle((n, n, n), O.derive_params(cfg), precision) for _ in pks]
+    for o, pk in zip(os_, pks):
+        o.set_temperature(pre)
+        o.set_fields(pk[:, 0].reshape(n, n, n).astype(np.uint8), *(pk[:, 5 + a].reshape(n, n, n) for a in range(3)),
+                     temperature=pk[:, 10].reshape(n, n, n))
+    for s in range(steps):
+        for o in os_:
+            o.step(1)
+        if s + 1 < steps and (s + 1) % every == 0:
+            os_[0].exchange_halo(os_[1], offset, halo)
+    return os_
+
+
+def test_oracle_halo_exchange_matches_golden():
+    """Two overlapping bricks with the reference's halo exchange between calls
+    (populations and temperature of the slabs), bit-identical to the
+    reference library's fixture."""
+    g = np.load(GOLDEN / "halo_12_12.npz")
+    cfg, pks, pre = O.halo_case(int(g["n"]))
+    os_ = _halo_oracles(cfg, pks, pre, int(g["steps"]), tuple(int(v) for v in g["offset"]), int(g["halo"]), int(g["every"]))
+    assert _bits_equal(os_[0].output(), g["out1"]) and _bits_equal(os_[1].output(), g["out2"])
+    assert _bits_equal(os_[0].temperature(), g["t1"]) and _bits_equal(os_[1].temperature(), g["t2"])
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("offset,halo,buoy", [((1, 0, 0), 2, False), ((0, -1, 1), 3, True), ((1, 1, 1), 1, True)])
+def test_oracle_halo_exchange_matches_reference_live(offset, halo, buoy):
+    n, steps, every = 12, 9, 2
+    cfg, pks, pre = O.halo_case(n, buoyancy=buoy)
+    ref = O.RefLib()
+    outs = ref.run_pair((n, n, n), cfg, pks, steps, offset, halo, exchange_every=every, temperature_states=(pre, pre))
+    os_ = _halo_oracles(cfg, pks, pre, steps, offset, halo, every)
+    for o, out, t in zip(os_, outs, ref.temperatures):
+        assert _bits_equal(o.output(), out)
+        assert _bits_equal(o.temperature(), t)
