@@ -198,6 +198,8 @@ SIGNATURES = {
     "aero_lbm_step_rect_cached_scaled": (_I, [_I, _I, _I, _LL, _F, _F32P]),
     "aero_lbm_has_context": (_I, [_LL]),
     "aero_lbm_context_realtime_cached_initialized": (_I, [_LL]),
+    "aero_lbm_exchange_halo": (_I, [_I, _LL, _LL, _I, _I, _I]),
+    "aero_lbm_exchange_halo_layers_rect": (_I, [_I, _I, _I, _I, _LL, _LL, _I, _I, _I]),
     "aero_lbm_get_temperature_state_rect": (_I, [_I, _I, _I, _LL, _F32P]),
     "aero_lbm_extract_flow_atlas_rect": (_I, [_I, _I, _I, _LL, _I, _F32P, _I]),
     "aero_lbm_get_flow_state_rect": (_I, [_I, _I, _I, _LL, _F32P]),

@@ -51,7 +51,7 @@ __device__ __forceinline__ void accumulate_cell(const float (&f)[27], double (&a
 __global__ void conservation_ab_kernel(int nx, int ny, int nz, const float* __restrict__ g,
                                        const uint32_t* __restrict__ flags, const uint8_t* __restrict__ obstacle,
                                        const float* __restrict__ ref_p, const FaceParams* __restrict__ F,
-                                       double* __restrict__ partials) {
+                                       double* __restrict__ partials, int direct) {
     const long long cells = (long long)nx * ny * nz;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x; cell < cells;
@@ -60,8 +60,13 @@ __global__ void conservation_ab_kernel(int nx, int ny, int nz, const float* __re
         if (w & kFlagSelfSolid) continue;
         const int z = (int)(cell % nz), y = (int)((cell / nz) % ny), x = (int)(cell / ((long long)ny * nz));
         float f[27];
-        const PullView v{g, obstacle, ref_p, F, cells, nx, ny, nz};
-        pull27(v, w, cell, x, y, z, f);
+        if (direct) {  // g holds the streamed state itself (after a halo exchange)
+#pragma unroll
+            for (int q = 0; q < 27; ++q) f[q] = g[(long long)q * cells + cell];
+        } else {
+            const PullView v{g, obstacle, ref_p, F, cells, nx, ny, nz};
+            pull27(v, w, cell, x, y, z, f);
+        }
         accumulate_cell(f, acc);
     }
     block_sum4(acc);
@@ -85,7 +90,7 @@ __global__ void conservation_ip_kernel(const typename S::T* __restrict__ f, IpAr
         const int own = pad_index(G, x, y, z);
         const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
         float fl[27];
-        ip_pull<S>(f, a, G, o, own, w, cell, x, y, z, a.parity, a.ref_p_prev, a.face_prev, fl);
+        ip_pull<S>(f, a, G, o, own, w, a.parity, fl);
         accumulate_cell(fl, acc);
     }
     block_sum4(acc);
@@ -115,9 +120,10 @@ int conservation_blocks(long long cells) {
 
 cudaError_t launch_conservation_ab(int nx, int ny, int nz, const float* g, const uint32_t* flags,
                                    const uint8_t* obstacle, const float* ref_p, const FaceParams* face,
-                                   double* partials, double* out, cudaStream_t s) {
+                                   double* partials, double* out, cudaStream_t s, int direct) {
     const int blocks = conservation_blocks((long long)nx * ny * nz);
-    conservation_ab_kernel<<<blocks, kConservationThreads, 0, s>>>(nx, ny, nz, g, flags, obstacle, ref_p, face, partials);
+    conservation_ab_kernel<<<blocks, kConservationThreads, 0, s>>>(nx, ny, nz, g, flags, obstacle, ref_p, face, partials,
+                                                                   direct);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -101,7 +101,7 @@ __device__ __forceinline__ void add_cell(const float (&f)[27], double (&acc)[4])
 __global__ void static_sums_ab_kernel(int nx, int ny, int nz, const float* __restrict__ g,
                                       const uint32_t* __restrict__ flags, const uint8_t* __restrict__ obstacle,
                                       const float* __restrict__ ref_p, const FaceParams* __restrict__ F,
-                                      double* __restrict__ partials) {
+                                      double* __restrict__ partials, int direct) {
     const long long cells = (long long)nx * ny * nz;
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -110,8 +110,13 @@ __global__ void static_sums_ab_kernel(int nx, int ny, int nz, const float* __res
         if (!(w & kFlagSelfSolid)) {
             const int z = (int)(cell % nz), y = (int)((cell / nz) % ny), x = (int)(cell / ((long long)ny * nz));
             float f[27];
-            const PullView v{g, obstacle, ref_p, F, cells, nx, ny, nz};
-            pull27(v, w, cell, x, y, z, f);
+            if (direct) {  // g holds the streamed state itself (after a halo exchange)
+#pragma unroll
+                for (int q = 0; q < 27; ++q) f[q] = g[(long long)q * cells + cell];
+            } else {
+                const PullView v{g, obstacle, ref_p, F, cells, nx, ny, nz};
+                pull27(v, w, cell, x, y, z, f);
+            }
             add_cell(f, acc);
         }
     }
@@ -136,7 +141,7 @@ __global__ void static_sums_ip_kernel(const typename S::T* __restrict__ f, IpArg
             const int own = pad_index(G, x, y, z);
             const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
             float fl[27];
-            ip_pull<S>(f, a, G, o, own, w, cell, x, y, z, a.parity, a.ref_p_prev, a.face_prev, fl);
+            ip_pull<S>(f, a, G, o, own, w, a.parity, fl);
             add_cell(fl, acc);
         }
     }
@@ -194,9 +199,10 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums_noalloc(long long conte
     cudaStream_t s = current_stream();
     const int blocks = (int)((c->cells + kStaticThreads - 1) / kStaticThreads);
     if (c->layout == 0) {
-        static_sums_ab_kernel<<<blocks, kStaticThreads, 0, s>>>(c->nx, c->ny, c->nz, c->g[c->cur], c->flags[c->slot],
+        const float* g = c->f_ready ? c->g[1 - c->cur] : c->g[c->cur];
+        static_sums_ab_kernel<<<blocks, kStaticThreads, 0, s>>>(c->nx, c->ny, c->nz, g, c->flags[c->slot],
                                                                 c->obstacle[c->slot], c->ref_p[c->slot],
-                                                                c->d_face[c->slot], scratch);
+                                                                c->d_face[c->slot], scratch, c->f_ready ? 1 : 0);
     } else {
         IpArgs a{};
         a.g = make_pad_geom(c->nx, c->ny, c->nz, c->periodic_mask);

@@ -17,15 +17,21 @@ cudaError_t launch_step_ab_exact(BrickDims d, const float* g_in, float* g_out, c
                                    stream);
 }
 
+cudaError_t launch_collide_ab_exact(BrickDims d, float* f_io, CellFields cur, ForceField force, CollideParams cp,
+                                 cudaStream_t stream) {
+    return launch_collide_ab_t<true>(d, f_io, cur, force, cp, stream);
+}
+
 cudaError_t launch_output_ab_exact(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
                                 const float* ref_p, const FaceParams* face, int stride, int out_channels,
-                                float velocity_scale, float* out, cudaStream_t stream) {
+                                float velocity_scale, float* out, cudaStream_t stream, int direct) {
     return launch_output_ab_t<true>(d, g, flags, obstacle, ref_p, face, stride, out_channels, velocity_scale, out,
-                                     stream);
+                                     stream, direct);
 }
 
 
 cudaError_t ip_init_f32_exact(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, true>::init(f, a, s); }
+cudaError_t ip_fill_f32_exact(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, true>::face_fill(f, a, s); }
 cudaError_t ip_step_f32_exact(float* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
     return IpLaunch<StoreF32, true>::step(f, a, transitions, fill, s);
 }

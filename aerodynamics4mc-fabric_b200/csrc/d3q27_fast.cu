@@ -16,15 +16,21 @@ cudaError_t launch_step_ab_fast(BrickDims d, const float* g_in, float* g_out, co
                                    stream);
 }
 
+cudaError_t launch_collide_ab_fast(BrickDims d, float* f_io, CellFields cur, ForceField force, CollideParams cp,
+                                 cudaStream_t stream) {
+    return launch_collide_ab_t<false>(d, f_io, cur, force, cp, stream);
+}
+
 cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
                                 const float* ref_p, const FaceParams* face, int stride, int out_channels,
-                                float velocity_scale, float* out, cudaStream_t stream) {
+                                float velocity_scale, float* out, cudaStream_t stream, int direct) {
     return launch_output_ab_t<false>(d, g, flags, obstacle, ref_p, face, stride, out_channels, velocity_scale, out,
-                                     stream);
+                                     stream, direct);
 }
 
 
 cudaError_t ip_init_f32_fast(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, false>::init(f, a, s); }
+cudaError_t ip_fill_f32_fast(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, false>::face_fill(f, a, s); }
 cudaError_t ip_step_f32_fast(float* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
     return IpLaunch<StoreF32, false>::step(f, a, transitions, fill, s);
 }
@@ -33,6 +39,7 @@ cudaError_t ip_output_f32_fast(const float* f, const IpArgs& a, int stride, int 
 }
 
 cudaError_t ip_init_f16_fast(__half* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF16Dev, false>::init(f, a, s); }
+cudaError_t ip_fill_f16_fast(__half* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF16Dev, false>::face_fill(f, a, s); }
 cudaError_t ip_step_f16_fast(__half* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
     return IpLaunch<StoreF16Dev, false>::step(f, a, transitions, fill, s);
 }
@@ -41,6 +48,7 @@ cudaError_t ip_output_f16_fast(const __half* f, const IpArgs& a, int stride, int
 }
 
 cudaError_t ip_init_i16_fast(short* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreI16Dev, false>::init(f, a, s); }
+cudaError_t ip_fill_i16_fast(short* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreI16Dev, false>::face_fill(f, a, s); }
 cudaError_t ip_step_i16_fast(short* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
     return IpLaunch<StoreI16Dev, false>::step(f, a, transitions, fill, s);
 }

@@ -55,36 +55,17 @@ __device__ __forceinline__ float ip_face_equilibrium(const FaceParams& F, int q,
     return feq27(q, rho, ux, uy, uz);
 }
 
-// Incoming populations of a fluid cell at parity p.
+// Incoming populations of a fluid cell at parity p, read between calls: every
+// call ends with the equilibrium-face pre-fill, so each incoming slot (the
+// face sources included) holds the cell's streamed population.
 template <class S>
 __device__ __forceinline__ void ip_pull(const typename S::T* __restrict__ f, const IpArgs& a, const PadGeom& G,
-                                        const NeighbourOffsets& o, int own, uint32_t w, long long cell, int x, int y,
-                                        int z, int p, const float* ref_p, const FaceParams* F, float (&fl)[27]) {
-    if (!(w & kFlagFaceSpecial)) {
-#pragma unroll
-        for (int q = 0; q < 27; ++q) {
-            int c, d;
-            incoming_slot(o, own, q, p, (w >> q) & 1u, c, d);
-            fl[q] = S::load(f + (long long)d * G.pcells + c, q, a.sc);
-        }
-        return;
-    }
+                                        const NeighbourOffsets& o, int own, uint32_t w, int p, float (&fl)[27]) {
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
-        const bool bb = (w >> q) & 1u;
-        // Periodic axes wrap first, then the first axis still outside picks
-        // the face (remap_hydrodynamic_coords + hydrodynamic_face_for_oob).
-        const int sx = axis_neighbour(x, -q_cx(q), G.nx, G.wrap[0]);
-        const int sy = axis_neighbour(y, -q_cy(q), G.ny, G.wrap[1]);
-        const int sz = axis_neighbour(z, -q_cz(q), G.nz, G.wrap[2]);
-        const bool oob = sx < 0 || sx >= G.nx || sy < 0 || sy >= G.ny || sz < 0 || sz >= G.nz;
-        if (!bb && oob) {
-            fl[q] = ip_face_equilibrium(*F, q, ref_p[cell], sx, sy, sz, G.nx, G.ny, G.nz);
-        } else {
-            int c, d;
-            incoming_slot(o, own, q, p, bb, c, d);
-            fl[q] = S::load(f + (long long)d * G.pcells + c, q, a.sc);
-        }
+        int c, d;
+        incoming_slot(o, own, q, p, (w >> q) & 1u, c, d);
+        fl[q] = S::load(f + (long long)d * G.pcells + c, q, a.sc);
     }
 }
 
@@ -479,7 +460,7 @@ __global__ void output_ip_kernel(const typename S::T* __restrict__ f, IpArgs a, 
         const int own = pad_index(G, x, y, z);
         const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
         float fl[27];
-        ip_pull<S>(f, a, G, o, own, w, cell, x, y, z, a.parity, a.ref_p_prev, a.face_prev, fl);
+        ip_pull<S>(f, a, G, o, own, w, a.parity, fl);
         if (kExact) exact::macro_out_exact(fl, false, scale, o4);
         else macro_out(fl, false, scale, o4);
     }

@@ -84,15 +84,20 @@ cudaError_t launch_step_ab_exact(BrickDims d, const float* g_in, float* g_out, c
 cudaError_t launch_step_ab_fast(BrickDims d, const float* g_in, float* g_out, const uint32_t* flags_prev,
                                 const uint8_t* obstacle_prev, const float* ref_p_prev, const FaceParams* face_prev,
                                 CellFields cur, ForceField force, CollideParams cp, cudaStream_t stream);
+// Collision of a streamed state held in f_io (the call after a halo exchange).
+cudaError_t launch_collide_ab_exact(BrickDims d, float* f_io, CellFields cur, ForceField force, CollideParams cp,
+                                    cudaStream_t stream);
+cudaError_t launch_collide_ab_fast(BrickDims d, float* f_io, CellFields cur, ForceField force, CollideParams cp,
+                                   cudaStream_t stream);
 // Macro output of the streamed state S(g): write_output semantics
 // (AoS, out_channels per cell; ux,uy,uz scaled; clamp(rho - 1)).
-// `face` points to device memory.
+// `face` points to device memory. direct: g already holds the streamed state.
 cudaError_t launch_output_ab_exact(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
                                    const float* ref_p, const FaceParams* face, int stride, int out_channels,
-                                   float velocity_scale, float* out, cudaStream_t stream);
+                                   float velocity_scale, float* out, cudaStream_t stream, int direct = 0);
 cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
                                   const float* ref_p, const FaceParams* face, int stride, int out_channels,
-                                  float velocity_scale, float* out, cudaStream_t stream);
+                                  float velocity_scale, float* out, cudaStream_t stream, int direct = 0);
 
 uint64_t kernel_launch_count();
 void count_launch();

@@ -241,6 +241,43 @@ cudaError_t launch_step_ab_t(BrickDims d, const float* g_in, float* g_out, const
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- collide only (two buffers)
+// The call after a halo exchange: the streamed state f (the pull of the last
+// call, with the exchanged slabs written in) already sits in f_io; collide
+// it in place.
+template <bool kExact>
+__global__ void __launch_bounds__(128) collide_ab_kernel(int nx, int ny, int nz, float* __restrict__ f_io,
+                                                         CellFields cur, ForceField force, CollideParams cp) {
+    const long long cells = (long long)nx * ny * nz;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= cells) return;
+    if (cur.obstacle[cell]) {
+        // the reference collides no solid cell; its f stays as streamed
+        record_u(cur, cell, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    float f[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) f[q] = f_io[(long long)q * cells + cell];
+    if (!collide_cell<kExact>(f, cp, cur, force, cell)) {
+        reseed_store_ab(f_io, cells, cell, cur, cp.max_speed);
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < 27; ++q) f_io[(long long)q * cells + cell] = f[q];
+}
+
+template <bool kExact>
+cudaError_t launch_collide_ab_t(BrickDims d, float* f_io, CellFields cur, ForceField force, CollideParams cp,
+                                cudaStream_t stream) {
+    if (d.cells <= 0) return cudaSuccess;
+    const int block = 128;
+    collide_ab_kernel<kExact><<<(unsigned)((d.cells + block - 1) / block), block, 0, stream>>>(d.nx, d.ny, d.nz, f_io,
+                                                                                             cur, force, cp);
+    count_launch();
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- output
 // write_output / strided extract semantics (jni.cpp:2535-2581, 9385-9446).
 __device__ __forceinline__ void macro_out(const float (&f)[27], bool solid, float scale, float* o) {
@@ -269,7 +306,7 @@ template <bool kExact>
 __global__ void output_ab_kernel(int nx, int ny, int nz, const float* __restrict__ g, const uint32_t* __restrict__ flags,
                                  const uint8_t* __restrict__ obstacle, const float* __restrict__ ref_p,
                                  const FaceParams* __restrict__ F, int stride, int sx, int sy, int sz, int out_ch,
-                                 float scale, float* __restrict__ out) {
+                                 float scale, float* __restrict__ out, int direct) {
     const long long n_out = (long long)sx * sy * sz;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_out) return;
@@ -282,7 +319,12 @@ __global__ void output_ab_kernel(int nx, int ny, int nz, const float* __restrict
     float f[27];
     const PullView v{g, obstacle, ref_p, F, cells, nx, ny, nz};
     const uint32_t w = flags[cell];
-    pull27(v, w, cell, x, y, z, f);
+    if (direct) {  // g holds the streamed state itself
+#pragma unroll
+        for (int q = 0; q < 27; ++q) f[q] = g[(long long)q * cells + cell];
+    } else {
+        pull27(v, w, cell, x, y, z, f);
+    }
     float o[4];
     if (kExact) exact::macro_out_exact(f, (w & kFlagSelfSolid) != 0, scale, o);
     else macro_out(f, (w & kFlagSelfSolid) != 0, scale, o);
@@ -294,13 +336,13 @@ __global__ void output_ab_kernel(int nx, int ny, int nz, const float* __restrict
 template <bool kExact>
 cudaError_t launch_output_ab_t(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
                              const float* ref_p, const FaceParams* face, int stride, int out_channels,
-                             float velocity_scale, float* out, cudaStream_t stream) {
+                             float velocity_scale, float* out, cudaStream_t stream, int direct = 0) {
     const int sx = (d.nx + stride - 1) / stride, sy = (d.ny + stride - 1) / stride, sz = (d.nz + stride - 1) / stride;
     const long long n = (long long)sx * sy * sz;
     if (n <= 0) return cudaSuccess;
     const int block = 128;
     output_ab_kernel<kExact><<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(
-        d.nx, d.ny, d.nz, g, flags, obstacle, ref_p, face, stride, sx, sy, sz, out_channels, velocity_scale, out);
+        d.nx, d.ny, d.nz, g, flags, obstacle, ref_p, face, stride, sx, sy, sz, out_channels, velocity_scale, out, direct);
     count_launch();
     return cudaGetLastError();
 }

@@ -1,0 +1,39 @@
+// Halo exchange between overlapping bricks (see halo.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "d3q27_kernels.cuh"
+#include "inplace27.cuh"
+
+namespace aero {
+
+// One direction of the exchange: per axis the source start, destination
+// start and size (cells).
+struct HaloSlab {
+    int src[3], dst[3], size[3];
+};
+
+// halo_exchange_slab_bounds with the reference's halo clamp
+// (max(1, min(halo_layers, n / 2 - 1)), core n - 2 halo > 0).
+bool halo_slabs(int n, int halo_layers, int ox, int oy, int oz, HaloSlab& first_to_second, HaloSlab& second_to_first);
+
+// An in-place context as the exchange sees it.
+struct HaloIpSide {
+    void* f;
+    PadGeom g;
+    const uint32_t* flags;  // classification of the last call (bounce bits, solid cells)
+    int parity;             // parity of the next step
+    Fp16Scale sc;
+};
+
+// storage: 0 FP32, 1 IEEE-half deviations, 2 16-bit fixed point (both sides alike).
+cudaError_t launch_halo_ip(int storage, const HaloIpSide& a, const HaloIpSide& b, const HaloSlab& ab,
+                           const HaloSlab& ba, cudaStream_t s);
+cudaError_t launch_materialise_ab(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
+                                  const float* ref_p, const FaceParams* face, float* f_out, cudaStream_t s);
+// comps component-major arrays of `cells` floats each, copied along one slab.
+cudaError_t launch_halo_soa(const float* a, float* b, long long cells, int ny, int nz, int comps, const HaloSlab& ab,
+                            cudaStream_t s);
+
+}  // namespace aero

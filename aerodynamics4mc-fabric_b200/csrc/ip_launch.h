@@ -25,6 +25,21 @@ cudaError_t ip_step_i16_fast(short* f, const IpArgs& a, bool transitions, bool f
 cudaError_t ip_output_i16_fast(const short* f, const IpArgs& a, int stride, int out_ch, float scale, float* out,
                                cudaStream_t s);
 
+cudaError_t ip_fill_f32_exact(float* f, const IpArgs& a, cudaStream_t s);
+cudaError_t ip_fill_f32_fast(float* f, const IpArgs& a, cudaStream_t s);
+cudaError_t ip_fill_f16_fast(__half* f, const IpArgs& a, cudaStream_t s);
+cudaError_t ip_fill_i16_fast(short* f, const IpArgs& a, cudaStream_t s);
+
+// Equilibrium-face pre-fill for the step of parity a.parity (see
+// face_fill_ip_kernel); run at the end of every call, so that between calls
+// every incoming slot holds the cell's streamed population.
+inline cudaError_t ip_fill(int v, void* f, const IpArgs& a, cudaStream_t s) {
+    if (v == kIpF32Exact) return ip_fill_f32_exact(static_cast<float*>(f), a, s);
+    if (v == kIpF32Fast) return ip_fill_f32_fast(static_cast<float*>(f), a, s);
+    if (v == kIpI16Fast) return ip_fill_i16_fast(static_cast<short*>(f), a, s);
+    return ip_fill_f16_fast(static_cast<__half*>(f), a, s);
+}
+
 inline cudaError_t ip_init(int v, void* f, const IpArgs& a, cudaStream_t s) {
     if (v == kIpF32Exact) return ip_init_f32_exact(static_cast<float*>(f), a, s);
     if (v == kIpF32Fast) return ip_init_f32_fast(static_cast<float*>(f), a, s);

@@ -21,6 +21,7 @@
 #include "d3q27_kernels.cuh"
 #include "ip_launch.h"
 #include "conservation.cuh"
+#include "halo.cuh"
 #include "runtime_internal.h"
 #include "thermal.cuh"
 
@@ -718,6 +719,11 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         if (!ctx.initialized) {
             auto launch = g_collision_mode == 0 ? launch_init_collide_exact : launch_init_collide_fast;
             if (!cuda_ok(launch(d, ctx.fields(new_slot), ctx.force_field(), cp, g_next, s), "init_collide")) return false;
+        } else if (ctx.f_ready) {
+            // a halo exchange left the streamed state in g_next: collide it there
+            auto launch = g_collision_mode == 0 ? launch_collide_ab_exact : launch_collide_ab_fast;
+            if (!cuda_ok(launch(d, g_next, ctx.fields(new_slot), ctx.force_field(), cp, s), "collide_ab")) return false;
+            ctx.f_ready = false;
         } else {
             auto launch = g_collision_mode == 0 ? launch_step_ab_exact : launch_step_ab_fast;
             if (!cuda_ok(launch(d, ctx.g[ctx.cur], g_next, ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
@@ -738,12 +744,7 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             ctx.parity = 1;
         } else {
             a.parity = ctx.parity;
-            bool fill = false;
-            for (int i = 0; i < 6; ++i) {
-                const int k = ctx.face_prev.kind[i];
-                fill |= k == kHydroVelocity || k == kHydroPressure || k == kHydroMovingWall;
-            }
-            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, have_packet, fill, s), "step_inplace")) return false;
+            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, have_packet, false, s), "step_inplace")) return false;
             ctx.parity ^= 1;
         }
     }
@@ -751,6 +752,21 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     ctx.face_prev = face_now;
     ctx.initialized = true;
     ctx.step_counter += 1;
+    if (ctx.layout == 1) {
+        // Equilibrium-face sources of the next step, written now: between calls
+        // every incoming slot then holds the cell's streamed population (the
+        // reference's f), which the halo exchange reads and writes.
+        bool fill = false;
+        for (int i = 0; i < 6; ++i) {
+            const int k = face_now.kind[i];
+            fill |= k == kHydroVelocity || k == kHydroPressure || k == kHydroMovingWall;
+        }
+        if (fill) {
+            IpArgs a = ip_args(ctx, new_slot, new_slot, cp);
+            a.parity = ctx.parity;
+            if (!cuda_ok(ip_fill(ctx.ip_variant, ctx.ip, a, s), "face_fill_inplace")) return false;
+        }
+    }
 
     if (out) return read_output(ctx, 1, g_cfg.output_channels, scale, out);
     return true;
@@ -761,8 +777,9 @@ bool output_device(Context& ctx, int stride, int out_ch, float scale, float* dev
     const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
     if (ctx.layout == 0) {
         auto launch = g_collision_mode == 0 ? launch_output_ab_exact : launch_output_ab_fast;
-        return cuda_ok(launch(d, ctx.g[ctx.cur], ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot],
-                              ctx.d_face[ctx.slot], stride, out_ch, scale, dev_out, s),
+        const float* g = ctx.f_ready ? ctx.g[1 - ctx.cur] : ctx.g[ctx.cur];
+        return cuda_ok(launch(d, g, ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot], ctx.d_face[ctx.slot],
+                              stride, out_ch, scale, dev_out, s, ctx.f_ready ? 1 : 0),
                        "output");
     }
     IpArgs a = ip_args(ctx, ctx.slot, ctx.slot, current_collide_params());
@@ -985,6 +1002,113 @@ AERO_LBM_B200_EXPORT int aero_lbm_set_temperature_state_rect(int nx, int ny, int
     return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
 }
 
+// exchange_context_halo_cpu_layers (jni.cpp:8266-8426) on device-resident
+// contexts; the argument checks of native_exchange_halo_rect_layers_impl
+// (jni.cpp:9693-9790). Both contexts must exist, be distinct, have the
+// requested cubic shape and use the same storage; a context that has not
+// stepped yet holds no populations and makes the call a no-op (the
+// reference returns true for an empty context).
+static bool exchange_halo(const char* who, int nx, int ny, int nz, int halo_layers, long long first_key,
+                          long long second_key, int ox, int oy, int oz) {
+    auto fail = [&](const std::string& m) {
+        set_error(std::string(who) + ": " + m);
+        return false;
+    };
+    if (!g_cfg.initialized) return fail("runtime not initialized");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return fail("invalid dimensions");
+    if (halo_layers <= 0) return fail("halo_layers must be positive");
+    if (ox < -1 || ox > 1 || oy < -1 || oy > 1 || oz < -1 || oz > 1) {
+        std::ostringstream o;
+        o << "invalid offset (" << ox << "," << oy << "," << oz << ")";
+        return fail(o.str());
+    }
+    if (ox == 0 && oy == 0 && oz == 0) return fail("zero offset is invalid");
+    if (nx != ny || ny != nz) {
+        std::ostringstream o;
+        o << "only cubic contexts are supported, got " << nx << "x" << ny << "x" << nz;
+        return fail(o.str());
+    }
+    if (halo_layers * 2 >= nx) {
+        std::ostringstream o;
+        o << "invalid halo layout nx=" << nx << " halo=" << halo_layers;
+        return fail(o.str());
+    }
+    Context* a = find_context(first_key);
+    Context* b = find_context(second_key);
+    if (!a || !b) {
+        std::ostringstream o;
+        o << "missing context(s) first=" << first_key << (a ? "" : " [missing]") << ", second=" << second_key
+          << (b ? "" : " [missing]");
+        return fail(o.str());
+    }
+    if (a == b) return fail("the two context keys are the same context");
+    for (Context* c : {a, b})
+        if (c->nx != nx || c->ny != ny || c->nz != nz) {
+            std::ostringstream o;
+            o << "context shape " << c->nx << "x" << c->ny << "x" << c->nz << " differs from the requested " << nx << "x"
+              << ny << "x" << nz;
+            return fail(o.str());
+        }
+    if (!a->initialized || !b->initialized) return true;
+    if (a->layout != b->layout || (a->layout == 1 && a->ip_variant != b->ip_variant))
+        return fail("the two contexts use different storage (layout or precision)");
+    HaloSlab ab, ba;
+    if (!halo_slabs(nx, halo_layers, ox, oy, oz, ab, ba)) return fail("halo slab bounds invalid");
+    cudaStream_t s = current_stream();
+    if (a->layout == 1) {
+        auto side = [](Context& c) {
+            return HaloIpSide{c.ip, make_pad_geom(c.nx, c.ny, c.nz, c.periodic_mask), c.flags[c.slot], c.parity,
+                              Fp16Scale{c.fp16_scale, c.fp16_scale > 0.0f ? 1.0f / c.fp16_scale : 0.0f}};
+        };
+        const int storage = a->ip_variant == kIpF16Fast ? 1 : (a->ip_variant == kIpI16Fast ? 2 : 0);
+        if (!cuda_ok(launch_halo_ip(storage, side(*a), side(*b), ab, ba, s), "halo_inplace")) return false;
+    } else {
+        for (Context* c : {a, b}) {
+            if (c->f_ready) continue;
+            const BrickDims d{c->nx, c->ny, c->nz, 0, c->cells};
+            if (!cuda_ok(launch_materialise_ab(d, c->g[c->cur], c->flags[c->slot], c->obstacle[c->slot],
+                                               c->ref_p[c->slot], c->d_face[c->slot], c->g[1 - c->cur], s),
+                         "halo_materialise")) return false;
+            c->f_ready = true;
+        }
+        if (!cuda_ok(launch_halo_soa(a->g[1 - a->cur], b->g[1 - b->cur], a->cells, ny, nz, 27, ab, s), "halo_f")) return false;
+        if (!cuda_ok(launch_halo_soa(b->g[1 - b->cur], a->g[1 - a->cur], b->cells, ny, nz, 27, ba, s), "halo_f")) return false;
+    }
+    if (!cuda_ok(launch_halo_soa(a->temperature, b->temperature, a->cells, ny, nz, 1, ab, s), "halo_temperature")) return false;
+    if (!cuda_ok(launch_halo_soa(b->temperature, a->temperature, b->cells, ny, nz, 1, ba, s), "halo_temperature")) return false;
+    return true;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo_layers_rect(int nx, int ny, int nz, int halo_layers, long long first_key,
+                                                            long long second_key, int ox, int oy, int oz) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    return exchange_halo("exchange_halo_layers_rect", nx, ny, nz, halo_layers, first_key, second_key, ox, oy, oz) ? 1 : 0;
+}
+
+// native_exchange_halo_impl (jni.cpp:9623-9691): the configured cubic grid and
+// max(1, n / 4) halo layers (exchange_context_halo_cpu, jni.cpp:8428-8430).
+AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo(int grid_size, long long first_key, long long second_key, int ox, int oy,
+                                                int oz) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_cfg.initialized) {
+        set_error("exchange_halo: runtime not initialized");
+        return 0;
+    }
+    if (g_cfg.nx != g_cfg.ny || g_cfg.ny != g_cfg.nz || grid_size != g_cfg.nx) {
+        std::ostringstream o;
+        o << "exchange_halo: grid size mismatch (requested=" << grid_size << ", configured=" << g_cfg.nx << "x"
+          << g_cfg.ny << "x" << g_cfg.nz << ")";
+        set_error(o.str());
+        return 0;
+    }
+    return exchange_halo("exchange_halo", grid_size, grid_size, grid_size, std::max(1, grid_size / 4), first_key,
+                         second_key, ox, oy, oz)
+               ? 1
+               : 0;
+}
+
 AERO_LBM_B200_EXPORT void aero_lbm_release_context(long long key) {
     std::lock_guard<std::recursive_mutex> lk(g_mutex);
     g_contexts.erase(key);
@@ -1174,8 +1298,9 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums(long long key, double* 
     double* dev_out = partials + (size_t)blocks * 4;
     cudaError_t e;
     if (c->layout == 0) {
-        e = launch_conservation_ab(c->nx, c->ny, c->nz, c->g[c->cur], c->flags[c->slot], c->obstacle[c->slot],
-                                   c->ref_p[c->slot], c->d_face[c->slot], partials, dev_out, s);
+        const float* g = c->f_ready ? c->g[1 - c->cur] : c->g[c->cur];
+        e = launch_conservation_ab(c->nx, c->ny, c->nz, g, c->flags[c->slot], c->obstacle[c->slot], c->ref_p[c->slot],
+                                   c->d_face[c->slot], partials, dev_out, s, c->f_ready ? 1 : 0);
     } else {
         IpArgs a = ip_args(*c, c->slot, c->slot, current_collide_params());
         a.parity = c->parity;

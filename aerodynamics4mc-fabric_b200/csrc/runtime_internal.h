@@ -60,6 +60,9 @@ struct Context {
     void* scratch = nullptr; // conservation-sum partials
     size_t scratch_cap = 0;
     int cur = 0;
+    // Two-buffer layout after a halo exchange: g[1 - cur] holds the streamed
+    // state (exchanged slabs included); the next call collides it directly.
+    bool f_ready = false;
     int slot = 0;
     bool allocated = false;
     bool initialized = false;

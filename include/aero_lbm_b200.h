@@ -164,6 +164,20 @@ AERO_LBM_B200_EXPORT int aero_lbm_step_rect_cached_scaled(int nx, int ny, int nz
 AERO_LBM_B200_EXPORT int aero_lbm_has_context(long long context_key);
 /* native/include/aero_lbm_capi.h:220 */
 AERO_LBM_B200_EXPORT int aero_lbm_context_realtime_cached_initialized(long long context_key);
+/* native/include/aero_lbm_capi.h:210-217 (jni.cpp:9623-9691, 8428-8430) — halo
+ * exchange between two stepped contexts of the configured cubic grid with
+ * max(1, grid_size / 4) halo layers. */
+AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo(int grid_size, long long first_context_key, long long second_context_key,
+                                                int offset_x, int offset_y, int offset_z);
+/* native/include/aero_lbm_capi.h:218-228 (jni.cpp:9693-9790, 8136-8426) — the
+ * second context lies at offset (offset_x, offset_y, offset_z) in {-1,0,1}^3
+ * (not all 0) from the first; each receives the other's streamed populations
+ * and temperature on the slab of halo_layers (clamped to n/2 - 1) layers.
+ * Cubic contexts only; returns 1 (no-op) while either context has not
+ * stepped; both contexts must use the same storage. */
+AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo_layers_rect(int nx, int ny, int nz, int halo_layers,
+                                                            long long first_context_key, long long second_context_key,
+                                                            int offset_x, int offset_y, int offset_z);
 /* native/include/aero_lbm_capi.h:241 */
 AERO_LBM_B200_EXPORT int aero_lbm_get_temperature_state_rect(int nx, int ny, int nz, long long context_key, float* out_temperature);
 /* native/include/aero_lbm_capi.h:262 (jni.cpp:9246-9450) — sample every stride cells
