@@ -200,6 +200,14 @@ SIGNATURES = {
     "aero_lbm_context_realtime_cached_initialized": (_I, [_LL]),
     "aero_lbm_exchange_halo": (_I, [_I, _LL, _LL, _I, _I, _I]),
     "aero_lbm_exchange_halo_layers_rect": (_I, [_I, _I, _I, _I, _LL, _LL, _I, _I, _I]),
+    "aero_lbm_step_rect_with_sparse_overlays": (_I, [_F32P, _I, _I, _I, _LL, ctypes.c_void_p, _F32P, _I, _F32P]),
+    "aero_lbm_shift_context": (_I, [_I, _LL, _I, _I, _I]),
+    "aero_lbm_context_compact_initialized": (_I, [_LL]),
+    "aero_lbm_sample_temperature_point_rect": (_I, [_I, _I, _I, _LL, _I, _I, _I, _F32P]),
+    "aero_lbm_sample_flow_point_rect": (_I, [_I, _I, _I, _LL, _I, _I, _I, _F32P]),
+    "aero_lbm_copy_flow_temperature_subrect": (_I, [_I, _I, _I, _LL, _I, _I, _I, _I, _I, _I, _F32P, _F32P]),
+    "aero_lbm_get_last_force": (_I, [_LL, _F32P, _F32P, _F32P]),
+    "aero_lbm_memory_info": (ctypes.c_char_p, []),
     "aero_lbm_get_temperature_state_rect": (_I, [_I, _I, _I, _LL, _F32P]),
     "aero_lbm_extract_flow_atlas_rect": (_I, [_I, _I, _I, _LL, _I, _F32P, _I]),
     "aero_lbm_get_flow_state_rect": (_I, [_I, _I, _I, _LL, _F32P]),

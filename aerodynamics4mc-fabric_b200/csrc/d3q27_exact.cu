@@ -23,9 +23,9 @@ cudaError_t launch_collide_ab_exact(BrickDims d, float* f_io, CellFields cur, Fo
 }
 
 cudaError_t launch_output_ab_exact(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
-                                const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                                const float* ref_p, const FaceParams* face, OutBox box, int out_channels,
                                 float velocity_scale, float* out, cudaStream_t stream, int direct) {
-    return launch_output_ab_t<true>(d, g, flags, obstacle, ref_p, face, stride, out_channels, velocity_scale, out,
+    return launch_output_ab_t<true>(d, g, flags, obstacle, ref_p, face, box, out_channels, velocity_scale, out,
                                      stream, direct);
 }
 
@@ -35,8 +35,8 @@ cudaError_t ip_fill_f32_exact(float* f, const IpArgs& a, cudaStream_t s) { retur
 cudaError_t ip_step_f32_exact(float* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
     return IpLaunch<StoreF32, true>::step(f, a, transitions, fill, s);
 }
-cudaError_t ip_output_f32_exact(const float* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
-    return IpLaunch<StoreF32, true>::output(f, a, stride, out_ch, scale, out, s);
+cudaError_t ip_output_f32_exact(const float* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out, cudaStream_t s) {
+    return IpLaunch<StoreF32, true>::output(f, a, box, out_ch, scale, out, s);
 }
 
 }  // namespace aero

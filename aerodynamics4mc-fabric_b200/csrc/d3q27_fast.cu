@@ -22,9 +22,9 @@ cudaError_t launch_collide_ab_fast(BrickDims d, float* f_io, CellFields cur, For
 }
 
 cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
-                                const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                                const float* ref_p, const FaceParams* face, OutBox box, int out_channels,
                                 float velocity_scale, float* out, cudaStream_t stream, int direct) {
-    return launch_output_ab_t<false>(d, g, flags, obstacle, ref_p, face, stride, out_channels, velocity_scale, out,
+    return launch_output_ab_t<false>(d, g, flags, obstacle, ref_p, face, box, out_channels, velocity_scale, out,
                                      stream, direct);
 }
 
@@ -34,8 +34,8 @@ cudaError_t ip_fill_f32_fast(float* f, const IpArgs& a, cudaStream_t s) { return
 cudaError_t ip_step_f32_fast(float* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
     return IpLaunch<StoreF32, false>::step(f, a, transitions, fill, s);
 }
-cudaError_t ip_output_f32_fast(const float* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
-    return IpLaunch<StoreF32, false>::output(f, a, stride, out_ch, scale, out, s);
+cudaError_t ip_output_f32_fast(const float* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out, cudaStream_t s) {
+    return IpLaunch<StoreF32, false>::output(f, a, box, out_ch, scale, out, s);
 }
 
 cudaError_t ip_init_f16_fast(__half* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF16Dev, false>::init(f, a, s); }
@@ -43,8 +43,8 @@ cudaError_t ip_fill_f16_fast(__half* f, const IpArgs& a, cudaStream_t s) { retur
 cudaError_t ip_step_f16_fast(__half* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
     return IpLaunch<StoreF16Dev, false>::step(f, a, transitions, fill, s);
 }
-cudaError_t ip_output_f16_fast(const __half* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
-    return IpLaunch<StoreF16Dev, false>::output(f, a, stride, out_ch, scale, out, s);
+cudaError_t ip_output_f16_fast(const __half* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out, cudaStream_t s) {
+    return IpLaunch<StoreF16Dev, false>::output(f, a, box, out_ch, scale, out, s);
 }
 
 cudaError_t ip_init_i16_fast(short* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreI16Dev, false>::init(f, a, s); }
@@ -52,8 +52,8 @@ cudaError_t ip_fill_i16_fast(short* f, const IpArgs& a, cudaStream_t s) { return
 cudaError_t ip_step_i16_fast(short* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
     return IpLaunch<StoreI16Dev, false>::step(f, a, transitions, fill, s);
 }
-cudaError_t ip_output_i16_fast(const short* f, const IpArgs& a, int stride, int out_ch, float scale, float* out, cudaStream_t s) {
-    return IpLaunch<StoreI16Dev, false>::output(f, a, stride, out_ch, scale, out, s);
+cudaError_t ip_output_i16_fast(const short* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out, cudaStream_t s) {
+    return IpLaunch<StoreI16Dev, false>::output(f, a, box, out_ch, scale, out, s);
 }
 
 }  // namespace aero

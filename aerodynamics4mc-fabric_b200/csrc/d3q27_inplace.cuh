@@ -30,12 +30,19 @@ struct IpArgs {
     int cells_per_thread;            // 1 one cell per thread, 2 two cells per thread (packed collision)
     int streamed;                    // factorised two-cell step: populations streamed by bulk async copies
     int* fault;                      // device word set to 1 by a streamed step whose copies never landed
+    // Populations of solid cells (27 x cells FP32, null = all at rest): the
+    // reference keeps a solid cell's streamed populations and flips them
+    // every call (jni.cpp:2209-2452: f_post = f, f'[q] = f_post[opp q]); they
+    // come back when the cell opens again. Stored at a canonical parity:
+    // entry (p ? opp(q) : q) holds population q at a step of parity p.
+    float* solid_f;
 };
+
 
 // Equilibrium value of a face (velocity / pressure / moving wall), the only
 // non-bounce-back faces the in-place layout accepts
 // (boundary_equilibrium_value, jni.cpp:1519-1561).
-__device__ __forceinline__ float ip_face_equilibrium(const FaceParams& F, int q, float ref_p, int sx, int sy, int sz,
+__device__ __forceinline__ float ip_face_equilibrium(const FaceParams& F, int q, float ref_p, int y, int sx, int sy, int sz,
                                                      int nx, int ny, int nz) {
     const int face = oob_face(sx, sy, sz, nx, ny, nz);
     const int kind = F.kind[face];
@@ -45,6 +52,10 @@ __device__ __forceinline__ float ip_face_equilibrium(const FaceParams& F, int q,
         rho = 1.0f + clampf_dev(F.pressure[face], -0.03f, 0.03f);
     } else {
         ux = F.velocity[face][0]; uy = F.velocity[face][1]; uz = F.velocity[face][2];
+        if (F.cylinder_inlet && sx < 0) {
+            ux = cylinder_inlet_ux(ny, y, F.velocity[face][0]);
+            uy = 0.0f; uz = 0.0f;
+        }
     }
     rho = clampf_dev(rho, 0.97f, 1.03f);
     const float s2 = ux * ux + uy * uy + uz * uz;
@@ -383,28 +394,43 @@ __global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
         if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) continue;
         int c, d;
         incoming_slot(o, own, q, a.parity, false, c, d);
-        S::store(f + (long long)d * G.pcells + c, q, ip_face_equilibrium(F, q, rp, sx, sy, sz, nx, ny, nz), a.sc);
+        S::store(f + (long long)d * G.pcells + c, q, ip_face_equilibrium(F, q, rp, y, sx, sy, sz, nx, ny, nz), a.sc);
     }
 }
 
 // Cells that were solid at the streaming call and are fluid now: start from
-// the rest equilibrium (the state a cell holds while solid since
-// initialisation), collide and push. Runs after step_ip_kernel of the same
-// parity; the slots it writes were only read (as bounce-back) by that launch.
+// the populations the cell held while solid (a.solid_f; the rest
+// equilibrium for a cell solid since initialisation), collide and push. Cells
+// that turn solid in this call keep their streamed populations in a.solid_f:
+// the step kernel pushed them uncollided, so they sit in the cell's outgoing
+// slots. Runs after step_ip_kernel of the same parity; the slots it writes
+// were only read (as bounce-back) by that launch.
 template <class S, bool kExact>
 __global__ void __launch_bounds__(128) transition_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom G = a.g;
     const long long cells = (long long)G.nx * G.ny * G.nz;
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= cells) return;
-    if (!(a.flags_prev[cell] & kFlagSelfSolid) || a.obstacle_cur[cell]) return;
+    const bool was_solid = (a.flags_prev[cell] & kFlagSelfSolid) != 0, solid = a.obstacle_cur[cell] != 0;
+    if (was_solid == solid) return;
     int x, y, z;
     cell_coords(G, cell, x, y, z);
     const int own = pad_index(G, x, y, z);
     const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
+    if (solid) {
+        if (!a.solid_f) return;
+#pragma unroll 1
+        for (int q = 0; q < 27; ++q) {
+            int c, d;
+            outgoing_slot(o, own, q, a.parity, c, d);
+            a.solid_f[(long long)solid_slot(q, a.parity) * cells + cell] = S::load(f + (long long)d * G.pcells + c, q, a.sc);
+        }
+        return;
+    }
     float fl[27];
 #pragma unroll
-    for (int q = 0; q < 27; ++q) fl[q] = q_w(q);
+    for (int q = 0; q < 27; ++q)
+        fl[q] = a.solid_f ? a.solid_f[(long long)solid_slot(q, a.parity) * cells + cell] : q_w(q);
     if (!collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
         reseed_push<S>(f, a, cell, x, y, z, a.parity);
         return;
@@ -443,16 +469,16 @@ __global__ void __launch_bounds__(128) init_ip_kernel(typename S::T* __restrict_
 // Macro output of the streamed state (what the next step would pull), with
 // write_output / strided-extract semantics. Read-only.
 template <class S, bool kExact>
-__global__ void output_ip_kernel(const typename S::T* __restrict__ f, IpArgs a, int stride, int ax_n, int ay_n, int az_n,
-                                 int out_ch, float scale, float* __restrict__ out) {
+__global__ void output_ip_kernel(const typename S::T* __restrict__ f, IpArgs a, OutBox b, int out_ch, float scale,
+                                 float* __restrict__ out) {
     const PadGeom G = a.g;
-    const long long n_out = (long long)ax_n * ay_n * az_n;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_out) return;
-    const int az = (int)(i % az_n);
-    const int ay = (int)((i / az_n) % ay_n);
-    const int ax = (int)(i / ((long long)ay_n * az_n));
-    const int x = min(G.nx - 1, ax * stride), y = min(G.ny - 1, ay * stride), z = min(G.nz - 1, az * stride);
+    if (i >= b.count()) return;
+    const int az = (int)(i % b.sz);
+    const int ay = (int)((i / b.sz) % b.sy);
+    const int ax = (int)(i / ((long long)b.sy * b.sz));
+    const int x = min(G.nx - 1, b.ox + ax * b.stride), y = min(G.ny - 1, b.oy + ay * b.stride),
+              z = min(G.nz - 1, b.oz + az * b.stride);
     const long long cell = ((long long)x * G.ny + y) * G.nz + z;
     const uint32_t w = a.flags_prev[cell];
     float o4[4] = {0.0f, 0.0f, 0.0f, 0.0f};

@@ -20,7 +20,27 @@ struct FaceParams {
     int wrap_hi[3];         // per axis: the max face wraps
     int disable_convective; // INHERIT_GAME faces use bounce-back instead of convective outflow
     float max_speed;
+    int cylinder_inlet;     // cylinder preset: the x- velocity face blows the parabolic profile
 };
+
+// cylinder_benchmark_inlet_ux (jni.cpp:214-220): 4 u_max s (1 - s) across the
+// channel, s = y / max(1, ny - 1); applied to velocity and moving-wall
+// sources beyond x- under the cylinder preset (jni.cpp:1536-1545). Rounded
+// operation by operation, as the reference evaluates it.
+__host__ __device__ inline float cylinder_inlet_ux(int ny, int y, float u_max) {
+    const float height = (float)(ny - 1 > 1 ? ny - 1 : 1);
+#ifdef __CUDA_ARCH__
+    const float denom = fmaxf(__fsub_rn(height, 0.0f), 1.0e-6f);
+    const float s = __fdiv_rn(__fsub_rn((float)y, 0.0f), denom);
+    if (s < 0.0f || s > 1.0f) return 0.0f;
+    return __fmul_rn(__fmul_rn(__fmul_rn(4.0f, u_max), s), __fsub_rn(1.0f, s));
+#else
+    const float denom = height - 0.0f > 1.0e-6f ? height - 0.0f : 1.0e-6f;
+    const float s = ((float)y - 0.0f) / denom;
+    if (s < 0.0f || s > 1.0f) return 0.0f;
+    return 4.0f * u_max * s * (1.0f - s);
+#endif
+}
 
 struct BrickDims {
     int nx, ny, nz;
@@ -69,6 +89,19 @@ struct ForceField {
     const float* fz;
 };
 
+// Region of a macro output: sample (a, b, c) of the sx x sy x sz result is the
+// cell (min(nx - 1, ox + a * stride), ...). A strided atlas has origin 0; a
+// sub-box or a point sample has stride 1.
+struct OutBox {
+    int ox, oy, oz;
+    int sx, sy, sz;
+    int stride;
+    __host__ __device__ long long count() const { return (long long)sx * sy * sz; }
+};
+inline OutBox strided_box(int nx, int ny, int nz, int stride) {
+    return OutBox{0, 0, 0, (nx + stride - 1) / stride, (ny + stride - 1) / stride, (nz + stride - 1) / stride, stride};
+}
+
 // Launch helpers (all asynchronous on `stream`; return the launch error).
 cudaError_t launch_ingest_packet(const float* packet, int in_channels, BrickDims d, CellFields out, cudaStream_t stream);
 cudaError_t launch_build_flags(const uint8_t* obstacle, BrickDims d, FaceParams face, uint32_t* flags, cudaStream_t stream);
@@ -93,10 +126,10 @@ cudaError_t launch_collide_ab_fast(BrickDims d, float* f_io, CellFields cur, For
 // (AoS, out_channels per cell; ux,uy,uz scaled; clamp(rho - 1)).
 // `face` points to device memory. direct: g already holds the streamed state.
 cudaError_t launch_output_ab_exact(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
-                                   const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                                   const float* ref_p, const FaceParams* face, OutBox box, int out_channels,
                                    float velocity_scale, float* out, cudaStream_t stream, int direct = 0);
 cudaError_t launch_output_ab_fast(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
-                                  const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                                  const float* ref_p, const FaceParams* face, OutBox box, int out_channels,
                                   float velocity_scale, float* out, cudaStream_t stream, int direct = 0);
 
 uint64_t kernel_launch_count();

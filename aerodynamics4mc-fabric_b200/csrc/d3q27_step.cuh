@@ -85,6 +85,10 @@ static __device__ __noinline__ float face_value(const float* __restrict__ g, con
                 rho = 1.0f + clampf_dev(F.pressure[face], -0.03f, 0.03f);
             } else {
                 ux = F.velocity[face][0]; uy = F.velocity[face][1]; uz = F.velocity[face][2];
+                if (F.cylinder_inlet && sx < 0) {
+                    ux = cylinder_inlet_ux(ny, y, F.velocity[face][0]);
+                    uy = 0.0f; uz = 0.0f;
+                }
             }
             rho = clampf_dev(rho, 0.97f, 1.03f);
             const float s2 = ux * ux + uy * uy + uz * uz;
@@ -305,15 +309,15 @@ __device__ __forceinline__ void macro_out(const float (&f)[27], bool solid, floa
 template <bool kExact>
 __global__ void output_ab_kernel(int nx, int ny, int nz, const float* __restrict__ g, const uint32_t* __restrict__ flags,
                                  const uint8_t* __restrict__ obstacle, const float* __restrict__ ref_p,
-                                 const FaceParams* __restrict__ F, int stride, int sx, int sy, int sz, int out_ch,
-                                 float scale, float* __restrict__ out, int direct) {
-    const long long n_out = (long long)sx * sy * sz;
+                                 const FaceParams* __restrict__ F, OutBox b, int out_ch, float scale,
+                                 float* __restrict__ out, int direct) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_out) return;
-    const int az = (int)(i % sz);
-    const int ay = (int)((i / sz) % sy);
-    const int ax = (int)(i / ((long long)sy * sz));
-    const int x = min(nx - 1, ax * stride), y = min(ny - 1, ay * stride), z = min(nz - 1, az * stride);
+    if (i >= b.count()) return;
+    const int az = (int)(i % b.sz);
+    const int ay = (int)((i / b.sz) % b.sy);
+    const int ax = (int)(i / ((long long)b.sy * b.sz));
+    const int x = min(nx - 1, b.ox + ax * b.stride), y = min(ny - 1, b.oy + ay * b.stride),
+              z = min(nz - 1, b.oz + az * b.stride);
     const long long cells = (long long)nx * ny * nz;
     const long long cell = ((long long)x * ny + y) * nz + z;
     float f[27];
@@ -335,14 +339,13 @@ __global__ void output_ab_kernel(int nx, int ny, int nz, const float* __restrict
 
 template <bool kExact>
 cudaError_t launch_output_ab_t(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,
-                             const float* ref_p, const FaceParams* face, int stride, int out_channels,
+                             const float* ref_p, const FaceParams* face, OutBox box, int out_channels,
                              float velocity_scale, float* out, cudaStream_t stream, int direct = 0) {
-    const int sx = (d.nx + stride - 1) / stride, sy = (d.ny + stride - 1) / stride, sz = (d.nz + stride - 1) / stride;
-    const long long n = (long long)sx * sy * sz;
+    const long long n = box.count();
     if (n <= 0) return cudaSuccess;
     const int block = 128;
     output_ab_kernel<kExact><<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(
-        d.nx, d.ny, d.nz, g, flags, obstacle, ref_p, face, stride, sx, sy, sz, out_channels, velocity_scale, out, direct);
+        d.nx, d.ny, d.nz, g, flags, obstacle, ref_p, face, box, out_channels, velocity_scale, out, direct);
     count_launch();
     return cudaGetLastError();
 }

@@ -13,10 +13,10 @@
 // the next step's parity between calls (the equilibrium-face sources are
 // pre-filled at the end of each call), so a cell's f is read and written
 // through the same slot map the step kernel pulls with (bounce-back bits of
-// the last classification). Solid cells of an in-place context store no
-// populations (their memory is link storage): a solid destination keeps
-// nothing, a solid source gives the rest equilibrium (what a never-fluid
-// solid cell holds in the reference). Two-buffer contexts materialise f
+// the last classification). Solid cells of an in-place context keep their
+// populations beside the lattice (IpArgs::solid_f, at a canonical parity;
+// rest equilibrium while that store does not exist yet), and the exchange
+// reads and writes them there. Two-buffer contexts materialise f
 // (the pull of their post-collision state) into the spare buffer first; the
 // next call then collides f directly.
 #include "halo.cuh"
@@ -36,6 +36,7 @@ struct IpSide {
     const uint32_t* flags;
     int parity;
     Fp16Scale sc;
+    float* solid_f;
 };
 
 template <class S>
@@ -48,13 +49,15 @@ __global__ void halo_ip_kernel(IpSide<S> src, IpSide<S> dst, HaloSlab slab) {
     const int dx = slab.dst[0] + lx, dy = slab.dst[1] + ly, dz = slab.dst[2] + lz;
     const long long dcell = ((long long)dx * dst.g.ny + dy) * dst.g.nz + dz;
     const uint32_t wd = dst.flags[dcell];
-    if (wd & kFlagSelfSolid) return;
+    const bool dst_solid = (wd & kFlagSelfSolid) != 0;
+    if (dst_solid && !dst.solid_f) return;  // never-opened solid cells: at rest, like the source would have to be
     const long long scell = ((long long)sx * src.g.ny + sy) * src.g.nz + sz;
     const uint32_t ws = src.flags[scell];
     const bool src_solid = (ws & kFlagSelfSolid) != 0;
     const NeighbourOffsets os = neighbour_offsets(src.g, sx, sy, sz);
     const NeighbourOffsets od = neighbour_offsets(dst.g, dx, dy, dz);
     const int own_s = pad_index(src.g, sx, sy, sz), own_d = pad_index(dst.g, dx, dy, dz);
+    const long long scells = (long long)src.g.nx * src.g.ny * src.g.nz, dcells = (long long)dst.g.nx * dst.g.ny * dst.g.nz;
 #pragma unroll 1
     for (int q = 0; q < 27; ++q) {
         float v = q_w(q);
@@ -62,6 +65,12 @@ __global__ void halo_ip_kernel(IpSide<S> src, IpSide<S> dst, HaloSlab slab) {
             int c, d;
             incoming_slot(os, own_s, q, src.parity, (ws >> q) & 1u, c, d);
             v = S::load(src.f + (long long)d * src.g.pcells + c, q, src.sc);
+        } else if (src.solid_f) {
+            v = src.solid_f[(long long)solid_slot(q, src.parity) * scells + scell];
+        }
+        if (dst_solid) {
+            dst.solid_f[(long long)solid_slot(q, dst.parity) * dcells + dcell] = v;
+            continue;
         }
         int c, d;
         incoming_slot(od, own_d, q, dst.parity, (wd >> q) & 1u, c, d);
@@ -105,8 +114,8 @@ unsigned blocks_for(const HaloSlab& s) {
 
 template <class S>
 cudaError_t halo_ip_t(const HaloIpSide& a, const HaloIpSide& b, const HaloSlab& ab, const HaloSlab& ba, cudaStream_t s) {
-    const IpSide<S> A{static_cast<typename S::T*>(a.f), a.g, a.flags, a.parity, a.sc};
-    const IpSide<S> B{static_cast<typename S::T*>(b.f), b.g, b.flags, b.parity, b.sc};
+    const IpSide<S> A{static_cast<typename S::T*>(a.f), a.g, a.flags, a.parity, a.sc, a.solid_f};
+    const IpSide<S> B{static_cast<typename S::T*>(b.f), b.g, b.flags, b.parity, b.sc, b.solid_f};
     halo_ip_kernel<S><<<blocks_for(ab), 128, 0, s>>>(A, B, ab);
     count_launch();
     halo_ip_kernel<S><<<blocks_for(ba), 128, 0, s>>>(B, A, ba);

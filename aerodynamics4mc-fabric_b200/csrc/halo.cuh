@@ -25,6 +25,7 @@ struct HaloIpSide {
     const uint32_t* flags;  // classification of the last call (bounce bits, solid cells)
     int parity;             // parity of the next step
     Fp16Scale sc;
+    float* solid_f;         // populations of solid cells (IpArgs::solid_f), or null
 };
 
 // storage: 0 FP32, 1 IEEE-half deviations, 2 16-bit fixed point (both sides alike).

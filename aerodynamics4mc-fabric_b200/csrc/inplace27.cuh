@@ -88,6 +88,11 @@ struct StoreI16Dev {
     }
 };
 
+// Populations of solid cells are kept beside the lattice at a canonical
+// parity: entry solid_slot(q, p) holds population q entering a step of
+// parity p (a solid cell's populations flip every call, as the parity does).
+__host__ __device__ __forceinline__ int solid_slot(int q, int parity) { return parity ? q_opp(q) : q; }
+
 // Geometry of one padded brick and the per-axis wrap rule.
 struct PadGeom {
     int nx, ny, nz;

@@ -50,11 +50,11 @@ struct IpLaunch {
         count_launch();
         return cudaGetLastError();
     }
-    static cudaError_t output(const typename S::T* f, const IpArgs& a, int stride, int out_ch, float scale, float* out,
+    static cudaError_t output(const typename S::T* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out,
                               cudaStream_t s) {
-        const int sx = (a.g.nx + stride - 1) / stride, sy = (a.g.ny + stride - 1) / stride, sz = (a.g.nz + stride - 1) / stride;
-        const long long n = (long long)sx * sy * sz;
-        output_ip_kernel<S, kExact><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a, stride, sx, sy, sz, out_ch, scale, out);
+        const long long n = box.count();
+        if (n <= 0) return cudaSuccess;
+        output_ip_kernel<S, kExact><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a, box, out_ch, scale, out);
         count_launch();
         return cudaGetLastError();
     }

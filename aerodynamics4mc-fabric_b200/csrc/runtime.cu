@@ -21,6 +21,7 @@
 #include "d3q27_kernels.cuh"
 #include "ip_launch.h"
 #include "conservation.cuh"
+#include "context_ops.cuh"
 #include "halo.cuh"
 #include "runtime_internal.h"
 #include "thermal.cuh"
@@ -372,6 +373,7 @@ FaceParams current_face_params() {
     }
     f.disable_convective = bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_CONVECTIVE_OUTFLOW) ? 1 : 0;
     f.max_speed = kMaxSpeed;
+    f.cylinder_inlet = (bench_active() && g_bench.preset == AERO_LBM_BENCHMARK_PRESET_CYLINDER_CROSSFLOW_2D) ? 1 : 0;
     return f;
 }
 
@@ -407,7 +409,14 @@ void Context::release_device() {
     fr(reinterpret_cast<void*&>(out));
     fr(reinterpret_cast<void*&>(force));
     fr(reinterpret_cast<void*&>(fault));
+    fr(reinterpret_cast<void*&>(force3));
+    fr(reinterpret_cast<void*&>(overlay_cells));
+    fr(reinterpret_cast<void*&>(overlay_values));
+    overlay_cap = 0;
+    force_valid = false;
+    f_ready = false;
     fr(ip);
+    fr(reinterpret_cast<void*&>(solid_f));
     fr(scratch);
     scratch_cap = 0;
     packet_cap = out_cap = 0;
@@ -443,6 +452,8 @@ bool Context::allocate(int nx_, int ny_, int nz_) {
     }
     allocated = true;
     initialized = false;
+    f_ready = false;
+    force_valid = false;
     slot = 0;
     cur = 0;
     step_counter = 0;
@@ -521,6 +532,7 @@ static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const Collide
     a.cells_per_thread = g_cells_per_thread;
     a.streamed = g_streamed_step;
     a.fault = ctx.fault;
+    a.solid_f = ctx.solid_f;
     return a;
 }
 
@@ -642,7 +654,8 @@ static float thermal_diffusivity() {
 }
 
 // One step of a context. packet may be null (cached step); out may be null.
-bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet) {
+bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet,
+                  const SparseOverlays* overlays) {
     cudaStream_t s = current_stream();
     const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
     const FaceParams face_now = current_face_params();
@@ -677,6 +690,25 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             if (!cuda_ok(cudaMemcpyAsync(ctx.packet, packet, bytes, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync(packet)")) return false;
         }
         if (!cuda_ok(launch_ingest_packet(ctx.packet, in_ch, d, ctx.fields(new_slot), s), "ingest_packet")) return false;
+        if (overlays && overlays->count > 0) {
+            // apply_sparse_payload_overlays (jni.cpp:1696-1721), right after the ingest
+            const int n = overlays->count;
+            if (ctx.overlay_cap < n) {
+                if (ctx.overlay_cells) cudaFree(ctx.overlay_cells);
+                if (ctx.overlay_values) cudaFree(ctx.overlay_values);
+                ctx.overlay_cells = nullptr;
+                ctx.overlay_values = nullptr;
+                ctx.overlay_cap = 0;
+                if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.overlay_cells), (size_t)n * sizeof(int)), "cudaMalloc(overlays)") ||
+                    !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.overlay_values), (size_t)n * 6 * sizeof(float)), "cudaMalloc(overlays)"))
+                    return false;
+                ctx.overlay_cap = n;
+            }
+            if (!cuda_ok(cudaMemcpyAsync(ctx.overlay_cells, overlays->cells, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s), "copy overlays") ||
+                !cuda_ok(cudaMemcpyAsync(ctx.overlay_values, overlays->values, (size_t)n * 6 * sizeof(float), cudaMemcpyHostToDevice, s), "copy overlays") ||
+                !cuda_ok(launch_apply_overlays(ctx.overlay_cells, ctx.overlay_values, n, ctx.fields(new_slot), ctx.cells, ctx.thermal, s), "apply_overlays"))
+                return false;
+        }
         if (!classify(ctx, new_slot, face_now, d, s)) return false;
         ctx.has_inputs = true;
     } else if (face_changed && ctx.initialized) {
@@ -743,6 +775,15 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             if (!cuda_ok(ip_init(ctx.ip_variant, ctx.ip, a, s), "init_inplace")) return false;
             ctx.parity = 1;
         } else {
+            if (have_packet && !ctx.solid_f) {
+                // the first call that can change the mask: solid cells so far
+                // have been solid since initialisation and hold the rest state
+                if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.solid_f), (size_t)ctx.cells * 27 * sizeof(float)),
+                             "cudaMalloc(solid populations)") ||
+                    !cuda_ok(launch_fill_rest(ctx.solid_f, ctx.cells, s), "fill solid populations"))
+                    return false;
+                a.solid_f = ctx.solid_f;
+            }
             a.parity = ctx.parity;
             if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, have_packet, false, s), "step_inplace")) return false;
             ctx.parity ^= 1;
@@ -752,6 +793,16 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     ctx.face_prev = face_now;
     ctx.initialized = true;
     ctx.step_counter += 1;
+    // compute_benchmark_force (jni.cpp:2454-2492) after the collision: only the
+    // cylinder preset reports a force; its outflow face keeps it on the
+    // two-buffer layout, whose state is the post-collision populations
+    ctx.force_valid = false;
+    if (bench_active() && g_bench.preset == AERO_LBM_BENCHMARK_PRESET_CYLINDER_CROSSFLOW_2D && ctx.layout == 0) {
+        if (!ctx.force3 && !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.force3), 3 * sizeof(double)), "cudaMalloc(force)"))
+            return false;
+        if (!cuda_ok(launch_cylinder_force(ctx.g[ctx.cur], ctx.obstacle[new_slot], d, ctx.force3, s), "cylinder_force")) return false;
+        ctx.force_valid = true;
+    }
     if (ctx.layout == 1) {
         // Equilibrium-face sources of the next step, written now: between calls
         // every incoming slot then holds the cell's streamed population (the
@@ -772,25 +823,33 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     return true;
 }
 
-bool output_device(Context& ctx, int stride, int out_ch, float scale, float* dev_out) {
+bool output_device(Context& ctx, OutBox box, int out_ch, float scale, float* dev_out) {
     cudaStream_t s = current_stream();
     const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
     if (ctx.layout == 0) {
         auto launch = g_collision_mode == 0 ? launch_output_ab_exact : launch_output_ab_fast;
         const float* g = ctx.f_ready ? ctx.g[1 - ctx.cur] : ctx.g[ctx.cur];
         return cuda_ok(launch(d, g, ctx.flags[ctx.slot], ctx.obstacle[ctx.slot], ctx.ref_p[ctx.slot], ctx.d_face[ctx.slot],
-                              stride, out_ch, scale, dev_out, s, ctx.f_ready ? 1 : 0),
+                              box, out_ch, scale, dev_out, s, ctx.f_ready ? 1 : 0),
                        "output");
     }
     IpArgs a = ip_args(ctx, ctx.slot, ctx.slot, current_collide_params());
     a.parity = ctx.parity;
-    return cuda_ok(ip_output(ctx.ip_variant, ctx.ip, a, stride, out_ch, scale, dev_out, s), "output_inplace");
+    return cuda_ok(ip_output(ctx.ip_variant, ctx.ip, a, box, out_ch, scale, dev_out, s), "output_inplace");
 }
 
+bool read_output_box(Context& ctx, OutBox box, int out_ch, float scale, float* host_out, float* host_temperature);
+
 bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out) {
+    return read_output_box(ctx, strided_box(ctx.nx, ctx.ny, ctx.nz, stride), out_ch, scale, host_out, nullptr);
+}
+
+// Output of a box; host_temperature (optional) receives the temperature of
+// the same cells as aero_lbm_copy_flow_temperature_subrect reads it.
+bool read_output_box(Context& ctx, OutBox box, int out_ch, float scale, float* host_out, float* host_temperature) {
     cudaStream_t s = current_stream();
-    const int sx = (ctx.nx + stride - 1) / stride, sy = (ctx.ny + stride - 1) / stride, sz = (ctx.nz + stride - 1) / stride;
-    const size_t bytes = (size_t)sx * sy * sz * out_ch * sizeof(float);
+    const size_t n = (size_t)box.count();
+    const size_t bytes = n * (out_ch + (host_temperature ? 1 : 0)) * sizeof(float);
     if (ctx.out_cap < bytes) {
         if (ctx.out) cudaFree(ctx.out);
         ctx.out = nullptr;
@@ -798,8 +857,17 @@ bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_
         if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.out), bytes), "cudaMalloc(output)")) return false;
         ctx.out_cap = bytes;
     }
-    if (!output_device(ctx, stride, out_ch, scale, ctx.out)) return false;
-    if (!cuda_ok(cudaMemcpyAsync(host_out, ctx.out, bytes, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(output)")) return false;
+    if (!output_device(ctx, box, out_ch, scale, ctx.out)) return false;
+    if (!cuda_ok(cudaMemcpyAsync(host_out, ctx.out, n * out_ch * sizeof(float), cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync(output)")) return false;
+    if (host_temperature) {
+        float* dev_t = ctx.out + n * out_ch;
+        const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
+        if (!cuda_ok(launch_gather_temperature(ctx.temperature, ctx.obstacle[ctx.slot], d, box, dev_t, s), "gather_temperature") ||
+            !cuda_ok(cudaMemcpyAsync(host_temperature, dev_t, n * sizeof(float), cudaMemcpyDeviceToHost, s),
+                     "cudaMemcpyAsync(temperature)"))
+            return false;
+    }
     int fault = 0;
     if (!cuda_ok(cudaMemcpyAsync(&fault, ctx.fault, sizeof(int), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(fault)")) return false;
     if (!cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize(output)")) return false;
@@ -858,7 +926,8 @@ bool do_init(int nx, int ny, int nz, int in_ch, int out_ch) {
     return true;
 }
 
-bool step_impl(const float* packet, int nx, int ny, int nz, long long key, float* out, float scale, bool cached) {
+bool step_impl(const float* packet, int nx, int ny, int nz, long long key, float* out, float scale, bool cached,
+               const SparseOverlays* overlays = nullptr) {
     const auto t0 = Clock::now();
     clear_error();
     if (!g_cfg.initialized) {
@@ -886,7 +955,7 @@ bool step_impl(const float* packet, int nx, int ny, int nz, long long key, float
         set_error("cached solver step: dimensions differ from the resident context");
         return false;
     }
-    const bool ok = step_context(*ctx, cached ? nullptr : packet, out, scale, true);
+    const bool ok = step_context(*ctx, cached ? nullptr : packet, out, scale, true, overlays);
     if (!ok && g_last_error.empty()) set_error("native_step_raw_dims: step failed");
     record_timing(0.0, 0.0, 0.0, ms_since(t0), cached);
     return ok;
@@ -1058,7 +1127,7 @@ static bool exchange_halo(const char* who, int nx, int ny, int nz, int halo_laye
     if (a->layout == 1) {
         auto side = [](Context& c) {
             return HaloIpSide{c.ip, make_pad_geom(c.nx, c.ny, c.nz, c.periodic_mask), c.flags[c.slot], c.parity,
-                              Fp16Scale{c.fp16_scale, c.fp16_scale > 0.0f ? 1.0f / c.fp16_scale : 0.0f}};
+                              Fp16Scale{c.fp16_scale, c.fp16_scale > 0.0f ? 1.0f / c.fp16_scale : 0.0f}, c.solid_f};
         };
         const int storage = a->ip_variant == kIpF16Fast ? 1 : (a->ip_variant == kIpI16Fast ? 2 : 0);
         if (!cuda_ok(launch_halo_ip(storage, side(*a), side(*b), ab, ba, s), "halo_inplace")) return false;
@@ -1107,6 +1176,253 @@ AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo(int grid_size, long long first_k
                          second_key, ox, oy, oz)
                ? 1
                : 0;
+}
+
+// native_step_raw_dims_with_sparse_overlays_impl (jni.cpp:8686-8745): a full
+// step whose ingested reference fields are overridden at `overlay_count`
+// cells (6 floats each: vx, vy, vz, p, T, source) before the collision.
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect_with_sparse_overlays(const float* packet, int nx, int ny, int nz, long long key,
+                                                                 const int* overlay_cells, const float* overlay_values,
+                                                                 int overlay_count, float* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (overlay_count < 0) {
+        set_error("native_step_raw_dims_sparse: invalid overlay count");
+        return 0;
+    }
+    if (overlay_count > 0 && (!overlay_cells || !overlay_values)) {
+        set_error("native_step_raw_dims_sparse: missing overlay data");
+        return 0;
+    }
+    const SparseOverlays ov{overlay_cells, overlay_values, overlay_count};
+    return step_impl(packet, nx, ny, nz, key, out, 1.0f, false, &ov) ? 1 : 0;
+}
+
+// native_shift_context_impl + shift_context_cpu_state (jni.cpp:9603-9616,
+// 8432-8478): the whole state moves by (dx, dy, dz) (new cell x holds old
+// cell x + d); cells shifted in from outside get the rest equilibrium, fluid,
+// zero reference fields and zero temperature. The classification is rebuilt
+// from the shifted mask with the last call's faces; the next call collides
+// the shifted streamed state.
+AERO_LBM_B200_EXPORT int aero_lbm_shift_context(int grid_size, long long key, int dx, int dy, int dz) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_cfg.initialized || g_cfg.nx != g_cfg.ny || g_cfg.ny != g_cfg.nz || grid_size != g_cfg.nx) {
+        set_error("shift_context: runtime not initialized or grid size mismatch");
+        return 0;
+    }
+    Context* c = find_context(key);
+    if (!c) {
+        set_error("shift_context: missing context");
+        return 0;
+    }
+    if (c->nx != g_cfg.nx || c->ny != g_cfg.ny || c->nz != g_cfg.nz) {
+        set_error("shift_context: context shape differs from the configured grid");
+        return 0;
+    }
+    if (dx == 0 && dy == 0 && dz == 0) return 1;
+    if (std::abs(dx) >= c->nx || std::abs(dy) >= c->ny || std::abs(dz) >= c->nz) {
+        set_error("shift_context: shift larger than the context");
+        return 0;
+    }
+    cudaStream_t s = current_stream();
+    const BrickDims d{c->nx, c->ny, c->nz, 0, c->cells};
+    const size_t cells = (size_t)c->cells;
+    float* tmp = nullptr;
+    if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&tmp), cells * 27 * sizeof(float)), "cudaMalloc(shift)")) return 0;
+    std::unique_ptr<float, decltype(&cudaFree)> tmp_guard(tmp, &cudaFree);
+    // one component-major field of `comps` floats per cell, shifted in place through tmp
+    auto shift_field = [&](float* p, int comps, float fill) {
+        if (!p) return true;
+        return cuda_ok(launch_shift_f32(p, tmp, d, comps, dx, dy, dz, fill, false, s), "shift") &&
+               cuda_ok(cudaMemcpyAsync(p, tmp, cells * comps * sizeof(float), cudaMemcpyDeviceToDevice, s), "shift copy");
+    };
+    if (!shift_field(c->temperature, 1, 0.0f) || !shift_field(c->temperature_next, 1, 0.0f) ||
+        !shift_field(c->temperature_scratch, 1, 0.0f) || !shift_field(c->u_last, 3, 0.0f))
+        return 0;
+    c->force_valid = false;
+    if (!c->initialized) return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
+    const int slot = c->slot;
+    IpView v{};
+    int storage = 0;
+    if (c->layout == 0) {
+        // populations first, through the classification they were streamed with
+        if (c->f_ready) {
+            if (!cuda_ok(launch_shift_f32(c->g[1 - c->cur], c->g[c->cur], d, 27, dx, dy, dz, 0.0f, true, s), "shift f")) return 0;
+            c->cur = 1 - c->cur;
+        } else {
+            if (!cuda_ok(launch_shift_materialise_ab(d, c->g[c->cur], c->flags[slot], c->obstacle[slot], c->ref_p[slot],
+                                                     c->d_face[slot], dx, dy, dz, c->g[1 - c->cur], s),
+                         "shift materialise")) return 0;
+            c->f_ready = true;
+        }
+    } else {
+        storage = c->ip_variant == kIpF16Fast ? 1 : (c->ip_variant == kIpI16Fast ? 2 : 0);
+        if (c->solid_f) {
+            if (!cuda_ok(launch_shift_f32(c->solid_f, tmp, d, 27, dx, dy, dz, 0.0f, true, s), "shift solid") ||
+                !cuda_ok(cudaMemcpyAsync(c->solid_f, tmp, cells * 27 * sizeof(float), cudaMemcpyDeviceToDevice, s),
+                         "shift solid copy"))
+                return 0;
+        }
+        v = IpView{c->ip, make_pad_geom(c->nx, c->ny, c->nz, c->periodic_mask), c->flags[slot], c->parity,
+                   Fp16Scale{c->fp16_scale, c->fp16_scale > 0.0f ? 1.0f / c->fp16_scale : 0.0f}};
+        if (!cuda_ok(launch_ip_gather_shifted(storage, v, dx, dy, dz, tmp, s), "shift gather")) return 0;
+    }
+    // the reference fields (the in-place populations wait in tmp; scalar
+    // shifts then go through the obstacle's spare slot and the spare buffer)
+    uint8_t* ob_tmp = c->obstacle[1 - slot];
+    if (!cuda_ok(launch_shift_u8(c->obstacle[slot], ob_tmp, d, dx, dy, dz, s), "shift obstacle") ||
+        !cuda_ok(cudaMemcpyAsync(c->obstacle[slot], ob_tmp, cells, cudaMemcpyDeviceToDevice, s), "shift obstacle copy"))
+        return 0;
+    float* f_tmp = c->ref_p[1 - slot];
+    auto shift_scalar = [&](float* p) {
+        if (!p) return true;
+        return cuda_ok(launch_shift_f32(p, f_tmp, d, 1, dx, dy, dz, 0.0f, false, s), "shift") &&
+               cuda_ok(cudaMemcpyAsync(p, f_tmp, cells * sizeof(float), cudaMemcpyDeviceToDevice, s), "shift copy");
+    };
+    if (!shift_scalar(c->ref_p[slot]) || !shift_scalar(c->ref_ux) || !shift_scalar(c->ref_uy) || !shift_scalar(c->ref_uz) ||
+        !shift_scalar(c->ref_temperature) || !shift_scalar(c->thermal_source))
+        return 0;
+    if (!cuda_ok(launch_build_flags(c->obstacle[slot], d, c->h_face[slot], c->flags[slot], s), "shift flags")) return 0;
+    if (c->layout == 1) {
+        v.flags = c->flags[slot];
+        if (!cuda_ok(launch_ip_scatter(storage, v, tmp, s), "shift scatter")) return 0;
+    }
+    return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
+}
+
+// The compact (heuristic) solver is not part of this library: no context is
+// ever compact-initialised (jni.cpp:10071-10078 answers 0 without it too).
+AERO_LBM_B200_EXPORT int aero_lbm_context_compact_initialized(long long) { return 0; }
+
+// native_sample_temperature_point_raw_dims_impl (jni.cpp:8899-8947, CPU
+// branch): the raw temperature state of one cell.
+AERO_LBM_B200_EXPORT int aero_lbm_sample_temperature_point_rect(int nx, int ny, int nz, long long key, int x, int y, int z,
+                                                                float* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_cfg.initialized || !out || nx <= 0 || ny <= 0 || nz <= 0 || x < 0 || y < 0 || z < 0 || x >= nx || y >= ny ||
+        z >= nz) {
+        set_error("sample_temperature_point: invalid arguments");
+        return 0;
+    }
+    Context* c = find_context(key);
+    if (!c || c->nx != nx || c->ny != ny || c->nz != nz) {
+        set_error("sample_temperature_point: no context of these dimensions");
+        return 0;
+    }
+    cudaStream_t s = current_stream();
+    const long long cell = ((long long)x * ny + y) * nz + z;
+    return cuda_ok(cudaMemcpyAsync(out, c->temperature + cell, sizeof(float), cudaMemcpyDeviceToHost, s), "copy temperature") &&
+                   cuda_ok(cudaStreamSynchronize(s), "sync")
+               ? 1
+               : 0;
+}
+
+// native_sample_flow_point_raw_dims_impl (jni.cpp:8949-9244, CPU branch):
+// write_output of one cell (velocity unscaled, clamp(rho - 1)); 0 on solids.
+AERO_LBM_B200_EXPORT int aero_lbm_sample_flow_point_rect(int nx, int ny, int nz, long long key, int x, int y, int z,
+                                                         float* out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_cfg.initialized || !out || nx <= 0 || ny <= 0 || nz <= 0 || x < 0 || y < 0 || z < 0 || x >= nx || y >= ny ||
+        z >= nz) {
+        set_error("sample_flow_point: invalid arguments");
+        return 0;
+    }
+    Context* c = find_context(key);
+    if (!c || !c->initialized || c->nx != nx || c->ny != ny || c->nz != nz) {
+        set_error("sample_flow_point: no initialized context of these dimensions");
+        return 0;
+    }
+    return read_output_box(*c, OutBox{x, y, z, 1, 1, 1, 1}, 4, 1.0f, out, nullptr) ? 1 : 0;
+}
+
+// native_copy_flow_temperature_subrect_raw_dims_impl (jni.cpp:9451-9526): the
+// flow (4 floats per cell) and the temperature (0 on solids, clamped) of the
+// box [offset, offset + copy) in cell order, x outermost.
+AERO_LBM_B200_EXPORT int aero_lbm_copy_flow_temperature_subrect(int nx, int ny, int nz, long long key, int ox, int oy, int oz,
+                                                                int cnx, int cny, int cnz, float* out_flow,
+                                                                float* out_temperature) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_cfg.initialized || !out_flow || !out_temperature || nx <= 0 || ny <= 0 || nz <= 0 || cnx <= 0 || cny <= 0 ||
+        cnz <= 0 || ox < 0 || oy < 0 || oz < 0 || ox + cnx > nx || oy + cny > ny || oz + cnz > nz) {
+        set_error("copy_flow_temperature_subrect: invalid arguments");
+        return 0;
+    }
+    Context* c = find_context(key);
+    if (!c || !c->initialized || c->nx != nx || c->ny != ny || c->nz != nz) {
+        set_error("copy_flow_temperature_subrect: no initialized context of these dimensions");
+        return 0;
+    }
+    return read_output_box(*c, OutBox{ox, oy, oz, cnx, cny, cnz, 1}, 4, 1.0f, out_flow, out_temperature) ? 1 : 0;
+}
+
+// aero_lbm_get_last_force (jni.cpp:10259-10267): the momentum-exchange force
+// of the last call (cylinder preset: sum / nz; otherwise 0).
+AERO_LBM_B200_EXPORT int aero_lbm_get_last_force(long long key, float* fx, float* fy, float* fz) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    Context* c = find_context(key);
+    if (!c) {
+        set_error("get_last_force: missing context");
+        return 0;
+    }
+    float f[3] = {0.0f, 0.0f, 0.0f};
+    if (c->force_valid) {
+        double h[3];
+        cudaStream_t s = current_stream();
+        if (!cuda_ok(cudaMemcpyAsync(h, c->force3, sizeof(h), cudaMemcpyDeviceToHost, s), "copy force") ||
+            !cuda_ok(cudaStreamSynchronize(s), "sync"))
+            return 0;
+        const double inv_depth = c->nz > 0 ? 1.0 / (double)c->nz : 1.0;
+        for (int k = 0; k < 3; ++k) f[k] = (float)(h[k] * inv_depth);
+    }
+    if (fx) *fx = f[0];
+    if (fy) *fy = f[1];
+    if (fz) *fz = f[2];
+    return 1;
+}
+
+// memory_info_string (jni.cpp:5436-5457): device bytes per category. The
+// categories follow the reference's names: d3q27_* for in-place contexts,
+// classic_* for two-buffer ones.
+AERO_LBM_B200_EXPORT const char* aero_lbm_memory_info(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    static std::string text;
+    unsigned long long ip_dist = 0, ip_solid = 0, ip_class = 0, ip_out = 0, ab_dist = 0, ab_payload = 0, ab_out = 0,
+                       temp = 0, contexts = 0, cells = 0;
+    for (const auto& kv : g_contexts) {
+        const Context& c = *kv.second;
+        if (!c.allocated) continue;
+        const unsigned long long n = (unsigned long long)c.cells;
+        contexts += 1;
+        cells += n;
+        const unsigned long long t = n * 4ull * (1 + (c.temperature_next ? 2 : 0) + (c.ref_temperature ? 2 : 0)) +
+                                     (c.u_last ? n * 12ull : 0);
+        temp += t;
+        if (c.layout == 1 && c.ip) {
+            const unsigned long long pc = (unsigned long long)(c.nx + 2) * (c.ny + 2) * (c.nz + 2);
+            ip_dist += pc * 27ull * (c.ip_variant == kIpF32Exact || c.ip_variant == kIpF32Fast ? 4ull : 2ull);
+            ip_solid += 2ull * n;
+            ip_class += 2ull * n * 4ull;
+            ip_out += c.out_cap;
+        } else {
+            ab_dist += 2ull * n * 27ull * 4ull;
+            ab_out += c.out_cap;
+        }
+        ab_payload += c.packet_cap;
+    }
+    const unsigned long long total = ip_dist + ip_solid + ip_class + ip_out + ab_dist + ab_payload + ab_out + temp;
+    text = "gpu_bytes(total=" + std::to_string(total) + ",d3q27_dist=" + std::to_string(ip_dist) +
+           ",d3q27_solid=" + std::to_string(ip_solid) + ",d3q27_class=" + std::to_string(ip_class) +
+           ",d3q27_fan=0,d3q27_active=0,d3q27_boundary=0,d3q27_output=" + std::to_string(ip_out) +
+           ",compact_state=0,compact_solid=0,compact_output=0,classic_payload=" + std::to_string(ab_payload) +
+           ",classic_dist=" + std::to_string(ab_dist) + ",classic_output=" + std::to_string(ab_out) +
+           ",classic_temperature=" + std::to_string(temp) + ",classic_thermal_dist=0,contexts=" +
+           std::to_string(contexts) + ",cells=" + std::to_string(cells) + ")";
+    return text.c_str();
 }
 
 AERO_LBM_B200_EXPORT void aero_lbm_release_context(long long key) {

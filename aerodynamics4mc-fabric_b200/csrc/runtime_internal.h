@@ -53,6 +53,7 @@ struct Context {
     int layout = 0;
     int ip_variant = 0;      // IpVariant when layout == 1
     void* ip = nullptr;      // padded population array (float or __half)
+    float* solid_f = nullptr;  // in-place: populations of solid cells (IpArgs::solid_f), from the first mask change on
     int parity = 0;          // slot-map parity of the next in-place step
     int periodic_mask = 0;   // axes wrapped by the in-place layout
     float fp16_scale = 0.0f; // per-brick FP16 deviation scale
@@ -63,6 +64,13 @@ struct Context {
     // Two-buffer layout after a halo exchange: g[1 - cur] holds the streamed
     // state (exchanged slabs included); the next call collides it directly.
     bool f_ready = false;
+    // compute_benchmark_force of the last call (cylinder preset): 3 device doubles
+    double* force3 = nullptr;
+    bool force_valid = false;
+    // device copies of a call's sparse payload overlays
+    int* overlay_cells = nullptr;
+    float* overlay_values = nullptr;
+    int overlay_cap = 0;
     int slot = 0;
     bool allocated = false;
     bool initialized = false;
@@ -100,12 +108,19 @@ Context* find_context(long long key);
 Context* get_or_create_context(long long key, int nx, int ny, int nz);
 void release_all_contexts();
 const RuntimeView runtime_view();
-bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet);
+// Sparse payload overlays of one call (host arrays; 6 values per cell).
+struct SparseOverlays {
+    const int* cells;
+    const float* values;
+    int count;
+};
+bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet,
+                  const SparseOverlays* overlays = nullptr);
 bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out);
 // Per-brick FP16 deviation scale for a brick whose speed stays below umax.
 float fp16_scale_for_speed(float umax);
 float i16_scale_for_speed(float umax);
 // Device-side output into `dev_out` (no copy, no synchronisation).
-bool output_device(Context& ctx, int stride, int out_ch, float scale, float* dev_out);
+bool output_device(Context& ctx, OutBox box, int out_ch, float scale, float* dev_out);
 
 }  // namespace aero

@@ -178,6 +178,42 @@ AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo(int grid_size, long long first_c
 AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo_layers_rect(int nx, int ny, int nz, int halo_layers,
                                                             long long first_context_key, long long second_context_key,
                                                             int offset_x, int offset_y, int offset_z);
+/* native/include/aero_lbm_capi.h:195-205 (jni.cpp:8686-8745, 1696-1721) — a
+ * full step whose ingested reference fields are replaced at overlay_count
+ * cells before the collision (6 floats per overlay: vx, vy, vz, p, T, source;
+ * cell indices outside the brick are skipped). */
+AERO_LBM_B200_EXPORT int aero_lbm_step_rect_with_sparse_overlays(const float* packet, int nx, int ny, int nz,
+                                                                 long long context_key, const int* overlay_cells,
+                                                                 const float* overlay_values, int overlay_count,
+                                                                 float* output_flow);
+/* native/include/aero_lbm_capi.h:206 (jni.cpp:9603-9616, 8432-8478) — move
+ * the whole state by (dx, dy, dz): new cell x holds old cell x + d; cells
+ * shifted in from outside are fluid at rest with zero fields. */
+AERO_LBM_B200_EXPORT int aero_lbm_shift_context(int grid_size, long long context_key, int dx, int dy, int dz);
+/* native/include/aero_lbm_capi.h:208 — always 0: no compact (heuristic)
+ * contexts exist in this library. */
+AERO_LBM_B200_EXPORT int aero_lbm_context_compact_initialized(long long context_key);
+/* native/include/aero_lbm_capi.h:230-239 (jni.cpp:8899-8947) — raw
+ * temperature state of one cell. */
+AERO_LBM_B200_EXPORT int aero_lbm_sample_temperature_point_rect(int nx, int ny, int nz, long long context_key, int sample_x,
+                                                                int sample_y, int sample_z, float* out_temperature);
+/* native/include/aero_lbm_capi.h:240-249 (jni.cpp:8949-9244) — write_output
+ * of one cell (4 floats, velocity unscaled). */
+AERO_LBM_B200_EXPORT int aero_lbm_sample_flow_point_rect(int nx, int ny, int nz, long long context_key, int sample_x,
+                                                         int sample_y, int sample_z, float* out_flow);
+/* native/include/aero_lbm_capi.h:259-272 (jni.cpp:9451-9526) — flow (4 floats
+ * per cell) and temperature (0 on solids, clamped to [-1, 1]) of a sub-box,
+ * x outermost. */
+AERO_LBM_B200_EXPORT int aero_lbm_copy_flow_temperature_subrect(int nx, int ny, int nz, long long context_key, int offset_x,
+                                                                int offset_y, int offset_z, int copy_nx, int copy_ny,
+                                                                int copy_nz, float* out_flow, float* out_temperature);
+/* native/include/aero_lbm_capi.h:275 (jni.cpp:10259-10267, 2454-2492) — the
+ * last call's momentum-exchange force on the cylinder (cylinder preset only,
+ * else 0). */
+AERO_LBM_B200_EXPORT int aero_lbm_get_last_force(long long context_key, float* out_fx, float* out_fy, float* out_fz);
+/* native/include/aero_lbm_capi.h:281 (jni.cpp:5436-5457) — device bytes per
+ * category, the reference's key set. */
+AERO_LBM_B200_EXPORT const char* aero_lbm_memory_info(void);
 /* native/include/aero_lbm_capi.h:241 */
 AERO_LBM_B200_EXPORT int aero_lbm_get_temperature_state_rect(int nx, int ny, int nz, long long context_key, float* out_temperature);
 /* native/include/aero_lbm_capi.h:262 (jni.cpp:9246-9450) — sample every stride cells

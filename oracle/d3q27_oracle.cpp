@@ -18,6 +18,9 @@
 //   stream_and_bounce       native/src/aero_lbm_jni.cpp:2415-2452
 //   write_output            native/src/aero_lbm_jni.cpp:2535-2581
 //   strided atlas extract   native/src/aero_lbm_jni.cpp:9246-9450
+//   sparse payload overlays native/src/aero_lbm_jni.cpp:1696-1721
+//   context shift           native/src/aero_lbm_jni.cpp:8067-8130, 8432-8478
+//   cylinder force          native/src/aero_lbm_jni.cpp:201-227, 2454-2492
 //   halo exchange           native/src/aero_lbm_jni.cpp:8136-8265 (slab bounds,
 //                           slab copies), 9692-9780 (layers entry point)
 //   temperature transport   native/src/aero_lbm_jni.cpp:2049-2143 (first-order
@@ -89,6 +92,7 @@ typedef struct OracleD3Q27Params {
     int internal_thermal_source;   // 1: the packet's source channel feeds the transport
     int packet_has_temperature;    // 1: the packet carries the temperature channel (>= 11 channels)
     int thermal_bfecc;             // 1: the BFECC branch (heated-cavity presets), 0: first-order
+    int cylinder_force;            // 1: the cylinder preset's momentum-exchange force after each collision
 } OracleD3Q27Params;
 
 }  // extern "C"
@@ -224,7 +228,16 @@ struct D3Q27Oracle {
         return f1 + conv_beta * (f1 - f2);
     }
 
-    T equilibrium_value(size_t cell, int q, int face) const {
+    // cylinder_benchmark_inlet_ux (jni.cpp:214-220)
+    T cylinder_inlet_ux(int y, T u_max) const {
+        const T height = T(float(std::max(1, ny - 1)));
+        const T denom = std::max(height - T(0), T(1.0e-6f));
+        const T s = (T(float(y)) - T(0)) / denom;
+        if (s < T(0) || s > T(1)) return T(0);
+        return T(4.0f) * u_max * s * (T(1.0f) - s);
+    }
+
+    T equilibrium_value(size_t cell, int q, int face, int y, int sx) const {
         T r = T(1.0) + clampv(ref_p[cell], p_min, p_max);
         T vx = T(0), vy = T(0), vz = T(0);
         const int kind = p.face_kind[face];
@@ -232,6 +245,12 @@ struct D3Q27Oracle {
             vx = T(p.face_velocity[face][0]);
             vy = T(p.face_velocity[face][1]);
             vz = T(p.face_velocity[face][2]);
+            // the cylinder preset's parabolic inflow (jni.cpp:1536-1545)
+            if (p.cylinder_force && sx < 0) {
+                vx = cylinder_inlet_ux(y, T(p.face_velocity[face][0]));
+                vy = T(0);
+                vz = T(0);
+            }
         } else if (kind == kPressureDirichlet) {
             r = T(1.0) + clampv(T(p.face_pressure[face]), p_min, p_max);
         }
@@ -254,7 +273,7 @@ struct D3Q27Oracle {
             case kMovingWall:
             case kVelocityDirichlet:
             case kPressureDirichlet:
-                return equilibrium_value(cell, q, face);
+                return equilibrium_value(cell, q, face, y, sx);
             case kSymmetry: {
                 const int ix = std::clamp(sx, 0, nx - 1);
                 const int iy = std::clamp(sy, 0, ny - 1);
@@ -707,11 +726,112 @@ struct D3Q27Oracle {
         o[1] = double(vx / r); o[2] = double(vy / r); o[3] = double(vz / r);
     }
 
+    // compute_benchmark_force (jni.cpp:2454-2492) with the disc of
+    // cylinder_benchmark_geometry / cylinder_benchmark_solid_cell
+    // (jni.cpp:201-227), evaluated in float like the reference.
+    float last_force[3] = {0.0f, 0.0f, 0.0f};
+    bool in_cylinder(int x, int y) const {
+        const float length_cells = float(std::max(1, nx - 1));
+        const float channel_height = float(std::max(1, ny - 1));
+        float diameter = std::max(2.5f, 0.1f / 2.2f * length_cells);
+        diameter = std::min(diameter, std::max(2.5f, channel_height - 4.0f));
+        const float radius = 0.5f * diameter;
+        const float cxf = 0.2f / 2.2f * length_cells;
+        const float cyf = 0.0f + 0.2f / 0.41f * channel_height;
+        const float dx = float(x) - cxf, dy = float(y) - cyf;
+        return dx * dx + dy * dy <= radius * radius;
+    }
+    void cylinder_force() {
+        last_force[0] = last_force[1] = last_force[2] = 0.0f;
+        if (!p.cylinder_force) return;
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    const size_t cell = cell_index(x, y, z);
+                    if (obstacle[cell]) continue;
+                    for (int q = 0; q < 27; ++q) {
+                        if (q == 13 || L.cz[q] != 0) continue;
+                        const int ex = x + L.cx[q], ey = y + L.cy[q];
+                        if (ex < 0 || ey < 0 || ex >= nx || ey >= ny) continue;
+                        if (!obstacle[cell_index(ex, ey, z)] || !in_cylinder(ex, ey)) continue;
+                        const double fq = double(f_post[di(cell, q)]);
+                        fx += 2.0 * fq * double(L.cx[q]);
+                        fy += 2.0 * fq * double(L.cy[q]);
+                        fz += 2.0 * fq * double(L.cz[q]);
+                    }
+                }
+        const double inv_depth = nz > 0 ? 1.0 / double(nz) : 1.0;
+        last_force[0] = float(fx * inv_depth);
+        last_force[1] = float(fy * inv_depth);
+        last_force[2] = float(fz * inv_depth);
+    }
+
+    // apply_sparse_payload_overlays (jni.cpp:1696-1721) after an ingest
+    // (load_fields): reference velocity, pressure, temperature and source of
+    // the listed cells. Without the transport the temperature is the
+    // collision's field, as load_fields treats it.
+    void apply_overlays(const int* cells_in, const float* values, int count) {
+        for (int i = 0; i < count; ++i) {
+            const int cell = cells_in[i];
+            if (cell < 0 || size_t(cell) >= cells) continue;
+            const float* v = values + size_t(i) * 6;
+            ref_ux[cell] = T(std::isfinite(v[0]) ? v[0] : 0.0f);
+            ref_uy[cell] = T(std::isfinite(v[1]) ? v[1] : 0.0f);
+            ref_uz[cell] = T(std::isfinite(v[2]) ? v[2] : 0.0f);
+            ref_p[cell] = T(std::min(0.03f, std::max(-0.03f, v[3])));
+            const float t = std::min(1.0f, std::max(-1.0f, v[4]));
+            if (p.thermal_transport) {
+                ref_temperature[cell] = T(t);
+                thermal_source[cell] = T(std::min(0.006f, std::max(-0.006f, v[5])));
+            } else {
+                temperature[cell] = T(t);
+            }
+        }
+    }
+
+    // shift_context_cpu_state (jni.cpp:8432-8478) with shift_scalar_field /
+    // shift_population_field (jni.cpp:8067-8130): new cell x takes old cell
+    // x + d; cells from outside get the fill (rest equilibrium, rho 1, else 0).
+    template <typename V>
+    void shift_field(std::vector<V>& a, int comps, int dx, int dy, int dz, const V* fill) {
+        if (a.size() != cells * size_t(comps)) return;
+        std::vector<V> out(a.size());
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    const int ox = x + dx, oy = y + dy, oz = z + dz;
+                    const bool in = ox >= 0 && ox < nx && oy >= 0 && oy < ny && oz >= 0 && oz < nz;
+                    const size_t c = cell_index(x, y, z);
+                    for (int k = 0; k < comps; ++k)
+                        out[size_t(k) * cells + c] = in ? a[size_t(k) * cells + cell_index(ox, oy, oz)] : fill[k];
+                }
+        a.swap(out);
+    }
+    bool shift(int dx, int dy, int dz) {
+        if (dx == 0 && dy == 0 && dz == 0) return true;
+        if (std::abs(dx) >= nx || std::abs(dy) >= ny || std::abs(dz) >= nz) return false;
+        Arr rest;
+        for (int q = 0; q < 27; ++q) rest[q] = feq(q, T(1), T(0), T(0), T(0));
+        const T zero = T(0), one = T(1);
+        const uint8_t fluid = 0;
+        shift_field(f, 27, dx, dy, dz, rest.data());
+        shift_field(f_post, 27, dx, dy, dz, rest.data());
+        shift_field(rho, 1, dx, dy, dz, &one);
+        for (auto* a : {&ux, &uy, &uz, &ref_ux, &ref_uy, &ref_uz, &ref_p, &ref_temperature, &thermal_source, &temperature,
+                        &temperature_next, &temperature_scratch})
+            shift_field(*a, 1, dx, dy, dz, &zero);
+        shift_field(obstacle, 1, dx, dy, dz, &fluid);
+        last_force[0] = last_force[1] = last_force[2] = 0.0f;
+        return true;
+    }
+
     void step() {
         if (!initialized) initialize();
         else if (p.thermal_transport) apply_temperature_reference();
         if (p.thermal_transport) update_temperature();
         collide();
+        cylinder_force();
         stream();
         ++steps_done;
     }
@@ -918,6 +1038,36 @@ int oracle_d3q27_exchange_halo(void* first, void* second, int ox, int oy, int oz
     if (ox < -1 || ox > 1 || oy < -1 || oy > 1 || oz < -1 || oz > 1 || (ox == 0 && oy == 0 && oz == 0)) return 0;
     return a->f32 ? exchange_halo(*a->f32, *b->f32, ox, oy, oz, halo_layers)
                   : exchange_halo(*a->f64, *b->f64, ox, oy, oz, halo_layers);
+}
+
+int oracle_d3q27_apply_overlays(void* handle, const int* cells, const float* values, int count) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || count < 0 || (count > 0 && (!cells || !values))) return 0;
+    if (h->f32) h->f32->apply_overlays(cells, values, count);
+    else h->f64->apply_overlays(cells, values, count);
+    return 1;
+}
+
+int oracle_d3q27_shift(void* handle, int dx, int dy, int dz) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h) return 0;
+    return (h->f32 ? h->f32->shift(dx, dy, dz) : h->f64->shift(dx, dy, dz)) ? 1 : 0;
+}
+
+int oracle_d3q27_get_obstacle(void* handle, uint8_t* out) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !out) return 0;
+    const auto& ob = h->f32 ? h->f32->obstacle : h->f64->obstacle;
+    std::copy(ob.begin(), ob.end(), out);
+    return 1;
+}
+
+int oracle_d3q27_last_force(void* handle, float* out3) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || !out3) return 0;
+    const float* f = h->f32 ? h->f32->last_force : h->f64->last_force;
+    for (int k = 0; k < 3; ++k) out3[k] = f[k];
+    return 1;
 }
 
 // Strided atlas (aero_lbm_extract_flow_atlas_rect semantics, scale 1).

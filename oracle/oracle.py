@@ -35,6 +35,7 @@ INHERIT_GAME = 0
 # thermal face kinds (native/include/aero_lbm_capi.h:57-62)
 THERMAL_INHERIT, THERMAL_DISABLED, THERMAL_PERIODIC, THERMAL_ADIABATIC, THERMAL_DIRICHLET, THERMAL_NEUMANN = 0, 1, 2, 3, 4, 5
 PRESET_HEATED_CAVITY_2D, PRESET_HEATED_CAVITY_3D = 5, 6  # native/include/aero_lbm_capi.h:41-42
+PRESET_CYLINDER_2D = 4  # native/include/aero_lbm_capi.h:40
 FLAG_DISABLE_CONVECTIVE_OUTFLOW = 1 << 3
 FLAG_DISABLE_SGS = 1 << 5
 FLAG_DISABLE_BUOYANCY = 1 << 7
@@ -79,6 +80,7 @@ class OracleParams(ctypes.Structure):
         ("internal_thermal_source", ctypes.c_int),
         ("packet_has_temperature", ctypes.c_int),
         ("thermal_bfecc", ctypes.c_int),
+        ("cylinder_force", ctypes.c_int),
     ]
 
 
@@ -120,10 +122,16 @@ def derive_params(cfg: dict) -> OracleParams:
         ra = max(f32(1.0e-6), f32(cfg.get("rayleigh", 1.0e5)))
         pr = max(f32(1.0e-6), f32(cfg.get("prandtl", 0.71)))
         nu = _clamp(f32(speed * length) * f32(np.sqrt(f32(pr / ra))), NU_MIN, NU_MAX)
+    elif int(cfg.get("preset", 0)) == PRESET_CYLINDER_2D:
+        # benchmark_reference_speed, cylinder branch (jni.cpp:830-843)
+        speed = _norm(cfg.get("initial_velocity", (0, 0, 0)))
+        if speed <= f32(1.0e-8):
+            speed = f32(f32(2.0) / f32(3.0)) * _norm(faces[0].get("velocity", (0, 0, 0)))
     else:
         speed = _norm(cfg.get("initial_velocity", (0, 0, 0)))
         for fc in faces:
             speed = max(speed, _norm(fc.get("velocity", (0, 0, 0))))
+    if not cavity:
         re = f32(cfg.get("reynolds", 100.0))
         if re <= f32(1.0e-6) or speed <= f32(1.0e-8):
             nu = _clamp(RUNTIME_NU0, NU_MIN, NU_MAX)
@@ -169,6 +177,7 @@ def derive_params(cfg: dict) -> OracleParams:
     p.initial_temperature = float(f32(cfg.get("initial_temperature", 0.0)))
     p.internal_thermal_source = 1 if cfg.get("thermal_source", False) else 0
     p.packet_has_temperature = 1 if int(cfg.get("packet_channels", 11)) > 10 else 0
+    p.cylinder_force = 1 if int(cfg.get("preset", 0)) == PRESET_CYLINDER_2D else 0
     return p
 
 
@@ -199,6 +208,10 @@ class Oracle:
             lib.oracle_d3q27_get_temperature.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.oracle_d3q27_set_temperature.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.oracle_d3q27_exchange_halo.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 4
+            lib.oracle_d3q27_apply_overlays.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+            lib.oracle_d3q27_shift.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 3
+            lib.oracle_d3q27_last_force.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.oracle_d3q27_get_obstacle.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             cls._lib = lib
         return cls._lib
 
@@ -240,6 +253,25 @@ class Oracle:
     def exchange_halo(self, other: "Oracle", offset, halo_layers: int):
         if not self.lib().oracle_d3q27_exchange_halo(self.h, other.h, *[int(v) for v in offset], int(halo_layers)):
             raise RuntimeError("oracle halo exchange failed")
+
+    def apply_overlays(self, cells, values):
+        c = np.ascontiguousarray(np.asarray(cells, np.int32).reshape(-1))
+        v = np.ascontiguousarray(np.asarray(values, np.float32).reshape(-1, 6))
+        if not self.lib().oracle_d3q27_apply_overlays(self.h, c.ctypes.data, v.ctypes.data, int(c.size)):
+            raise RuntimeError("oracle overlays failed")
+
+    def shift(self, dx: int, dy: int, dz: int) -> bool:
+        return bool(self.lib().oracle_d3q27_shift(self.h, int(dx), int(dy), int(dz)))
+
+    def mask(self) -> np.ndarray:
+        out = np.zeros(self.cells, np.uint8)
+        self.lib().oracle_d3q27_get_obstacle(self.h, out.ctypes.data)
+        return out
+
+    def last_force(self) -> np.ndarray:
+        out = np.zeros(3, np.float32)
+        self.lib().oracle_d3q27_last_force(self.h, out.ctypes.data)
+        return out
 
     def set_temperature(self, t):
         arr = np.ascontiguousarray(np.asarray(t, np.float32).reshape(-1))
@@ -428,6 +460,196 @@ class RefLib:
             lib.aero_lbm_get_temperature_state_rect(nx, ny, nz, key, t.ctypes.data)
             self.temperatures.append(t)
         return [o.reshape(-1, 4) for o in outs]
+
+
+    def run_script(self, dims, cfg: dict, packet: np.ndarray, script, key: int = 1, temperature_state=None):
+        """A context driven through a list of calls (see ``run_script_oracle``
+        for the actions); returns the recorded results in order."""
+        nx, ny, nz = dims
+        lib = self.lib
+        vp, i, ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+        lib.aero_lbm_step_rect_with_sparse_overlays.argtypes = [vp, i, i, i, ll, vp, vp, i, vp]
+        lib.aero_lbm_get_flow_state_rect.argtypes = [i, i, i, ll, vp]
+        lib.aero_lbm_shift_context.argtypes = [i, ll, i, i, i]
+        lib.aero_lbm_get_last_force.argtypes = [ll, vp, vp, vp]
+        lib.aero_lbm_sample_flow_point_rect.argtypes = [i, i, i, ll, i, i, i, vp]
+        lib.aero_lbm_sample_temperature_point_rect.argtypes = [i, i, i, ll, i, i, i, vp]
+        lib.aero_lbm_copy_flow_temperature_subrect.argtypes = [i, i, i, ll] + [i] * 6 + [vp, vp]
+        if not lib.aero_lbm_init_rect(nx, ny, nz, packet.shape[1], 4):
+            raise RuntimeError(lib.aero_lbm_last_error())
+        c = config_struct(RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
+        if not lib.aero_lbm_benchmark_set_config(ctypes.byref(c)):
+            raise RuntimeError("set_config failed")
+        cells = nx * ny * nz
+        if temperature_state is not None:
+            t = np.ascontiguousarray(np.asarray(temperature_state, np.float32).reshape(-1))
+            if not lib.aero_lbm_set_temperature_state_rect(nx, ny, nz, key, t.ctypes.data):
+                raise RuntimeError(lib.aero_lbm_last_error())
+        pk = np.ascontiguousarray(packet, dtype=np.float32)
+        results = []
+        for act in script:
+            kind = act[0]
+            if kind == "step":
+                ov = act[1] if len(act) > 1 else None
+                if ov is None:
+                    ok = lib.aero_lbm_step_rect(pk.ctypes.data, nx, ny, nz, key, None)
+                else:
+                    oc = np.ascontiguousarray(ov[0], np.int32)
+                    vals = np.ascontiguousarray(ov[1], np.float32)
+                    ok = lib.aero_lbm_step_rect_with_sparse_overlays(pk.ctypes.data, nx, ny, nz, key, oc.ctypes.data,
+                                                                     vals.ctypes.data, int(oc.size), None)
+                if not ok:
+                    raise RuntimeError(lib.aero_lbm_last_error())
+            elif kind == "flow":
+                out = np.zeros(cells * 4, np.float32)
+                if not lib.aero_lbm_get_flow_state_rect(nx, ny, nz, key, out.ctypes.data):
+                    raise RuntimeError(lib.aero_lbm_last_error())
+                results.append(out.reshape(-1, 4))
+            elif kind == "temp":
+                t = np.zeros(cells, np.float32)
+                lib.aero_lbm_get_temperature_state_rect(nx, ny, nz, key, t.ctypes.data)
+                results.append(t)
+            elif kind == "shift":
+                if not lib.aero_lbm_shift_context(nx, key, *act[1:4]):
+                    raise RuntimeError("shift failed")
+            elif kind == "force":
+                f = np.zeros(3, np.float32)
+                lib.aero_lbm_get_last_force(key, f[0:].ctypes.data, f[1:].ctypes.data, f[2:].ctypes.data)
+                results.append(f)
+            elif kind == "point":
+                fl = np.zeros(4, np.float32)
+                t = np.zeros(1, np.float32)
+                if not (lib.aero_lbm_sample_flow_point_rect(nx, ny, nz, key, *act[1:4], fl.ctypes.data) and
+                        lib.aero_lbm_sample_temperature_point_rect(nx, ny, nz, key, *act[1:4], t.ctypes.data)):
+                    raise RuntimeError("point sample failed")
+                results.append((fl, t))
+            elif kind == "subrect":
+                n = int(np.prod(act[4:7]))
+                fl = np.zeros(n * 4, np.float32)
+                t = np.zeros(n, np.float32)
+                if not lib.aero_lbm_copy_flow_temperature_subrect(nx, ny, nz, key, *act[1:7], fl.ctypes.data, t.ctypes.data):
+                    raise RuntimeError("subrect copy failed")
+                results.append((fl.reshape(-1, 4), t))
+            else:
+                raise ValueError(kind)
+        return results
+
+
+def run_script_oracle(o: "Oracle", cfg: dict, packet: np.ndarray, script):
+    """The same call list on the oracle. Actions: ("step", overlays|None) with
+    overlays = (cells int32, values float32 x 6); ("flow",) write_output of
+    the streamed state; ("temp",) temperature state; ("shift", dx, dy, dz);
+    ("force",) last_force; ("point", x, y, z) -> (flow 4, [T]); ("subrect",
+    ox, oy, oz, cx, cy, cz) -> (flow cells x 4, T with solids 0, clamped)."""
+    n = o.dims
+    pk = np.asarray(packet, np.float32)
+    obst = pk[:, 0] > 0.5
+    transport = bool(derive_params(cfg).thermal_transport)
+    results = []
+    for act in script:
+        kind = act[0]
+        if kind == "step":
+            o.set_fields(obst.reshape(n).astype(np.uint8), *(pk[:, 5 + a].reshape(n) for a in range(3)),
+                         pressure=pk[:, 8].reshape(n),
+                         temperature=pk[:, 10].reshape(n) if pk.shape[1] > 10 else None)
+            if transport:
+                o.set_thermal_source(pk[:, 9] if (pk.shape[1] > 9 and cfg.get("thermal_source", False))
+                                     else np.zeros(pk.shape[0], np.float32))
+            ov = act[1] if len(act) > 1 else None
+            if ov is not None:
+                o.apply_overlays(ov[0], ov[1])
+            o.step(1)
+        elif kind == "flow":
+            results.append(o.output())
+        elif kind == "temp":
+            results.append(o.temperature())
+        elif kind == "shift":
+            if not o.shift(*act[1:4]):
+                raise RuntimeError("oracle shift failed")
+        elif kind == "force":
+            results.append(o.last_force())
+        elif kind == "point":
+            x, y, z = act[1:4]
+            cell = (x * n[1] + y) * n[2] + z
+            results.append((o.output()[cell].copy(), o.temperature()[cell:cell + 1].copy()))
+        elif kind == "subrect":
+            ox, oy, oz, cx, cy, cz = act[1:7]
+            flow = o.output().reshape(n + (4,))[ox:ox + cx, oy:oy + cy, oz:oz + cz].reshape(-1, 4)
+            t = o.temperature().reshape(n)[ox:ox + cx, oy:oy + cy, oz:oz + cz].reshape(-1)
+            solid = o.mask().reshape(n)[ox:ox + cx, oy:oy + cy, oz:oz + cz].reshape(-1) != 0
+            t = np.where(solid, np.float32(0), np.nan_to_num(np.clip(t, -1, 1), nan=0.0, posinf=0.0, neginf=0.0))
+            results.append((flow.copy(), t.astype(np.float32)))
+        else:
+            raise ValueError(kind)
+    return results
+
+
+def context_ops_script(n: int, seed: int = 23):
+    """A call list over the per-context entry points around the step: four
+    steps, a read of flow and temperature, a shift, point and sub-box reads,
+    steps with sparse overlays (40 cells plus two out-of-range indices), a
+    second shift, a step and the last force."""
+    rng = np.random.default_rng(seed)
+    cells = np.concatenate([rng.choice(n ** 3, 40, replace=False), [-1, n ** 3 + 5]]).astype(np.int32)
+    k = cells.size
+    vals = np.stack([rng.uniform(-0.05, 0.05, k), rng.uniform(-0.05, 0.05, k), rng.uniform(-0.05, 0.05, k),
+                     rng.uniform(-0.05, 0.05, k), rng.uniform(-1.5, 1.5, k), rng.uniform(-0.01, 0.01, k)],
+                    1).astype(np.float32)
+    ov = (cells, vals)
+    return ([("step",)] * 4 + [("flow",), ("temp",), ("shift", 1, -2, 0), ("flow",), ("temp",), ("point", 3, 4, 5),
+            ("subrect", 2, 3, 1, 5, 4, 6), ("step",), ("step", ov), ("step", ov), ("flow",), ("temp",),
+            ("shift", -3, 0, 2), ("step",), ("flow",), ("temp",), ("point", 0, 0, 0), ("force",)])
+
+
+CYLINDER_SCRIPT = [("step",), ("force",)] * 5 + [("flow",)]
+
+
+def load_results(path) -> list:
+    """The recorded results of a script fixture (r<i> or the pair r<i>_0, r<i>_1)."""
+    g = np.load(path)
+    out = []
+    for i in range(int(g["count"])):
+        out.append((g[f"r{i}_0"], g[f"r{i}_1"]) if f"r{i}_0" in g.files else g[f"r{i}"])
+    return out
+
+
+def results_equal(a, b) -> list:
+    """Per result: bit-identical (float32 views compared as integers)?"""
+    flags = []
+    for x, y in zip(a, b):
+        if isinstance(x, tuple):
+            flags.append(all(np.array_equal(np.asarray(p, np.float32).view(np.uint32),
+                                            np.asarray(q, np.float32).view(np.uint32)) for p, q in zip(x, y)))
+        else:
+            flags.append(np.array_equal(np.asarray(x, np.float32).view(np.uint32), np.asarray(y, np.float32).view(np.uint32)))
+    return flags
+
+
+def cylinder_case(nx: int = 44, ny: int = 20, nz: int = 3, sgs: bool = True):
+    """The 2-D cylinder crossflow preset (native/src/aero_lbm_jni.cpp:341-…,
+    geometry 201-227) as a configuration: inflow 0.12 at x-, convective
+    outflow at x+, walls y, periodic z, Re 100, u0 = (0.08, 0, 0); the packet
+    marks the disc of cylinder_benchmark_solid_cell solid. Returns the config
+    and the packet."""
+    length_cells = np.float32(max(1, nx - 1))
+    channel_height = np.float32(max(1, ny - 1))
+    diameter = max(np.float32(2.5), np.float32(np.float32(0.1) / np.float32(2.2)) * length_cells)
+    diameter = min(diameter, max(np.float32(2.5), np.float32(channel_height - np.float32(4.0))))
+    radius = np.float32(np.float32(0.5) * diameter)
+    cxf = np.float32(np.float32(np.float32(0.2) / np.float32(2.2)) * length_cells)
+    cyf = np.float32(np.float32(0.0) + np.float32(np.float32(0.2) / np.float32(0.41)) * channel_height)
+    xs = np.arange(nx, dtype=np.float32)[:, None] - cxf
+    ys = np.arange(ny, dtype=np.float32)[None, :] - cyf
+    disc = (xs * xs + ys * ys) <= radius * radius
+    obst = np.repeat(disc[:, :, None], nz, axis=2).astype(np.uint8)
+    u = (np.where(obst == 0, np.float32(0.08), np.float32(0)).astype(np.float32), np.zeros(obst.shape, np.float32),
+         np.zeros(obst.shape, np.float32))
+    faces = [{"kind": VELOCITY, "velocity": (0.12, 0, 0)}, {"kind": CONVECTIVE},
+             {"kind": BOUNCE_BACK}, {"kind": BOUNCE_BACK},
+             {"kind": PERIODIC, "thermal": THERMAL_PERIODIC}, {"kind": PERIODIC, "thermal": THERMAL_PERIODIC}]
+    cfg = {"preset": PRESET_CYLINDER_2D, "reynolds": 100.0, "initial_velocity": (0.08, 0.0, 0.0), "faces": faces,
+           "sgs": sgs, "buoyancy": False, "thermal_source": False}
+    return cfg, packet_from(obst, *u)
 
 
 # ---------------------------------------------------------------- configs

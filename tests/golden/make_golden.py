@@ -26,6 +26,15 @@ Fixtures:
                   offset (1, -1, 0), aero_lbm_exchange_halo_layers_rect after
                   every third of 12 calls; both write_output results and
                   temperature states.
+  ctxops_12.npz   the per-context entry points around the step
+                  (oracle.context_ops_script: steps, shifts, sparse overlays,
+                  point and sub-box reads, the last force) on
+                  oracle.thermal_case(12, seed 21) with the transport; every
+                  recorded result in order (r<i>, or r<i>_0 / r<i>_1 for pairs).
+  cylinder_44x20x3.npz the cylinder crossflow preset (oracle.cylinder_case:
+                  parabolic inflow, convective outflow, the disc as the mask):
+                  the momentum-exchange force after each of 5 calls and the
+                  final flow (oracle.CYLINDER_SCRIPT).
   thermal_12_20.npz buoyancy on with the reference's temperature transport:
                   oracle.thermal_case(12, seed 11) (every thermal face kind,
                   packet source channel, state preloaded), 20 steps; the
@@ -108,6 +117,34 @@ def halo_fixture(ref) -> None:
     print("halo_12_12 written")
 
 
+def save_results(path, results, **meta) -> None:
+    arrays = {}
+    for i, r in enumerate(results):
+        if isinstance(r, tuple):
+            for j, a in enumerate(r):
+                arrays[f"r{i}_{j}"] = a
+        else:
+            arrays[f"r{i}"] = r
+    np.savez_compressed(path, count=len(results), **arrays, **meta)
+
+
+def ctxops_fixture(ref) -> None:
+    n, seed = 12, 21
+    obst, u, temp, src, cfg, pre = O.thermal_case(n, seed)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+    res = ref.run_script((n, n, n), cfg, pk, O.context_ops_script(n), temperature_state=pre)
+    save_results(OUT / "ctxops_12.npz", res, n=n, seed=seed, input_sha256=digest(pk, pre))
+    print("ctxops_12 written")
+
+
+def cylinder_fixture(ref) -> None:
+    dims = (44, 20, 3)
+    cfg, pk = O.cylinder_case(*dims)
+    res = ref.run_script(dims, cfg, pk, O.CYLINDER_SCRIPT)
+    save_results(OUT / "cylinder_44x20x3.npz", res, dims=np.array(dims), input_sha256=digest(pk))
+    print("cylinder_44x20x3 written")
+
+
 def main() -> int:
     O.build(ref=True)
     ref = O.RefLib()
@@ -119,6 +156,10 @@ def main() -> int:
             cavity_fixture(ref)
         if only in "halo_12_12":
             halo_fixture(ref)
+        if only in "ctxops_12":
+            ctxops_fixture(ref)
+        if only in "cylinder_44x20x3":
+            cylinder_fixture(ref)
         return 0
     for name, n, steps in (("c1_16_200", 16, 200), ("c1_32_1000", 32, 1000)):
         seed = 1234
@@ -144,6 +185,8 @@ def main() -> int:
     thermal_fixture(ref)
     cavity_fixture(ref)
     halo_fixture(ref)
+    ctxops_fixture(ref)
+    cylinder_fixture(ref)
     return 0
 
 

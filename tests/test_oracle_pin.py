@@ -195,3 +195,55 @@ def test_oracle_halo_exchange_matches_reference_live(offset, halo, buoy):
     for o, out, t in zip(os_, outs, ref.temperatures):
         assert _bits_equal(o.output(), out)
         assert _bits_equal(o.temperature(), t)
+
+
+def _ctxops_oracle(n, seed, script=None):
+    obst, u, temp, src, cfg, pre = O.thermal_case(n, seed)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    return O.run_script_oracle(o, cfg, pk, script or O.context_ops_script(n)), (cfg, pk, pre)
+
+
+def test_oracle_context_ops_match_golden():
+    """Shifts, sparse overlays, point and sub-box reads around the step
+    (fixture ctxops_12.npz from the reference library), bit for bit."""
+    g = np.load(GOLDEN / "ctxops_12.npz")
+    res, _ = _ctxops_oracle(int(g["n"]), int(g["seed"]))
+    ref = O.load_results(GOLDEN / "ctxops_12.npz")
+    assert len(res) == len(ref) and all(O.results_equal(res, ref))
+
+
+def test_oracle_cylinder_force_matches_golden():
+    """The cylinder preset: parabolic inflow and the momentum-exchange force
+    after each call (fixture cylinder_44x20x3.npz), bit for bit."""
+    dims = (44, 20, 3)
+    cfg, pk = O.cylinder_case(*dims)
+    o = O.Oracle(dims, O.derive_params(cfg), "f32")
+    res = O.run_script_oracle(o, cfg, pk, O.CYLINDER_SCRIPT)
+    ref = O.load_results(GOLDEN / "cylinder_44x20x3.npz")
+    assert all(O.results_equal(res, ref))
+    assert abs(float(res[0][0])) > 0.0  # the disc does feel a force
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("seed,script", [(31, None),
+                                         (32, [("step",)] * 3 + [("shift", 0, 0, -5), ("point", 11, 11, 11),
+                                                                 ("subrect", 0, 0, 0, 12, 12, 12), ("step",),
+                                                                 ("shift", 11, 0, 0), ("flow",), ("temp",)])])
+def test_oracle_context_ops_match_reference_live(seed, script):
+    n = 12
+    res, (cfg, pk, pre) = _ctxops_oracle(n, seed, script)
+    ref = O.RefLib().run_script((n, n, n), cfg, pk, script or O.context_ops_script(n), temperature_state=pre)
+    assert all(O.results_equal(res, ref))
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+def test_oracle_cylinder_force_matches_reference_live():
+    dims = (30, 16, 2)
+    cfg, pk = O.cylinder_case(*dims, sgs=False)
+    script = [("step",), ("force",)] * 3 + [("flow",)]
+    o = O.Oracle(dims, O.derive_params(cfg), "f32")
+    res = O.run_script_oracle(o, cfg, pk, script)
+    ref = O.RefLib().run_script(dims, cfg, pk, script)
+    assert all(O.results_equal(res, ref))
