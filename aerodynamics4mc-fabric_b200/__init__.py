@@ -200,6 +200,10 @@ SIGNATURES = {
     "aero_lbm_context_realtime_cached_initialized": (_I, [_LL]),
     "aero_lbm_exchange_halo": (_I, [_I, _LL, _LL, _I, _I, _I]),
     "aero_lbm_exchange_halo_layers_rect": (_I, [_I, _I, _I, _I, _LL, _LL, _I, _I, _I]),
+    "aero_lbm_patch_d3q27_f16_static_cells_rect": (_I, [_I, _I, _I, _LL, _I, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p]),
+    "aero_lbm_set_d3q27_f16_boundary_shell_rect": (_I, [_I, _I, _I, _LL, _F32P, _I, _I, _I, _F]),
+    "aero_lbm_clear_d3q27_f16_boundary_shell_rect": (_I, [_LL]),
     "aero_lbm_step_rect_with_sparse_overlays": (_I, [_F32P, _I, _I, _I, _LL, ctypes.c_void_p, _F32P, _I, _F32P]),
     "aero_lbm_shift_context": (_I, [_I, _LL, _I, _I, _I]),
     "aero_lbm_context_compact_initialized": (_I, [_LL]),

@@ -16,12 +16,16 @@
 #include <sstream>
 #include <string>
 #include <unordered_map>
+#include <vector>
+
+#include <cuda_fp16.h>
 
 #include "../../include/aero_lbm_b200.h"
 #include "d3q27_kernels.cuh"
 #include "ip_launch.h"
 #include "conservation.cuh"
 #include "context_ops.cuh"
+#include "edits.cuh"
 #include "halo.cuh"
 #include "runtime_internal.h"
 #include "thermal.cuh"
@@ -413,6 +417,12 @@ void Context::release_device() {
     fr(reinterpret_cast<void*&>(overlay_cells));
     fr(reinterpret_cast<void*&>(overlay_values));
     overlay_cap = 0;
+    fr(reinterpret_cast<void*&>(patch_cells));
+    fr(reinterpret_cast<void*&>(patch_solid));
+    patch_cap = 0;
+    pending_slot = -1;
+    fr(shell);
+    shell_count = 0;
     force_valid = false;
     f_ready = false;
     fr(ip);
@@ -516,6 +526,12 @@ static bool inplace_faces_ok(const FaceParams& f) {
         return false;
     }
     return true;
+}
+
+// Storage of an in-place context for the kernels that take it as a number:
+// 0 FP32, 1 IEEE-half deviations, 2 16-bit fixed point.
+static int ip_storage(const Context& ctx) {
+    return ctx.ip_variant == kIpF16Fast ? 1 : (ctx.ip_variant == kIpI16Fast ? 2 : 0);
 }
 
 static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const CollideParams& cp) {
@@ -711,6 +727,10 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         }
         if (!classify(ctx, new_slot, face_now, d, s)) return false;
         ctx.has_inputs = true;
+    } else if (ctx.pending_slot >= 0) {
+        // block edits staged the mask of this call (aero_lbm_patch_d3q27_f16_static_cells_rect)
+        new_slot = ctx.pending_slot;
+        if (face_changed && !classify(ctx, new_slot, face_now, d, s)) return false;
     } else if (face_changed && ctx.initialized) {
         // Same inputs, new faces: rebuild the classification into the other slot.
         new_slot = 1 - ctx.slot;
@@ -775,7 +795,8 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             if (!cuda_ok(ip_init(ctx.ip_variant, ctx.ip, a, s), "init_inplace")) return false;
             ctx.parity = 1;
         } else {
-            if (have_packet && !ctx.solid_f) {
+            const bool transitions = have_packet || ctx.pending_slot >= 0;
+            if (transitions && !ctx.solid_f) {
                 // the first call that can change the mask: solid cells so far
                 // have been solid since initialisation and hold the rest state
                 if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.solid_f), (size_t)ctx.cells * 27 * sizeof(float)),
@@ -785,11 +806,12 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
                 a.solid_f = ctx.solid_f;
             }
             a.parity = ctx.parity;
-            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, have_packet, false, s), "step_inplace")) return false;
+            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, transitions, false, s), "step_inplace")) return false;
             ctx.parity ^= 1;
         }
     }
     ctx.slot = new_slot;
+    ctx.pending_slot = -1;
     ctx.face_prev = face_now;
     ctx.initialized = true;
     ctx.step_counter += 1;
@@ -816,6 +838,13 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             IpArgs a = ip_args(ctx, new_slot, new_slot, cp);
             a.parity = ctx.parity;
             if (!cuda_ok(ip_fill(ctx.ip_variant, ctx.ip, a, s), "face_fill_inplace")) return false;
+        }
+        if (ctx.shell_count > 0) {
+            IpArgs a = ip_args(ctx, new_slot, new_slot, cp);
+            a.parity = ctx.parity;
+            if (!cuda_ok(launch_shell_relax(ip_storage(ctx), ctx.ip, a, static_cast<const ShellCell*>(ctx.shell),
+                                            ctx.shell_count, ctx.shell_layers, ctx.shell_relax, s),
+                         "boundary_shell")) return false;
         }
     }
 
@@ -1221,6 +1250,10 @@ AERO_LBM_B200_EXPORT int aero_lbm_shift_context(int grid_size, long long key, in
         return 0;
     }
     if (dx == 0 && dy == 0 && dz == 0) return 1;
+    if (c->pending_slot >= 0) {
+        set_error("shift_context: block edits are staged for the next call; step once before shifting");
+        return 0;
+    }
     if (std::abs(dx) >= c->nx || std::abs(dy) >= c->ny || std::abs(dz) >= c->nz) {
         set_error("shift_context: shift larger than the context");
         return 0;
@@ -1289,6 +1322,189 @@ AERO_LBM_B200_EXPORT int aero_lbm_shift_context(int grid_size, long long key, in
         if (!cuda_ok(launch_ip_scatter(storage, v, tmp, s), "shift scatter")) return 0;
     }
     return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
+}
+
+// Block edits (patch_d3q27_f16_static_cells, jni.cpp:6156-6260, 4725-4778,
+// 9905-9960) on an in-place context that has stepped: the mask of the next
+// call is the current one with the patched cells set solid / fluid, and every
+// patched cell restarts at rest (its incoming populations, or its stored
+// populations while it is solid). The next call, cached or not, steps with
+// mask transitions; a call with a packet replaces the staged mask. Fan
+// directions are accepted and ignored (fans are not modelled).
+AERO_LBM_B200_EXPORT int aero_lbm_patch_d3q27_f16_static_cells_rect(int nx, int ny, int nz, long long key, int count,
+                                                                    const int* cells, const uint8_t* solid,
+                                                                    const uint8_t* fan_dir) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_cfg.initialized) {
+        set_error("patch_d3q27_f16_static_cells: runtime is not initialized");
+        return 0;
+    }
+    if (count <= 0) return 1;
+    if (!cells || !solid || !fan_dir) {
+        set_error("patch_d3q27_f16_static_cells: missing patch arrays");
+        return 0;
+    }
+    if (nx <= 0 || ny <= 0 || nz <= 0 || nx != g_cfg.nx || ny != g_cfg.ny || nz != g_cfg.nz) {
+        set_error("patch_d3q27_f16_static_cells: invalid dimensions");
+        return 0;
+    }
+    Context* c = find_context(key);
+    if (!c) {
+        set_error("patch_d3q27_f16_static_cells: context not found");
+        return 0;
+    }
+    if (c->nx != nx || c->ny != ny || c->nz != nz) {
+        set_error("patch_d3q27_f16_static_cells: context shape mismatch");
+        return 0;
+    }
+    if (!c->initialized || c->layout != 1) {
+        set_error("patch_d3q27_f16_static_cells: needs an in-place context that has stepped");
+        return 0;
+    }
+    cudaStream_t s = current_stream();
+    if (c->patch_cap < count) {
+        if (c->patch_cells) cudaFree(c->patch_cells);
+        if (c->patch_solid) cudaFree(c->patch_solid);
+        c->patch_cells = nullptr;
+        c->patch_solid = nullptr;
+        c->patch_cap = 0;
+        if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&c->patch_cells), (size_t)count * sizeof(int)), "cudaMalloc(patch)") ||
+            !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&c->patch_solid), (size_t)count), "cudaMalloc(patch)"))
+            return 0;
+        c->patch_cap = count;
+    }
+    if (!cuda_ok(cudaMemcpyAsync(c->patch_cells, cells, (size_t)count * sizeof(int), cudaMemcpyHostToDevice, s), "copy patch") ||
+        !cuda_ok(cudaMemcpyAsync(c->patch_solid, solid, (size_t)count, cudaMemcpyHostToDevice, s), "copy patch"))
+        return 0;
+    const int target = 1 - c->slot;
+    const BrickDims d{c->nx, c->ny, c->nz, 0, c->cells};
+    const uint8_t* base = c->obstacle[c->pending_slot >= 0 ? c->pending_slot : c->slot];
+    if (c->pending_slot < 0 &&
+        !cuda_ok(cudaMemcpyAsync(c->ref_p[target], c->ref_p[c->slot], (size_t)c->cells * sizeof(float),
+                                 cudaMemcpyDeviceToDevice, s), "copy pressure proxy"))
+        return 0;
+    if (!cuda_ok(launch_patch_mask(base, c->obstacle[target], c->cells, c->patch_cells, c->patch_solid, count, s),
+                 "patch mask") ||
+        !classify(*c, target, c->face_prev, d, s))
+        return 0;
+    IpArgs a = ip_args(*c, c->slot, c->slot, current_collide_params());
+    a.parity = c->parity;
+    if (!cuda_ok(launch_patch_reset(ip_storage(*c), c->ip, a, c->patch_cells, count, s), "patch reset")) return 0;
+    c->pending_slot = target;
+    return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
+}
+
+// upload_d3q27_f16_boundary_shell (jni.cpp:6449-6540): fluid cells within
+// shell_layers of a face in face_mask (bit i: x-, x+, y-, y+, z-, z+) get a
+// layer (1 outermost) and a target (the flow state's velocity, speed-clamped,
+// and pressure, rounded to half precision); after every later call their
+// state is relaxed toward it (edits.cuh). Needs an in-place context that has
+// stepped. A zero mask, layer count or relaxation clears the shell.
+AERO_LBM_B200_EXPORT int aero_lbm_set_d3q27_f16_boundary_shell_rect(int nx, int ny, int nz, long long key,
+                                                                    const float* flow, int channels, int face_mask,
+                                                                    int shell_layers, float relaxation) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    if (!g_cfg.initialized) {
+        set_error("set_d3q27_f16_boundary_shell: runtime is not initialized");
+        return 0;
+    }
+    if (nx <= 0 || ny <= 0 || nz <= 0 || nx != g_cfg.nx || ny != g_cfg.ny || nz != g_cfg.nz) {
+        set_error("set_d3q27_f16_boundary_shell: invalid dimensions");
+        return 0;
+    }
+    if (!flow || channels < 4) {
+        set_error("set_d3q27_f16_boundary_shell: missing flow state");
+        return 0;
+    }
+    Context* c = find_context(key);
+    if (!c) {
+        set_error("set_d3q27_f16_boundary_shell: context not found");
+        return 0;
+    }
+    if (c->nx != nx || c->ny != ny || c->nz != nz) {
+        set_error("set_d3q27_f16_boundary_shell: context shape mismatch");
+        return 0;
+    }
+    auto clear = [&]() {
+        if (c->shell) cudaFree(c->shell);
+        c->shell = nullptr;
+        c->shell_count = 0;
+        c->shell_layers = 0;
+        c->shell_relax = 0.0f;
+        return 1;
+    };
+    if (face_mask == 0 || shell_layers <= 0 || !(relaxation > 0.0f)) return clear();
+    if (!c->initialized || c->layout != 1) {
+        set_error("set_d3q27_f16_boundary_shell: needs an in-place context that has stepped");
+        return 0;
+    }
+    const int layers = std::max(1, std::min({shell_layers, nx, ny, nz}));
+    const float relax = clampf_h(finite_or(relaxation, 0.0f), 0.0f, 0.5f);
+    if (relax <= 0.0f) return clear();
+    cudaStream_t s = current_stream();
+    std::vector<uint8_t> solid((size_t)c->cells);
+    const uint8_t* mask = c->obstacle[c->pending_slot >= 0 ? c->pending_slot : c->slot];
+    if (!cuda_ok(cudaMemcpyAsync(solid.data(), mask, solid.size(), cudaMemcpyDeviceToHost, s), "copy mask") ||
+        !cuda_ok(cudaStreamSynchronize(s), "sync"))
+        return 0;
+    auto half_round = [](float v) { return __half2float(__float2half_rn(v)); };
+    std::vector<ShellCell> list;
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const long long cell = ((long long)x * ny + y) * nz + z;
+                if (solid[(size_t)cell]) continue;
+                int best = layers + 1;
+                if ((face_mask & 1) && x < layers) best = std::min(best, x + 1);
+                if ((face_mask & 2) && x >= nx - layers) best = std::min(best, nx - x);
+                if ((face_mask & 4) && y < layers) best = std::min(best, y + 1);
+                if ((face_mask & 8) && y >= ny - layers) best = std::min(best, ny - y);
+                if ((face_mask & 16) && z < layers) best = std::min(best, z + 1);
+                if ((face_mask & 32) && z >= nz - layers) best = std::min(best, nz - z);
+                if (best > layers) continue;
+                const float* v = flow + (size_t)cell * (size_t)channels;
+                float vx = finite_or(v[0], 0.0f), vy = finite_or(v[1], 0.0f), vz = finite_or(v[2], 0.0f);
+                const float p = clampf_h(finite_or(v[3], 0.0f), -0.03f, 0.03f);
+                const float s2 = vx * vx + vy * vy + vz * vz;
+                if (!std::isfinite(s2) || s2 > kMaxSpeed * kMaxSpeed) {
+                    if (!std::isfinite(s2) || s2 <= 0.0f) {
+                        vx = vy = vz = 0.0f;
+                    } else {
+                        const float k = kMaxSpeed / std::sqrt(s2);
+                        vx *= k; vy *= k; vz *= k;
+                    }
+                }
+                list.push_back(ShellCell{(int)cell, best, half_round(vx), half_round(vy), half_round(vz), half_round(p)});
+            }
+    clear();
+    if (list.empty()) return 1;
+    if (!cuda_ok(cudaMalloc(&c->shell, list.size() * sizeof(ShellCell)), "cudaMalloc(shell)")) return 0;
+    if (!cuda_ok(cudaMemcpyAsync(c->shell, list.data(), list.size() * sizeof(ShellCell), cudaMemcpyHostToDevice, s),
+                 "copy shell") ||
+        !cuda_ok(cudaStreamSynchronize(s), "sync"))
+        return 0;
+    c->shell_count = (int)list.size();
+    c->shell_layers = layers;
+    c->shell_relax = relax;
+    return 1;
+}
+
+// clear_d3q27_f16_boundary_shell (jni.cpp:6443-6447, 10024-10037): 1 also
+// when the context does not exist.
+AERO_LBM_B200_EXPORT int aero_lbm_clear_d3q27_f16_boundary_shell_rect(long long key) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    clear_error();
+    Context* c = find_context(key);
+    if (c) {
+        if (c->shell) cudaFree(c->shell);
+        c->shell = nullptr;
+        c->shell_count = 0;
+        c->shell_layers = 0;
+        c->shell_relax = 0.0f;
+    }
+    return 1;
 }
 
 // The compact (heuristic) solver is not part of this library: no context is

@@ -71,6 +71,17 @@ struct Context {
     int* overlay_cells = nullptr;
     float* overlay_values = nullptr;
     int overlay_cap = 0;
+    // Block edits staged for the next call (its mask and classification in
+    // this slot), or -1.
+    int pending_slot = -1;
+    int* patch_cells = nullptr;
+    uint8_t* patch_solid = nullptr;
+    int patch_cap = 0;
+    // Boundary-reference shell (in-place): cells, layers, relaxation.
+    void* shell = nullptr;
+    int shell_count = 0;
+    int shell_layers = 0;
+    float shell_relax = 0.0f;
     int slot = 0;
     bool allocated = false;
     bool initialized = false;

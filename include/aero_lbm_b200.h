@@ -178,6 +178,26 @@ AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo(int grid_size, long long first_c
 AERO_LBM_B200_EXPORT int aero_lbm_exchange_halo_layers_rect(int nx, int ny, int nz, int halo_layers,
                                                             long long first_context_key, long long second_context_key,
                                                             int offset_x, int offset_y, int offset_z);
+/* native/include/aero_lbm_capi.h:173-182 (jni.cpp:6156-6260, 9905-9960) — block
+ * edits on an in-place context that has stepped: the next call's mask is the
+ * current one with cell_indices[i] set to solid_values[i] (later entries win),
+ * and every patched cell restarts at rest. fan_dir_values must be given and
+ * is ignored (no fan model). */
+AERO_LBM_B200_EXPORT int aero_lbm_patch_d3q27_f16_static_cells_rect(int nx, int ny, int nz, long long context_key,
+                                                                    int patch_count, const int* cell_indices,
+                                                                    const uint8_t* solid_values,
+                                                                    const uint8_t* fan_dir_values);
+/* native/include/aero_lbm_capi.h:183-193 (jni.cpp:6449-6540, 9962-10022) — a
+ * boundary-reference shell: fluid cells within shell_layers of the faces in
+ * face_mask (bit i: x-, x+, y-, y+, z-, z+) are relaxed after every call
+ * toward the given flow state (flow_channels >= 4: ux, uy, uz, p) with
+ * strength relaxation (<= 0.5) x (1 - (layer - 1) / layers)^2. In-place
+ * contexts that have stepped; a zero mask, layer count or relaxation clears. */
+AERO_LBM_B200_EXPORT int aero_lbm_set_d3q27_f16_boundary_shell_rect(int nx, int ny, int nz, long long context_key,
+                                                                    const float* flow_state, int flow_channels,
+                                                                    int face_mask, int shell_layers, float relaxation);
+/* native/include/aero_lbm_capi.h:194 — remove the shell (1 also without a context). */
+AERO_LBM_B200_EXPORT int aero_lbm_clear_d3q27_f16_boundary_shell_rect(long long context_key);
 /* native/include/aero_lbm_capi.h:195-205 (jni.cpp:8686-8745, 1696-1721) — a
  * full step whose ingested reference fields are replaced at overlay_count
  * cells before the collision (6 floats per overlay: vx, vy, vz, p, T, source;

@@ -21,6 +21,10 @@
 //   sparse payload overlays native/src/aero_lbm_jni.cpp:1696-1721
 //   context shift           native/src/aero_lbm_jni.cpp:8067-8130, 8432-8478
 //   cylinder force          native/src/aero_lbm_jni.cpp:201-227, 2454-2492
+//   block edits, shell      native/src/aero_lbm_jni.cpp:6156-6260, 6449-6540 (the
+//                           library's own formulation: patched cells restart at
+//                           rest; the shell relaxes mass and momentum toward its
+//                           targets by an equilibrium shift after every call)
 //   halo exchange           native/src/aero_lbm_jni.cpp:8136-8265 (slab bounds,
 //                           slab copies), 9692-9780 (layers entry point)
 //   temperature transport   native/src/aero_lbm_jni.cpp:2049-2143 (first-order
@@ -826,6 +830,98 @@ struct D3Q27Oracle {
         return true;
     }
 
+    // Block edits: mask entries set, patched cells' streamed populations at rest.
+    void apply_patch(const int* cells_in, const uint8_t* solid, int count) {
+        for (int i = 0; i < count; ++i) {
+            const int c = cells_in[i];
+            if (c < 0 || size_t(c) >= cells) continue;
+            obstacle[c] = solid[i] ? 1 : 0;
+            for (int q = 0; q < 27; ++q) f[di(c, q)] = feq(q, T(1), T(0), T(0), T(0));
+        }
+    }
+
+    // Boundary-reference shell (upload_d3q27_f16_boundary_shell's layer and
+    // target rules, jni.cpp:6449-6540; targets rounded to half precision).
+    struct ShellCell { size_t cell; int layer; float ux, uy, uz, p; };
+    std::vector<ShellCell> shell;
+    int shell_layers = 0;
+    float shell_relax = 0.0f;
+    static float half_round(float v) { return float(static_cast<_Float16>(v)); }
+    void set_shell(const float* flow, int channels, int face_mask, int layers_in, float relaxation) {
+        shell.clear();
+        shell_layers = 0;
+        shell_relax = 0.0f;
+        if (!flow || channels < 4 || face_mask == 0 || layers_in <= 0 || !(relaxation > 0.0f)) return;
+        const int layers = std::max(1, std::min({layers_in, nx, ny, nz}));
+        const float relax = std::min(0.5f, std::max(0.0f, std::isfinite(relaxation) ? relaxation : 0.0f));
+        if (relax <= 0.0f) return;
+        const float ms = 0.57735026919f * 0.60f;
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    const size_t c = cell_index(x, y, z);
+                    if (obstacle[c]) continue;
+                    int best = layers + 1;
+                    if ((face_mask & 1) && x < layers) best = std::min(best, x + 1);
+                    if ((face_mask & 2) && x >= nx - layers) best = std::min(best, nx - x);
+                    if ((face_mask & 4) && y < layers) best = std::min(best, y + 1);
+                    if ((face_mask & 8) && y >= ny - layers) best = std::min(best, ny - y);
+                    if ((face_mask & 16) && z < layers) best = std::min(best, z + 1);
+                    if ((face_mask & 32) && z >= nz - layers) best = std::min(best, nz - z);
+                    if (best > layers) continue;
+                    const float* v = flow + c * size_t(channels);
+                    auto fin = [](float a) { return std::isfinite(a) ? a : 0.0f; };
+                    float vx = fin(v[0]), vy = fin(v[1]), vz = fin(v[2]);
+                    const float pr = std::min(0.03f, std::max(-0.03f, fin(v[3])));
+                    const float s2 = vx * vx + vy * vy + vz * vz;
+                    if (!std::isfinite(s2) || s2 > ms * ms) {
+                        if (!std::isfinite(s2) || s2 <= 0.0f) {
+                            vx = vy = vz = 0.0f;
+                        } else {
+                            const float k = ms / std::sqrt(s2);
+                            vx *= k; vy *= k; vz *= k;
+                        }
+                    }
+                    shell.push_back({c, best, half_round(vx), half_round(vy), half_round(vz), half_round(pr)});
+                }
+        shell_layers = layers;
+        shell_relax = relax;
+    }
+    void relax_shell() {
+        const T ms = T(p.max_speed);
+        for (const ShellCell& sc : shell) {
+            if (obstacle[sc.cell]) continue;
+            T r = T(0), jx = T(0), jy = T(0), jz = T(0);
+            for (int q = 0; q < 27; ++q) {
+                const T fq = f[di(sc.cell, q)];
+                r += fq;
+                jx += fq * T(L.cx[q]); jy += fq * T(L.cy[q]); jz += fq * T(L.cz[q]);
+            }
+            if (!(std::isfinite(double(r)) && std::isfinite(double(jx)) && std::isfinite(double(jy)) && std::isfinite(double(jz))))
+                continue;
+            r = clampv(r, rho_min, rho_max);
+            T vx = jx / r, vy = jy / r, vz = jz / r;
+            const T s2 = vx * vx + vy * vy + vz * vz;
+            if (!std::isfinite(double(s2)) || s2 > ms * ms) {
+                if (!std::isfinite(double(s2)) || s2 <= T(0)) {
+                    vx = vy = vz = T(0);
+                } else {
+                    const T k = ms / std::sqrt(s2);
+                    vx *= k; vy *= k; vz *= k;
+                }
+            }
+            const T t = T(1) - T(float(sc.layer - 1)) / std::max(T(1), T(float(shell_layers)));
+            const T alpha = clampv(T(shell_relax) * t * t, T(0), T(0.5f));
+            const T rt = clampv(T(1) + clampv(T(sc.p), p_min, p_max), rho_min, rho_max);
+            const T nx_ = vx + alpha * (T(sc.ux) - vx), ny_ = vy + alpha * (T(sc.uy) - vy), nz_ = vz + alpha * (T(sc.uz) - vz);
+            const T nr = r + alpha * (rt - r);
+            for (int q = 0; q < 27; ++q) {
+                T& fq = f[di(sc.cell, q)];
+                fq = fq + (feq(q, nr, nx_, ny_, nz_) - feq(q, r, vx, vy, vz));
+            }
+        }
+    }
+
     void step() {
         if (!initialized) initialize();
         else if (p.thermal_transport) apply_temperature_reference();
@@ -833,6 +929,7 @@ struct D3Q27Oracle {
         collide();
         cylinder_force();
         stream();
+        if (!shell.empty()) relax_shell();
         ++steps_done;
     }
 };
@@ -1052,6 +1149,22 @@ int oracle_d3q27_shift(void* handle, int dx, int dy, int dz) {
     auto* h = static_cast<Handle*>(handle);
     if (!h) return 0;
     return (h->f32 ? h->f32->shift(dx, dy, dz) : h->f64->shift(dx, dy, dz)) ? 1 : 0;
+}
+
+int oracle_d3q27_patch_cells(void* handle, const int* cells, const uint8_t* solid, int count) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h || count < 0 || (count > 0 && (!cells || !solid))) return 0;
+    if (h->f32) h->f32->apply_patch(cells, solid, count);
+    else h->f64->apply_patch(cells, solid, count);
+    return 1;
+}
+
+int oracle_d3q27_set_shell(void* handle, const float* flow, int channels, int face_mask, int layers, float relaxation) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h) return 0;
+    if (h->f32) h->f32->set_shell(flow, channels, face_mask, layers, relaxation);
+    else h->f64->set_shell(flow, channels, face_mask, layers, relaxation);
+    return 1;
 }
 
 int oracle_d3q27_get_obstacle(void* handle, uint8_t* out) {

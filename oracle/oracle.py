@@ -212,6 +212,8 @@ class Oracle:
             lib.oracle_d3q27_shift.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 3
             lib.oracle_d3q27_last_force.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.oracle_d3q27_get_obstacle.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.oracle_d3q27_patch_cells.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+            lib.oracle_d3q27_set_shell.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 3 + [ctypes.c_float]
             cls._lib = lib
         return cls._lib
 
@@ -262,6 +264,18 @@ class Oracle:
 
     def shift(self, dx: int, dy: int, dz: int) -> bool:
         return bool(self.lib().oracle_d3q27_shift(self.h, int(dx), int(dy), int(dz)))
+
+    def patch_cells(self, cells, solid):
+        c = np.ascontiguousarray(np.asarray(cells, np.int32).reshape(-1))
+        s = np.ascontiguousarray(np.asarray(solid, np.uint8).reshape(-1))
+        if not self.lib().oracle_d3q27_patch_cells(self.h, c.ctypes.data, s.ctypes.data, int(c.size)):
+            raise RuntimeError("oracle patch failed")
+
+    def set_shell(self, flow, face_mask: int, layers: int, relaxation: float):
+        fl = np.ascontiguousarray(np.asarray(flow, np.float32).reshape(self.cells, -1))
+        self._shell_flow = fl
+        self.lib().oracle_d3q27_set_shell(self.h, fl.ctypes.data, fl.shape[1], int(face_mask), int(layers),
+                                          float(relaxation))
 
     def mask(self) -> np.ndarray:
         out = np.zeros(self.cells, np.uint8)
@@ -537,7 +551,9 @@ class RefLib:
 
 def run_script_oracle(o: "Oracle", cfg: dict, packet: np.ndarray, script):
     """The same call list on the oracle. Actions: ("step", overlays|None) with
-    overlays = (cells int32, values float32 x 6); ("flow",) write_output of
+    overlays = (cells int32, values float32 x 6); ("cached",) a step with the
+    resident inputs; ("patch", cells, solid) block edits; ("shell", flow
+    cells x 4, face_mask, layers, relaxation); ("flow",) write_output of
     the streamed state; ("temp",) temperature state; ("shift", dx, dy, dz);
     ("force",) last_force; ("point", x, y, z) -> (flow 4, [T]); ("subrect",
     ox, oy, oz, cx, cy, cz) -> (flow cells x 4, T with solids 0, clamped)."""
@@ -559,6 +575,12 @@ def run_script_oracle(o: "Oracle", cfg: dict, packet: np.ndarray, script):
             if ov is not None:
                 o.apply_overlays(ov[0], ov[1])
             o.step(1)
+        elif kind == "cached":
+            o.step(1)
+        elif kind == "patch":
+            o.patch_cells(act[1], act[2])
+        elif kind == "shell":
+            o.set_shell(act[1], act[2], act[3], act[4])
         elif kind == "flow":
             results.append(o.output())
         elif kind == "temp":
@@ -604,6 +626,12 @@ def context_ops_script(n: int, seed: int = 23):
 CYLINDER_SCRIPT = [("step",), ("force",)] * 5 + [("flow",)]
 
 
+def feq_rest(q: int) -> float:
+    """Rest equilibrium weight of direction q (q = (ix*3+iy)*3+iz)."""
+    w1 = (1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0)
+    return float(np.float32(np.float32(np.float32(w1[q // 9]) * np.float32(w1[(q // 3) % 3])) * np.float32(w1[q % 3])))
+
+
 def load_results(path) -> list:
     """The recorded results of a script fixture (r<i> or the pair r<i>_0, r<i>_1)."""
     g = np.load(path)
@@ -623,6 +651,31 @@ def results_equal(a, b) -> list:
         else:
             flags.append(np.array_equal(np.asarray(x, np.float32).view(np.uint32), np.asarray(y, np.float32).view(np.uint32)))
     return flags
+
+
+def edits_script(n: int, seed: int = 43):
+    """Block edits and the boundary shell between steps: patches that close
+    fluid cells, open solid ones, reset fluid cells (duplicates and an
+    out-of-range index included), cached steps, a shell on three faces, a
+    second round of patches, the shell cleared."""
+    rng = np.random.default_rng(seed)
+
+    def patches(k):
+        cells = np.concatenate([rng.choice(n ** 3, k, replace=False), [n ** 3 + 7]]).astype(np.int32)
+        cells = np.concatenate([cells, cells[:3]])
+        solid = (rng.random(cells.size) < 0.4).astype(np.uint8)
+        return cells, solid
+
+    flow = np.zeros((n ** 3, 4), np.float32)
+    flow[:, 0] = 0.02 + rng.uniform(-0.005, 0.005, n ** 3)
+    flow[:, 1] = 0.01
+    flow[:, 2] = rng.uniform(-0.01, 0.01, n ** 3)
+    flow[:, 3] = 0.001
+    p1, p2, p3 = patches(30), patches(20), patches(25)
+    return ([("step",)] * 3 + [("patch",) + p1, ("cached",), ("cached",), ("flow",), ("temp",),
+                               ("shell", flow, 0b010011, 3, 0.3), ("step",), ("step",), ("flow",),
+                               ("patch",) + p2, ("patch",) + p3, ("cached",), ("flow",), ("temp",),
+                               ("shell", flow, 0, 3, 0.3), ("step",), ("flow",), ("temp",)])
 
 
 def cylinder_case(nx: int = 44, ny: int = 20, nz: int = 3, sgs: bool = True):

@@ -1,9 +1,10 @@
 """The per-context entry points around the step on the GPU: sparse payload
 overlays (aero_lbm_step_rect_with_sparse_overlays), the whole-state shift
 (aero_lbm_shift_context), point samples, sub-box copies, the cylinder
-preset's force (aero_lbm_get_last_force), memory_info and
-context_compact_initialized (native/src/aero_lbm_jni.cpp:1696-1721,
-2454-2492, 8432-8478, 8686-8745, 8899-9244, 9451-9526, 10039-10300).
+preset's force (aero_lbm_get_last_force), memory_info,
+context_compact_initialized, block edits and the boundary shell of in-place
+bricks (native/src/aero_lbm_jni.cpp:1696-1721, 2454-2492, 6156-6540,
+8432-8478, 8686-8745, 8899-9244, 9451-9526, 9905-10300).
 
 The reference-order FP32 path is bit-identical to the reference library's
 fixtures (ctxops_12.npz, cylinder_44x20x3.npz) in both layouts and launch
@@ -59,6 +60,19 @@ def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mod
                     vals = np.ascontiguousarray(ov[1], np.float32)
                     assert gpu.aero_lbm_step_rect_with_sparse_overlays(_fp(pk), nx, ny, nz, key, oc.ctypes.data, _fp(vals),
                                                                        int(oc.size), None) == 1, aero_b200.last_error(gpu)
+            elif kind == "cached":
+                assert gpu.aero_lbm_step_rect_cached(nx, ny, nz, key, None) == 1, aero_b200.last_error(gpu)
+            elif kind == "patch":
+                c = np.ascontiguousarray(act[1], np.int32)
+                sv = np.ascontiguousarray(act[2], np.uint8)
+                fan = np.zeros(c.size, np.uint8)
+                assert gpu.aero_lbm_patch_d3q27_f16_static_cells_rect(nx, ny, nz, key, int(c.size), c.ctypes.data,
+                                                                      sv.ctypes.data, fan.ctypes.data) == 1, \
+                    aero_b200.last_error(gpu)
+            elif kind == "shell":
+                fl = np.ascontiguousarray(act[1], np.float32)
+                assert gpu.aero_lbm_set_d3q27_f16_boundary_shell_rect(nx, ny, nz, key, _fp(fl), fl.shape[1], act[2],
+                                                                      act[3], act[4]) == 1, aero_b200.last_error(gpu)
             elif kind == "flow":
                 results.append(ctx.flow_state())
             elif kind == "temp":
@@ -88,7 +102,7 @@ def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mod
     finally:
         gpu.aero_lbm_b200_set_cells_per_thread(2)
         gpu.aero_lbm_set_realtime_solver_mode(0)
-    assert len(results) == sum(1 for a in script if a[0] not in ("step", "shift"))
+    assert len(results) == sum(1 for a in script if a[0] not in ("step", "shift", "cached", "patch", "shell"))
     return results
 
 
@@ -133,7 +147,7 @@ def test_context_ops_fp16_against_fp64(gpu):
     o = O.Oracle((n, n, n), O.derive_params(cfg), "f64")
     o.set_temperature(pre)
     ref = O.run_script_oracle(o, cfg, pk, script)
-    kinds = [a[0] for a in script if a[0] not in ("step", "shift")]
+    kinds = [a[0] for a in script if a[0] not in ("step", "shift", "cached", "patch", "shell")]
     for kind, a, b in zip(kinds, res, ref):
         if kind == "flow":
             e = O.flow_errors(a, b)
@@ -191,3 +205,75 @@ def test_context_ops_argument_checks(gpu):
         assert total >= n ** 3 * 27 * 2
     finally:
         ctx.release()
+
+
+@pytest.mark.parametrize("cpt", [1, 2])
+def test_block_edits_and_shell_match_oracle(gpu, cpt):
+    """In-place FP32 (reference-order collision): block edits between calls
+    (cached steps after them, duplicates, out-of-range indices, solid cells
+    opened and fluid ones closed) and the boundary shell, bit-identical to
+    the oracle's restatement of the same operations."""
+    n = 12
+    obst, u, temp, src, cfg, pre = O.thermal_case(n, 41)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+    script = O.edits_script(n)
+    res = run_script_gpu(gpu, (n, n, n), cfg, pk, script, key=860 + cpt, streaming=2, cpt=cpt, temperature_state=pre)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    flags = O.results_equal(res, O.run_script_oracle(o, cfg, pk, script))
+    assert all(flags), flags
+
+
+def test_block_edits_and_shell_fp16_against_fp64(gpu):
+    n = 12
+    obst, u, temp, src, cfg, pre = O.thermal_case(n, 41)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+    script = O.edits_script(n)
+    res = run_script_gpu(gpu, (n, n, n), cfg, pk, script, key=865, streaming=2, solver_mode=3, temperature_state=pre)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f64")
+    o.set_temperature(pre)
+    ref = O.run_script_oracle(o, cfg, pk, script)
+    kinds = [a[0] for a in script if a[0] in ("flow", "temp", "point", "subrect", "force")]
+    for kind, a, b in zip(kinds, res, ref):
+        if kind == "flow":
+            e = O.flow_errors(a, b)
+            assert e["u"] <= 1e-3 and e["rho"] <= 1e-4, e
+        elif kind == "temp":
+            assert float(np.max(np.abs(a - b))) <= 1e-3
+
+
+def test_block_edits_and_shell_argument_checks(gpu):
+    n = 12
+    obst, u, temp, src, cfg, pre = O.thermal_case(n, 41)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+    c = np.array([5, 6], np.int32)
+    sv = np.array([1, 0], np.uint8)
+    fan = np.zeros(2, np.uint8)
+    flow = np.zeros((n ** 3, 4), np.float32)
+    patch = gpu.aero_lbm_patch_d3q27_f16_static_cells_rect
+    shell = gpu.aero_lbm_set_d3q27_f16_boundary_shell_rect
+    for streaming, key in ((1, 870), (2, 871)):
+        gpu.aero_lbm_b200_set_streaming_mode(streaming)
+        ctx = aero_b200.LbmContext((n, n, n), key=key, lib=gpu)
+        ctx.configure(lbm_cases.product_config(gpu, cfg))
+        try:
+            assert patch(n, n, n, key, 2, c.ctypes.data, sv.ctypes.data, fan.ctypes.data) == 0  # no context yet
+            ctx.step(pk, output=False)
+            assert patch(n, n, n, key, 0, None, None, None) == 1
+            assert patch(n, n, n, key, 2, c.ctypes.data, sv.ctypes.data, None) == 0
+            assert "missing patch arrays" in aero_b200.last_error(gpu)
+            assert patch(n, n, n + 1, key, 2, c.ctypes.data, sv.ctypes.data, fan.ctypes.data) == 0
+            assert shell(n, n, n, key, _fp(flow), 3, 1, 2, 0.2) == 0
+            assert shell(n, n, n, key, _fp(flow), 4, 0, 2, 0.2) == 1  # empty mask clears
+            ok = streaming == 2
+            assert patch(n, n, n, key, 2, c.ctypes.data, sv.ctypes.data, fan.ctypes.data) == (1 if ok else 0)
+            assert shell(n, n, n, key, _fp(flow), 4, 1, 2, 0.2) == (1 if ok else 0)
+            if ok:
+                # staged edits block a shift until the next call
+                assert gpu.aero_lbm_shift_context(n, key, 1, 0, 0) == 0
+                assert gpu.aero_lbm_step_rect_cached(n, n, n, key, None) == 1
+                assert gpu.aero_lbm_shift_context(n, key, 1, 0, 0) == 1
+            assert gpu.aero_lbm_clear_d3q27_f16_boundary_shell_rect(key) == 1
+            assert gpu.aero_lbm_clear_d3q27_f16_boundary_shell_rect(99999) == 1
+        finally:
+            ctx.release()

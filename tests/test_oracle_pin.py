@@ -247,3 +247,43 @@ def test_oracle_cylinder_force_matches_reference_live():
     res = O.run_script_oracle(o, cfg, pk, script)
     ref = O.RefLib().run_script(dims, cfg, pk, script)
     assert all(O.results_equal(res, ref))
+
+
+def test_oracle_block_edits_and_shell_behaviour():
+    """Block edits and the boundary shell have no CPU twin in the reference
+    (its CPU build answers "OpenCL disabled"), so the oracle's restatement is
+    their specification: a patched cell restarts at rest with the new mask,
+    and the shell pulls the shell cells' velocity toward the target, more
+    strongly in the outer layer, while a cleared shell leaves the step as it
+    was."""
+    n = 12
+    obst, u, temp, src, cfg, pre = O.thermal_case(n, 41)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+
+    def run(script):
+        o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+        o.set_temperature(pre)
+        return o, O.run_script_oracle(o, cfg, pk, script)
+
+    cell = int(np.flatnonzero(obst.reshape(-1) == 0)[100])
+    o, res = run([("step",)] * 2 + [("patch", [cell], [0]), ("flow",)])
+    f = o.populations()[:, cell]
+    w = np.array([O.feq_rest(q) for q in range(27)])
+    assert np.allclose(f, w, rtol=0, atol=1e-7)
+    assert abs(res[0][cell]).max() == 0.0  # at rest: no velocity, no pressure
+    o, _ = run([("step",)] * 2 + [("patch", [cell], [1])])
+    assert o.mask()[cell] == 1
+
+    target = np.zeros((n ** 3, 4), np.float32)
+    target[:, 1] = 0.05
+    base = [("step",)] * 2
+    _, plain = run(base + [("cached",)] * 6 + [("flow",)])
+    _, shelled = run(base + [("shell", target, 0b000001, 3, 0.4)] + [("cached",)] * 6 + [("flow",)])
+    _, cleared = run(base + [("shell", target, 0b000001, 3, 0.4), ("shell", target, 0, 3, 0.4)] + [("cached",)] * 6
+                     + [("flow",)])
+    uy_plain = plain[0].reshape(n, n, n, 4)[..., 1]
+    uy_shell = shelled[0].reshape(n, n, n, 4)[..., 1]
+    fluid = obst == 0
+    gain = [float(np.mean((uy_shell - uy_plain)[x][fluid[x]])) for x in range(4)]
+    assert gain[0] > gain[1] > gain[2] > 0.0 and gain[0] > 1e-3, gain
+    assert _bits_equal(cleared[0], plain[0])
