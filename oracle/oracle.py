@@ -43,12 +43,15 @@ FLAG_DISABLE_BUOYANCY = 1 << 7
 
 def build(ref: bool | None = None) -> None:
     """Compile liboracle.so (always) and the reference library (when its
-    sources are present and ``ref`` is not False)."""
+    sources are present and ``ref`` is not False); with the product library
+    built, also the reference's brick service over both libraries."""
     subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
     if ref is None:
         ref = REFERENCE_SOURCE.exists()
     if ref:
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REFERENCE_SOURCE}"], check=True)
+        if (HERE.parent / "aerodynamics4mc-fabric_b200" / "libaero_lbm_b200.so").exists():
+            subprocess.run(["make", "-s", "-C", str(HERE), "sim", f"REF={REFERENCE_SOURCE}"], check=True)
 
 
 # ---------------------------------------------------------------- parameter derivation
@@ -703,6 +706,123 @@ def cylinder_case(nx: int = 44, ny: int = 20, nz: int = 3, sgs: bool = True):
     cfg = {"preset": PRESET_CYLINDER_2D, "reynolds": 100.0, "initial_velocity": (0.08, 0.0, 0.0), "faces": faces,
            "sgs": sgs, "buoyancy": False, "thermal_source": False}
     return cfg, packet_from(obst, *u)
+
+
+# ---------------------------------------------------------------- the reference's brick service
+SIM_REF_LIB = REF_LIB.parent / "libaero_sim_ref.so"
+SIM_B200_LIB = REF_LIB.parent / "libaero_sim_b200.so"
+
+
+class BrickService:
+    """The reference's brick-world service (its simulation bridge, built by
+    `make -C oracle sim`), driven through its C ABI. ``libaero_sim_ref.so``
+    runs it over the reference's CPU step; ``libaero_sim_b200.so`` is the same
+    service source linked against libaero_lbm_b200.so."""
+
+    def __init__(self, path: Path):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} missing (build with `make -C oracle sim`)")
+        lib = ctypes.CDLL(str(path))
+        vp, i, ll, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_float
+        for name, args in (
+                ("aero_lbm_simulation_create_service", [vp]),
+                ("aero_lbm_simulation_ensure_brick_world_runtime", [ll, ll, i, f, f]),
+                ("aero_lbm_simulation_set_brick_world_solver_mode", [ll, ll, i]),
+                ("aero_lbm_simulation_set_brick_world_exact_active_hints", [ll, ll, i, vp, i]),
+                ("aero_lbm_simulation_upload_brick_world_static_brick_with_sources",
+                 [ll, ll, i, i, i, i, vp, vp, vp, vp, vp, vp, vp, vp]),
+                ("aero_lbm_simulation_upload_brick_world_dynamic_brick", [ll, ll, i, i, i, i, vp, vp, vp]),
+                ("aero_lbm_simulation_step_brick_world_runtime", [ll, ll, i]),
+                ("aero_lbm_simulation_copy_brick_world_packed_flow_atlas", [ll, ll, i, i, i, i, i, vp, i]),
+                ("aero_lbm_simulation_copy_brick_world_dynamic_brick", [ll, ll, i, i, i, i, vp, vp, vp]),
+                ("aero_lbm_simulation_get_brick_world_runtime_status", [ll, ll, vp, i])):
+            getattr(lib, name).argtypes = args
+            getattr(lib, name).restype = ctypes.c_int
+        lib.aero_lbm_simulation_release_service.argtypes = [ll]
+        lib.aero_lbm_simulation_last_error.restype = ctypes.c_char_p
+        self.lib = lib
+
+    def _ok(self, v):
+        if not v:
+            raise RuntimeError(self.lib.aero_lbm_simulation_last_error())
+
+    def run(self, world: dict) -> dict:
+        """world: n, bricks [(bx, by, bz)], solver_mode, steps, dx, dt, and per
+        brick the static obstacle (n^3 u8) and dynamic flow (n^3 x 4), air and
+        surface temperature. Returns per brick the stride-4 packed atlas and
+        the dynamic brick after ``steps`` ticks, and the runtime status."""
+        lib, n = self.lib, int(world["n"])
+        key = ctypes.c_longlong(0)
+        self._ok(lib.aero_lbm_simulation_create_service(ctypes.byref(key)))
+        svc, wk = key.value, 1
+        try:
+            self._ok(lib.aero_lbm_simulation_ensure_brick_world_runtime(svc, wk, n, world["dx"], world["dt"]))
+            self._ok(lib.aero_lbm_simulation_set_brick_world_solver_mode(svc, wk, int(world["solver_mode"])))
+            coords = np.ascontiguousarray(np.array(world["bricks"], np.int32).reshape(-1))
+            self._ok(lib.aero_lbm_simulation_set_brick_world_exact_active_hints(svc, wk, n, coords.ctypes.data,
+                                                                                len(world["bricks"])))
+            cells = n ** 3
+            zeros_u8 = np.zeros(cells, np.uint8)
+            zeros_u16 = np.zeros(cells, np.uint16)
+            zeros_f = np.zeros(cells, np.float32)
+            faces = np.zeros(cells * 6, np.uint8)
+            keep = []
+            for b, (bx, by, bz) in enumerate(world["bricks"]):
+                ob = np.ascontiguousarray(world["obstacle"][b], np.uint8)
+                self._ok(lib.aero_lbm_simulation_upload_brick_world_static_brick_with_sources(
+                    svc, wk, n, bx, by, bz, ob.ctypes.data, zeros_u8.ctypes.data, zeros_u16.ctypes.data,
+                    zeros_f.ctypes.data, None, None, faces.ctypes.data, faces.ctypes.data))
+                fl = np.ascontiguousarray(world["flow"][b], np.float32)
+                at = np.ascontiguousarray(world["air_t"][b], np.float32)
+                st = np.ascontiguousarray(world["surface_t"][b], np.float32)
+                keep += [ob, fl, at, st]
+                self._ok(lib.aero_lbm_simulation_upload_brick_world_dynamic_brick(
+                    svc, wk, n, bx, by, bz, fl.ctypes.data, at.ctypes.data, st.ctypes.data))
+            self._ok(lib.aero_lbm_simulation_step_brick_world_runtime(svc, wk, int(world["steps"])))
+            out = {"atlas": [], "flow": [], "air_t": []}
+            s = (n + 3) // 4
+            for bx, by, bz in world["bricks"]:
+                atlas = np.zeros(s ** 3 * 4, np.int16)
+                self._ok(lib.aero_lbm_simulation_copy_brick_world_packed_flow_atlas(svc, wk, n, bx, by, bz, 4,
+                                                                                    atlas.ctypes.data, atlas.size))
+                fl = np.zeros(cells * 4, np.float32)
+                at = np.zeros(cells, np.float32)
+                st = np.zeros(cells, np.float32)
+                self._ok(lib.aero_lbm_simulation_copy_brick_world_dynamic_brick(svc, wk, n, bx, by, bz, fl.ctypes.data,
+                                                                                at.ctypes.data, st.ctypes.data))
+                out["atlas"].append(atlas)
+                out["flow"].append(fl.reshape(-1, 4))
+                out["air_t"].append(at)
+            status = np.zeros(8, np.int32)
+            lib.aero_lbm_simulation_get_brick_world_runtime_status(svc, wk, status.ctypes.data, 8)
+            out["status"] = status
+            return out
+        finally:
+            lib.aero_lbm_simulation_release_service(svc)
+
+
+def brick_world_case(n: int = 16, steps: int = 6, seed: int = 51, solver_mode: int = 1):
+    """Four face-adjacent bricks (2 x 2 in x-z) of n^3 cells: a solid ground
+    layer in the lower bricks plus 5 % random solids, a seeded flow of about
+    0.05 (lattice units), small air temperature deviations."""
+    rng = np.random.default_rng(seed)
+    bricks = [(0, 0, 0), (1, 0, 0), (0, 0, 1), (1, 0, 1)]
+    cells = n ** 3
+    obstacle, flow, air_t, surface_t = [], [], [], []
+    for _ in bricks:
+        ob = (rng.random((n, n, n)) < 0.05).astype(np.uint8)
+        ob[:, 0, :] = 1
+        obstacle.append(ob.reshape(-1))
+        fl = np.zeros((cells, 4), np.float32)
+        fl[:, 0] = 0.05 + rng.uniform(-0.01, 0.01, cells)
+        fl[:, 1] = rng.uniform(-0.005, 0.005, cells)
+        fl[:, 2] = 0.02 + rng.uniform(-0.01, 0.01, cells)
+        fl[ob.reshape(-1) != 0] = 0.0
+        flow.append(fl)
+        air_t.append(rng.uniform(-0.05, 0.05, cells).astype(np.float32))
+        surface_t.append(np.zeros(cells, np.float32))
+    return {"n": n, "bricks": bricks, "solver_mode": solver_mode, "steps": steps, "dx": 1.0, "dt": 0.05,
+            "obstacle": obstacle, "flow": flow, "air_t": air_t, "surface_t": surface_t}
 
 
 # ---------------------------------------------------------------- configs

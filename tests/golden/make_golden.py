@@ -35,6 +35,10 @@ Fixtures:
                   parabolic inflow, convective outflow, the disc as the mask):
                   the momentum-exchange force after each of 5 calls and the
                   final flow (oracle.CYLINDER_SCRIPT).
+  brickworld_16x4_6.npz the reference's brick-world service (its simulation
+                  bridge over its CPU step, oracle.BrickService) on
+                  oracle.brick_world_case(): four 16^3 bricks, 6 ticks in the
+                  classic solver mode; packed atlases, dynamic bricks, status.
   thermal_12_20.npz buoyancy on with the reference's temperature transport:
                   oracle.thermal_case(12, seed 11) (every thermal face kind,
                   packet source channel, state preloaded), 20 steps; the
@@ -145,6 +149,15 @@ def cylinder_fixture(ref) -> None:
     print("cylinder_44x20x3 written")
 
 
+def brickworld_fixture() -> None:
+    w = O.brick_world_case()
+    r = O.BrickService(O.SIM_REF_LIB).run(w)
+    np.savez_compressed(OUT / "brickworld_16x4_6.npz", atlas=np.stack(r["atlas"]), flow=np.stack(r["flow"]),
+                        air_t=np.stack(r["air_t"]), status=r["status"], steps=w["steps"], n=w["n"],
+                        input_sha256=digest(*w["obstacle"], *w["flow"], *w["air_t"]))
+    print("brickworld_16x4_6 written")
+
+
 def main() -> int:
     O.build(ref=True)
     ref = O.RefLib()
@@ -160,6 +173,8 @@ def main() -> int:
             ctxops_fixture(ref)
         if only in "cylinder_44x20x3":
             cylinder_fixture(ref)
+        if only in "brickworld_16x4_6":
+            brickworld_fixture()
         return 0
     for name, n, steps in (("c1_16_200", 16, 200), ("c1_32_1000", 32, 1000)):
         seed = 1234
@@ -187,6 +202,7 @@ def main() -> int:
     halo_fixture(ref)
     ctxops_fixture(ref)
     cylinder_fixture(ref)
+    brickworld_fixture()
     return 0
 
 
