@@ -38,7 +38,80 @@ struct CollideParams {
     int enable_buoyancy;
     int gravity_axis;       // axis the buoyant force points along (+): 0 x, 1 y, 2 z
     int zero_bits;          // always 0 (value-initialised): a run-time zero for collide27_exact_x2.cuh
+    // Game-runtime terms of the reference collide (jni.cpp:2256-2322,
+    // 2401-2411); all off in benchmark mode with the default flags.
+    int runtime_terms;          // any of them active: the kernels take one cell per thread
+    float fan_beta;             // 0.07 with fan forcing (kFanBeta), else 0
+    float fan_noise_amp;        // 0.02 (kFanNoiseAmp), 0 with DISABLE_FAN_NOISE
+    float fan_target_scale;     // 1 / (m/s per lattice velocity)
+    int sponge;                 // sponge toward rest in the 4 outer layers
+    float state_nudge;          // runtime mode 0.08: velocity nudge toward the packet state, 8 outer layers
+    int nx, ny, nz;             // brick of the call (edge distances)
+    unsigned long long step;    // the context's call counter (fan noise)
 };
+
+// Per-cell inputs of the runtime terms (filled by the caller when
+// CollideParams::runtime_terms is set).
+struct CellExtras {
+    float fan_mask, fan_x, fan_y, fan_z;  // packet fan channels (mask 0: no fan)
+    float noise;                          // fan_noise_amp * hash_signed_noise(cell, step)
+    float nudge;                          // state nudge factor of the cell
+    float ref_x, ref_y, ref_z;            // packet reference velocity
+};
+
+// hash_signed_noise (jni.cpp:1318-1328): splitmix-style 64-bit hash of
+// (cell, tick) to a float in [-1, 1].
+__host__ __device__ inline float signed_noise(unsigned long long cell, unsigned long long tick) {
+    unsigned long long x = cell * 0x9E3779B97F4A7C15ULL ^ tick * 0xD1B54A32D192ED03ULL;
+    x ^= x >> 30;
+    x *= 0xBF58476D1CE4E5B9ULL;
+    x ^= x >> 27;
+    x *= 0x94D049BB133111EBULL;
+    x ^= x >> 31;
+    const float u = (float)(x & 0x00FFFFFFULL) * (1.0f / 16777215.0f);
+    return 2.0f * u - 1.0f;
+}
+
+__device__ __forceinline__ int edge_distance(int x, int y, int z, int nx, int ny, int nz) {
+    return min(min(min(x, y), min(z, nx - 1 - x)), min(ny - 1 - y, nz - 1 - z));
+}
+// effective_runtime_state_nudge (jni.cpp:683-694): base (8 - d)^2 / 64 inside 8 layers
+__device__ __forceinline__ float state_nudge_at(const CollideParams& P, int d) {
+    if (P.state_nudge <= 0.0f || d >= 8) return 0.0f;
+    const float eta = (float)(8 - d) / 8.0f;
+    return P.state_nudge * eta * eta;
+}
+// effective_sponge_alpha (jni.cpp:787-794): 0.03 (4 - d)^2 / 16 inside 4 layers
+__device__ __forceinline__ float sponge_alpha_at(const CollideParams& P, int d) {
+    if (!P.sponge || d >= 4) return 0.0f;
+    const float eta = (float)(4 - d) / 4.0f;
+    return fminf(0.95f, fmaxf(0.0f, 0.03f * eta * eta));
+}
+
+// Fan force (jni.cpp:2256-2286): push toward the fan's target speed along its
+// direction, damp the perpendicular velocity, soften above 0.24.
+__device__ __forceinline__ void fan_force(const CellExtras& e, const CollideParams& P, float rs, float ux, float uy,
+                                          float uz, float& fx, float& fy, float& fz) {
+    const float speed_pre = sqrtf(ux * ux + uy * uy + uz * uz);
+    const float fan_norm = sqrtf(e.fan_x * e.fan_x + e.fan_y * e.fan_y + e.fan_z * e.fan_z);
+    if (!(fan_norm > 1e-8f)) return;
+    const float inv_norm = 1.0f / fan_norm;
+    const float noise = 1.0f + e.noise;
+    const float target = fminf(0.28f, fmaxf(0.0f, fan_norm * P.fan_target_scale * fmaxf(0.0f, noise)));
+    const float nx = e.fan_x * inv_norm, ny = e.fan_y * inv_norm, nz = e.fan_z * inv_norm;
+    const float u_para = ux * nx + uy * ny + uz * nz;
+    const float px = ux - u_para * nx, py = uy - u_para * ny, pz = uz - u_para * nz;
+    const float axial = fmaxf(0.0f, target - u_para);
+    float damp = 1.0f;
+    if (speed_pre > 0.24f) {
+        const float r = (speed_pre - 0.24f) / fmaxf(1e-4f, 0.04f);
+        damp = 1.0f / (1.0f + r * r);
+    }
+    const float beta = e.fan_mask * P.fan_beta * damp;
+    fx = beta * rs * (axial * nx - 1.0f * px);
+    fy = beta * rs * (axial * ny - 1.0f * py);
+    fz = beta * rs * (axial * nz - 1.0f * pz);
+}
 
 // Reference clamp constants (jni.cpp:118-132).
 constexpr float kNuShearMin = 1.0e-8f;
@@ -188,7 +261,8 @@ __device__ __forceinline__ void reseed_state(const ReseedSource& r, float max_sp
 // when unused). Returns false, leaving f untouched, when the input is not
 // finite: the caller then reseeds the cell (out of line, see reseed_state).
 __device__ __forceinline__ bool collide27(float (&f)[27], const CollideParams& P, const float* temperature,
-                                          float cfx, float cfy, float cfz, CollideOut& out) {
+                                          float cfx, float cfy, float cfz, CollideOut& out,
+                                          const CellExtras* ex = nullptr) {
     RawMoments m;
     raw_moments27<true>(f, m);
     const float rho = m.r000;
@@ -199,6 +273,7 @@ __device__ __forceinline__ bool collide27(float (&f)[27], const CollideParams& P
     float ux = m.r100 * ir, uy = m.r010 * ir, uz = m.r001 * ir;
 
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    if (ex && P.fan_beta > 0.0f && ex->fan_mask > 0.0f) fan_force(*ex, P, rs, ux, uy, uz, fx, fy, fz);
     if (P.enable_buoyancy) {
         const float add = rs * clampf_dev(P.buoy_beta * __ldg(temperature), -P.buoy_fmax, P.buoy_fmax);
         if (P.gravity_axis == 0) fx += add;
@@ -211,6 +286,12 @@ __device__ __forceinline__ bool collide27(float (&f)[27], const CollideParams& P
     ux += 0.5f * (fx * ir);
     uy += 0.5f * (fy * ir);
     uz += 0.5f * (fz * ir);
+    if (ex && P.state_nudge > 0.0f) {
+        const float sn = ex->nudge;
+        ux = (1.0f - sn) * ux + sn * ex->ref_x;
+        uy = (1.0f - sn) * uy + sn * ex->ref_y;
+        uz = (1.0f - sn) * uz + sn * ex->ref_z;
+    }
     const float s2 = ux * ux + uy * uy + uz * uz;
     if (!(isfinite(ux) && isfinite(uy) && isfinite(uz) && isfinite(s2))) return false;
     if (s2 > P.max_speed * P.max_speed) {

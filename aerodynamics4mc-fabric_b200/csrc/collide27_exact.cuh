@@ -75,7 +75,8 @@ struct ExactOut {
 // forcing, no edge nudge, no sponge). Returns false, with f untouched, when
 // the input is not finite; the caller reseeds the cell.
 __device__ __forceinline__ bool collide27_exact(float (&f)[27], const CollideParams& P, const float* temperature,
-                                                float cfx, float cfy, float cfz, CollideOut& out) {
+                                                float cfx, float cfy, float cfz, CollideOut& out,
+                                                const CellExtras* ex = nullptr) {
     bool bad = false;
 #pragma unroll
     for (int q = 0; q < 27; ++q) bad |= !isfinite(f[q]);
@@ -91,6 +92,7 @@ __device__ __forceinline__ bool collide27_exact(float (&f)[27], const CollidePar
     float uz = mom_z * inv_rho;
     if (!isfinite(rho_safe) || !isfinite(inv_rho) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz)) return false;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    if (ex && P.fan_beta > 0.0f && ex->fan_mask > 0.0f) fan_force(*ex, P, rho_safe, ux, uy, uz, fx, fy, fz);
     if (P.enable_buoyancy) {
         const float buoy = rclamp(P.buoy_beta * __ldg(temperature), -P.buoy_fmax, P.buoy_fmax);
         const float add = rho_safe * buoy;
@@ -110,6 +112,14 @@ __device__ __forceinline__ bool collide27_exact(float (&f)[27], const CollidePar
         ux += 0.5f * (fx * inv_rho);
         uy += 0.5f * (fy * inv_rho);
         uz += 0.5f * (fz * inv_rho);
+        if (!isfinite(ux) || !isfinite(uy) || !isfinite(uz)) return false;
+    }
+    if (ex && P.state_nudge > 0.0f) {
+        // runtime-mode state nudge (jni.cpp:2314-2322)
+        const float sn = ex->nudge;
+        ux = (1.0f - sn) * ux + sn * ex->ref_x;
+        uy = (1.0f - sn) * uy + sn * ex->ref_y;
+        uz = (1.0f - sn) * uz + sn * ex->ref_z;
         if (!isfinite(ux) || !isfinite(uy) || !isfinite(uz)) return false;
     }
     const float speed2 = ux * ux + uy * uy + uz * uz;

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
         fl[q] = S::load(f + (d * G.pcells + c), q, a.sc);
     }
     if (a.obstacle_cur[cell]) record_u(a.cur, cell, 0.0f, 0.0f, 0.0f);
-    if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
+    if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell, x, y, z)) {
         reseed_push<S>(f, a, cell, x, y, z, kParity);
         return;
     }
@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(128) transition_ip_kernel(typename S::T* __res
 #pragma unroll
     for (int q = 0; q < 27; ++q)
         fl[q] = a.solid_f ? a.solid_f[(long long)solid_slot(q, a.parity) * cells + cell] : q_w(q);
-    if (!collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
+    if (!collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell, x, y, z)) {
         reseed_push<S>(f, a, cell, x, y, z, a.parity);
         return;
     }
@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(128) init_ip_kernel(typename S::T* __restrict_
     float fl[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q) fl[q] = feq27(q, rho, ux, uy, uz);
-    if (!collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell)) {
+    if (!collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell, x, y, z)) {
         reseed_push<S>(f, a, cell, x, y, z, 0);
         return;
     }

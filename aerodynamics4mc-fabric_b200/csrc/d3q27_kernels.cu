@@ -77,6 +77,13 @@ __global__ void ingest_packet_kernel(const float* __restrict__ packet, int in_ch
     out.ref_uy[cell] = isfinite(vy) ? vy : 0.0f;
     out.ref_uz[cell] = isfinite(vz) ? vz : 0.0f;
     out.ref_p[cell] = clampf_dev(p[kChStateP], -0.03f, 0.03f);
+    if (out.fan_mask) {
+        // ingest_payload's fan channels (jni.cpp:1674-1678)
+        out.fan_mask[cell] = clampf_dev(p[1], 0.0f, 1.0f);
+        out.fan_ux[cell] = isfinite(p[2]) ? p[2] : 0.0f;
+        out.fan_uy[cell] = isfinite(p[3]) ? p[3] : 0.0f;
+        out.fan_uz[cell] = isfinite(p[4]) ? p[4] : 0.0f;
+    }
     const float t = in_ch > kChStateTemp ? p[kChStateTemp] : 0.0f;
     if (out.ref_temperature) {
         // transported temperature: the packet's field is the reference

@@ -73,6 +73,11 @@ struct CellFields {
     float* thermal_source = nullptr;
     float* u_last = nullptr;
     long long cells = 0;  // SoA stride of u_last
+    // Packet fan channels (mask clamped to [0, 1]; null: fan forcing off).
+    float* fan_mask = nullptr;
+    float* fan_ux = nullptr;
+    float* fan_uy = nullptr;
+    float* fan_uz = nullptr;
 };
 
 // Velocity a collision leaves for the next call's temperature advection.

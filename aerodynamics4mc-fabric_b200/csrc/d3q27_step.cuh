@@ -28,16 +28,42 @@ __device__ __forceinline__ int oob_face(int sx, int sy, int sz, int nx, int ny, 
 }
 
 // Collide one fluid cell; false = non-finite input, the caller reseeds.
+// (x, y, z): the cell's coordinates, for the runtime terms' edge layers.
 template <bool kExact>
 __device__ __forceinline__ bool collide_cell(float (&f)[27], const CollideParams& cp, const CellFields& cur,
-                                             const ForceField& force, long long cell) {
+                                             const ForceField& force, long long cell, int x, int y, int z) {
     CollideOut o;
     const float cfx = force.fx ? force.fx[cell] : 0.0f;
     const float cfy = force.fy ? force.fy[cell] : 0.0f;
     const float cfz = force.fz ? force.fz[cell] : 0.0f;
-    const bool ok = kExact ? exact::collide27_exact(f, cp, cur.temperature + cell, cfx, cfy, cfz, o)
-                           : collide27(f, cp, cur.temperature + cell, cfx, cfy, cfz, o);
+    CellExtras ex;
+    const CellExtras* exp = nullptr;
+    int d = 0;
+    if (cp.runtime_terms) {
+        d = edge_distance(x, y, z, cp.nx, cp.ny, cp.nz);
+        ex.fan_mask = cur.fan_mask ? cur.fan_mask[cell] : 0.0f;
+        ex.fan_x = cur.fan_mask ? cur.fan_ux[cell] : 0.0f;
+        ex.fan_y = cur.fan_mask ? cur.fan_uy[cell] : 0.0f;
+        ex.fan_z = cur.fan_mask ? cur.fan_uz[cell] : 0.0f;
+        ex.noise = cp.fan_noise_amp * signed_noise((unsigned long long)cell, cp.step);
+        ex.nudge = state_nudge_at(cp, d);
+        ex.ref_x = cur.ref_ux[cell];
+        ex.ref_y = cur.ref_uy[cell];
+        ex.ref_z = cur.ref_uz[cell];
+        exp = &ex;
+    }
+    const bool ok = kExact ? exact::collide27_exact(f, cp, cur.temperature + cell, cfx, cfy, cfz, o, exp)
+                           : collide27(f, cp, cur.temperature + cell, cfx, cfy, cfz, o, exp);
     if (ok) record_u(cur, cell, o.ux, o.uy, o.uz);
+    if (ok && cp.runtime_terms) {
+        const float alpha = sponge_alpha_at(cp, d);
+        if (alpha > 0.0f) {
+            // sponge toward the rest state (jni.cpp:2401-2411)
+            const float keep = 1.0f - alpha;
+#pragma unroll
+            for (int q = 0; q < 27; ++q) f[q] = keep * f[q] + alpha * feq27(q, 1.0f, 0.0f, 0.0f, 0.0f);
+        }
+    }
     return ok;
 }
 
@@ -188,7 +214,9 @@ __global__ void __launch_bounds__(128) init_collide_kernel(int nx, int ny, int n
 #pragma unroll
     for (int q = 0; q < 27; ++q) f[q] = feq27(q, rho, ux, uy, uz);
     if (solid) record_u(cur, cell, 0.0f, 0.0f, 0.0f);
-    if (!solid && !collide_cell<kExact>(f, cp, cur, force, cell)) {
+    int x, y, z;
+    cell_xyz32(cell, ny, nz, x, y, z);
+    if (!solid && !collide_cell<kExact>(f, cp, cur, force, cell, x, y, z)) {
         reseed_store_ab(g_out, cells, cell, cur, cp.max_speed);
         return;
     }
@@ -224,7 +252,7 @@ __global__ void __launch_bounds__(128) step_ab_kernel(int nx, int ny, int nz, co
     const PullView v{g_in, obstacle_prev, ref_p_prev, F, cells, nx, ny, nz};
     pull27(v, flags_prev[cell], cell, x, y, z, f);
     if (cur.obstacle[cell]) record_u(cur, cell, 0.0f, 0.0f, 0.0f);
-    if (!cur.obstacle[cell] && !collide_cell<kExact>(f, cp, cur, force, cell)) {
+    if (!cur.obstacle[cell] && !collide_cell<kExact>(f, cp, cur, force, cell, x, y, z)) {
         reseed_store_ab(g_out, cells, cell, cur, cp.max_speed);
         return;
     }
@@ -263,7 +291,9 @@ __global__ void __launch_bounds__(128) collide_ab_kernel(int nx, int ny, int nz,
     float f[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q) f[q] = f_io[(long long)q * cells + cell];
-    if (!collide_cell<kExact>(f, cp, cur, force, cell)) {
+    int x, y, z;
+    cell_xyz32(cell, ny, nz, x, y, z);
+    if (!collide_cell<kExact>(f, cp, cur, force, cell, x, y, z)) {
         reseed_store_ab(f_io, cells, cell, cur, cp.max_speed);
         return;
     }

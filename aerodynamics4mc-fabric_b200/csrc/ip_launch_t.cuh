@@ -30,10 +30,12 @@ struct IpLaunch {
             if (e != cudaSuccess) return e;
         }
         step_timer_begin(s);
-        if (!kExact && a.cells_per_thread == 2 && a.streamed && IpaLaunch<S>::eligible(a)) {
+        // the runtime terms (fans, state nudge, sponge) exist in the one-cell kernel only
+        const int cpt = a.cp.runtime_terms ? 1 : a.cells_per_thread;
+        if (!kExact && cpt == 2 && a.streamed && IpaLaunch<S>::eligible(a)) {
             cudaError_t e = IpaLaunch<S>::step(f, a, s);
             if (e != cudaSuccess) return e;
-        } else if (a.cells_per_thread == 2) {
+        } else if (cpt == 2) {
             const int lb = line_block((a.g.nz + 1) / 2);
             if (a.parity == 0) step_ip2_kernel<S, kExact, 0><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
             else step_ip2_kernel<S, kExact, 1><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);

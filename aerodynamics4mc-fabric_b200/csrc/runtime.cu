@@ -356,6 +356,15 @@ CollideParams current_collide_params() {
     p.enable_sgs = !bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_SGS);
     p.enable_buoyancy = !bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_BUOYANCY);
     p.gravity_axis = g_gravity_axis >= 0 ? g_gravity_axis : 1;
+    // game-runtime terms (effective_enable_fan_forcing / _fan_noise_amp /
+    // _sponge_alpha / _runtime_state_nudge, jni.cpp:676-822): on outside
+    // benchmark mode, and in benchmark mode when their DISABLE flag is clear
+    p.fan_beta = bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_FAN_FORCING) ? 0.0f : 0.07f;
+    p.fan_noise_amp = bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_FAN_NOISE) ? 0.0f : 0.02f;
+    p.fan_target_scale = 1.0f / (1.0f / (1.0f / 20.0f));
+    p.sponge = bench_flag(AERO_LBM_BENCHMARK_FLAG_DISABLE_SPONGE) ? 0 : 1;
+    p.state_nudge = bench_active() ? 0.0f : 0.08f;
+    p.runtime_terms = (p.fan_beta > 0.0f || p.sponge || p.state_nudge > 0.0f) ? 1 : 0;
     return p;
 }
 
@@ -427,6 +436,7 @@ void Context::release_device() {
     f_ready = false;
     fr(ip);
     fr(reinterpret_cast<void*&>(solid_f));
+    fr(reinterpret_cast<void*&>(fan_mask));
     fr(scratch);
     scratch_cap = 0;
     packet_cap = out_cap = 0;
@@ -472,6 +482,12 @@ bool Context::allocate(int nx_, int ny_, int nz_) {
 
 CellFields Context::fields(int s) const {
     CellFields c{obstacle[s], ref_ux, ref_uy, ref_uz, ref_p[s], temperature};
+    if (fan_mask) {
+        c.fan_mask = fan_mask;
+        c.fan_ux = fan_mask + cells;
+        c.fan_uy = fan_mask + 2 * cells;
+        c.fan_uz = fan_mask + 3 * cells;
+    }
     if (thermal) {
         c.ref_temperature = ref_temperature;
         c.thermal_source = thermal_source;
@@ -675,7 +691,19 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     cudaStream_t s = current_stream();
     const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
     const FaceParams face_now = current_face_params();
-    const CollideParams cp = current_collide_params();
+    CollideParams cp = current_collide_params();
+    cp.nx = ctx.nx;
+    cp.ny = ctx.ny;
+    cp.nz = ctx.nz;
+    cp.step = ctx.step_counter;
+    if (cp.fan_beta > 0.0f && !ctx.fan_mask) {
+        // packet fan channels, kept from the ingest for the collision
+        if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.fan_mask), (size_t)ctx.cells * 4 * sizeof(float)),
+                     "cudaMalloc(fans)") ||
+            !cuda_ok(cudaMemsetAsync(ctx.fan_mask, 0, (size_t)ctx.cells * 4 * sizeof(float), current_stream()),
+                     "cudaMemset(fans)"))
+            return false;
+    }
     // The reference updates the temperature before every collision
     // (run_cpu_step, jni.cpp:8480-8507); it reaches the flow through the
     // buoyancy force.

@@ -53,7 +53,8 @@ struct Context {
     int layout = 0;
     int ip_variant = 0;      // IpVariant when layout == 1
     void* ip = nullptr;      // padded population array (float or __half)
-    float* solid_f = nullptr;  // in-place: populations of solid cells (IpArgs::solid_f), from the first mask change on
+    float* solid_f = nullptr;
+    float* fan_mask = nullptr;  // packet fan channels, 4 x cells (mask, ux, uy, uz), while fan forcing is on  // in-place: populations of solid cells (IpArgs::solid_f), from the first mask change on
     int parity = 0;          // slot-map parity of the next in-place step
     int periodic_mask = 0;   // axes wrapped by the in-place layout
     float fp16_scale = 0.0f; // per-brick FP16 deviation scale

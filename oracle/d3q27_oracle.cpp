@@ -14,7 +14,8 @@
 //   bounce/boundary values  native/src/aero_lbm_jni.cpp:1475-1602
 //   payload ingest          native/src/aero_lbm_jni.cpp:1671-1694
 //   initialisation          native/src/aero_lbm_jni.cpp:1752-1781
-//   collide                 native/src/aero_lbm_jni.cpp:2209-2413
+//   collide                 native/src/aero_lbm_jni.cpp:2209-2413 (fan forcing,
+//                           state nudge and sponge: 676-694, 787-822, 1318-1328)
 //   stream_and_bounce       native/src/aero_lbm_jni.cpp:2415-2452
 //   write_output            native/src/aero_lbm_jni.cpp:2535-2581
 //   strided atlas extract   native/src/aero_lbm_jni.cpp:9246-9450
@@ -97,6 +98,10 @@ typedef struct OracleD3Q27Params {
     int packet_has_temperature;    // 1: the packet carries the temperature channel (>= 11 channels)
     int thermal_bfecc;             // 1: the BFECC branch (heated-cavity presets), 0: first-order
     int cylinder_force;            // 1: the cylinder preset's momentum-exchange force after each collision
+    int fan_forcing;               // 1: fan force from the packet's fan channels (runtime mode, or benchmark flag clear)
+    double fan_noise_amp;          // fan target noise amplitude (0.02; 0 with DISABLE_FAN_NOISE)
+    int sponge;                    // 1: post-collision sponge toward rest in the 4 outer layers
+    double state_nudge;            // runtime mode: 0.08 (velocity nudge toward the packet state, 8 outer layers)
 } OracleD3Q27Params;
 
 }  // extern "C"
@@ -129,6 +134,7 @@ inline T clampv(T v, T lo, T hi) { return std::min(hi, std::max(lo, v)); }
 template <typename T>
 struct D3Q27Oracle {
     using Arr = std::array<T, 27>;
+    using value_type_t = T;
     Lattice<T> L;
     int nx = 0, ny = 0, nz = 0;
     size_t cells = 0;
@@ -147,6 +153,7 @@ struct D3Q27Oracle {
     std::vector<T> temperature_next, ref_temperature, thermal_source, temperature_scratch;
     std::vector<T> force_x, force_y, force_z;  // optional per-cell force density
     std::vector<uint8_t> obstacle;
+    std::vector<T> fan_mask, fan_ux, fan_uy, fan_uz;  // packet fan channels (empty: none)
     bool initialized = false;
     uint64_t steps_done = 0;
 
@@ -557,6 +564,39 @@ struct D3Q27Oracle {
     }
 
     // ---- collide (native/src/aero_lbm_jni.cpp:2209-2413, benchmark mode: no fan, nudge or sponge)
+    // hash_signed_noise (jni.cpp:1318-1328)
+    static float signed_noise(uint64_t cell, uint64_t tick) {
+        uint64_t x = cell * 0x9E3779B97F4A7C15ULL ^ tick * 0xD1B54A32D192ED03ULL;
+        x ^= x >> 30;
+        x *= 0xBF58476D1CE4E5B9ULL;
+        x ^= x >> 27;
+        x *= 0x94D049BB133111EBULL;
+        x ^= x >> 31;
+        const float u = float(x & 0x00FFFFFFULL) * (1.0f / 16777215.0f);
+        return 2.0f * u - 1.0f;
+    }
+    int edge_distance(size_t cell) const {
+        const int x = int(cell / (size_t(ny) * nz)), y = int((cell / nz) % ny), z = int(cell % nz);
+        return std::min({x, y, z, nx - 1 - x, ny - 1 - y, nz - 1 - z});
+    }
+    // effective_runtime_state_nudge (jni.cpp:683-694)
+    T state_nudge_at(size_t cell) const {
+        const float base = float(p.state_nudge);
+        if (base <= 0.0f) return T(0);
+        const int d = edge_distance(cell);
+        if (d >= 8) return T(0);
+        const float eta = float(8 - d) / float(8);
+        return T(base * eta * eta);
+    }
+    // effective_sponge_alpha (jni.cpp:787-794)
+    T sponge_at(size_t cell) const {
+        if (!p.sponge) return T(0);
+        const int d = edge_distance(cell);
+        if (d >= 4) return T(0);
+        const float eta = float(4 - d) / float(4);
+        return T(std::min(0.95f, std::max(0.0f, 0.03f * eta * eta)));
+    }
+
     void collide() {
         const T ms = T(p.max_speed);
         const T tau_s_base = T(p.tau_shear), tau_n_base = T(p.tau_normal);
@@ -591,6 +631,32 @@ struct D3Q27Oracle {
                 continue;
             }
             T fx = T(0), fy = T(0), fz = T(0);
+            if (p.fan_forcing && !fan_mask.empty() && fan_mask[cell] > T(0)) {
+                // fan forcing (jni.cpp:2256-2286) with the reference's constants
+                const T speed_pre = std::sqrt(vx * vx + vy * vy + vz * vz);
+                const T fnx = fan_ux[cell], fny = fan_uy[cell], fnz = fan_uz[cell];
+                const T fan_norm = std::sqrt(fnx * fnx + fny * fny + fnz * fnz);
+                if (fan_norm > T(1e-8f)) {
+                    const T inv_norm = T(1.0f) / fan_norm;
+                    const T noise = T(1.0f) + T(float(p.fan_noise_amp)) * T(signed_noise(cell, steps_done));
+                    const float velocity_scale = 1.0f / (1.0f / 20.0f);
+                    const T target_scale = T(1.0f / velocity_scale);
+                    const T target = clampv(fan_norm * target_scale * std::max(T(0.0f), noise), T(0.0f), T(0.28f));
+                    const T ex = fnx * inv_norm, ey = fny * inv_norm, ez = fnz * inv_norm;
+                    const T u_para = vx * ex + vy * ey + vz * ez;
+                    const T px = vx - u_para * ex, py = vy - u_para * ey, pz = vz - u_para * ez;
+                    const T axial = std::max(T(0.0f), target - u_para);
+                    T damp = T(1.0f);
+                    if (speed_pre > T(0.24f)) {
+                        const T rr = (speed_pre - T(0.24f)) / std::max(T(1e-4f), T(0.04f));
+                        damp = T(1.0f) / (T(1.0f) + rr * rr);
+                    }
+                    const T beta = fan_mask[cell] * T(0.07f) * damp;
+                    fx = beta * rs * (axial * ex - T(1.0f) * px);
+                    fy = beta * rs * (axial * ey - T(1.0f) * py);
+                    fz = beta * rs * (axial * ez - T(1.0f) * pz);
+                }
+            }
             if (p.enable_buoyancy) {
                 const T b = clampv(T(p.buoyancy_beta) * temperature[cell], -T(p.buoyancy_force_max), T(p.buoyancy_force_max));
                 const T add = rs * b;
@@ -609,6 +675,14 @@ struct D3Q27Oracle {
             vx += T(0.5) * dux;
             vy += T(0.5) * duy;
             vz += T(0.5) * duz;
+            if (p.state_nudge > 0.0) {
+                // effective_runtime_state_nudge toward the packet state (jni.cpp:2314-2322)
+                const T sn = state_nudge_at(cell);
+                vx = (T(1.0f) - sn) * vx + sn * ref_ux[cell];
+                vy = (T(1.0f) - sn) * vy + sn * ref_uy[cell];
+                vz = (T(1.0f) - sn) * vz + sn * ref_uz[cell];
+                if (!std::isfinite(vx) || !std::isfinite(vy) || !std::isfinite(vz)) { reseed(cell); continue; }
+            }
             const T s2 = vx * vx + vy * vy + vz * vz;
             if (!std::isfinite(s2)) { reseed(cell); continue; }
             if (s2 > ms * ms) {
@@ -663,6 +737,15 @@ struct D3Q27Oracle {
             const T uxc = mxc / rcs, uyc = myc / rcs, uzc = mzc / rcs;
             for (int q = 0; q < 27; ++q) fc[q] += feq(q, rs, vx, vy, vz) - feq(q, rcs, uxc, uyc, uzc);
             for (int q = 0; q < 27; ++q) f_post[di(cell, q)] = fc[q] + guo(q, vx, vy, vz, fx, fy, fz, om_o);
+            const T alpha = sponge_at(cell);
+            if (alpha > T(0)) {
+                // sponge toward the rest state (jni.cpp:2401-2411)
+                const T keep = T(1.0f) - alpha;
+                for (int q = 0; q < 27; ++q) {
+                    T& fr = f_post[di(cell, q)];
+                    fr = keep * fr + alpha * feq(q, T(1.0f), T(0.0f), T(0.0f), T(0.0f));
+                }
+            }
         }
     }
 
@@ -1149,6 +1232,29 @@ int oracle_d3q27_shift(void* handle, int dx, int dy, int dz) {
     auto* h = static_cast<Handle*>(handle);
     if (!h) return 0;
     return (h->f32 ? h->f32->shift(dx, dy, dz) : h->f64->shift(dx, dy, dz)) ? 1 : 0;
+}
+
+// The packet's fan channels (ingest_payload, jni.cpp:1674-1678): mask clamped
+// to [0, 1], velocities with non-finite values as 0; null clears them.
+int oracle_d3q27_set_fans(void* handle, const float* mask, const float* vx, const float* vy, const float* vz) {
+    auto* h = static_cast<Handle*>(handle);
+    if (!h) return 0;
+    auto load = [&](auto& o) {
+        using T = typename std::decay_t<decltype(o)>::value_type_t;
+        if (!mask || !vx || !vy || !vz) {
+            o.fan_mask.clear(); o.fan_ux.clear(); o.fan_uy.clear(); o.fan_uz.clear();
+            return;
+        }
+        o.fan_mask.resize(o.cells); o.fan_ux.resize(o.cells); o.fan_uy.resize(o.cells); o.fan_uz.resize(o.cells);
+        auto fin = [](float v) { return std::isfinite(v) ? v : 0.0f; };
+        for (size_t c = 0; c < o.cells; ++c) {
+            o.fan_mask[c] = T(std::min(1.0f, std::max(0.0f, mask[c])));
+            o.fan_ux[c] = T(fin(vx[c])); o.fan_uy[c] = T(fin(vy[c])); o.fan_uz[c] = T(fin(vz[c]));
+        }
+    };
+    if (h->f32) load(*h->f32);
+    else load(*h->f64);
+    return 1;
 }
 
 int oracle_d3q27_patch_cells(void* handle, const int* cells, const uint8_t* solid, int count) {

@@ -36,6 +36,7 @@ INHERIT_GAME = 0
 THERMAL_INHERIT, THERMAL_DISABLED, THERMAL_PERIODIC, THERMAL_ADIABATIC, THERMAL_DIRICHLET, THERMAL_NEUMANN = 0, 1, 2, 3, 4, 5
 PRESET_HEATED_CAVITY_2D, PRESET_HEATED_CAVITY_3D = 5, 6  # native/include/aero_lbm_capi.h:41-42
 PRESET_CYLINDER_2D = 4  # native/include/aero_lbm_capi.h:40
+FLAG_DISABLE_FAN_FORCING, FLAG_DISABLE_FAN_NOISE, FLAG_DISABLE_SPONGE = 1 << 0, 1 << 1, 1 << 2
 FLAG_DISABLE_CONVECTIVE_OUTFLOW = 1 << 3
 FLAG_DISABLE_SGS = 1 << 5
 FLAG_DISABLE_BUOYANCY = 1 << 7
@@ -84,6 +85,10 @@ class OracleParams(ctypes.Structure):
         ("packet_has_temperature", ctypes.c_int),
         ("thermal_bfecc", ctypes.c_int),
         ("cylinder_force", ctypes.c_int),
+        ("fan_forcing", ctypes.c_int),
+        ("fan_noise_amp", ctypes.c_double),
+        ("sponge", ctypes.c_int),
+        ("state_nudge", ctypes.c_double),
     ]
 
 
@@ -181,6 +186,12 @@ def derive_params(cfg: dict) -> OracleParams:
     p.internal_thermal_source = 1 if cfg.get("thermal_source", False) else 0
     p.packet_has_temperature = 1 if int(cfg.get("packet_channels", 11)) > 10 else 0
     p.cylinder_force = 1 if int(cfg.get("preset", 0)) == PRESET_CYLINDER_2D else 0
+    # fan forcing, fan noise and the sponge: off unless the config clears their
+    # DISABLE flags (the default config sets them)
+    p.fan_forcing = 1 if cfg.get("fans", False) else 0
+    p.fan_noise_amp = float(f32(0.02)) if (cfg.get("fans", False) and cfg.get("fan_noise", False)) else 0.0
+    p.sponge = 1 if cfg.get("sponge", False) else 0
+    p.state_nudge = 0.0
     return p
 
 
@@ -216,6 +227,7 @@ class Oracle:
             lib.oracle_d3q27_last_force.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.oracle_d3q27_get_obstacle.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.oracle_d3q27_patch_cells.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+            lib.oracle_d3q27_set_fans.argtypes = [ctypes.c_void_p] * 5
             lib.oracle_d3q27_set_shell.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 3 + [ctypes.c_float]
             cls._lib = lib
         return cls._lib
@@ -267,6 +279,12 @@ class Oracle:
 
     def shift(self, dx: int, dy: int, dz: int) -> bool:
         return bool(self.lib().oracle_d3q27_shift(self.h, int(dx), int(dy), int(dz)))
+
+    def set_fans(self, mask, vx, vy, vz):
+        arrs = [self._p(v, np.float32) for v in (mask, vx, vy, vz)]
+        self._keep_fans = [a for a, _ in arrs]
+        if not self.lib().oracle_d3q27_set_fans(self.h, *[p for _, p in arrs]):
+            raise RuntimeError("oracle set_fans failed")
 
     def patch_cells(self, cells, solid):
         c = np.ascontiguousarray(np.asarray(cells, np.int32).reshape(-1))
@@ -367,6 +385,10 @@ def config_struct(struct_type, cfg: dict, default_fn):
         flags &= ~(1 << 6)
     if cfg.get("disable_convective", False):
         flags |= FLAG_DISABLE_CONVECTIVE_OUTFLOW
+    for key, bit in (("fans", FLAG_DISABLE_FAN_FORCING), ("fan_noise", FLAG_DISABLE_FAN_NOISE),
+                     ("sponge", FLAG_DISABLE_SPONGE)):
+        if key in cfg:
+            flags = (flags & ~bit) if cfg[key] else (flags | bit)
     c.flags = flags
     c.reynolds_number = cfg.get("reynolds", 100.0)
     c.initial_temperature = cfg.get("initial_temperature", 0.0)
@@ -574,6 +596,8 @@ def run_script_oracle(o: "Oracle", cfg: dict, packet: np.ndarray, script):
             if transport:
                 o.set_thermal_source(pk[:, 9] if (pk.shape[1] > 9 and cfg.get("thermal_source", False))
                                      else np.zeros(pk.shape[0], np.float32))
+            if cfg.get("fans", False):
+                o.set_fans(pk[:, 1], pk[:, 2], pk[:, 3], pk[:, 4])
             ov = act[1] if len(act) > 1 else None
             if ov is not None:
                 o.apply_overlays(ov[0], ov[1])
@@ -627,6 +651,7 @@ def context_ops_script(n: int, seed: int = 23):
 
 
 CYLINDER_SCRIPT = [("step",), ("force",)] * 5 + [("flow",)]
+FAN_SCRIPT = [("step",)] * 6 + [("flow",), ("temp",)] + [("step",)] * 6 + [("flow",)]
 
 
 def feq_rest(q: int) -> float:
@@ -679,6 +704,22 @@ def edits_script(n: int, seed: int = 43):
                                ("shell", flow, 0b010011, 3, 0.3), ("step",), ("step",), ("flow",),
                                ("patch",) + p2, ("patch",) + p3, ("cached",), ("flow",), ("temp",),
                                ("shell", flow, 0, 3, 0.3), ("step",), ("flow",), ("temp",)])
+
+
+def fan_case(n: int = 12, seed: int = 61, noise: bool = True, sponge: bool = True):
+    """The thermal case with the fan forcing, fan noise and sponge of the
+    reference's collide switched on (their DISABLE flags cleared): 3 % of the
+    fluid cells carry a fan (mask U(0.3, 1), direction and speed up to 3 m/s,
+    so the target exceeds the soft cap in places)."""
+    obst, u, temp, src, cfg, pre = thermal_case(n, seed)
+    rng = np.random.default_rng(seed + 1)
+    dims = (n, n, n)
+    fan = (rng.random(dims) < 0.03) & (obst == 0)
+    mask = np.where(fan, rng.uniform(0.3, 1.0, dims), 0.0).astype(np.float32)
+    fv = [np.where(fan, rng.uniform(-3.0, 3.0, dims), 0.0).astype(np.float32) for _ in range(3)]
+    cfg = dict(cfg, fans=True, fan_noise=noise, sponge=sponge)
+    pk = packet_from(obst, *u, temperature=temp, source=src, fans=(mask, *fv))
+    return cfg, pk, pre
 
 
 def cylinder_case(nx: int = 44, ny: int = 20, nz: int = 3, sgs: bool = True):
@@ -849,7 +890,8 @@ def c1_config(tau: float = 0.55, u0: float = 0.05, sgs: bool = True) -> dict:
     }
 
 
-def packet_from(obstacle, ux, uy, uz, pressure=None, temperature=None, channels: int = 11, source=None) -> np.ndarray:
+def packet_from(obstacle, ux, uy, uz, pressure=None, temperature=None, channels: int = 11, source=None,
+                fans=None) -> np.ndarray:
     cells = obstacle.size
     pk = np.zeros((cells, channels), dtype=np.float32)
     pk[:, 0] = (obstacle.reshape(-1) != 0)
@@ -862,6 +904,9 @@ def packet_from(obstacle, ux, uy, uz, pressure=None, temperature=None, channels:
         pk[:, 10] = np.asarray(temperature, np.float32).reshape(-1)
     if source is not None and channels > 9:
         pk[:, 9] = np.asarray(source, np.float32).reshape(-1)
+    if fans is not None:  # (mask, vx, vy, vz): channels 1-4
+        for c, v in enumerate(fans):
+            pk[:, 1 + c] = np.asarray(v, np.float32).reshape(-1)
     return pk
 
 

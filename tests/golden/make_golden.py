@@ -39,6 +39,9 @@ Fixtures:
                   bridge over its CPU step, oracle.BrickService) on
                   oracle.brick_world_case(): four 16^3 bricks, 6 ticks in the
                   classic solver mode; packed atlases, dynamic bricks, status.
+  fans_12_12.npz  the fan forcing, fan noise and sponge of the reference's
+                  collide switched on in benchmark mode (oracle.fan_case(12,
+                  seed 61)): flow and temperature after 6 calls, flow after 12.
   thermal_12_20.npz buoyancy on with the reference's temperature transport:
                   oracle.thermal_case(12, seed 11) (every thermal face kind,
                   packet source channel, state preloaded), 20 steps; the
@@ -158,6 +161,13 @@ def brickworld_fixture() -> None:
     print("brickworld_16x4_6 written")
 
 
+def fans_fixture(ref) -> None:
+    cfg, pk, pre = O.fan_case(12, 61)
+    res = ref.run_script((12, 12, 12), cfg, pk, O.FAN_SCRIPT, temperature_state=pre)
+    save_results(OUT / "fans_12_12.npz", res, input_sha256=digest(pk, pre))
+    print("fans_12_12 written")
+
+
 def main() -> int:
     O.build(ref=True)
     ref = O.RefLib()
@@ -175,6 +185,8 @@ def main() -> int:
             cylinder_fixture(ref)
         if only in "brickworld_16x4_6":
             brickworld_fixture()
+        if only in "fans_12_12":
+            fans_fixture(ref)
         return 0
     for name, n, steps in (("c1_16_200", 16, 200), ("c1_32_1000", 32, 1000)):
         seed = 1234
@@ -203,6 +215,7 @@ def main() -> int:
     ctxops_fixture(ref)
     cylinder_fixture(ref)
     brickworld_fixture()
+    fans_fixture(ref)
     return 0
 
 

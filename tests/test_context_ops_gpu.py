@@ -277,3 +277,30 @@ def test_block_edits_and_shell_argument_checks(gpu):
             assert gpu.aero_lbm_clear_d3q27_f16_boundary_shell_rect(99999) == 1
         finally:
             ctx.release()
+
+
+@pytest.mark.parametrize("streaming,cpt", [(1, 1), (2, 1), (2, 2)])
+def test_fans_and_sponge_match_reference_golden(gpu, streaming, cpt):
+    """Fan forcing with noise and the sponge (their DISABLE flags cleared), in
+    both layouts; the runtime terms take the one-cell kernels whatever the
+    launch-shape setting. Bit-identical to fixture fans_12_12.npz."""
+    cfg, pk, pre = O.fan_case(12, 61)
+    res = run_script_gpu(gpu, (12, 12, 12), cfg, pk, O.FAN_SCRIPT, key=880 + 2 * streaming + cpt, streaming=streaming,
+                         cpt=cpt, temperature_state=pre)
+    flags = O.results_equal(res, O.load_results(GOLDEN / "fans_12_12.npz"))
+    assert all(flags), flags
+
+
+def test_fans_and_sponge_fp16_against_fp64(gpu):
+    cfg, pk, pre = O.fan_case(12, 61)
+    res = run_script_gpu(gpu, (12, 12, 12), cfg, pk, O.FAN_SCRIPT, key=890, streaming=2, solver_mode=3,
+                         temperature_state=pre)
+    o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f64")
+    o.set_temperature(pre)
+    ref = O.run_script_oracle(o, cfg, pk, O.FAN_SCRIPT)
+    for kind, a, b in zip(("flow", "temp", "flow"), res, ref):
+        if kind == "flow":
+            e = O.flow_errors(a, b)
+            assert e["u"] <= 1e-3 and e["rho"] <= 1e-4, e
+        else:
+            assert float(np.max(np.abs(a - b))) <= 1e-3

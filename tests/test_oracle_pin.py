@@ -287,3 +287,25 @@ def test_oracle_block_edits_and_shell_behaviour():
     gain = [float(np.mean((uy_shell - uy_plain)[x][fluid[x]])) for x in range(4)]
     assert gain[0] > gain[1] > gain[2] > 0.0 and gain[0] > 1e-3, gain
     assert _bits_equal(cleared[0], plain[0])
+
+
+def test_oracle_fans_and_sponge_match_golden():
+    """Fan forcing (with noise) and the sponge of the reference's collide,
+    bit for bit against fixture fans_12_12.npz."""
+    cfg, pk, pre = O.fan_case(12, 61)
+    o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    res = O.run_script_oracle(o, cfg, pk, O.FAN_SCRIPT)
+    assert all(O.results_equal(res, O.load_results(GOLDEN / "fans_12_12.npz")))
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("noise,sponge,seed", [(True, True, 62), (False, True, 63), (True, False, 64)])
+def test_oracle_fans_and_sponge_match_reference_live(noise, sponge, seed):
+    cfg, pk, pre = O.fan_case(12, seed, noise, sponge)
+    script = [("step",)] * 5 + [("flow",), ("temp",)]
+    o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    res = O.run_script_oracle(o, cfg, pk, script)
+    ref = O.RefLib().run_script((12, 12, 12), cfg, pk, script, temperature_state=pre)
+    assert all(O.results_equal(res, ref))
