@@ -1,4 +1,6 @@
 // Per-context operations between or around steps (see context_ops.cuh).
+// Built with --fmad=false: the shifted pull evaluates the face rules
+// operation by operation, like the reference-order step kernel.
 // Each is one or two small launches on the caller's stream; none is on the
 // per-step path except the overlays (a sparse scatter after the ingest) and
 // the cylinder force (one read pass, only under that benchmark preset).

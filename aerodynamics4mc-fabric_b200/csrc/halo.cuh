@@ -1,4 +1,4 @@
-// Halo exchange between overlapping bricks (see halo.cu).
+// Halo exchange between overlapping bricks (see halo_exact.cu).
 #pragma once
 
 #include <cuda_runtime.h>

@@ -18,7 +18,9 @@
 // rest equilibrium while that store does not exist yet), and the exchange
 // reads and writes them there. Two-buffer contexts materialise f
 // (the pull of their post-collision state) into the spare buffer first; the
-// next call then collides f directly.
+// next call then collides f directly. Built with --fmad=false: that pull
+// evaluates the face rules (convective outflow, equilibria) operation by
+// operation, as the step kernel of the reference-order collision does.
 #include "halo.cuh"
 
 #include <algorithm>

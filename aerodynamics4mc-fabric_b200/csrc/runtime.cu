@@ -680,6 +680,8 @@ static ThermalFaces current_thermal_faces() {
     return t;
 }
 static float thermal_diffusivity() {
+    // runtime_molecular_alpha0 (jni.cpp:931-933): air's diffusivity nu / Pr in lattice units
+    if (!bench_active()) return std::max(1.0e-8f, (1.50e-5f / 0.71f) * (1.0f / 20.0f) / (1.0f * 1.0f));
     if (!heated_cavity()) return kThermalDiffusivity;
     const float pr = std::max(1.0e-6f, finite_or(g_bench.prandtl_number, 0.71f));
     return base_nu_shear() / pr;
@@ -775,7 +777,13 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             const ThermalInitArgs ti{ctx.cells, ctx.temperature, ctx.u_last, ctx.obstacle[new_slot], ctx.ref_temperature,
                                      ctx.ref_ux, ctx.ref_uy, ctx.ref_uz, g_bench.initial_temperature, bench_active() ? 1 : 0};
             if (!cuda_ok(launch_thermal_init(ti, s), "thermal_init")) return false;
+        } else if (!bench_active() && in_ch > 10) {
+            const ThermalNudgeArgs tn{ctx.nx, ctx.ny, ctx.nz, ctx.temperature, ctx.obstacle[new_slot], ctx.ref_temperature,
+                                      cp.state_nudge};
+            if (!cuda_ok(launch_thermal_reference_nudge(tn, s), "thermal_reference")) return false;
         }
+        // should_update_temperature (jni.cpp:2191-2196): every other call in runtime mode
+        const bool update = bench_active() || ctx.step_counter % 2 == 0;
         ThermalArgs ta{};
         ta.nx = ctx.nx; ta.ny = ctx.ny; ta.nz = ctx.nz; ta.cells = ctx.cells;
         ta.t = ctx.temperature;
@@ -791,8 +799,14 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         // nudges or fans either)
         ta.bfecc = (!bench_active() || heated_cavity()) ? 1 : 0;
         ta.scratch = ctx.temperature_scratch;
-        if (!cuda_ok(launch_thermal_update(ta, s), "thermal_update")) return false;
-        std::swap(ctx.temperature, ta.bfecc ? ctx.temperature_scratch : ctx.temperature_next);
+        ta.dt = bench_active() ? 1.0f : 2.0f;
+        ta.turbulent = (!bench_active() && cp.enable_sgs) ? 1 : 0;
+        ta.sgs_c2 = cp.sgs_c2;
+        ta.nu0 = clamp_nu(kRuntimeMolecularNu0);
+        if (update) {
+            if (!cuda_ok(launch_thermal_update(ta, s), "thermal_update")) return false;
+            std::swap(ctx.temperature, ta.bfecc ? ctx.temperature_scratch : ctx.temperature_next);
+        }
     }
     if (ctx.layout == 0) {
         float* g_next = ctx.g[1 - ctx.cur];
@@ -1200,8 +1214,16 @@ static bool exchange_halo(const char* who, int nx, int ny, int nz, int halo_laye
         if (!cuda_ok(launch_halo_soa(a->g[1 - a->cur], b->g[1 - b->cur], a->cells, ny, nz, 27, ab, s), "halo_f")) return false;
         if (!cuda_ok(launch_halo_soa(b->g[1 - b->cur], a->g[1 - a->cur], b->cells, ny, nz, 27, ba, s), "halo_f")) return false;
     }
-    if (!cuda_ok(launch_halo_soa(a->temperature, b->temperature, a->cells, ny, nz, 1, ab, s), "halo_temperature")) return false;
-    if (!cuda_ok(launch_halo_soa(b->temperature, a->temperature, b->cells, ny, nz, 1, ba, s), "halo_temperature")) return false;
+    // should_exchange_temperature_halo (jni.cpp:2198-2207): in runtime mode the
+    // temperature moves every other call; its slabs are exchanged only when
+    // either context updated it in its last call
+    auto updated_last = [](const Context* c) {
+        return bench_active() || c->step_counter == 0 || (c->step_counter - 1) % 2 == 0;
+    };
+    if (updated_last(a) || updated_last(b)) {
+        if (!cuda_ok(launch_halo_soa(a->temperature, b->temperature, a->cells, ny, nz, 1, ab, s), "halo_temperature")) return false;
+        if (!cuda_ok(launch_halo_soa(b->temperature, a->temperature, b->cells, ny, nz, 1, ba, s), "halo_temperature")) return false;
+    }
     return true;
 }
 

@@ -51,7 +51,27 @@ struct ThermalArgs {
     ThermalFaces faces;
     int bfecc;                  // 1: the BFECC branch (heated-cavity presets); the result lands in scratch
     float* scratch;             // BFECC: third state buffer
+    // Runtime mode (benchmark off): the BFECC update runs every other call
+    // with dt = 2 and adds a local eddy diffusivity nu_t / 0.85 from the last
+    // collision's velocity gradients (runtime_local_turbulent_nu and
+    // effective_local_thermal_diffusivity, jni.cpp:1972-2047).
+    float dt;                   // effective_thermal_dt: 1, or 2 in runtime mode
+    int turbulent;              // add the local eddy diffusivity
+    float sgs_c2;               // Smagorinsky C^2 of the eddy viscosity
+    float nu0;                  // runtime molecular viscosity (its cap is 5 nu0)
 };
+
+// Runtime mode, every call after the first (apply_runtime_temperature_reference,
+// jni.cpp:8037-8064): solid cells hold 0; fluid cells in the 8 outer layers
+// move toward the packet temperature by the state nudge factor.
+struct ThermalNudgeArgs {
+    int nx, ny, nz;
+    float* t;
+    const uint8_t* obstacle;
+    const float* ref_t;
+    float nudge;                // 0.08
+};
+cudaError_t launch_thermal_reference_nudge(const ThermalNudgeArgs& a, cudaStream_t s);
 
 // First call of a context: the state and the velocity the first update
 // advects with (initialize_distributions, jni.cpp:1752-1781). benchmark: a

@@ -139,6 +139,42 @@ __device__ __noinline__ float th_sample_far(const ThermalArgs& a, float px, floa
     return th_sample(a, a.t, px, py, pz, fallback);
 }
 
+// runtime_local_turbulent_nu (jni.cpp:1972-2031): 0 next to a solid face
+// neighbour; else C^2 |S| (capped at 5 nu0) from central differences of the
+// last collision's velocity, a solid or outside neighbour giving the centre's
+// value.
+__device__ __forceinline__ float vel_or_self(const ThermalArgs& a, const float* v, int x, int y, int z, float self) {
+    if (x < 0 || y < 0 || z < 0 || x >= a.nx || y >= a.ny || z >= a.nz) return self;
+    const long long c = ((long long)x * a.ny + y) * a.nz + z;
+    return a.obstacle[c] ? self : v[c];
+}
+__device__ __noinline__ float eddy_nu(const ThermalArgs& a, int x, int y, int z) {
+    const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    for (int i = 0; i < 6; ++i) {
+        const int p = x + off[i][0], q = y + off[i][1], r = z + off[i][2];
+        if (p < 0 || q < 0 || r < 0 || p >= a.nx || q >= a.ny || r >= a.nz) continue;
+        if (a.obstacle[((long long)p * a.ny + q) * a.nz + r]) return 0.0f;
+    }
+    const long long cc = ((long long)x * a.ny + y) * a.nz + z;
+    float d[3][3];
+    for (int k = 0; k < 3; ++k) {
+        const float* v = a.u + (long long)k * a.cells;
+        const float self = v[cc];
+        d[k][0] = 0.5f * (vel_or_self(a, v, x + 1, y, z, self) - vel_or_self(a, v, x - 1, y, z, self));
+        d[k][1] = 0.5f * (vel_or_self(a, v, x, y + 1, z, self) - vel_or_self(a, v, x, y - 1, z, self));
+        d[k][2] = 0.5f * (vel_or_self(a, v, x, y, z + 1, self) - vel_or_self(a, v, x, y, z - 1, self));
+    }
+    const float sxx = d[0][0], syy = d[1][1], szz = d[2][2];
+    const float sxy = 0.5f * (d[0][1] + d[1][0]);
+    const float sxz = 0.5f * (d[0][2] + d[2][0]);
+    const float syz = 0.5f * (d[1][2] + d[2][1]);
+    const float smag = sqrtf(exact::rmax(0.0f, 2.0f * (sxx * sxx + syy * syy + szz * szz) +
+                                                     4.0f * (sxy * sxy + sxz * sxz + syz * syz)));
+    float nut = a.sgs_c2 * smag;
+    nut = exact::rmin(nut, 5.0f * a.nu0);
+    return exact::rmax(0.0f, nut);
+}
+
 // ---- BFECC branch (jni.cpp:2050-2135): one thread per cell, line grid.
 __device__ __forceinline__ bool th_line_cell(const ThermalArgs& a, int& x, int& y, int& z, int& cell) {
     z = blockIdx.x * blockDim.x + threadIdx.x;
@@ -156,7 +192,7 @@ __global__ void __launch_bounds__(128) bfecc_forward_kernel(ThermalArgs a) {
         a.scratch[cell] = 0.0f;
         return;
     }
-    const float dt = 1.0f;
+    const float dt = a.dt;
     const float ux = a.u[cell], uy = a.u[a.cells + cell], uz = a.u[2 * a.cells + cell];
     a.scratch[cell] = th_sample(a, a.t, (float)x - dt * ux, (float)y - dt * uy, (float)z - dt * uz, a.t[cell]);
 }
@@ -169,7 +205,7 @@ __global__ void __launch_bounds__(128) bfecc_correct_kernel(ThermalArgs a) {
         a.t_next[cell] = 0.0f;
         return;
     }
-    const float dt = 1.0f;
+    const float dt = a.dt;
     const float tc = a.t[cell];
     const float ux = a.u[cell], uy = a.u[a.cells + cell], uz = a.u[2 * a.cells + cell];
     const float back = th_sample(a, a.scratch, (float)x + dt * ux, (float)y + dt * uy, (float)z + dt * uz, a.scratch[cell]);
@@ -184,7 +220,7 @@ __global__ void __launch_bounds__(128) bfecc_final_kernel(ThermalArgs a) {
         a.scratch[cell] = 0.0f;
         return;
     }
-    const float dt = 1.0f, cooling = 0.0f;
+    const float dt = a.dt, cooling = 0.0f;
     const float tc = a.t[cell];
     const float ux = a.u[cell], uy = a.u[a.cells + cell], uz = a.u[2 * a.cells + cell];
     float adv = th_sample(a, a.t_next, (float)x - dt * ux, (float)y - dt * uy, (float)z - dt * uz, a.t_next[cell]);
@@ -203,7 +239,28 @@ __global__ void __launch_bounds__(128) bfecc_final_kernel(ThermalArgs a) {
     const float t_sum = n0 + n1 + n2 + n3 + n4 + n5;
     const float lap = t_sum - 6.0f * tc;
     const float src = a.source ? exact::rclamp(a.source[cell], -0.006f, 0.006f) : 0.0f;
-    a.scratch[cell] = exact::rclamp(adv + dt * (a.alpha * lap + src - cooling * adv), -1.0f, 1.0f);
+    const float alpha = a.turbulent ? a.alpha + eddy_nu(a, x, y, z) / exact::rmax(1.0e-6f, 0.85f) : a.alpha;
+    a.scratch[cell] = exact::rclamp(adv + dt * (alpha * lap + src - cooling * adv), -1.0f, 1.0f);
+}
+
+__global__ void thermal_reference_nudge_kernel(ThermalNudgeArgs a) {
+    const long long cells = (long long)a.nx * a.ny * a.nz;
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= cells) return;
+    if (a.obstacle[cell]) {
+        a.t[cell] = 0.0f;
+        return;
+    }
+    int x, y, z;
+    cell_xyz32(cell, a.ny, a.nz, x, y, z);
+    const int d = min(min(min(x, y), min(z, a.nx - 1 - x)), min(a.ny - 1 - y, a.nz - 1 - z));
+    if (d >= 8) return;
+    const float eta = (float)(8 - d) / 8.0f;
+    const float n = a.nudge * eta * eta;
+    if (n <= 0.0f) return;
+    const float rt = exact::rclamp(a.ref_t[cell], -1.0f, 1.0f);
+    const float keep = 1.0f - n;
+    a.t[cell] = exact::rclamp(a.t[cell] * keep + rt * n, -1.0f, 1.0f);
 }
 
 template <int kKind>
@@ -336,6 +393,14 @@ __global__ void thermal_init_kernel(ThermalInitArgs a) {
 cudaError_t launch_thermal_init(const ThermalInitArgs& a, cudaStream_t s) {
     if (a.cells <= 0) return cudaSuccess;
     thermal_init_kernel<<<(unsigned)((a.cells + 255) / 256), 256, 0, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_thermal_reference_nudge(const ThermalNudgeArgs& a, cudaStream_t s) {
+    const long long cells = (long long)a.nx * a.ny * a.nz;
+    if (cells <= 0) return cudaSuccess;
+    thermal_reference_nudge_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }

@@ -102,6 +102,7 @@ typedef struct OracleD3Q27Params {
     double fan_noise_amp;          // fan target noise amplitude (0.02; 0 with DISABLE_FAN_NOISE)
     int sponge;                    // 1: post-collision sponge toward rest in the 4 outer layers
     double state_nudge;            // runtime mode: 0.08 (velocity nudge toward the packet state, 8 outer layers)
+    int runtime_mode;              // 1: benchmark mode off (jni.cpp:8037-8064, 1972-2047, 2191-2196)
 } OracleD3Q27Params;
 
 }  // extern "C"
@@ -320,7 +321,7 @@ struct D3Q27Oracle {
             if (p.thermal_transport) {
                 // benchmark mode: a zero state takes initial_temperature, a
                 // non-zero fluid state the packet's reference temperature
-                if (std::fabs(temperature[cell]) < T(1e-8f)) temperature[cell] = clampv(T(float(p.initial_temperature)), t_min, t_max);
+                if (!p.runtime_mode && std::fabs(temperature[cell]) < T(1e-8f)) temperature[cell] = clampv(T(float(p.initial_temperature)), t_min, t_max);
                 else if (!obstacle[cell]) temperature[cell] = clampv(ref_temperature[cell], t_min, t_max);
                 temperature[cell] = clampv(temperature[cell], t_min, t_max);
                 temperature_next[cell] = temperature[cell];
@@ -378,8 +379,59 @@ struct D3Q27Oracle {
     // (the runtime nudge toward the packet is zero in benchmark mode).
     void apply_temperature_reference() {
         if (!p.packet_has_temperature) return;
-        for (size_t cell = 0; cell < cells; ++cell)
-            if (obstacle[cell]) temperature[cell] = temperature_next[cell] = T(0);
+        for (size_t cell = 0; cell < cells; ++cell) {
+            if (obstacle[cell]) {
+                temperature[cell] = temperature_next[cell] = T(0);
+                continue;
+            }
+            // runtime mode: nudge toward the packet temperature in the outer
+            // layers (apply_runtime_temperature_reference, jni.cpp:8037-8064)
+            const T n = state_nudge_at(cell);
+            if (n <= T(0)) continue;
+            const T rt = clampv(ref_temperature[cell], t_min, t_max);
+            const T keep = T(1.0f) - n;
+            temperature[cell] = clampv(T(temperature[cell] * keep + rt * n), t_min, t_max);
+            temperature_next[cell] = temperature[cell];
+        }
+    }
+    // runtime_local_turbulent_nu (jni.cpp:1972-2031): Smagorinsky eddy
+    // viscosity from central differences of the last collision's velocity
+    // (a solid or outside neighbour gives the centre's value); 0 next to a
+    // solid cell.
+    T velocity_or_self(const std::vector<T>& v, int x, int y, int z, T self) const {
+        if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return self;
+        const size_t c = cell_index(x, y, z);
+        return obstacle[c] ? self : v[c];
+    }
+    T local_turbulent_nu(int x, int y, int z) const {
+        if (!p.enable_sgs) return T(0);
+        const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        for (const auto& o : off) {
+            const int a = x + o[0], b = y + o[1], c = z + o[2];
+            if (a < 0 || b < 0 || c < 0 || a >= nx || b >= ny || c >= nz) continue;
+            if (obstacle[cell_index(a, b, c)]) return T(0);
+        }
+        const size_t cc = cell_index(x, y, z);
+        const std::vector<T>* comp[3] = {&ux, &uy, &uz};
+        T d[3][3];
+        for (int k = 0; k < 3; ++k) {
+            const T self = (*comp[k])[cc];
+            d[k][0] = T(0.5f) * (velocity_or_self(*comp[k], x + 1, y, z, self) - velocity_or_self(*comp[k], x - 1, y, z, self));
+            d[k][1] = T(0.5f) * (velocity_or_self(*comp[k], x, y + 1, z, self) - velocity_or_self(*comp[k], x, y - 1, z, self));
+            d[k][2] = T(0.5f) * (velocity_or_self(*comp[k], x, y, z + 1, self) - velocity_or_self(*comp[k], x, y, z - 1, self));
+        }
+        const T sxx = d[0][0], syy = d[1][1], szz = d[2][2];
+        const T sxy = T(0.5f) * (d[0][1] + d[1][0]);
+        const T sxz = T(0.5f) * (d[0][2] + d[2][0]);
+        const T syz = T(0.5f) * (d[1][2] + d[2][1]);
+        const T smag = std::sqrt(std::max(T(0.0f), T(2.0f) * (sxx * sxx + syy * syy + szz * szz) +
+                                                      T(4.0f) * (sxy * sxy + sxz * sxz + syz * syz)));
+        // runtime_molecular_nu0 (jni.cpp:927-929): the clamped runtime molecular
+        // viscosity, without the collision's 1e-6 floor
+        const T nu0 = T(std::min((0.95f - 0.5f) / 3.0f, std::max(1.0e-8f, 1.50e-5f * (1.0f / 20.0f) / (1.0f * 1.0f))));
+        T nut = T(float(p.sgs_c2)) * smag;
+        nut = std::min(nut, T(float(p.sgs_nut_max_ratio)) * nu0);
+        return std::max(T(0.0f), nut);
     }
     void local_bounds(int x, int y, int z, T& lo, T& hi) const {
         const T c = temperature[cell_index(x, y, z)];
@@ -396,7 +448,8 @@ struct D3Q27Oracle {
     // of that, the error-corrected field advected again and limited to the
     // local min/max of the state, then diffusion + source (dt = 1).
     void update_temperature_bfecc() {
-        const T dt = T(1.0f), cooling = T(0.0f);
+        // effective_thermal_dt (jni.cpp:907-909): the update stride, 2 in runtime mode
+        const T dt = T(p.runtime_mode ? 2.0f : 1.0f), cooling = T(0.0f);
         const T alpha = T(float(p.thermal_diffusivity));
         for (int x = 0; x < nx; ++x)
             for (int y = 0; y < ny; ++y)
@@ -433,7 +486,10 @@ struct D3Q27Oracle {
                                     thermal_neighbour(temperature, x, y, z + 1, tc) + thermal_neighbour(temperature, x, y, z - 1, tc);
                     const T lap = t_sum - T(6.0f) * tc;
                     const T src = p.internal_thermal_source ? clampv(thermal_source[cell], T(-0.006f), T(0.006f)) : T(0);
-                    temperature_scratch[cell] = clampv(T(adv + dt * (alpha * lap + src - cooling * adv)), t_min, t_max);
+                    // effective_local_thermal_diffusivity (jni.cpp:2033-2047)
+                    const T a_loc = p.runtime_mode ? T(alpha + local_turbulent_nu(x, y, z) / std::max(T(1.0e-6f), T(0.85f)))
+                                                   : alpha;
+                    temperature_scratch[cell] = clampv(T(adv + dt * (a_loc * lap + src - cooling * adv)), t_min, t_max);
                 }
         temperature.swap(temperature_scratch);
         temperature_next = temperature;
@@ -1008,7 +1064,9 @@ struct D3Q27Oracle {
     void step() {
         if (!initialized) initialize();
         else if (p.thermal_transport) apply_temperature_reference();
-        if (p.thermal_transport) update_temperature();
+        // should_update_temperature (jni.cpp:2191-2196): every call, every
+        // other call in runtime mode
+        if (p.thermal_transport && (!p.runtime_mode || steps_done % 2 == 0)) update_temperature();
         collide();
         cylinder_force();
         stream();
@@ -1068,8 +1126,15 @@ int exchange_halo(D3Q27Oracle<T>& a, D3Q27Oracle<T>& b, int ox, int oy, int oz, 
     };
     copy(a, b, s1, d2);
     copy(b, a, s2, d1);
-    copy_t(a, b, s1, d2);
-    copy_t(b, a, s2, d1);
+    // should_exchange_temperature_halo (jni.cpp:2198-2207): with the runtime
+    // mode's every-other-call update, only after a call that moved it
+    auto updated_last = [](const D3Q27Oracle<T>& o) {
+        return !o.p.runtime_mode || o.steps_done == 0 || (o.steps_done - 1) % 2 == 0;
+    };
+    if (updated_last(a) || updated_last(b)) {
+        copy_t(a, b, s1, d2);
+        copy_t(b, a, s2, d1);
+    }
     a.temperature_next = a.temperature;
     b.temperature_next = b.temperature;
     return 1;

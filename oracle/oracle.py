@@ -89,6 +89,7 @@ class OracleParams(ctypes.Structure):
         ("fan_noise_amp", ctypes.c_double),
         ("sponge", ctypes.c_int),
         ("state_nudge", ctypes.c_double),
+        ("runtime_mode", ctypes.c_int),
     ]
 
 
@@ -192,7 +193,46 @@ def derive_params(cfg: dict) -> OracleParams:
     p.fan_noise_amp = float(f32(0.02)) if (cfg.get("fans", False) and cfg.get("fan_noise", False)) else 0.0
     p.sponge = 1 if cfg.get("sponge", False) else 0
     p.state_nudge = 0.0
+    if not cfg.get("benchmark", True):
+        runtime_params(p)
     return p
+
+
+def runtime_params(p: OracleParams) -> None:
+    """Benchmark mode off (aero_lbm_benchmark_reset_config): the reference's
+    game-runtime constants (jni.cpp:87-168, 676-1031): molecular viscosity
+    and diffusivity of air at 1 m cells and 1/20 s steps, SGS, buoyancy,
+    fans with noise, sponge, state nudge, the temperature transport (BFECC,
+    every other call, local eddy diffusivity) and the default config's faces
+    (INHERIT_GAME: convective outflow, thermal self)."""
+    nu = _clamp(RUNTIME_NU0, NU_MIN, NU_MAX)
+    p.tau_shear = float(_clamp(f32(0.5) + f32(3.0) * nu, TAU_MIN, TAU_MAX))
+    p.tau_normal = float(_clamp(f32(0.5) + f32(3.0) * RUNTIME_NU0, TAU_MIN, TAU_MAX))
+    p.nu0 = float(max(f32(1e-6), nu))
+    p.sgs_c2 = float(f32(f32(0.025) * f32(0.025)))
+    p.enable_sgs = 1
+    p.enable_buoyancy = 1
+    p.buoyancy_beta = float(BOUSSINESQ_BETA)
+    p.gravity_axis = 1
+    for i in range(3):
+        p.body_force[i] = 0.0
+    for i in range(6):
+        p.face_kind[i] = INHERIT_GAME
+        p.thermal_kind[i] = THERMAL_INHERIT
+        p.face_pressure[i] = 0.0
+        for a in range(3):
+            p.face_velocity[i][a] = 0.0
+    p.disable_convective_outflow = 0
+    p.thermal_transport = 1
+    p.thermal_bfecc = 1
+    alpha0 = f32(f32(f32(1.50e-5) / f32(0.71)) * f32(f32(1.0) / f32(20.0))) / f32(f32(1.0) * f32(1.0))
+    p.thermal_diffusivity = float(max(f32(1.0e-8), alpha0))
+    p.internal_thermal_source = 1
+    p.fan_forcing = 1
+    p.fan_noise_amp = float(f32(0.02))
+    p.sponge = 1
+    p.state_nudge = float(f32(0.08))
+    p.runtime_mode = 1
 
 
 # ---------------------------------------------------------------- oracle (restatement)
@@ -475,9 +515,12 @@ class RefLib:
         lib.aero_lbm_exchange_halo_layers_rect.restype = ctypes.c_int
         if not lib.aero_lbm_init_rect(nx, ny, nz, packets[0].shape[1], 4):
             raise RuntimeError(lib.aero_lbm_last_error())
-        c = config_struct(RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
-        if not lib.aero_lbm_benchmark_set_config(ctypes.byref(c)):
-            raise RuntimeError("set_config failed")
+        if cfg.get("benchmark", True):
+            c = config_struct(RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
+            if not lib.aero_lbm_benchmark_set_config(ctypes.byref(c)):
+                raise RuntimeError("set_config failed")
+        else:
+            lib.aero_lbm_benchmark_reset_config()
         for key, ts in zip(keys, temperature_states):
             if ts is not None:
                 t = np.ascontiguousarray(np.asarray(ts, np.float32).reshape(-1))
@@ -516,9 +559,12 @@ class RefLib:
         lib.aero_lbm_copy_flow_temperature_subrect.argtypes = [i, i, i, ll] + [i] * 6 + [vp, vp]
         if not lib.aero_lbm_init_rect(nx, ny, nz, packet.shape[1], 4):
             raise RuntimeError(lib.aero_lbm_last_error())
-        c = config_struct(RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
-        if not lib.aero_lbm_benchmark_set_config(ctypes.byref(c)):
-            raise RuntimeError("set_config failed")
+        if cfg.get("benchmark", True):
+            c = config_struct(RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
+            if not lib.aero_lbm_benchmark_set_config(ctypes.byref(c)):
+                raise RuntimeError("set_config failed")
+        else:
+            lib.aero_lbm_benchmark_reset_config()
         cells = nx * ny * nz
         if temperature_state is not None:
             t = np.ascontiguousarray(np.asarray(temperature_state, np.float32).reshape(-1))
@@ -652,6 +698,8 @@ def context_ops_script(n: int, seed: int = 23):
 
 CYLINDER_SCRIPT = [("step",), ("force",)] * 5 + [("flow",)]
 FAN_SCRIPT = [("step",)] * 6 + [("flow",), ("temp",)] + [("step",)] * 6 + [("flow",)]
+RUNTIME_SCRIPT = ([("step",)] + [("flow",), ("temp",)] + [("step",)] * 2 + [("flow",), ("temp",)] + [("step",)] * 5
+                  + [("flow",), ("temp",)])
 
 
 def feq_rest(q: int) -> float:
@@ -719,6 +767,19 @@ def fan_case(n: int = 12, seed: int = 61, noise: bool = True, sponge: bool = Tru
     fv = [np.where(fan, rng.uniform(-3.0, 3.0, dims), 0.0).astype(np.float32) for _ in range(3)]
     cfg = dict(cfg, fans=True, fan_noise=noise, sponge=sponge)
     pk = packet_from(obst, *u, temperature=temp, source=src, fans=(mask, *fv))
+    return cfg, pk, pre
+
+
+def runtime_case(n: int = 12, seed: int = 71, fans: bool = True):
+    """Benchmark mode off (the reference's game runtime, as its brick service
+    runs it): the thermal case's brick and fields with fans on 3 % of the
+    fluid cells; the faces are the default config's (convective outflow)."""
+    cfg, pk, pre = fan_case(n, seed)
+    if not fans:
+        pk = pk.copy()
+        pk[:, 1:5] = 0.0
+    cfg = {"benchmark": False, "faces": cfg["faces"], "fans": True, "thermal_transport": True,
+           "thermal_source": True}
     return cfg, pk, pre
 
 

@@ -42,6 +42,10 @@ Fixtures:
   fans_12_12.npz  the fan forcing, fan noise and sponge of the reference's
                   collide switched on in benchmark mode (oracle.fan_case(12,
                   seed 61)): flow and temperature after 6 calls, flow after 12.
+  runtime_12_8.npz benchmark mode off (the reference's game runtime:
+                  fans, noise, sponge, state nudge, every-other-call BFECC
+                  transport with eddy diffusivity, convective outflow faces),
+                  oracle.runtime_case(12, seed 71), oracle.RUNTIME_SCRIPT.
   thermal_12_20.npz buoyancy on with the reference's temperature transport:
                   oracle.thermal_case(12, seed 11) (every thermal face kind,
                   packet source channel, state preloaded), 20 steps; the
@@ -168,6 +172,13 @@ def fans_fixture(ref) -> None:
     print("fans_12_12 written")
 
 
+def runtime_fixture(ref) -> None:
+    cfg, pk, pre = O.runtime_case(12, 71)
+    res = ref.run_script((12, 12, 12), cfg, pk, O.RUNTIME_SCRIPT, temperature_state=pre)
+    save_results(OUT / "runtime_12_8.npz", res, input_sha256=digest(pk, pre))
+    print("runtime_12_8 written")
+
+
 def main() -> int:
     O.build(ref=True)
     ref = O.RefLib()
@@ -187,6 +198,8 @@ def main() -> int:
             brickworld_fixture()
         if only in "fans_12_12":
             fans_fixture(ref)
+        if only in "runtime_12_8":
+            runtime_fixture(ref)
         return 0
     for name, n, steps in (("c1_16_200", 16, 200), ("c1_32_1000", 32, 1000)):
         seed = 1234
@@ -216,6 +229,7 @@ def main() -> int:
     cylinder_fixture(ref)
     brickworld_fixture()
     fans_fixture(ref)
+    runtime_fixture(ref)
     return 0
 
 

@@ -33,12 +33,13 @@ def _fp(a):
     return a.ctypes.data_as(_F32P)
 
 
-def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mode=0, temperature_state=None):
+def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mode=0, temperature_state=None,
+                   collision=0):
     """The product driven through the same call list as oracle.run_script_oracle."""
     nx, ny, nz = dims
     gpu.aero_lbm_b200_set_physics_overrides(-1.0, -1.0, -1)
     gpu.aero_lbm_b200_set_streaming_mode(streaming)
-    gpu.aero_lbm_b200_set_collision_mode(0)
+    gpu.aero_lbm_b200_set_collision_mode(collision)
     gpu.aero_lbm_set_realtime_solver_mode(solver_mode)
     assert gpu.aero_lbm_b200_set_cells_per_thread(cpt) == 1
     pk = np.ascontiguousarray(pk, np.float32)
@@ -46,7 +47,10 @@ def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mod
     results = []
     try:
         ctx = aero_b200.LbmContext(dims, key=key, lib=gpu)
-        ctx.configure(lbm_cases.product_config(gpu, cfg))
+        if cfg.get("benchmark", True):
+            ctx.configure(lbm_cases.product_config(gpu, cfg))
+        else:
+            gpu.aero_lbm_benchmark_reset_config()  # the game runtime (benchmark mode off)
         if temperature_state is not None:
             ctx.set_temperature_state(temperature_state)
         for act in script:
@@ -102,6 +106,7 @@ def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mod
     finally:
         gpu.aero_lbm_b200_set_cells_per_thread(2)
         gpu.aero_lbm_set_realtime_solver_mode(0)
+        gpu.aero_lbm_b200_set_collision_mode(0)
     assert len(results) == sum(1 for a in script if a[0] not in ("step", "shift", "cached", "patch", "shell"))
     return results
 
@@ -304,3 +309,26 @@ def test_fans_and_sponge_fp16_against_fp64(gpu):
             assert e["u"] <= 1e-3 and e["rho"] <= 1e-4, e
         else:
             assert float(np.max(np.abs(a - b))) <= 1e-3
+
+
+@pytest.mark.parametrize("collision", [0, 1])
+def test_runtime_mode_matches_reference_golden(gpu, collision):
+    """Benchmark mode off, as the reference's brick service runs the step:
+    fans with noise, sponge, state nudge, the every-other-call BFECC
+    transport with eddy diffusivity, convective outflow faces (two-buffer
+    layout). The reference-order collision is bit-identical to fixture
+    runtime_12_8.npz; the factorised one agrees to FP32 rounding."""
+    cfg, pk, pre = O.runtime_case(12, 71)
+    res = run_script_gpu(gpu, (12, 12, 12), cfg, pk, O.RUNTIME_SCRIPT, key=900 + collision, streaming=0,
+                         temperature_state=pre, collision=collision)
+    ref = O.load_results(GOLDEN / "runtime_12_8.npz")
+    if collision == 0:
+        flags = O.results_equal(res, ref)
+        assert all(flags), flags
+    else:
+        for kind, a, b in zip(("flow", "temp") * 3, res, ref):
+            if kind == "flow":
+                e = O.flow_errors(a, b)
+                assert e["u"] <= 1e-5 and e["rho"] <= 1e-6, e
+            else:
+                assert float(np.max(np.abs(a - b))) <= 1e-5

@@ -167,3 +167,38 @@ def test_halo_exchange_argument_checks(gpu):
     finally:
         c1.release()
         c2.release()
+
+
+def test_halo_exchange_runtime_mode_matches_oracle(gpu):
+    """Benchmark mode off: the temperature slabs move only after a call that
+    updated the temperature (every other call); the two-buffer layout."""
+    n, steps, offset, halo = 12, 7, (1, 0, 0), 2
+    cfg, pk1, pre = O.runtime_case(n, 74)
+    _, pk2, _ = O.runtime_case(n, 75)
+    gpu.aero_lbm_b200_set_streaming_mode(0)
+    gpu.aero_lbm_b200_set_collision_mode(0)
+    c1 = aero_b200.LbmContext((n, n, n), key=790, lib=gpu)
+    gpu.aero_lbm_benchmark_reset_config()
+    c2 = aero_b200.LbmContext((n, n, n), key=791, lib=gpu, init=False)
+    os_ = []
+    for _ in range(2):
+        o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+        o.set_temperature(pre)
+        os_.append(o)
+    try:
+        for c in (c1, c2):
+            c.set_temperature_state(pre)
+        for s in range(steps):
+            last = s + 1 == steps
+            outs = [c.step(pk, output=last) for c, pk in zip((c1, c2), (pk1, pk2))]
+            for o, pk in zip(os_, (pk1, pk2)):
+                O.run_script_oracle(o, cfg, pk, [("step",)])
+            if not last:
+                assert gpu.aero_lbm_exchange_halo_layers_rect(n, n, n, halo, 790, 791, *offset) == 1
+                os_[0].exchange_halo(os_[1], offset, halo)
+        for c, o, out in zip((c1, c2), os_, outs):
+            assert_bits(out, o.output())
+            assert np.array_equal(c.temperature_state().view(np.uint32), o.temperature().view(np.uint32))
+    finally:
+        c1.release()
+        c2.release()

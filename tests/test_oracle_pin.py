@@ -309,3 +309,51 @@ def test_oracle_fans_and_sponge_match_reference_live(noise, sponge, seed):
     res = O.run_script_oracle(o, cfg, pk, script)
     ref = O.RefLib().run_script((12, 12, 12), cfg, pk, script, temperature_state=pre)
     assert all(O.results_equal(res, ref))
+
+
+def test_oracle_runtime_mode_matches_golden():
+    """Benchmark mode off (the game runtime the brick service uses), bit for
+    bit against fixture runtime_12_8.npz."""
+    cfg, pk, pre = O.runtime_case(12, 71)
+    o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    res = O.run_script_oracle(o, cfg, pk, O.RUNTIME_SCRIPT)
+    assert all(O.results_equal(res, O.load_results(GOLDEN / "runtime_12_8.npz")))
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("seed,fans", [(72, True), (73, False)])
+def test_oracle_runtime_mode_matches_reference_live(seed, fans):
+    cfg, pk, pre = O.runtime_case(12, seed, fans)
+    script = [("step",)] * 4 + [("flow",), ("temp",)] + [("step",)] * 3 + [("flow",), ("temp",)]
+    o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    res = O.run_script_oracle(o, cfg, pk, script)
+    ref = O.RefLib().run_script((12, 12, 12), cfg, pk, script, temperature_state=pre)
+    assert all(O.results_equal(res, ref))
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("every", [1, 2, 3])
+def test_oracle_runtime_halo_matches_reference_live(every):
+    """Halo exchange in runtime mode: the temperature slabs move only after a
+    call that updated the temperature (every other call there)."""
+    n, steps, offset, halo = 12, 7, (1, 0, 0), 2
+    cfg, pk1, pre = O.runtime_case(n, 74)
+    _, pk2, _ = O.runtime_case(n, 75)
+    ref = O.RefLib()
+    outs = ref.run_pair((n, n, n), cfg, [pk1, pk2], steps, offset, halo, exchange_every=every,
+                        temperature_states=(pre, pre))
+    os_ = []
+    for pk in (pk1, pk2):
+        o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+        o.set_temperature(pre)
+        os_.append(o)
+    for s in range(steps):
+        for o, pk in zip(os_, (pk1, pk2)):
+            O.run_script_oracle(o, cfg, pk, [("step",)])
+        if s + 1 < steps and (s + 1) % every == 0:
+            os_[0].exchange_halo(os_[1], offset, halo)
+    for o, out, t in zip(os_, outs, ref.temperatures):
+        assert _bits_equal(o.output(), out)
+        assert _bits_equal(o.temperature(), t)
