@@ -107,29 +107,49 @@ cudaError_t launch_ingest_packet(const float* packet, int in_channels, BrickDims
 
 // Pull classification (see lattice.cuh for the bit layout). Mirrors the
 // branch structure of stream_and_bounce (jni.cpp:2415-2452) and
-// benchmark_hydrodynamic_boundary_value (jni.cpp:1563-1602).
-__global__ void build_flags_kernel(const uint8_t* __restrict__ obstacle, int nx, int ny, int nz, FaceParams F,
-                                   uint32_t* __restrict__ flags) {
-    const long long cells = (long long)nx * ny * nz;
-    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= cells) return;
-    const int z = (int)(cell % nz);
-    const int y = (int)((cell / nz) % ny);
-    const int x = (int)(cell / ((long long)ny * nz));
+// benchmark_hydrodynamic_boundary_value (jni.cpp:1563-1602). A block stages
+// its 32 x 4 x 2 cells' mask with a one-cell halo in shared memory (periodic
+// sides wrapped while staging, 2 = outside a non-periodic face), so the 27
+// neighbour tests of a cell read shared memory instead of issuing 27
+// dependent global loads.
+constexpr int kFlagTz = 32, kFlagTy = 4, kFlagTx = 2;
+__global__ void __launch_bounds__(kFlagTz * kFlagTy * kFlagTx) build_flags_kernel(
+    const uint8_t* __restrict__ obstacle, int nx, int ny, int nz, FaceParams F, uint32_t* __restrict__ flags) {
+    constexpr int SZ = kFlagTz + 2, SY = kFlagTy + 2, SX = kFlagTx + 2;
+    __shared__ uint8_t tile[SX * SY * SZ];
+    const int z0 = blockIdx.x * kFlagTz, y0 = blockIdx.y * kFlagTy, x0 = blockIdx.z * kFlagTx;
+    const int tid = (threadIdx.z * kFlagTy + threadIdx.y) * kFlagTz + threadIdx.x;
+    for (int i = tid; i < SX * SY * SZ; i += kFlagTz * kFlagTy * kFlagTx) {
+        const int tz = i % SZ, ty = (i / SZ) % SY, tx = i / (SZ * SY);
+        int gx = x0 + tx - 1, gy = y0 + ty - 1, gz = z0 + tz - 1;
+        uint8_t v = 2;
+        if (wrap_coord(gx, nx, F.wrap_lo[0], F.wrap_hi[0]) && wrap_coord(gy, ny, F.wrap_lo[1], F.wrap_hi[1]) &&
+            wrap_coord(gz, nz, F.wrap_lo[2], F.wrap_hi[2]))
+            v = obstacle[((long long)gx * ny + gy) * nz + gz] ? 1 : 0;
+        tile[i] = v;
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.z, y = y0 + threadIdx.y, z = z0 + threadIdx.x;
+    if (x >= nx || y >= ny || z >= nz) return;
+    const long long cell = ((long long)x * ny + y) * nz + z;
+    const int own = ((threadIdx.z + 1) * SY + threadIdx.y + 1) * SZ + threadIdx.x + 1;
     uint32_t w = 0;
-    if (obstacle[cell]) {
+    if (tile[own] == 1) {
         w = kFlagSelfSolid;
     } else {
-#pragma unroll 1
+#pragma unroll
         for (int q = 0; q < 27; ++q) {
-            int sx = x - q_cx(q), sy = y - q_cy(q), sz = z - q_cz(q);
-            const bool inx = wrap_coord(sx, nx, F.wrap_lo[0], F.wrap_hi[0]);
-            const bool iny = wrap_coord(sy, ny, F.wrap_lo[1], F.wrap_hi[1]);
-            const bool inz = wrap_coord(sz, nz, F.wrap_lo[2], F.wrap_hi[2]);
-            if (inx && iny && inz) {
-                if (obstacle[((long long)sx * ny + sy) * nz + sz]) w |= 1u << q;
-            } else {
-                const int kind = F.kind[oob_face(sx, sy, sz, nx, ny, nz)];
+            const uint8_t v = tile[own - (q_cx(q) * SY + q_cy(q)) * SZ - q_cz(q)];
+            if (v == 1) {
+                w |= 1u << q;
+            } else if (v == 2) {
+                // the first axis outside a non-periodic face picks the face (oob_face)
+                const int sx = x - q_cx(q), sy = y - q_cy(q), sz = z - q_cz(q);
+                int face;
+                if ((sx < 0 && !F.wrap_lo[0]) || (sx >= nx && !F.wrap_hi[0])) face = sx < 0 ? kFaceXMin : kFaceXMax;
+                else if ((sy < 0 && !F.wrap_lo[1]) || (sy >= ny && !F.wrap_hi[1])) face = sy < 0 ? kFaceYMin : kFaceYMax;
+                else face = sz < 0 ? kFaceZMin : kFaceZMax;
+                const int kind = F.kind[face];
                 if (kind == kHydroBounceBack || (kind == kHydroInheritGame && F.disable_convective)) w |= 1u << q;
                 else w |= kFlagFaceSpecial;
             }
@@ -140,9 +160,10 @@ __global__ void build_flags_kernel(const uint8_t* __restrict__ obstacle, int nx,
 
 cudaError_t launch_build_flags(const uint8_t* obstacle, BrickDims d, FaceParams face, uint32_t* flags, cudaStream_t stream) {
     if (d.cells <= 0) return cudaSuccess;
-    const int block = 256;
-    const long long grid = (d.cells + block - 1) / block;
-    build_flags_kernel<<<(unsigned)grid, block, 0, stream>>>(obstacle, d.nx, d.ny, d.nz, face, flags);
+    const dim3 block(kFlagTz, kFlagTy, kFlagTx);
+    const dim3 grid((unsigned)((d.nz + kFlagTz - 1) / kFlagTz), (unsigned)((d.ny + kFlagTy - 1) / kFlagTy),
+                    (unsigned)((d.nx + kFlagTx - 1) / kFlagTx));
+    build_flags_kernel<<<grid, block, 0, stream>>>(obstacle, d.nx, d.ny, d.nz, face, flags);
     count_launch();
     return cudaGetLastError();
 }
