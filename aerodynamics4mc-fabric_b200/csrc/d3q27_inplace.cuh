@@ -360,21 +360,22 @@ template <class S>
 __global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom G = a.g;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
-    const long long fx_n = (long long)ny * nz, fy_n = (long long)nx * nz, fz_n = (long long)nx * ny;
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    // 32-bit index arithmetic: a face of a brick has far fewer than 2^31 cells
+    const unsigned fx_n = (unsigned)ny * nz, fy_n = (unsigned)nx * nz, fz_n = (unsigned)nx * ny;
+    unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     int x, y, z;
     if (i < 2 * fx_n) {
         x = i < fx_n ? 0 : nx - 1;
-        const long long r = i % fx_n;
-        y = (int)(r / nz); z = (int)(r % nz);
+        const unsigned r = i < fx_n ? i : i - fx_n;
+        y = (int)(r / (unsigned)nz); z = (int)(r - (unsigned)y * nz);
     } else if ((i -= 2 * fx_n) < 2 * fy_n) {
         y = i < fy_n ? 0 : ny - 1;
-        const long long r = i % fy_n;
-        x = (int)(r / nz); z = (int)(r % nz);
+        const unsigned r = i < fy_n ? i : i - fy_n;
+        x = (int)(r / (unsigned)nz); z = (int)(r - (unsigned)x * nz);
     } else if ((i -= 2 * fy_n) < 2 * fz_n) {
         z = i < fz_n ? 0 : nz - 1;
-        const long long r = i % fz_n;
-        x = (int)(r / ny); y = (int)(r % ny);
+        const unsigned r = i < fz_n ? i : i - fz_n;
+        x = (int)(r / (unsigned)ny); y = (int)(r - (unsigned)x * ny);
     } else {
         return;
     }
@@ -385,7 +386,8 @@ __global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const int own = pad_index(G, x, y, z);
     const FaceParams& F = *a.face_prev;
     const float rp = a.ref_p_prev[cell];
-#pragma unroll 1
+    // unrolled: the direction constants fold and the 27 tests issue independently
+#pragma unroll
     for (int q = 0; q < 27; ++q) {
         if ((w >> q) & 1u) continue;
         const int sx = axis_neighbour(x, -q_cx(q), nx, G.wrap[0]);
