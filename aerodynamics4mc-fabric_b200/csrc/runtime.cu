@@ -437,6 +437,12 @@ void Context::release_device() {
     fr(ip);
     fr(reinterpret_cast<void*&>(solid_f));
     fr(reinterpret_cast<void*&>(fan_mask));
+    if (fill_done) cudaEventDestroy(fill_done);
+    if (fill_fork) cudaEventDestroy(fill_fork);
+    if (fill_stream) cudaStreamDestroy(fill_stream);
+    fill_done = fill_fork = nullptr;
+    fill_stream = nullptr;
+    fill_recorded = false;
     fr(scratch);
     scratch_cap = 0;
     packet_cap = out_cap = 0;
@@ -548,6 +554,11 @@ static bool inplace_faces_ok(const FaceParams& f) {
 // 0 FP32, 1 IEEE-half deviations, 2 16-bit fixed point.
 static int ip_storage(const Context& ctx) {
     return ctx.ip_variant == kIpF16Fast ? 1 : (ctx.ip_variant == kIpI16Fast ? 2 : 0);
+}
+
+bool join_fill(Context& ctx, cudaStream_t s) {
+    if (!ctx.fill_recorded) return true;
+    return cuda_ok(cudaStreamWaitEvent(s, ctx.fill_done, 0), "wait for the face pre-fill");
 }
 
 static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const CollideParams& cp) {
@@ -831,6 +842,7 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
                       "(symmetry or convective outflow); release and re-create the context");
             return false;
         }
+        if (!join_fill(ctx, s)) return false;
         IpArgs a = ip_args(ctx, ctx.slot, new_slot, cp);
         if (!ctx.initialized) {
             a.parity = 0;
@@ -877,11 +889,24 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             fill |= k == kHydroVelocity || k == kHydroPressure || k == kHydroMovingWall;
         }
         if (fill) {
+            // on the context's fill stream, forked after the step: it overlaps
+            // the next call's temperature update (the step waits for it)
+            if (!ctx.fill_stream &&
+                (!cuda_ok(cudaStreamCreateWithFlags(&ctx.fill_stream, cudaStreamNonBlocking), "fill stream") ||
+                 !cuda_ok(cudaEventCreateWithFlags(&ctx.fill_fork, cudaEventDisableTiming), "fill event") ||
+                 !cuda_ok(cudaEventCreateWithFlags(&ctx.fill_done, cudaEventDisableTiming), "fill event")))
+                return false;
             IpArgs a = ip_args(ctx, new_slot, new_slot, cp);
             a.parity = ctx.parity;
-            if (!cuda_ok(ip_fill(ctx.ip_variant, ctx.ip, a, s), "face_fill_inplace")) return false;
+            if (!cuda_ok(cudaEventRecord(ctx.fill_fork, s), "fork fill") ||
+                !cuda_ok(cudaStreamWaitEvent(ctx.fill_stream, ctx.fill_fork, 0), "fork fill") ||
+                !cuda_ok(ip_fill(ctx.ip_variant, ctx.ip, a, ctx.fill_stream), "face_fill_inplace") ||
+                !cuda_ok(cudaEventRecord(ctx.fill_done, ctx.fill_stream), "join fill"))
+                return false;
+            ctx.fill_recorded = true;
         }
         if (ctx.shell_count > 0) {
+            if (!join_fill(ctx, s)) return false;
             IpArgs a = ip_args(ctx, new_slot, new_slot, cp);
             a.parity = ctx.parity;
             if (!cuda_ok(launch_shell_relax(ip_storage(ctx), ctx.ip, a, static_cast<const ShellCell*>(ctx.shell),
@@ -904,6 +929,7 @@ bool output_device(Context& ctx, OutBox box, int out_ch, float scale, float* dev
                               box, out_ch, scale, dev_out, s, ctx.f_ready ? 1 : 0),
                        "output");
     }
+    if (!join_fill(ctx, s)) return false;
     IpArgs a = ip_args(ctx, ctx.slot, ctx.slot, current_collide_params());
     a.parity = ctx.parity;
     return cuda_ok(ip_output(ctx.ip_variant, ctx.ip, a, box, out_ch, scale, dev_out, s), "output_inplace");
@@ -1201,6 +1227,7 @@ static bool exchange_halo(const char* who, int nx, int ny, int nz, int halo_laye
                               Fp16Scale{c.fp16_scale, c.fp16_scale > 0.0f ? 1.0f / c.fp16_scale : 0.0f}, c.solid_f};
         };
         const int storage = a->ip_variant == kIpF16Fast ? 1 : (a->ip_variant == kIpI16Fast ? 2 : 0);
+        if (!join_fill(*a, s) || !join_fill(*b, s)) return false;
         if (!cuda_ok(launch_halo_ip(storage, side(*a), side(*b), ab, ba, s), "halo_inplace")) return false;
     } else {
         for (Context* c : {a, b}) {
@@ -1347,6 +1374,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_shift_context(int grid_size, long long key, in
                          "shift solid copy"))
                 return 0;
         }
+        if (!join_fill(*c, s)) return 0;
         v = IpView{c->ip, make_pad_geom(c->nx, c->ny, c->nz, c->periodic_mask), c->flags[slot], c->parity,
                    Fp16Scale{c->fp16_scale, c->fp16_scale > 0.0f ? 1.0f / c->fp16_scale : 0.0f}};
         if (!cuda_ok(launch_ip_gather_shifted(storage, v, dx, dy, dz, tmp, s), "shift gather")) return 0;
@@ -1440,7 +1468,8 @@ AERO_LBM_B200_EXPORT int aero_lbm_patch_d3q27_f16_static_cells_rect(int nx, int 
         return 0;
     IpArgs a = ip_args(*c, c->slot, c->slot, current_collide_params());
     a.parity = c->parity;
-    if (!cuda_ok(launch_patch_reset(ip_storage(*c), c->ip, a, c->patch_cells, count, s), "patch reset")) return 0;
+    if (!join_fill(*c, s) ||
+        !cuda_ok(launch_patch_reset(ip_storage(*c), c->ip, a, c->patch_cells, count, s), "patch reset")) return 0;
     c->pending_slot = target;
     return cuda_ok(cudaStreamSynchronize(s), "sync") ? 1 : 0;
 }
@@ -1886,7 +1915,8 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums(long long key, double* 
     } else {
         IpArgs a = ip_args(*c, c->slot, c->slot, current_collide_params());
         a.parity = c->parity;
-        e = launch_conservation_ip(c->ip_variant, c->ip, a, partials, dev_out, s);
+        e = join_fill(*c, s) ? launch_conservation_ip(c->ip_variant, c->ip, a, partials, dev_out, s)
+                             : cudaErrorUnknown;
     }
     if (!cuda_ok(e, "conservation kernels")) return 0;
     if (!cuda_ok(cudaMemcpyAsync(out4, dev_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy sums")) return 0;

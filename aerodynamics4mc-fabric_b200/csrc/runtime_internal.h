@@ -54,6 +54,12 @@ struct Context {
     int ip_variant = 0;      // IpVariant when layout == 1
     void* ip = nullptr;      // padded population array (float or __half)
     float* solid_f = nullptr;
+    // The equilibrium-face pre-fill at the end of a call runs on its own
+    // stream, overlapping the next call's temperature update; anything that
+    // touches the in-place populations joins it first (join_fill).
+    cudaStream_t fill_stream = nullptr;
+    cudaEvent_t fill_fork = nullptr, fill_done = nullptr;
+    bool fill_recorded = false;
     float* fan_mask = nullptr;  // packet fan channels, 4 x cells (mask, ux, uy, uz), while fan forcing is on  // in-place: populations of solid cells (IpArgs::solid_f), from the first mask change on
     int parity = 0;          // slot-map parity of the next in-place step
     int periodic_mask = 0;   // axes wrapped by the in-place layout
@@ -134,5 +140,7 @@ float fp16_scale_for_speed(float umax);
 float i16_scale_for_speed(float umax);
 // Device-side output into `dev_out` (no copy, no synchronisation).
 bool output_device(Context& ctx, OutBox box, int out_ch, float scale, float* dev_out);
+// Order stream s after the context's last equilibrium-face pre-fill.
+bool join_fill(Context& ctx, cudaStream_t s);
 
 }  // namespace aero
