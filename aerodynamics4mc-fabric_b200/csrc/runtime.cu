@@ -805,9 +805,8 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         ta.alpha = thermal_diffusivity();
         ta.faces = current_thermal_faces();
         // thermal_bfecc_active (jni.cpp:871-873); outside benchmark mode the
-        // reference also strides the update and uses a turbulent local
-        // diffusivity, which this runtime does not model (no runtime-mode
-        // nudges or fans either)
+        // update also runs every other call with dt = 2 and a local eddy
+        // diffusivity (effective_thermal_dt, effective_local_thermal_diffusivity)
         ta.bfecc = (!bench_active() || heated_cavity()) ? 1 : 0;
         ta.scratch = ctx.temperature_scratch;
         ta.dt = bench_active() ? 1.0f : 2.0f;
