@@ -89,8 +89,19 @@ __global__ void ingest_packet_kernel(const float* __restrict__ packet, int in_ch
         // transported temperature: the packet's field is the reference
         // temperature, channel 9 the source (ingest_payload, jni.cpp:1683-1693)
         out.ref_temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
-        const float src = in_ch > kChThermalSource ? p[kChThermalSource] : 0.0f;
-        out.thermal_source[cell] = clampf_dev(src, -0.006f, 0.006f);
+        float src;
+        if (in_ch > kChThermalSource) {
+            src = clampf_dev(p[kChThermalSource], -0.006f, 0.006f);
+        } else {
+            // no source channel: the fan-driven source of thermal_source_term
+            // (jni.cpp:1783-1797), rounded operation by operation
+            const float m = clampf_dev(p[1], 0.0f, 1.0f);
+            const float fx = isfinite(p[2]) ? p[2] : 0.0f, fy = isfinite(p[3]) ? p[3] : 0.0f,
+                        fz = isfinite(p[4]) ? p[4] : 0.0f;
+            const float n = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)), __fmul_rn(fz, fz)));
+            src = (m > 0.0f && n > 1e-8f) ? __fmul_rn(m, clampf_dev(__fmul_rn(n, 0.0012f), 0.0f, 0.006f)) : 0.0f;
+        }
+        out.thermal_source[cell] = src;
     } else {
         out.temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
     }

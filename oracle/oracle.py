@@ -620,6 +620,17 @@ class RefLib:
         return results
 
 
+def fan_thermal_source(pk: np.ndarray) -> np.ndarray:
+    """thermal_source_term without a source channel (native/src/aero_lbm_jni.cpp:
+    1783-1797): mask * clamp(|fan velocity| * 0.0012, 0, 0.006), in float32."""
+    m = np.minimum(np.float32(1), np.maximum(np.float32(0), pk[:, 1].astype(np.float32)))
+    m = np.where(np.isnan(pk[:, 1]), np.float32(0), m)
+    f = [np.where(np.isfinite(pk[:, c]), pk[:, c], 0).astype(np.float32) for c in (2, 3, 4)]
+    n = np.sqrt((f[0] * f[0] + f[1] * f[1]) + f[2] * f[2]).astype(np.float32)
+    capped = np.minimum(np.float32(0.006), np.maximum(np.float32(0), (n * np.float32(0.0012)).astype(np.float32)))
+    return np.where((m > 0) & (n > np.float32(1e-8)), (m * capped).astype(np.float32), np.float32(0)).astype(np.float32)
+
+
 def run_script_oracle(o: "Oracle", cfg: dict, packet: np.ndarray, script):
     """The same call list on the oracle. Actions: ("step", overlays|None) with
     overlays = (cells int32, values float32 x 6); ("cached",) a step with the
@@ -640,8 +651,13 @@ def run_script_oracle(o: "Oracle", cfg: dict, packet: np.ndarray, script):
                          pressure=pk[:, 8].reshape(n),
                          temperature=pk[:, 10].reshape(n) if pk.shape[1] > 10 else None)
             if transport:
-                o.set_thermal_source(pk[:, 9] if (pk.shape[1] > 9 and cfg.get("thermal_source", False))
-                                     else np.zeros(pk.shape[0], np.float32))
+                if not cfg.get("thermal_source", False):
+                    src = np.zeros(pk.shape[0], np.float32)
+                elif pk.shape[1] > 9:
+                    src = pk[:, 9]
+                else:
+                    src = fan_thermal_source(pk)
+                o.set_thermal_source(src)
             if cfg.get("fans", False):
                 o.set_fans(pk[:, 1], pk[:, 2], pk[:, 3], pk[:, 4])
             ov = act[1] if len(act) > 1 else None
@@ -770,7 +786,7 @@ def fan_case(n: int = 12, seed: int = 61, noise: bool = True, sponge: bool = Tru
     return cfg, pk, pre
 
 
-def runtime_case(n: int = 12, seed: int = 71, fans: bool = True):
+def runtime_case(n: int = 12, seed: int = 71, fans: bool = True, channels: int = 11):
     """Benchmark mode off (the reference's game runtime, as its brick service
     runs it): the thermal case's brick and fields with fans on 3 % of the
     fluid cells; the faces are the default config's (convective outflow)."""
@@ -779,8 +795,8 @@ def runtime_case(n: int = 12, seed: int = 71, fans: bool = True):
         pk = pk.copy()
         pk[:, 1:5] = 0.0
     cfg = {"benchmark": False, "faces": cfg["faces"], "fans": True, "thermal_transport": True,
-           "thermal_source": True}
-    return cfg, pk, pre
+           "thermal_source": True, "packet_channels": channels}
+    return cfg, np.ascontiguousarray(pk[:, :channels]), pre
 
 
 def cylinder_case(nx: int = 44, ny: int = 20, nz: int = 3, sgs: bool = True):

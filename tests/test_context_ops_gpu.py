@@ -46,7 +46,7 @@ def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mod
     cells = nx * ny * nz
     results = []
     try:
-        ctx = aero_b200.LbmContext(dims, key=key, lib=gpu)
+        ctx = aero_b200.LbmContext(dims, input_channels=pk.shape[1], key=key, lib=gpu)
         if cfg.get("benchmark", True):
             ctx.configure(lbm_cases.product_config(gpu, cfg))
         else:
@@ -332,3 +332,16 @@ def test_runtime_mode_matches_reference_golden(gpu, collision):
                 assert e["u"] <= 1e-5 and e["rho"] <= 1e-6, e
             else:
                 assert float(np.max(np.abs(a - b))) <= 1e-5
+
+
+@pytest.mark.parametrize("channels", [9, 10])
+def test_short_packets_match_oracle(gpu, channels):
+    """Runtime mode with 9- or 10-channel packets: no temperature channel, and
+    with 9 channels the temperature source derived from the fan channels."""
+    cfg, pk, pre = O.runtime_case(12, 77, True, channels)
+    script = [("step",)] * 3 + [("flow",), ("temp",)] + [("step",)] * 2 + [("flow",), ("temp",)]
+    res = run_script_gpu(gpu, (12, 12, 12), cfg, pk, script, key=910 + channels, streaming=0, temperature_state=pre)
+    o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    flags = O.results_equal(res, O.run_script_oracle(o, cfg, pk, script))
+    assert all(flags), flags

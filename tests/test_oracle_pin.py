@@ -357,3 +357,18 @@ def test_oracle_runtime_halo_matches_reference_live(every):
     for o, out, t in zip(os_, outs, ref.temperatures):
         assert _bits_equal(o.output(), out)
         assert _bits_equal(o.temperature(), t)
+
+
+@pytest.mark.skipif(not O.REF_LIB.exists(), reason="reference library not built here")
+@pytest.mark.parametrize("channels", [9, 10])
+def test_oracle_short_packets_match_reference_live(channels):
+    """Packets without the temperature channel (10) or also without the source
+    channel (9): the reference temperature is 0 and, with 9 channels, the
+    transport's source comes from the fan channels."""
+    cfg, pk, pre = O.runtime_case(12, 77, True, channels)
+    script = [("step",)] * 3 + [("flow",), ("temp",)] + [("step",)] * 2 + [("flow",), ("temp",)]
+    o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    res = O.run_script_oracle(o, cfg, pk, script)
+    ref = O.RefLib().run_script((12, 12, 12), cfg, pk, script, temperature_state=pre)
+    assert all(O.results_equal(res, ref))
