@@ -32,8 +32,8 @@ cudaError_t launch_output_ab_exact(BrickDims d, const float* g, const uint32_t* 
 
 cudaError_t ip_init_f32_exact(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, true>::init(f, a, s); }
 cudaError_t ip_fill_f32_exact(float* f, const IpArgs& a, cudaStream_t s) { return IpLaunch<StoreF32, true>::face_fill(f, a, s); }
-cudaError_t ip_step_f32_exact(float* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
-    return IpLaunch<StoreF32, true>::step(f, a, transitions, fill, s);
+cudaError_t ip_step_f32_exact(float* f, const IpArgs& a, bool transitions, cudaStream_t s) {
+    return IpLaunch<StoreF32, true>::step(f, a, transitions, s);
 }
 cudaError_t ip_output_f32_exact(const float* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out, cudaStream_t s) {
     return IpLaunch<StoreF32, true>::output(f, a, box, out_ch, scale, out, s);

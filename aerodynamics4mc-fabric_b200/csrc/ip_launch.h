@@ -9,19 +9,19 @@ namespace aero {
 enum IpVariant { kIpF32Exact = 0, kIpF32Fast = 1, kIpF16Fast = 2, kIpI16Fast = 3 };
 
 cudaError_t ip_init_f32_exact(float* f, const IpArgs& a, cudaStream_t s);
-cudaError_t ip_step_f32_exact(float* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s);
+cudaError_t ip_step_f32_exact(float* f, const IpArgs& a, bool transitions, cudaStream_t s);
 cudaError_t ip_output_f32_exact(const float* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out,
                                 cudaStream_t s);
 cudaError_t ip_init_f32_fast(float* f, const IpArgs& a, cudaStream_t s);
-cudaError_t ip_step_f32_fast(float* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s);
+cudaError_t ip_step_f32_fast(float* f, const IpArgs& a, bool transitions, cudaStream_t s);
 cudaError_t ip_output_f32_fast(const float* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out,
                                cudaStream_t s);
 cudaError_t ip_init_f16_fast(__half* f, const IpArgs& a, cudaStream_t s);
-cudaError_t ip_step_f16_fast(__half* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s);
+cudaError_t ip_step_f16_fast(__half* f, const IpArgs& a, bool transitions, cudaStream_t s);
 cudaError_t ip_output_f16_fast(const __half* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out,
                                cudaStream_t s);
 cudaError_t ip_init_i16_fast(short* f, const IpArgs& a, cudaStream_t s);
-cudaError_t ip_step_i16_fast(short* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s);
+cudaError_t ip_step_i16_fast(short* f, const IpArgs& a, bool transitions, cudaStream_t s);
 cudaError_t ip_output_i16_fast(const short* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out,
                                cudaStream_t s);
 
@@ -46,11 +46,11 @@ inline cudaError_t ip_init(int v, void* f, const IpArgs& a, cudaStream_t s) {
     if (v == kIpI16Fast) return ip_init_i16_fast(static_cast<short*>(f), a, s);
     return ip_init_f16_fast(static_cast<__half*>(f), a, s);
 }
-inline cudaError_t ip_step(int v, void* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
-    if (v == kIpF32Exact) return ip_step_f32_exact(static_cast<float*>(f), a, transitions, fill, s);
-    if (v == kIpF32Fast) return ip_step_f32_fast(static_cast<float*>(f), a, transitions, fill, s);
-    if (v == kIpI16Fast) return ip_step_i16_fast(static_cast<short*>(f), a, transitions, fill, s);
-    return ip_step_f16_fast(static_cast<__half*>(f), a, transitions, fill, s);
+inline cudaError_t ip_step(int v, void* f, const IpArgs& a, bool transitions, cudaStream_t s) {
+    if (v == kIpF32Exact) return ip_step_f32_exact(static_cast<float*>(f), a, transitions, s);
+    if (v == kIpF32Fast) return ip_step_f32_fast(static_cast<float*>(f), a, transitions, s);
+    if (v == kIpI16Fast) return ip_step_i16_fast(static_cast<short*>(f), a, transitions, s);
+    return ip_step_f16_fast(static_cast<__half*>(f), a, transitions, s);
 }
 inline cudaError_t ip_output(int v, const void* f, const IpArgs& a, OutBox box, int out_ch, float scale, float* out,
                              cudaStream_t s) {

@@ -23,12 +23,8 @@ struct IpLaunch {
         count_launch();
         return cudaGetLastError();
     }
-    static cudaError_t step(typename S::T* f, const IpArgs& a, bool transitions, bool fill, cudaStream_t s) {
+    static cudaError_t step(typename S::T* f, const IpArgs& a, bool transitions, cudaStream_t s) {
         const long long cells = (long long)a.g.nx * a.g.ny * a.g.nz;
-        if (fill) {
-            cudaError_t e = face_fill(f, a, s);
-            if (e != cudaSuccess) return e;
-        }
         step_timer_begin(s);
         // the runtime terms (fans, state nudge, sponge) exist in the one-cell kernel only
         const int cpt = a.cp.runtime_terms ? 1 : a.cells_per_thread;

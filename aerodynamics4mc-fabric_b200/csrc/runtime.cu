@@ -859,7 +859,7 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
                 a.solid_f = ctx.solid_f;
             }
             a.parity = ctx.parity;
-            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, transitions, false, s), "step_inplace")) return false;
+            if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, transitions, s), "step_inplace")) return false;
             ctx.parity ^= 1;
         }
     }
