@@ -437,6 +437,8 @@ void Context::release_device() {
     fr(ip);
     fr(reinterpret_cast<void*&>(solid_f));
     fr(reinterpret_cast<void*&>(fan_mask));
+    if (copy_done) cudaEventDestroy(copy_done);
+    copy_done = nullptr;
     if (fill_done) cudaEventDestroy(fill_done);
     if (fill_fork) cudaEventDestroy(fill_fork);
     if (fill_stream) cudaStreamDestroy(fill_stream);
@@ -747,6 +749,13 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             if (!cuda_ok(cudaMemcpyAsync(ctx.packet, packet, bytes, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync(packet)")) return false;
         }
         if (!cuda_ok(launch_ingest_packet(ctx.packet, in_ch, d, ctx.fields(new_slot), s), "ingest_packet")) return false;
+        if (host_packet) {
+            // the caller owns its packet again when the call returns: remember
+            // when the copies from host memory (a pinned buffer is read by DMA
+            // after cudaMemcpyAsync returns) have finished
+            if (!ctx.copy_done && !cuda_ok(cudaEventCreateWithFlags(&ctx.copy_done, cudaEventDisableTiming), "copy event"))
+                return false;
+        }
         if (overlays && overlays->count > 0) {
             // apply_sparse_payload_overlays (jni.cpp:1696-1721), right after the ingest
             const int n = overlays->count;
@@ -766,6 +775,7 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
                 !cuda_ok(launch_apply_overlays(ctx.overlay_cells, ctx.overlay_values, n, ctx.fields(new_slot), ctx.cells, ctx.thermal, s), "apply_overlays"))
                 return false;
         }
+        if (host_packet && !cuda_ok(cudaEventRecord(ctx.copy_done, s), "copy event")) return false;
         if (!classify(ctx, new_slot, face_now, d, s)) return false;
         ctx.has_inputs = true;
     } else if (ctx.pending_slot >= 0) {
@@ -915,6 +925,7 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     }
 
     if (out) return read_output(ctx, 1, g_cfg.output_channels, scale, out);
+    if (have_packet && host_packet && !cuda_ok(cudaEventSynchronize(ctx.copy_done), "wait for the packet copy")) return false;
     return true;
 }
 

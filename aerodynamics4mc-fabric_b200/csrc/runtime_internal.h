@@ -60,6 +60,7 @@ struct Context {
     cudaStream_t fill_stream = nullptr;
     cudaEvent_t fill_fork = nullptr, fill_done = nullptr;
     bool fill_recorded = false;
+    cudaEvent_t copy_done = nullptr;  // a call's host-to-device input copies (returned only once read)
     float* fan_mask = nullptr;  // packet fan channels, 4 x cells (mask, ux, uy, uz), while fan forcing is on  // in-place: populations of solid cells (IpArgs::solid_f), from the first mask change on
     int parity = 0;          // slot-map parity of the next in-place step
     int periodic_mask = 0;   // axes wrapped by the in-place layout
