@@ -183,6 +183,7 @@ _F32P = ctypes.POINTER(ctypes.c_float)
 _I16P = ctypes.POINTER(ctypes.c_int16)
 _U8P = ctypes.POINTER(ctypes.c_uint8)
 _I32P = ctypes.POINTER(ctypes.c_int)
+_U16P = ctypes.POINTER(ctypes.c_uint16)
 _LL = ctypes.c_longlong
 _I = ctypes.c_int
 _F = ctypes.c_float
@@ -283,6 +284,31 @@ SIGNATURES = {
     "aero_lbm_b200_adjoint_last_error": (ctypes.c_char_p, []),
     "aero_lbm_b200_adjoint_collide_vjp_host": (_I, [_I, ctypes.POINTER(AeroLbmB200AdjointConfig), ctypes.POINTER(ctypes.c_double), ctypes.c_double,
                                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    # brick-world service ABI
+    "aero_lbm_simulation_create_service": (_I, [ctypes.POINTER(_LL)]),
+    "aero_lbm_simulation_release_service": (None, [_LL]),
+    "aero_lbm_simulation_set_focus": (_I, [_LL, _I, _I, _I, _I]),
+    "aero_lbm_simulation_submit_world_deltas": (_I, [_LL, ctypes.c_void_p, _I]),
+    "aero_lbm_simulation_ensure_brick_world_runtime": (_I, [_LL, _LL, _I, _F, _F]),
+    "aero_lbm_simulation_set_brick_world_solver_mode": (_I, [_LL, _LL, _I]),
+    "aero_lbm_simulation_set_brick_world_active_hints": (_I, [_LL, _LL, _I, _I32P, _I]),
+    "aero_lbm_simulation_set_brick_world_exact_active_hints": (_I, [_LL, _LL, _I, _I32P, _I]),
+    "aero_lbm_simulation_get_brick_world_runtime_status": (_I, [_LL, _LL, _I32P, _I]),
+    "aero_lbm_simulation_step_brick_world_runtime": (_I, [_LL, _LL, _I]),
+    "aero_lbm_simulation_get_brick_world_resident_brick_count": (_I, [_LL, _LL]),
+    "aero_lbm_simulation_copy_brick_world_resident_bricks": (_I, [_LL, _LL, _I32P, _I]),
+    "aero_lbm_simulation_get_brick_world_active_brick_count": (_I, [_LL, _LL]),
+    "aero_lbm_simulation_copy_brick_world_active_bricks": (_I, [_LL, _LL, _I32P, _I]),
+    "aero_lbm_simulation_upload_brick_world_static_brick": (_I, [_LL, _LL, _I, _I, _I, _I, _U8P, _U8P, _U16P, _F32P, _U8P, _U8P]),
+    "aero_lbm_simulation_upload_brick_world_static_brick_with_sources": (
+        _I, [_LL, _LL, _I, _I, _I, _I, _U8P, _U8P, _U16P, _F32P, _U8P, _F32P, _U8P, _U8P]),
+    "aero_lbm_simulation_queue_brick_world_static_brick_upload": (_I, [_LL, _LL, _I, _I, _I, _I, _U8P, _U8P, _U16P, _F32P, _U8P, _U8P]),
+    "aero_lbm_simulation_copy_brick_world_dynamic_brick": (_I, [_LL, _LL, _I, _I, _I, _I, _F32P, _F32P, _F32P]),
+    "aero_lbm_simulation_copy_brick_world_packed_flow_atlas": (_I, [_LL, _LL, _I, _I, _I, _I, _I, _I16P, _I]),
+    "aero_lbm_simulation_upload_brick_world_dynamic_brick": (_I, [_LL, _LL, _I, _I, _I, _I, _F32P, _F32P, _F32P]),
+    "aero_lbm_simulation_upload_brick_world_boundary_reference_brick": (_I, [_LL, _LL, _I, _I, _I, _I, _F32P, _F32P, _F32P]),
+    "aero_lbm_simulation_runtime_info": (ctypes.c_char_p, []),
+    "aero_lbm_simulation_last_error": (ctypes.c_char_p, []),
     # wind-tunnel ABI
     "aero_solver_default_grid": (None, [ctypes.POINTER(AeroGridDesc)]),
     "aero_solver_default_boundary": (None, [ctypes.POINTER(AeroBoundaryDesc)]),
@@ -370,6 +396,116 @@ def declared_symbols(header: Path = HEADER_PATH) -> list[str]:
 
     text = "\n".join(l for l in header.read_text().splitlines() if not l.lstrip().startswith("#"))
     return sorted(set(re.findall(r"AERO_LBM_B200_EXPORT\s+[^;(]*?\b(\w+)\s*\(", text)))
+
+
+class AeroLbmWorldDelta(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("type", "x", "y", "z", "data0", "data1", "data2", "data3")] + \
+               [(n, ctypes.c_float) for n in ("value0", "value1", "value2", "value3")]
+
+
+def _ptr(a: np.ndarray, ctype):
+    assert a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+class BrickWorldService:
+    """The brick-world service (aero_lbm_simulation_*), what the mod's
+    NativeSimulationBridge drives: one world of equal cubic bricks keyed by
+    brick coordinates, stepped together; dynamic bricks are 4 floats per cell
+    (ux, uy, uz, pressure proxy) plus air and surface temperature; the packed
+    atlas is 4 int16 per sample."""
+
+    def __init__(self, lib: ctypes.CDLL | None = None):
+        self.lib = lib or load_library()
+        key = ctypes.c_longlong(0)
+        self._ok(self.lib.aero_lbm_simulation_create_service(ctypes.byref(key)))
+        self.key = key.value
+
+    def _ok(self, v):
+        if not v:
+            raise RuntimeError(self.error())
+        return v
+
+    def error(self) -> str:
+        m = self.lib.aero_lbm_simulation_last_error()
+        return m.decode("utf-8", "replace") if m else ""
+
+    def ensure_world(self, world: int, brick_size: int, dx: float = 1.0, dt: float = 0.05, solver_mode: int = 1):
+        self._ok(self.lib.aero_lbm_simulation_ensure_brick_world_runtime(self.key, world, brick_size, dx, dt))
+        self._ok(self.lib.aero_lbm_simulation_set_brick_world_solver_mode(self.key, world, solver_mode))
+        self.n = brick_size
+
+    def set_hints(self, world: int, coords, exact: bool = True):
+        c = np.ascontiguousarray(np.asarray(coords, np.int32).reshape(-1))
+        fn = self.lib.aero_lbm_simulation_set_brick_world_exact_active_hints if exact \
+            else self.lib.aero_lbm_simulation_set_brick_world_active_hints
+        self._ok(fn(self.key, world, self.n, _ptr(c, ctypes.c_int), c.size // 3))
+
+    def upload_static(self, world: int, coord, obstacle, surface_kind=None, open_face_mask=None, emitter=None,
+                      source_fan=None, source_emitter=None):
+        cells = self.n ** 3
+        ob = np.ascontiguousarray(np.asarray(obstacle, np.uint8).reshape(-1))
+        sk = np.ascontiguousarray(np.zeros(cells, np.uint8) if surface_kind is None else np.asarray(surface_kind, np.uint8).reshape(-1))
+        of = np.ascontiguousarray(np.zeros(cells, np.uint16) if open_face_mask is None else np.asarray(open_face_mask, np.uint16).reshape(-1))
+        em = np.ascontiguousarray(np.zeros(cells, np.float32) if emitter is None else np.asarray(emitter, np.float32).reshape(-1))
+        faces = np.zeros(cells * 6, np.uint8)
+        sf = None if source_fan is None else np.ascontiguousarray(np.asarray(source_fan, np.uint8).reshape(-1))
+        se = None if source_emitter is None else np.ascontiguousarray(np.asarray(source_emitter, np.float32).reshape(-1))
+        self._ok(self.lib.aero_lbm_simulation_upload_brick_world_static_brick_with_sources(
+            self.key, world, self.n, *coord, _ptr(ob, ctypes.c_uint8), _ptr(sk, ctypes.c_uint8), _ptr(of, ctypes.c_uint16),
+            _ptr(em, ctypes.c_float), None if sf is None else _ptr(sf, ctypes.c_uint8),
+            None if se is None else _ptr(se, ctypes.c_float), _ptr(faces, ctypes.c_uint8), _ptr(faces, ctypes.c_uint8)))
+
+    def _dynamic_args(self, flow, air, surface):
+        cells = self.n ** 3
+        f = np.ascontiguousarray(np.asarray(flow, np.float32).reshape(-1))
+        a = np.ascontiguousarray(np.asarray(air, np.float32).reshape(-1))
+        s = np.ascontiguousarray(np.zeros(cells, np.float32) if surface is None else np.asarray(surface, np.float32).reshape(-1))
+        return f, a, s
+
+    def upload_dynamic(self, world: int, coord, flow, air, surface=None):
+        f, a, s = self._dynamic_args(flow, air, surface)
+        self._ok(self.lib.aero_lbm_simulation_upload_brick_world_dynamic_brick(self.key, world, self.n, *coord, fptr(f), fptr(a), fptr(s)))
+
+    def upload_reference(self, world: int, coord, flow, air, surface=None):
+        f, a, s = self._dynamic_args(flow, air, surface)
+        self._ok(self.lib.aero_lbm_simulation_upload_brick_world_boundary_reference_brick(
+            self.key, world, self.n, *coord, fptr(f), fptr(a), fptr(s)))
+
+    def submit_deltas(self, deltas):
+        arr = (AeroLbmWorldDelta * len(deltas))(*[AeroLbmWorldDelta(*d) for d in deltas])
+        self._ok(self.lib.aero_lbm_simulation_submit_world_deltas(self.key, ctypes.cast(arr, ctypes.c_void_p), len(deltas)))
+
+    def step(self, world: int, steps: int = 1):
+        self._ok(self.lib.aero_lbm_simulation_step_brick_world_runtime(self.key, world, steps))
+
+    def atlas(self, world: int, coord, stride: int = 4, out: np.ndarray | None = None) -> np.ndarray:
+        res = (self.n + stride - 1) // stride
+        out = np.zeros(res ** 3 * 4, np.int16) if out is None else out
+        self._ok(self.lib.aero_lbm_simulation_copy_brick_world_packed_flow_atlas(
+            self.key, world, self.n, *coord, stride, out.ctypes.data_as(_I16P), out.size))
+        return out
+
+    def dynamic(self, world: int, coord):
+        cells = self.n ** 3
+        f = np.zeros(cells * 4, np.float32)
+        a = np.zeros(cells, np.float32)
+        s = np.zeros(cells, np.float32)
+        self._ok(self.lib.aero_lbm_simulation_copy_brick_world_dynamic_brick(self.key, world, self.n, *coord, fptr(f), fptr(a), fptr(s)))
+        return f.reshape(-1, 4), a, s
+
+    def status(self, world: int) -> np.ndarray:
+        st = np.zeros(8, np.int32)
+        self._ok(self.lib.aero_lbm_simulation_get_brick_world_runtime_status(self.key, world, _ptr(st, ctypes.c_int), 8))
+        return st
+
+    def runtime_info(self) -> str:
+        return self.lib.aero_lbm_simulation_runtime_info().decode()
+
+    def release(self):
+        if self.key:
+            self.lib.aero_lbm_simulation_release_service(self.key)
+            self.key = 0
 
 
 class LbmContext:

@@ -65,46 +65,12 @@ bool step_timer_read(double* total_ms, int* launches) {
 }
 
 // ---------------------------------------------------------------- ingest
-// Packet semantics of ingest_payload (native/src/aero_lbm_jni.cpp:1671-1694).
+// Packet semantics of ingest_payload (native/src/aero_lbm_jni.cpp:1671-1694),
+// per cell in ingest_cell (d3q27_kernels.cuh).
 __global__ void ingest_packet_kernel(const float* __restrict__ packet, int in_ch, long long cells, CellFields out) {
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= cells) return;
-    const float* p = packet + cell * in_ch;
-    const float ob = p[kChObstacle];
-    out.obstacle[cell] = ob > 0.5f ? 1 : 0;
-    const float vx = p[kChStateVx], vy = p[kChStateVy], vz = p[kChStateVz];
-    out.ref_ux[cell] = isfinite(vx) ? vx : 0.0f;
-    out.ref_uy[cell] = isfinite(vy) ? vy : 0.0f;
-    out.ref_uz[cell] = isfinite(vz) ? vz : 0.0f;
-    out.ref_p[cell] = clampf_dev(p[kChStateP], -0.03f, 0.03f);
-    if (out.fan_mask) {
-        // ingest_payload's fan channels (jni.cpp:1674-1678)
-        out.fan_mask[cell] = clampf_dev(p[1], 0.0f, 1.0f);
-        out.fan_ux[cell] = isfinite(p[2]) ? p[2] : 0.0f;
-        out.fan_uy[cell] = isfinite(p[3]) ? p[3] : 0.0f;
-        out.fan_uz[cell] = isfinite(p[4]) ? p[4] : 0.0f;
-    }
-    const float t = in_ch > kChStateTemp ? p[kChStateTemp] : 0.0f;
-    if (out.ref_temperature) {
-        // transported temperature: the packet's field is the reference
-        // temperature, channel 9 the source (ingest_payload, jni.cpp:1683-1693)
-        out.ref_temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
-        float src;
-        if (in_ch > kChThermalSource) {
-            src = clampf_dev(p[kChThermalSource], -0.006f, 0.006f);
-        } else {
-            // no source channel: the fan-driven source of thermal_source_term
-            // (jni.cpp:1783-1797), rounded operation by operation
-            const float m = clampf_dev(p[1], 0.0f, 1.0f);
-            const float fx = isfinite(p[2]) ? p[2] : 0.0f, fy = isfinite(p[3]) ? p[3] : 0.0f,
-                        fz = isfinite(p[4]) ? p[4] : 0.0f;
-            const float n = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)), __fmul_rn(fz, fz)));
-            src = (m > 0.0f && n > 1e-8f) ? __fmul_rn(m, clampf_dev(__fmul_rn(n, 0.0012f), 0.0f, 0.006f)) : 0.0f;
-        }
-        out.thermal_source[cell] = src;
-    } else {
-        out.temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
-    }
+    ingest_cell(packet + cell * in_ch, in_ch, cell, out);
 }
 
 cudaError_t launch_ingest_packet(const float* packet, int in_channels, BrickDims d, CellFields out, cudaStream_t stream) {
@@ -112,6 +78,30 @@ cudaError_t launch_ingest_packet(const float* packet, int in_channels, BrickDims
     const int block = 256;
     const long long grid = (d.cells + block - 1) / block;
     ingest_packet_kernel<<<(unsigned)grid, block, 0, stream>>>(packet, in_channels, d.cells, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Largest reference speed over fluid cells (the per-brick 16-bit storage
+// scale of a context whose first inputs were built on the device). Non-
+// negative floats order like their bit patterns, so an integer max suffices.
+__global__ void max_fluid_speed_kernel(CellFields f, long long cells, unsigned int* out_bits) {
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float s = 0.0f;
+    if (cell < cells && f.obstacle[cell] == 0) {
+        const float ux = f.ref_ux[cell], uy = f.ref_uy[cell], uz = f.ref_uz[cell];
+        const float s2 = ux * ux + uy * uy + uz * uz;
+        if (isfinite(s2)) s = sqrtf(s2);
+    }
+    for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_xor_sync(0xffffffffu, s, o));
+    if ((threadIdx.x & 31) == 0 && s > 0.0f) atomicMax(out_bits, __float_as_uint(s));
+}
+
+cudaError_t launch_max_fluid_speed(CellFields f, long long cells, unsigned int* out_bits, cudaStream_t stream) {
+    if (cells <= 0) return cudaSuccess;
+    const int block = 256;
+    const long long grid = (cells + block - 1) / block;
+    max_fluid_speed_kernel<<<(unsigned)grid, block, 0, stream>>>(f, cells, out_bits);
     count_launch();
     return cudaGetLastError();
 }

@@ -88,6 +88,56 @@ __device__ __forceinline__ void record_u(const CellFields& c, long long cell, fl
     c.u_last[2 * c.cells + cell] = uz;
 }
 
+// One cell of ingest_payload (native/src/aero_lbm_jni.cpp:1671-1694): the
+// packet's in_ch channels of this cell (p) into the per-cell fields. Shared by
+// the packet ingest kernel and kernels that build a call's inputs on the
+// device, so both sanitise and clamp identically.
+__device__ __forceinline__ void ingest_cell(const float* p, int in_ch, long long cell, const CellFields& out) {
+    const float ob = p[kChObstacle];
+    out.obstacle[cell] = ob > 0.5f ? 1 : 0;
+    const float vx = p[kChStateVx], vy = p[kChStateVy], vz = p[kChStateVz];
+    out.ref_ux[cell] = isfinite(vx) ? vx : 0.0f;
+    out.ref_uy[cell] = isfinite(vy) ? vy : 0.0f;
+    out.ref_uz[cell] = isfinite(vz) ? vz : 0.0f;
+    out.ref_p[cell] = clampf_dev(p[kChStateP], -0.03f, 0.03f);
+    if (out.fan_mask) {
+        // ingest_payload's fan channels (jni.cpp:1674-1678)
+        out.fan_mask[cell] = clampf_dev(p[1], 0.0f, 1.0f);
+        out.fan_ux[cell] = isfinite(p[2]) ? p[2] : 0.0f;
+        out.fan_uy[cell] = isfinite(p[3]) ? p[3] : 0.0f;
+        out.fan_uz[cell] = isfinite(p[4]) ? p[4] : 0.0f;
+    }
+    const float t = in_ch > kChStateTemp ? p[kChStateTemp] : 0.0f;
+    if (out.ref_temperature) {
+        // transported temperature: the packet's field is the reference
+        // temperature, channel 9 the source (ingest_payload, jni.cpp:1683-1693)
+        out.ref_temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
+        float src;
+        if (in_ch > kChThermalSource) {
+            src = clampf_dev(p[kChThermalSource], -0.006f, 0.006f);
+        } else {
+            // no source channel: the fan-driven source of thermal_source_term
+            // (jni.cpp:1783-1797), rounded operation by operation
+            const float m = clampf_dev(p[1], 0.0f, 1.0f);
+            const float fx = isfinite(p[2]) ? p[2] : 0.0f, fy = isfinite(p[3]) ? p[3] : 0.0f,
+                        fz = isfinite(p[4]) ? p[4] : 0.0f;
+            const float n = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)), __fmul_rn(fz, fz)));
+            src = (m > 0.0f && n > 1e-8f) ? __fmul_rn(m, clampf_dev(__fmul_rn(n, 0.0012f), 0.0f, 0.006f)) : 0.0f;
+        }
+        out.thermal_source[cell] = src;
+    } else {
+        out.temperature[cell] = clampf_dev(t, -1.0f, 1.0f);
+    }
+}
+
+// A kernel that writes one call's inputs straight into a context's per-cell
+// fields (in place of a host packet's copy and ingest_packet_kernel): the
+// device-resident brick service builds its packets this way.
+struct DeviceFill {
+    cudaError_t (*launch)(const CellFields& out, const BrickDims& d, cudaStream_t s, void* user);
+    void* user;
+};
+
 struct ForceField {
     const float* fx;      // optional per-cell force density (SoA); null = none
     const float* fy;
@@ -109,6 +159,9 @@ inline OutBox strided_box(int nx, int ny, int nz, int stride) {
 
 // Launch helpers (all asynchronous on `stream`; return the launch error).
 cudaError_t launch_ingest_packet(const float* packet, int in_channels, BrickDims d, CellFields out, cudaStream_t stream);
+// Largest |u| of the fluid cells' reference velocity (fields after an ingest),
+// as float bits into *out_bits (cleared first by the caller).
+cudaError_t launch_max_fluid_speed(CellFields f, long long cells, unsigned int* out_bits, cudaStream_t stream);
 cudaError_t launch_build_flags(const uint8_t* obstacle, BrickDims d, FaceParams face, uint32_t* flags, cudaStream_t stream);
 // *_exact: reference-order collision (bit-identical to the reference CPU step);
 // *_fast: factorised collision (agrees to FP32 rounding).

@@ -603,7 +603,7 @@ float i16_scale_for_speed(float umax) {
 }
 
 // First step of a context: pick the layout, the in-place variant and allocate.
-static bool choose_layout(Context& ctx, const FaceParams& face, const float* packet, bool host_packet) {
+static bool choose_layout(Context& ctx, const FaceParams& face, const float* packet, bool host_packet, int in_slot) {
     const bool local = inplace_faces_ok(face);
     const bool want_fp16 = g_realtime_solver_mode == AERO_LBM_REALTIME_SOLVER_D3Q27_FP16_INPLACE_EXPERIMENTAL;
     int layout = 0;
@@ -653,6 +653,22 @@ static bool choose_layout(Context& ctx, const FaceParams& face, const float* pac
                 const float s2 = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
                 if (std::isfinite(s2)) umax = std::max(umax, std::sqrt(s2));
             }
+        } else if (ctx.has_inputs) {
+            // inputs that live on the device (a device packet or a device
+            // build): the largest reference speed of the ingested fluid cells
+            cudaStream_t s = current_stream();
+            unsigned int* d_bits = nullptr;
+            unsigned int bits = 0;
+            const bool ok = cuda_ok(cudaMalloc(reinterpret_cast<void**>(&d_bits), sizeof(unsigned int)), "cudaMalloc(max speed)") &&
+                            cuda_ok(cudaMemsetAsync(d_bits, 0, sizeof(unsigned int), s), "cudaMemset(max speed)") &&
+                            cuda_ok(launch_max_fluid_speed(ctx.fields(in_slot), ctx.cells, d_bits, s), "max speed") &&
+                            cuda_ok(cudaMemcpyAsync(&bits, d_bits, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "copy max speed") &&
+                            cuda_ok(cudaStreamSynchronize(s), "sync max speed");
+            if (d_bits) cudaFree(d_bits);
+            if (!ok) return false;
+            float dev_umax = 0.0f;
+            std::memcpy(&dev_umax, &bits, sizeof(float));
+            if (std::isfinite(dev_umax)) umax = std::max(umax, dev_umax);
         }
         ctx.fp16_scale = ctx.ip_variant == kIpI16Fast ? i16_scale_for_speed(umax) : fp16_scale_for_speed(umax);
     }
@@ -702,7 +718,7 @@ static float thermal_diffusivity() {
 
 // One step of a context. packet may be null (cached step); out may be null.
 bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet,
-                  const SparseOverlays* overlays) {
+                  const SparseOverlays* overlays, const DeviceFill* fill) {
     cudaStream_t s = current_stream();
     const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
     const FaceParams face_now = current_face_params();
@@ -725,7 +741,8 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     ctx.thermal = g_thermal_mode == 1 || (g_thermal_mode == -1 && cp.enable_buoyancy);
     if (ctx.thermal && !ensure_thermal(ctx)) return false;
     const int in_ch = g_cfg.input_channels;
-    const bool have_packet = packet != nullptr;
+    const bool have_packet = packet != nullptr || fill != nullptr;
+    if (fill) host_packet = false;
     if (!have_packet && !ctx.has_inputs) {
         set_error("cached step requested before any packet was uploaded for this context");
         return false;
@@ -736,19 +753,24 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     if (have_packet) {
         new_slot = ctx.initialized ? 1 - ctx.slot : ctx.slot;
         const size_t bytes = (size_t)ctx.cells * in_ch * sizeof(float);
-        if (ctx.packet_cap < bytes) {
-            if (ctx.packet) cudaFree(ctx.packet);
-            ctx.packet = nullptr;
-            ctx.packet_cap = 0;
-            if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.packet), bytes), "cudaMalloc(packet)")) return false;
-            ctx.packet_cap = bytes;
-        }
-        if (host_packet) {
-            if (!cuda_ok(cudaMemcpyAsync(ctx.packet, packet, bytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(packet)")) return false;
+        if (fill) {
+            // the inputs are built on the device straight into the fields
+            if (!cuda_ok(fill->launch(ctx.fields(new_slot), d, s, fill->user), "device input fill")) return false;
         } else {
-            if (!cuda_ok(cudaMemcpyAsync(ctx.packet, packet, bytes, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync(packet)")) return false;
+            if (ctx.packet_cap < bytes) {
+                if (ctx.packet) cudaFree(ctx.packet);
+                ctx.packet = nullptr;
+                ctx.packet_cap = 0;
+                if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.packet), bytes), "cudaMalloc(packet)")) return false;
+                ctx.packet_cap = bytes;
+            }
+            if (host_packet) {
+                if (!cuda_ok(cudaMemcpyAsync(ctx.packet, packet, bytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(packet)")) return false;
+            } else {
+                if (!cuda_ok(cudaMemcpyAsync(ctx.packet, packet, bytes, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync(packet)")) return false;
+            }
+            if (!cuda_ok(launch_ingest_packet(ctx.packet, in_ch, d, ctx.fields(new_slot), s), "ingest_packet")) return false;
         }
-        if (!cuda_ok(launch_ingest_packet(ctx.packet, in_ch, d, ctx.fields(new_slot), s), "ingest_packet")) return false;
         if (host_packet) {
             // the caller owns its packet again when the call returns: remember
             // when the copies from host memory (a pinned buffer is read by DMA
@@ -792,7 +814,7 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         if (!classify(ctx, new_slot, face_now, d, s)) return false;
     }
 
-    if (!ctx.initialized && !choose_layout(ctx, face_now, packet, host_packet)) return false;
+    if (!ctx.initialized && !choose_layout(ctx, face_now, packet, host_packet, new_slot)) return false;
     if (ctx.thermal) {
         if (!ctx.initialized) {
             const ThermalInitArgs ti{ctx.cells, ctx.temperature, ctx.u_last, ctx.obstacle[new_slot], ctx.ref_temperature,
@@ -1069,6 +1091,28 @@ bool step_impl(const float* packet, int nx, int ny, int nz, long long key, float
 }
 
 }  // namespace
+
+bool aero::step_rect_device(long long key, int nx, int ny, int nz, const DeviceFill& fill) {
+    const auto t0 = Clock::now();
+    clear_error();
+    if (!g_cfg.initialized) {
+        set_error("native_step_raw_dims: runtime not initialized");
+        return false;
+    }
+    if (nx <= 0 || ny <= 0 || nz <= 0) {
+        set_error("native_step_raw_dims: invalid dimensions");
+        return false;
+    }
+    Context* ctx = get_or_create_context(key, nx, ny, nz);
+    if (!ctx) {
+        if (g_last_error.empty()) set_error("native_step_raw_dims: failed to allocate or acquire context");
+        return false;
+    }
+    const bool ok = step_context(*ctx, nullptr, nullptr, 1.0f, false, nullptr, &fill);
+    if (!ok && g_last_error.empty()) set_error("native_step_raw_dims: step failed");
+    record_timing(0.0, 0.0, 0.0, ms_since(t0), false);
+    return ok;
+}
 
 extern "C" {
 

@@ -133,8 +133,14 @@ struct SparseOverlays {
     const float* values;
     int count;
 };
+// One call of a context. packet: the call's input packet (host or device
+// memory, host_packet saying which), or null for a cached call; fill (optional)
+// builds the call's inputs on the device instead of a packet.
 bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet,
-                  const SparseOverlays* overlays = nullptr);
+                  const SparseOverlays* overlays = nullptr, const DeviceFill* fill = nullptr);
+// aero_lbm_step_rect for a call whose inputs `fill` builds on the device:
+// the same context lookup / creation, checks and timing record; no output.
+bool step_rect_device(long long key, int nx, int ny, int nz, const DeviceFill& fill);
 bool read_output(Context& ctx, int stride, int out_ch, float scale, float* host_out);
 // Per-brick FP16 deviation scale for a brick whose speed stays below umax.
 float fp16_scale_for_speed(float umax);

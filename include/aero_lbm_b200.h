@@ -507,6 +507,107 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_collide_vjp_host(int precision, c
                                                                 const double* cell_force, const double* lam_out,
                                                                 double* f_out, double* lam_in, double* lam_force);
 
+/* ---- brick-world service ABI (native/include/aero_lbm_capi.h:151-164, 303-466, 695-696;
+ * implemented by native/src/aero_lbm_simulation_bridge.cpp:4562-5535, 6866-7022) ----
+ * The entry points the mod's ClientL2Solver reaches through JNI. One service
+ * (key 1) holds brick worlds keyed by the caller; each world has one brick
+ * size, its bricks are keyed by brick coordinates. Brick state lives on the
+ * device between ticks: a tick builds each brick's inputs and refreshes its
+ * dynamic state with kernels, and reads back one flag word per brick; the
+ * packed atlas is quantised on the device. Regions (server L2), nested
+ * feedback, atlases by key and the analysis codec are not part of this
+ * library. Return convention as the reference: 1 ok, 0 error (message by
+ * aero_lbm_simulation_last_error), counts -1 on error. */
+typedef struct AeroLbmWorldDelta {
+    int type;
+    int x;
+    int y;
+    int z;
+    int data0;
+    int data1;
+    int data2;
+    int data3;
+    float value0;
+    float value1;
+    float value2;
+    float value3;
+} AeroLbmWorldDelta;
+
+/* capi.h:303-304 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_create_service(long long* out_service_key);
+AERO_LBM_B200_EXPORT void aero_lbm_simulation_release_service(long long service_key);
+/* capi.h:305-311 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_set_focus(long long service_key, int block_x, int block_y, int block_z,
+                                                       int radius_blocks);
+/* capi.h:312-316: brick deltas (types 1-5, 8 cell patch, 9 queued upload, 10
+ * source patch) apply at the world's next step; type 6 drops the world */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_submit_world_deltas(long long service_key, const AeroLbmWorldDelta* deltas,
+                                                                 int delta_count);
+/* capi.h:317-323 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_ensure_brick_world_runtime(long long service_key, long long world_key,
+                                                                        int brick_size, float dx_meters, float dt_seconds);
+/* capi.h:324-328 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_set_brick_world_solver_mode(long long service_key, long long world_key,
+                                                                         int solver_mode);
+/* capi.h:329-342 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_set_brick_world_active_hints(long long service_key, long long world_key,
+                                                                          int brick_size, const int* brick_coords,
+                                                                          int brick_count);
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_set_brick_world_exact_active_hints(long long service_key, long long world_key,
+                                                                                int brick_size, const int* brick_coords,
+                                                                                int brick_count);
+/* capi.h:343-348: status[8] = brick size, bricks, hinted, active,
+ * geometry-dirty, forcing-dirty, pending re-init, epoch */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_get_brick_world_runtime_status(long long service_key, long long world_key,
+                                                                            int* out_status, int status_count);
+/* capi.h:349-353 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_step_brick_world_runtime(long long service_key, long long world_key,
+                                                                      int step_count);
+/* capi.h:354-373 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_get_brick_world_resident_brick_count(long long service_key, long long world_key);
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_copy_brick_world_resident_bricks(long long service_key, long long world_key,
+                                                                              int* out_coords, int brick_capacity);
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_get_brick_world_active_brick_count(long long service_key, long long world_key);
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_copy_brick_world_active_bricks(long long service_key, long long world_key,
+                                                                            int* out_coords, int brick_capacity);
+/* capi.h:374-417 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_upload_brick_world_static_brick(
+    long long service_key, long long world_key, int brick_size, int brick_x, int brick_y, int brick_z,
+    const uint8_t* obstacle, const uint8_t* surface_kind, const uint16_t* open_face_mask, const float* emitter_power_watts,
+    const uint8_t* face_sky_exposure, const uint8_t* face_direct_exposure);
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_upload_brick_world_static_brick_with_sources(
+    long long service_key, long long world_key, int brick_size, int brick_x, int brick_y, int brick_z,
+    const uint8_t* obstacle, const uint8_t* surface_kind, const uint16_t* open_face_mask, const float* emitter_power_watts,
+    const uint8_t* source_fan_dir, const float* source_emitter_power_watts, const uint8_t* face_sky_exposure,
+    const uint8_t* face_direct_exposure);
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_queue_brick_world_static_brick_upload(
+    long long service_key, long long world_key, int brick_size, int brick_x, int brick_y, int brick_z,
+    const uint8_t* obstacle, const uint8_t* surface_kind, const uint16_t* open_face_mask, const float* emitter_power_watts,
+    const uint8_t* face_sky_exposure, const uint8_t* face_direct_exposure);
+/* capi.h:435-456 */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_copy_brick_world_dynamic_brick(long long service_key, long long world_key,
+                                                                            int brick_size, int brick_x, int brick_y,
+                                                                            int brick_z, float* out_flow_state,
+                                                                            float* out_air_temperature,
+                                                                            float* out_surface_temperature);
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_copy_brick_world_packed_flow_atlas(long long service_key, long long world_key,
+                                                                                int brick_size, int brick_x, int brick_y,
+                                                                                int brick_z, int sample_stride,
+                                                                                int16_t* out_packed_flow,
+                                                                                int packed_value_count);
+/* capi.h:457-466 (dynamic upload: simulation_bridge.cpp:5412-5477) */
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_upload_brick_world_dynamic_brick(long long service_key, long long world_key,
+                                                                              int brick_size, int brick_x, int brick_y,
+                                                                              int brick_z, const float* flow_state,
+                                                                              const float* air_temperature,
+                                                                              const float* surface_temperature);
+AERO_LBM_B200_EXPORT int aero_lbm_simulation_upload_brick_world_boundary_reference_brick(
+    long long service_key, long long world_key, int brick_size, int brick_x, int brick_y, int brick_z,
+    const float* flow_state, const float* air_temperature, const float* surface_temperature);
+/* capi.h:695-696 */
+AERO_LBM_B200_EXPORT const char* aero_lbm_simulation_runtime_info(void);
+AERO_LBM_B200_EXPORT const char* aero_lbm_simulation_last_error(void);
+
 /* ---- wind-tunnel ABI (native/include/aero_solver_capi.h:1-115) ---- */
 enum {
     AERO_SOLVER_ABI_VERSION = 1,

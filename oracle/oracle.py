@@ -919,6 +919,201 @@ class BrickService:
             lib.aero_lbm_simulation_release_service(svc)
 
 
+class WorldDelta(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("type", "x", "y", "z", "data0", "data1", "data2", "data3")] + \
+               [(n, ctypes.c_float) for n in ("value0", "value1", "value2", "value3")]
+
+
+def run_brick_script(path: Path, script: list) -> list:
+    """Run a list of brick-world service operations through the C ABI of the
+    library at ``path`` (the reference's service, or any library exporting
+    aero_lbm_simulation_*) and return what the reading operations returned, in
+    order. Operations (tuples): ("ensure", world, n, dx, dt), ("mode", world,
+    m), ("hints", world, n, coords, exact), ("static", world, n, coord,
+    obstacle, surface_kind, open_faces, emitter, source_fan|None,
+    source_emitter|None), ("queue_static", world, n, coord, obstacle,
+    surface_kind, open_faces, emitter), ("dynamic" | "reference", world, n,
+    coord, flow, air, surface), ("deltas", [12-tuples]), ("step", world,
+    count), ("atlas", world, n, coord, stride), ("copy", world, n, coord),
+    ("status", world), ("coords", world, resident). Every operation's return
+    code is recorded too, so failures must match as well."""
+    lib = ctypes.CDLL(str(path))
+    vp, i, ll, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_float
+    sig = {
+        "aero_lbm_simulation_create_service": [vp],
+        "aero_lbm_simulation_ensure_brick_world_runtime": [ll, ll, i, f, f],
+        "aero_lbm_simulation_set_brick_world_solver_mode": [ll, ll, i],
+        "aero_lbm_simulation_set_brick_world_active_hints": [ll, ll, i, vp, i],
+        "aero_lbm_simulation_set_brick_world_exact_active_hints": [ll, ll, i, vp, i],
+        "aero_lbm_simulation_upload_brick_world_static_brick_with_sources": [ll, ll, i, i, i, i] + [vp] * 8,
+        "aero_lbm_simulation_queue_brick_world_static_brick_upload": [ll, ll, i, i, i, i] + [vp] * 6,
+        "aero_lbm_simulation_upload_brick_world_dynamic_brick": [ll, ll, i, i, i, i, vp, vp, vp],
+        "aero_lbm_simulation_upload_brick_world_boundary_reference_brick": [ll, ll, i, i, i, i, vp, vp, vp],
+        "aero_lbm_simulation_submit_world_deltas": [ll, vp, i],
+        "aero_lbm_simulation_step_brick_world_runtime": [ll, ll, i],
+        "aero_lbm_simulation_copy_brick_world_packed_flow_atlas": [ll, ll, i, i, i, i, i, vp, i],
+        "aero_lbm_simulation_copy_brick_world_dynamic_brick": [ll, ll, i, i, i, i, vp, vp, vp],
+        "aero_lbm_simulation_get_brick_world_runtime_status": [ll, ll, vp, i],
+        "aero_lbm_simulation_get_brick_world_resident_brick_count": [ll, ll],
+        "aero_lbm_simulation_get_brick_world_active_brick_count": [ll, ll],
+        "aero_lbm_simulation_copy_brick_world_resident_bricks": [ll, ll, vp, i],
+        "aero_lbm_simulation_copy_brick_world_active_bricks": [ll, ll, vp, i],
+    }
+    for name, args in sig.items():
+        getattr(lib, name).argtypes = args
+        getattr(lib, name).restype = ctypes.c_int
+    lib.aero_lbm_simulation_release_service.argtypes = [ll]
+    lib.aero_lbm_simulation_last_error.restype = ctypes.c_char_p
+    key = ctypes.c_longlong(0)
+    assert lib.aero_lbm_simulation_create_service(ctypes.byref(key)) == 1
+    svc = key.value
+    keep, out = [], []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(np.asarray(a, dt).reshape(-1))
+        keep.append(a)
+        return a.ctypes.data
+
+    try:
+        for op in script:
+            kind = op[0]
+            if kind == "ensure":
+                out.append(("rc", lib.aero_lbm_simulation_ensure_brick_world_runtime(svc, *op[1:])))
+            elif kind == "mode":
+                out.append(("rc", lib.aero_lbm_simulation_set_brick_world_solver_mode(svc, op[1], op[2])))
+            elif kind == "hints":
+                _, w, n, coords, exact = op
+                fn = lib.aero_lbm_simulation_set_brick_world_exact_active_hints if exact else \
+                    lib.aero_lbm_simulation_set_brick_world_active_hints
+                out.append(("rc", fn(svc, w, n, arr(coords, np.int32), len(coords))))
+            elif kind in ("static", "queue_static"):
+                w, n, c = op[1], op[2], op[3]
+                cells = n ** 3
+                faces = arr(np.zeros(cells * 6, np.uint8), np.uint8)
+                ob, sk, of, em = arr(op[4], np.uint8), arr(op[5], np.uint8), arr(op[6], np.uint16), arr(op[7], np.float32)
+                if kind == "static":
+                    sf = None if op[8] is None else arr(op[8], np.uint8)
+                    se = None if op[9] is None else arr(op[9], np.float32)
+                    out.append(("rc", lib.aero_lbm_simulation_upload_brick_world_static_brick_with_sources(
+                        svc, w, n, *c, ob, sk, of, em, sf, se, faces, faces)))
+                else:
+                    out.append(("rc", lib.aero_lbm_simulation_queue_brick_world_static_brick_upload(
+                        svc, w, n, *c, ob, sk, of, em, faces, faces)))
+            elif kind in ("dynamic", "reference"):
+                w, n, c, fl, air, sf = op[1:]
+                fn = lib.aero_lbm_simulation_upload_brick_world_dynamic_brick if kind == "dynamic" else \
+                    lib.aero_lbm_simulation_upload_brick_world_boundary_reference_brick
+                out.append(("rc", fn(svc, w, n, *c, arr(fl, np.float32), arr(air, np.float32), arr(sf, np.float32))))
+            elif kind == "deltas":
+                ds = (WorldDelta * len(op[1]))(*[WorldDelta(*d) for d in op[1]])
+                keep.append(ds)
+                out.append(("rc", lib.aero_lbm_simulation_submit_world_deltas(svc, ctypes.addressof(ds), len(op[1]))))
+            elif kind == "step":
+                rc = lib.aero_lbm_simulation_step_brick_world_runtime(svc, op[1], op[2])
+                out.append(("step", rc, b"" if rc else lib.aero_lbm_simulation_last_error()))
+            elif kind == "atlas":
+                w, n, c, stride = op[1:]
+                res = (n + stride - 1) // stride
+                a = np.zeros(res ** 3 * 4, np.int16)
+                rc = lib.aero_lbm_simulation_copy_brick_world_packed_flow_atlas(svc, w, n, *c, stride, a.ctypes.data, a.size)
+                out.append(("atlas", rc, a))
+            elif kind == "copy":
+                w, n, c = op[1:]
+                cells = n ** 3
+                fl, air, sf = np.zeros(cells * 4, np.float32), np.zeros(cells, np.float32), np.zeros(cells, np.float32)
+                rc = lib.aero_lbm_simulation_copy_brick_world_dynamic_brick(svc, w, n, *c, fl.ctypes.data, air.ctypes.data,
+                                                                            sf.ctypes.data)
+                out.append(("copy", rc, fl, air, sf))
+            elif kind == "status":
+                st = np.zeros(8, np.int32)
+                rc = lib.aero_lbm_simulation_get_brick_world_runtime_status(svc, op[1], st.ctypes.data, 8)
+                out.append(("status", rc, st))
+            elif kind == "coords":
+                w, resident = op[1], op[2]
+                cnt = (lib.aero_lbm_simulation_get_brick_world_resident_brick_count if resident else
+                       lib.aero_lbm_simulation_get_brick_world_active_brick_count)(svc, w)
+                buf = np.zeros(max(cnt, 0) * 3, np.int32)
+                got = (lib.aero_lbm_simulation_copy_brick_world_resident_bricks if resident else
+                       lib.aero_lbm_simulation_copy_brick_world_active_bricks)(svc, w, buf.ctypes.data, max(cnt, 0))
+                rows = sorted(map(tuple, buf.reshape(-1, 3).tolist()))
+                out.append(("coords", cnt, got, rows))
+            else:
+                raise ValueError(kind)
+    finally:
+        lib.aero_lbm_simulation_release_service(svc)
+    return out
+
+
+def brick_world_rich_script(n: int = 12, seed: int = 57) -> list:
+    """A brick-world session exercising the service's bookkeeping around the
+    step: an L-shaped set of bricks (one not hinted), dynamic uploads for some
+    bricks only (the others seed from their neighbours' means or from a
+    boundary reference), fan surface kinds and heat emitters in the static
+    fields, source fields rebuilt into fan footprints and plumes, a boundary
+    reference, world deltas (a cell patch and a source patch), a queued static
+    upload and a mid-run dynamic upload; reads after each phase."""
+    rng = np.random.default_rng(seed)
+    cells = n ** 3
+    W = 1
+    bricks = [(0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 0, 1), (1, 0, 1), (0, 1, 0)]
+    hinted = bricks[:5]
+
+    def obstacle():
+        ob = (rng.random((n, n, n)) < 0.05).astype(np.uint8)
+        ob[:, 0, :] = 1
+        return ob.reshape(-1)
+
+    def flow(scale=1.0):
+        fl = np.zeros((cells, 4), np.float32)
+        fl[:, 0] = scale * (0.05 + rng.uniform(-0.01, 0.01, cells))
+        fl[:, 1] = scale * rng.uniform(-0.005, 0.005, cells)
+        fl[:, 2] = scale * (0.02 + rng.uniform(-0.01, 0.01, cells))
+        fl[:, 3] = rng.uniform(-0.002, 0.002, cells)
+        return fl
+
+    def temps():
+        return rng.uniform(-0.05, 0.05, cells).astype(np.float32), rng.uniform(0, 0.02, cells).astype(np.float32)
+
+    s = [("ensure", W, n, 1.0, 0.05), ("mode", W, 1), ("hints", W, n, hinted, True), ("status", W)]
+    zeros_u8 = np.zeros(cells, np.uint8)
+    zeros_u16 = np.zeros(cells, np.uint16)
+    zeros_f = np.zeros(cells, np.float32)
+    for b in bricks:
+        ob = obstacle()
+        sk, of, em, sf, se = zeros_u8.copy(), zeros_u16.copy(), zeros_f.copy(), None, None
+        if b == (0, 0, 0):
+            sk.reshape(n, n, n)[2:4, 3:6, 3:6] = 33  # fans blowing +x
+        if b == (1, 0, 0):
+            em.reshape(n, n, n)[5:7, 2, 5:7] = 400.0
+            of.reshape(n, n, n)[:, 1, :] = 2
+        if b == (0, 0, 1):
+            sf = zeros_u8.copy()
+            sf.reshape(n, n, n)[4, 3, 4] = 2  # a fan block pointing +x
+            se = zeros_f.copy()
+            se.reshape(n, n, n)[7, 2, 7] = 600.0
+        s.append(("static", W, n, b, ob, sk, of, em, sf, se))
+    for b in [(0, 0, 0), (1, 0, 0), (0, 0, 1)]:
+        air, surf = temps()
+        s.append(("dynamic", W, n, b, flow(), air, surf))
+    air, surf = temps()
+    s.append(("reference", W, n, (2, 0, 0), flow(0.8), air, surf))
+    reads = lambda: [("status", W), ("coords", W, True), ("coords", W, False)] + \
+        [("atlas", W, n, b, 4) for b in hinted] + [("copy", W, n, b) for b in hinted]
+    s += [("step", W, 3)] + reads()
+    # world deltas: a cell patch that solidifies a fluid cell of (1,0,0), a
+    # source patch placing a fan block in (0,0,0), a queued static upload
+    wx, wy, wz = 1 * n + 6, 5, 6
+    s.append(("deltas", [(8, wx, wy, wz, W, 0x1, 0, 0, 0.0, 0.0, 0.0, 0.0),
+                         (10, 3, 6, 4, W, 0x0 | (0 << 8) | (2 << 16), 0, 0, 0.0, 0.0, 0.0, 0.0)]))
+    ob = obstacle()
+    s.append(("queue_static", W, n, (1, 0, 1), ob, zeros_u8, zeros_u16, zeros_f))
+    s += [("step", W, 3)] + reads()
+    air, surf = temps()
+    s.append(("dynamic", W, n, (0, 0, 0), flow(1.2), air, surf))
+    s += [("step", W, 2)] + reads() + [("atlas", W, n, (1, 0, 0), 3)]
+    return s
+
+
 def brick_world_case(n: int = 16, steps: int = 6, seed: int = 51, solver_mode: int = 1):
     """Four face-adjacent bricks (2 x 2 in x-z) of n^3 cells: a solid ground
     layer in the lower bricks plus 5 % random solids, a seeded flow of about
