@@ -113,10 +113,11 @@ def c1_plain_fp32(n: int = 32, seed: int = 1234, tau: float = 0.55, steps: int =
 
 def c2_terrain_boussinesq(n: int = 128, seed: int = 2024, tau: float = 0.55, steps: int = 1000) -> BrickCase:
     """One n^3 brick over a seeded 4-octave heightmap (amplitude 24 cells at
-    n=128, scaled with n), inflow u=(0.08,0.02,0) at x=0, far-field
-    equilibrium outflow at x=n-1 and on the lid, periodic y, bounce-back
-    ground. Boussinesq along +z with g*beta = 1e-4 and T = -1e-3 z plus a
-    Gaussian warm bubble (amplitude 0.01, radius 8, centre (n/2, n/2, 20))."""
+    n=128, scaled with n), inflow u=(0.08,0.02,0) at x=0 (velocity face),
+    convective outflow at x=n-1, a far-field equilibrium lid at the inflow
+    velocity, periodic y, bounce-back ground. Boussinesq along +z with
+    g*beta = 1e-4 and T = -1e-3 z plus a Gaussian warm bubble (amplitude
+    0.01, radius 8, centre (n/2, n/2, 20))."""
     s = n / 128.0
     h = value_noise_heightmap(n, n, 4, 24.0 * s, seed)
     z = np.arange(n)[None, None, :]
@@ -130,7 +131,7 @@ def c2_terrain_boussinesq(n: int = 128, seed: int = 2024, tau: float = 0.55, ste
     r2 = np.sum((g - centre) ** 2, -1)
     temp = (-1e-3 * g[..., 2] + 0.01 * np.exp(-r2 / (2 * (8.0 * s) ** 2))).astype(np.float32)
     far = {"kind": VELOCITY, "velocity": u_in}
-    faces = [far, far, {"kind": PERIODIC}, {"kind": PERIODIC}, {"kind": BOUNCE_BACK}, far]
+    faces = [far, {"kind": CONVECTIVE}, {"kind": PERIODIC}, {"kind": PERIODIC}, {"kind": BOUNCE_BACK}, far]
     return BrickCase("c2-terrain-boussinesq", (n, n, n), obstacle, u, temp, faces, tau, u_in, sgs=True,
                      smagorinsky_c=0.1, buoyancy=True, buoyancy_beta=1e-4, gravity_axis=2, steps=steps)
 

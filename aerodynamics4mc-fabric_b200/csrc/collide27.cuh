@@ -256,7 +256,8 @@ __device__ __forceinline__ void reseed_state(const ReseedSource& r, float max_sp
     }
 }
 
-// Collide one fluid cell in place. `temperature` feeds buoyancy (read only
+// Collide one fluid cell in place. `temperature` (the cell's entry of the
+// temperature field, or a caller's local value) feeds buoyancy (read only
 // when buoyancy is on); cfx/cfy/cfz is an extra per-cell force density (zero
 // when unused). Returns false, leaving f untouched, when the input is not
 // finite: the caller then reseeds the cell (out of line, see reseed_state).
@@ -275,7 +276,7 @@ __device__ __forceinline__ bool collide27(float (&f)[27], const CollideParams& P
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     if (ex && P.fan_beta > 0.0f && ex->fan_mask > 0.0f) fan_force(*ex, P, rs, ux, uy, uz, fx, fy, fz);
     if (P.enable_buoyancy) {
-        const float add = rs * clampf_dev(P.buoy_beta * __ldg(temperature), -P.buoy_fmax, P.buoy_fmax);
+        const float add = rs * clampf_dev(P.buoy_beta * *temperature, -P.buoy_fmax, P.buoy_fmax);
         if (P.gravity_axis == 0) fx += add;
         else if (P.gravity_axis == 1) fy += add;
         else fz += add;

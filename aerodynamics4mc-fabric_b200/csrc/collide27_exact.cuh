@@ -94,7 +94,7 @@ __device__ __forceinline__ bool collide27_exact(float (&f)[27], const CollidePar
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     if (ex && P.fan_beta > 0.0f && ex->fan_mask > 0.0f) fan_force(*ex, P, rho_safe, ux, uy, uz, fx, fy, fz);
     if (P.enable_buoyancy) {
-        const float buoy = rclamp(P.buoy_beta * __ldg(temperature), -P.buoy_fmax, P.buoy_fmax);
+        const float buoy = rclamp(P.buoy_beta * *temperature, -P.buoy_fmax, P.buoy_fmax);
         const float add = rho_safe * buoy;
         if (P.gravity_axis == 0) fx += add;
         else if (P.gravity_axis == 1) fy += add;

@@ -13,10 +13,12 @@ namespace aero {
 // apply_sparse_payload_overlays (jni.cpp:1696-1721): overlay i (6 floats:
 // vx, vy, vz, p, T, source) replaces the ingested reference fields of cell
 // cells[i]; indices outside [0, cells) are skipped. With the temperature
-// transport on, T and the source go to the packet reference channels, else T
-// is the collision's temperature field (as the ingest does).
+// transport on (thermal 1), T and the source go to the packet reference
+// channels; thermal 2 (packets without a source channel) keeps the cells'
+// fan-driven source; thermal 0: T is the collision's temperature field (as
+// the ingest does).
 cudaError_t launch_apply_overlays(const int* cells, const float* values, int count, CellFields f, long long n_cells,
-                                  bool thermal, cudaStream_t s);
+                                  int thermal, cudaStream_t s);
 
 // Shift of a component-major field: dst[k][x] = src[k][x + d] inside the
 // brick, else fill (shift_scalar_field / shift_population_field,

@@ -13,6 +13,10 @@ namespace {
 
 constexpr int kOverlayChannels = 6;  // vx, vy, vz, p, T, source (jni.cpp:75-81)
 
+// thermal: 0 the overlay's temperature is the collision's field; 1 it is the
+// transport's reference temperature and the overlay's source replaces the
+// cell's; 2 as 1 but the cell keeps its fan-driven source (9-channel packets:
+// thermal_source_term, jni.cpp:1783-1797, ignores the stored source then)
 __global__ void apply_overlays_kernel(const int* __restrict__ cells, const float* __restrict__ values, int count,
                                       CellFields f, long long n_cells, int thermal) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -26,7 +30,7 @@ __global__ void apply_overlays_kernel(const int* __restrict__ cells, const float
     f.ref_p[cell] = clampf_dev(v[3], -0.03f, 0.03f);
     if (thermal) {
         f.ref_temperature[cell] = clampf_dev(v[4], -1.0f, 1.0f);
-        f.thermal_source[cell] = clampf_dev(v[5], -0.006f, 0.006f);
+        if (thermal == 1) f.thermal_source[cell] = clampf_dev(v[5], -0.006f, 0.006f);
     } else {
         f.temperature[cell] = clampf_dev(v[4], -1.0f, 1.0f);
     }
@@ -243,9 +247,9 @@ cudaError_t ip_scatter_t(const IpView& v, const float* tmp, cudaStream_t s) {
 }  // namespace
 
 cudaError_t launch_apply_overlays(const int* cells, const float* values, int count, CellFields f, long long n_cells,
-                                  bool thermal, cudaStream_t s) {
+                                  int thermal, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
-    apply_overlays_kernel<<<(unsigned)((count + 127) / 128), 128, 0, s>>>(cells, values, count, f, n_cells, thermal ? 1 : 0);
+    apply_overlays_kernel<<<(unsigned)((count + 127) / 128), 128, 0, s>>>(cells, values, count, f, n_cells, thermal);
     count_launch();
     return cudaGetLastError();
 }

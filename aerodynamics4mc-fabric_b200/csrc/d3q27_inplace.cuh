@@ -13,6 +13,7 @@
 #include "collide27_x2.cuh"
 #include "collide27_exact_x2.cuh"
 #include "inplace27.cuh"
+#include "thermal_fused.cuh"
 
 namespace aero {
 
@@ -30,6 +31,11 @@ struct IpArgs {
     int cells_per_thread;            // 1 one cell per thread, 2 two cells per thread (packed collision)
     int streamed;                    // factorised two-cell step: populations streamed by bulk async copies
     int* fault;                      // device word set to 1 by a streamed step whose copies never landed
+    // Temperature transport computed by the step kernel itself (1) before each
+    // collision (thermal_fused.cuh), or by a separate pass (0); the launch
+    // then provides fused_smem_bytes(block span) of dynamic shared memory.
+    int transport;
+    FusedTransport tr;
     // Populations of solid cells (27 x cells FP32, null = all at rest): the
     // reference keeps a solid cell's streamed populations and flips them
     // every call (jni.cpp:2209-2452: f_post = f, f'[q] = f_post[opp q]); they
@@ -164,12 +170,32 @@ inline dim3 line_grid(const PadGeom& g, int block, int cells_per_thread = 1) {
 // Threads per block of the line launch: a multiple of 32 covering n, at most 128.
 inline int line_block(int n) { return n >= 128 ? 128 : ((n + 31) / 32) * 32; }
 
+// Shared memory of the fused temperature transport for a block covering
+// `span` cells of a line: nine staged rows of span + 2 values and codes.
+inline size_t fused_smem_bytes(int span) { return (size_t)9 * (span + 2) * (sizeof(float) + 1); }
+
+template <int kCells>
+__device__ __forceinline__ void fused_transport(const IpArgs& a, int x, int y, int z_begin, int span,
+                                                const int (&zs)[kCells], float (&tn)[kCells]) {
+    extern __shared__ float fused_sv[];
+    const int W = span + 2;
+    thermal_fused::update_cells<kCells>(a.tr, a.obstacle_cur, a.g.nx, a.g.ny, a.g.nz, x, y, z_begin, span, zs, tn,
+                                        fused_sv, reinterpret_cast<unsigned char*>(fused_sv + 9 * W));
+}
+
 template <class S, bool kExact, int kParity>
 __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom G = a.g;
     int x, y, z;
     long long cell;
-    if (!line_cell(G, x, y, z, cell)) return;
+    const bool in_line = line_cell(G, x, y, z, cell);
+    float tn[1] = {0.0f};
+    if (a.transport) {
+        const int z_begin = blockIdx.x * blockDim.x;
+        const int zs[1] = {z};
+        fused_transport<1>(a, x, y, z_begin, min((int)blockDim.x, G.nz - z_begin), zs, tn);
+    }
+    if (!in_line) return;
     const uint32_t w = a.flags_prev[cell];
     if (w & kFlagSelfSolid) {  // memory of a solid cell is link storage; transitions run separately
         record_u(a.cur, cell, 0.0f, 0.0f, 0.0f);
@@ -185,7 +211,7 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
         fl[q] = S::load(f + (d * G.pcells + c), q, a.sc);
     }
     if (a.obstacle_cur[cell]) record_u(a.cur, cell, 0.0f, 0.0f, 0.0f);
-    if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell, x, y, z)) {
+    if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell, x, y, z, a.transport ? tn : nullptr)) {
         reseed_push<S>(f, a, cell, x, y, z, kParity);
         return;
     }
@@ -261,8 +287,14 @@ template <class S, bool kExact, int kParity>
 __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_MIN_BLOCKS) step_ip2_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom& G = a.g;
     const int z0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (z0 >= G.nz) return;
     const int y = blockIdx.y, x = blockIdx.z;
+    float tn[2] = {0.0f, 0.0f};
+    if (a.transport) {
+        const int z_begin = 2 * blockIdx.x * blockDim.x;
+        const int zs[2] = {z0, z0 + 1};
+        fused_transport<2>(a, x, y, z_begin, min(2 * (int)blockDim.x, G.nz - z_begin), zs, tn);
+    }
+    if (z0 >= G.nz) return;
     const long long cell0 = ((long long)x * G.ny + y) * G.nz + z0;
     const bool has1 = z0 + 1 < G.nz;
     const uint32_t w0 = a.flags_prev[cell0];
@@ -299,7 +331,9 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
         }
     }
     const float* temp = a.cur.temperature;
-    const F2 t = a.cp.enable_buoyancy ? f2(temp[cell0], has1 ? temp[cell0 + 1] : 0.0f) : f2(0.0f);
+    const F2 t = !a.cp.enable_buoyancy ? f2(0.0f)
+                 : a.transport         ? f2(tn[0], tn[1])
+                                       : f2(temp[cell0], has1 ? temp[cell0 + 1] : 0.0f);
     F2 cfx = f2(0.0f), cfy = f2(0.0f), cfz = f2(0.0f);
     if (a.force.fx) {
         cfx = f2(a.force.fx[cell0], has1 ? a.force.fx[cell0 + 1] : 0.0f);
@@ -350,12 +384,64 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
     }
 }
 
-// Before a step of parity p: write the equilibrium value of every incoming
-// population whose source lies outside an equilibrium face into the slot the
-// pulling cell reads at parity p (a ghost-cell slot, or for positive
-// directions the cell's own slot that only the never-updated ghost would
-// write). One thread per cell of the six boundary layers; cells on edges are
-// visited once per face and write identical values.
+// Source of incoming population q of boundary cell (x, y, z) whose pull
+// source (sx, sy, sz) lies outside a face that is neither periodic nor
+// bounce-back, for the step of parity p (benchmark_hydrodynamic_boundary_value,
+// jni.cpp:1494-1602). Equilibrium faces need only the face's state. Symmetry
+// copies the post-collision population q of the clamped source cell;
+// convective outflow extrapolates it from the two cells inward along the
+// face normal, f1 + 0.15 (f1 - f2) (f1 alone when the second cell is solid);
+// a solid source cell (f1's) gives the half-way bounce-back value. The
+// post-collision populations are those the last step left: when the fill
+// runs they still sit in their outgoing slots of parity p ^ 1, and the
+// bounce-back value in the cell's flipped slot of parity p. Products and sums
+// round separately (the reference's order).
+template <class S>
+__device__ __forceinline__ float ip_face_source(const typename S::T* __restrict__ f, const IpArgs& a, const PadGeom& G,
+                                                const NeighbourOffsets& o, int own, long long cell, int x, int y, int z,
+                                                int q, int sx, int sy, int sz, int p) {
+    const FaceParams& F = *a.face_prev;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const int face = oob_face(sx, sy, sz, nx, ny, nz);
+    const int kind = F.kind[face];
+    if (kind == kHydroVelocity || kind == kHydroPressure || kind == kHydroMovingWall)
+        return ip_face_equilibrium(F, q, a.ref_p_prev[cell], y, sx, sy, sz, nx, ny, nz);
+    int c, d;
+    incoming_slot(o, own, q, p, true, c, d);
+    const float bounced = S::load(f + (long long)d * G.pcells + c, q, a.sc);
+    // post-collision population q of cell (ix, iy, iz) after the last step
+    auto post = [&](int ix, int iy, int iz) {
+        int pc, pd;
+        outgoing_slot(neighbour_offsets(G, ix, iy, iz), pad_index(G, ix, iy, iz), q, p ^ 1, pc, pd);
+        return S::load(f + (long long)pd * G.pcells + pc, q, a.sc);
+    };
+    auto solid = [&](int ix, int iy, int iz) { return a.obstacle_cur[((long long)ix * ny + iy) * nz + iz] != 0; };
+    if (kind == kHydroSymmetry) {
+        const int ix = min(max(sx, 0), nx - 1), iy = min(max(sy, 0), ny - 1), iz = min(max(sz, 0), nz - 1);
+        return solid(ix, iy, iz) ? bounced : post(ix, iy, iz);
+    }
+    if (kind == kHydroInheritGame && F.disable_convective) return bounced;
+    const int dx = (sx < 0 || sx >= nx) ? q_cx(q) : 0;
+    const int dy = (sy < 0 || sy >= ny) ? q_cy(q) : 0;
+    const int dz = (sz < 0 || sz >= nz) ? q_cz(q) : 0;
+    const int x1 = min(max(x + dx, 0), nx - 1), y1 = min(max(y + dy, 0), ny - 1), z1 = min(max(z + dz, 0), nz - 1);
+    if (solid(x1, y1, z1)) return bounced;
+    const float f1 = post(x1, y1, z1);
+    const int x2 = min(max(x + 2 * dx, 0), nx - 1), y2 = min(max(y + 2 * dy, 0), ny - 1), z2 = min(max(z + 2 * dz, 0), nz - 1);
+    if (solid(x2, y2, z2)) return f1;
+    const float f2 = post(x2, y2, z2);
+    return __fadd_rn(f1, __fmul_rn(0.15f, __fsub_rn(f1, f2)));
+}
+
+// Before a step of parity p: write the source of every incoming population
+// whose pull source lies outside a face that is neither periodic nor
+// bounce-back (ip_face_source) into the slot the pulling cell reads at parity
+// p (a ghost-cell slot, or for positive directions the cell's own slot that
+// only the never-updated ghost would write). These slots are written by no
+// step and read by no other fill thread, so the fill runs right after the
+// step that produced the post-collision populations it reads. One thread per
+// cell of the six boundary layers; cells on edges are visited once per face
+// and write identical values.
 template <class S>
 __global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom G = a.g;
@@ -384,8 +470,6 @@ __global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     if ((w & kFlagSelfSolid) || !(w & kFlagFaceSpecial)) return;
     const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
     const int own = pad_index(G, x, y, z);
-    const FaceParams& F = *a.face_prev;
-    const float rp = a.ref_p_prev[cell];
     // unrolled: the direction constants fold and the 27 tests issue independently
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
@@ -394,9 +478,10 @@ __global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
         const int sy = axis_neighbour(y, -q_cy(q), ny, G.wrap[1]);
         const int sz = axis_neighbour(z, -q_cz(q), nz, G.wrap[2]);
         if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) continue;
+        const float v = ip_face_source<S>(f, a, G, o, own, cell, x, y, z, q, sx, sy, sz, a.parity);
         int c, d;
         incoming_slot(o, own, q, a.parity, false, c, d);
-        S::store(f + (long long)d * G.pcells + c, q, ip_face_equilibrium(F, q, rp, y, sx, sy, sz, nx, ny, nz), a.sc);
+        S::store(f + (long long)d * G.pcells + c, q, v, a.sc);
     }
 }
 

@@ -28,10 +28,14 @@ __device__ __forceinline__ int oob_face(int sx, int sy, int sz, int nx, int ny, 
 }
 
 // Collide one fluid cell; false = non-finite input, the caller reseeds.
-// (x, y, z): the cell's coordinates, for the runtime terms' edge layers.
+// (x, y, z): the cell's coordinates, for the runtime terms' edge layers;
+// temperature: the cell's buoyancy temperature when the caller computed it
+// (fused transport), else null (read from cur.temperature).
 template <bool kExact>
 __device__ __forceinline__ bool collide_cell(float (&f)[27], const CollideParams& cp, const CellFields& cur,
-                                             const ForceField& force, long long cell, int x, int y, int z) {
+                                             const ForceField& force, long long cell, int x, int y, int z,
+                                             const float* temperature = nullptr) {
+    const float* tp = temperature ? temperature : cur.temperature + cell;
     CollideOut o;
     const float cfx = force.fx ? force.fx[cell] : 0.0f;
     const float cfy = force.fy ? force.fy[cell] : 0.0f;
@@ -52,8 +56,8 @@ __device__ __forceinline__ bool collide_cell(float (&f)[27], const CollideParams
         ex.ref_z = cur.ref_uz[cell];
         exp = &ex;
     }
-    const bool ok = kExact ? exact::collide27_exact(f, cp, cur.temperature + cell, cfx, cfy, cfz, o, exp)
-                           : collide27(f, cp, cur.temperature + cell, cfx, cfy, cfz, o, exp);
+    const bool ok = kExact ? exact::collide27_exact(f, cp, tp, cfx, cfy, cfz, o, exp)
+                           : collide27(f, cp, tp, cfx, cfy, cfz, o, exp);
     if (ok) record_u(cur, cell, o.ux, o.uy, o.uz);
     if (ok && cp.runtime_terms) {
         const float alpha = sponge_alpha_at(cp, d);

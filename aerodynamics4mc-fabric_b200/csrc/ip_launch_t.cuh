@@ -3,6 +3,8 @@
 // d3q27_fast.cu).
 #pragma once
 
+#include <algorithm>
+
 #include "d3q27_async.cuh"
 
 namespace aero {
@@ -28,17 +30,19 @@ struct IpLaunch {
         step_timer_begin(s);
         // the runtime terms (fans, state nudge, sponge) exist in the one-cell kernel only
         const int cpt = a.cp.runtime_terms ? 1 : a.cells_per_thread;
-        if (!kExact && cpt == 2 && a.streamed && IpaLaunch<S>::eligible(a)) {
+        if (!kExact && cpt == 2 && a.streamed && !a.transport && IpaLaunch<S>::eligible(a)) {
             cudaError_t e = IpaLaunch<S>::step(f, a, s);
             if (e != cudaSuccess) return e;
         } else if (cpt == 2) {
             const int lb = line_block((a.g.nz + 1) / 2);
-            if (a.parity == 0) step_ip2_kernel<S, kExact, 0><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
-            else step_ip2_kernel<S, kExact, 1><<<line_grid(a.g, lb, 2), lb, 0, s>>>(f, a);
+            const size_t smem = a.transport ? fused_smem_bytes(std::min(2 * lb, a.g.nz)) : 0;
+            if (a.parity == 0) step_ip2_kernel<S, kExact, 0><<<line_grid(a.g, lb, 2), lb, smem, s>>>(f, a);
+            else step_ip2_kernel<S, kExact, 1><<<line_grid(a.g, lb, 2), lb, smem, s>>>(f, a);
         } else {
             const int lb = line_block(a.g.nz);
-            if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
-            else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, 0, s>>>(f, a);
+            const size_t smem = a.transport ? fused_smem_bytes(std::min(lb, a.g.nz)) : 0;
+            if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, smem, s>>>(f, a);
+            else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, smem, s>>>(f, a);
         }
         step_timer_end(s);
         count_launch();

@@ -53,8 +53,9 @@ RuntimeConfig g_cfg;
 std::recursive_mutex g_mutex;  // guards every entry point (the caller is one worker thread)
 int g_thermal_mode = -1;      // temperature transport: -1 with buoyancy, 0 never (packet field), 1 always
 int g_streamed_step = 0;      // factorised two-cell in-place step: bulk-copy streamed kernel where eligible (opt-in)
+int g_fused_transport = 1;    // in-place steps compute the first-order temperature transport themselves
 int g_cells_per_thread = 2;    // in-place step: 1 one cell per thread, 2 two cells per thread (packed collision)
-int g_fp16_format = 0;         // 16-bit storage: 0 IEEE half deviations, 1 fixed-point deviations
+int g_fp16_format = 1;         // 16-bit storage: 0 IEEE half deviations, 1 fixed-point deviations (default)
 std::unordered_map<long long, std::unique_ptr<Context>> g_contexts;
 std::string g_last_error;
 std::string g_timing_text;
@@ -536,20 +537,27 @@ const RuntimeView runtime_view() {
     return RuntimeView{g_cfg.initialized, g_cfg.nx, g_cfg.ny, g_cfg.nz, g_cfg.input_channels, g_cfg.output_channels};
 }
 
-// The in-place layout needs faces whose pulled value is local to the pulling
-// cell (periodic on both sides of an axis, bounce-back, equilibrium faces).
+// Faces the in-place layout takes: periodic on both sides of an axis,
+// bounce-back, and the faces whose pulled values the end-of-call fill writes
+// (equilibrium faces, symmetry, convective outflow: face_fill_ip_kernel). The
+// cylinder preset stays on the two-buffer layout, whose state its
+// momentum-exchange force reads.
 static bool inplace_faces_ok(const FaceParams& f) {
     for (int a = 0; a < 3; ++a)
         if (f.wrap_lo[a] != f.wrap_hi[a]) return false;
+    return !(bench_active() && g_bench.preset == AERO_LBM_BENCHMARK_PRESET_CYLINDER_CROSSFLOW_2D);
+}
+
+// Some face needs the end-of-call fill (a kind other than periodic and
+// bounce-back, which the step kernel resolves itself).
+static bool faces_need_fill(const FaceParams& f) {
     for (int i = 0; i < 6; ++i) {
         const int k = f.kind[i];
-        if (k == kHydroPeriodic || k == kHydroBounceBack || k == kHydroVelocity || k == kHydroPressure ||
-            k == kHydroMovingWall)
-            continue;
+        if (k == kHydroPeriodic || k == kHydroBounceBack) continue;
         if (k == kHydroInheritGame && f.disable_convective) continue;
-        return false;
+        return true;
     }
-    return true;
+    return false;
 }
 
 // Storage of an in-place context for the kernels that take it as a number:
@@ -609,7 +617,7 @@ static bool choose_layout(Context& ctx, const FaceParams& face, const float* pac
     int layout = 0;
     if (g_stream_mode == 2) {
         if (!local) {
-            set_error("in-place streaming requested but a face is symmetry or convective outflow (non-local)");
+            set_error("in-place streaming requested but an axis is periodic on one side only, or the cylinder preset is set");
             return false;
         }
         layout = 1;
@@ -740,6 +748,8 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
     // buoyancy force.
     ctx.thermal = g_thermal_mode == 1 || (g_thermal_mode == -1 && cp.enable_buoyancy);
     if (ctx.thermal && !ensure_thermal(ctx)) return false;
+    bool fused_transport = false;
+    FusedTransport transport{};
     const int in_ch = g_cfg.input_channels;
     const bool have_packet = packet != nullptr || fill != nullptr;
     if (fill) host_packet = false;
@@ -794,7 +804,8 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
             }
             if (!cuda_ok(cudaMemcpyAsync(ctx.overlay_cells, overlays->cells, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s), "copy overlays") ||
                 !cuda_ok(cudaMemcpyAsync(ctx.overlay_values, overlays->values, (size_t)n * 6 * sizeof(float), cudaMemcpyHostToDevice, s), "copy overlays") ||
-                !cuda_ok(launch_apply_overlays(ctx.overlay_cells, ctx.overlay_values, n, ctx.fields(new_slot), ctx.cells, ctx.thermal, s), "apply_overlays"))
+                !cuda_ok(launch_apply_overlays(ctx.overlay_cells, ctx.overlay_values, n, ctx.fields(new_slot), ctx.cells,
+                                                  ctx.thermal ? (in_ch > kChThermalSource ? 1 : 2) : 0, s), "apply_overlays"))
                 return false;
         }
         if (host_packet && !cuda_ok(cudaEventRecord(ctx.copy_done, s), "copy event")) return false;
@@ -845,7 +856,20 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         ta.turbulent = (!bench_active() && cp.enable_sgs) ? 1 : 0;
         ta.sgs_c2 = cp.sgs_c2;
         ta.nu0 = clamp_nu(kRuntimeMolecularNu0);
-        if (update) {
+        // The first-order branch runs inside the in-place step kernel
+        // (thermal_fused.cuh) once the context has stepped: the state is
+        // swapped here, the kernel reads the old one and writes the new one.
+        fused_transport = update && ctx.initialized && ctx.layout == 1 && !ta.bfecc && ta.dt == 1.0f && !ta.turbulent &&
+                          g_fused_transport;
+        if (fused_transport) {
+            transport.t = ctx.temperature;
+            std::swap(ctx.temperature, ctx.temperature_next);
+            transport.t_next = ctx.temperature;
+            transport.u = ctx.u_last;
+            transport.source = ta.source;
+            transport.alpha = ta.alpha;
+            transport.faces = ta.faces;
+        } else if (update) {
             if (!cuda_ok(launch_thermal_update(ta, s), "thermal_update")) return false;
             std::swap(ctx.temperature, ta.bfecc ? ctx.temperature_scratch : ctx.temperature_next);
         }
@@ -891,6 +915,10 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
                 a.solid_f = ctx.solid_f;
             }
             a.parity = ctx.parity;
+            if (fused_transport) {
+                a.transport = 1;
+                a.tr = transport;
+            }
             if (!cuda_ok(ip_step(ctx.ip_variant, ctx.ip, a, transitions, s), "step_inplace")) return false;
             ctx.parity ^= 1;
         }
@@ -914,12 +942,7 @@ bool step_context(Context& ctx, const float* packet, float* out, float scale, bo
         // Equilibrium-face sources of the next step, written now: between calls
         // every incoming slot then holds the cell's streamed population (the
         // reference's f), which the halo exchange reads and writes.
-        bool fill = false;
-        for (int i = 0; i < 6; ++i) {
-            const int k = face_now.kind[i];
-            fill |= k == kHydroVelocity || k == kHydroPressure || k == kHydroMovingWall;
-        }
-        if (fill) {
+        if (faces_need_fill(face_now)) {
             // on the context's fill stream, forked after the step: it overlaps
             // the next call's temperature update (the step waits for it)
             if (!ctx.fill_stream &&
@@ -2001,6 +2024,16 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_thermal_transport(int mode) {
         return 0;
     }
     g_thermal_mode = mode;
+    return 1;
+}
+
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_fused_transport(int on) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    if (on != 0 && on != 1) {
+        set_error("set_fused_transport: 0 (separate pass) or 1 (inside the in-place step)");
+        return 0;
+    }
+    g_fused_transport = on;
     return 1;
 }
 

@@ -329,11 +329,18 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_thermal_transport(int mode);
  * current one, 0 = per-thread loads (default; faster on B200). Same
  * arithmetic, bit-identical results. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streamed_step(int on);
+/* Where the first-order temperature transport of in-place contexts runs:
+ * 1 (default) inside the step kernel, each cell updating its own temperature
+ * right before its collision; 0 as a separate pass before the step. Same
+ * arithmetic, bit-identical results; the heated-cavity and game-runtime
+ * (BFECC) transports always run as separate passes. */
+AERO_LBM_B200_EXPORT int aero_lbm_b200_set_fused_transport(int on);
 /* Format of the 16-bit deviation storage chosen by
  * aero_lbm_set_realtime_solver_mode(3), for contexts created afterwards:
- * 0 = IEEE half of (f - w) * S / w with a power-of-two per-brick S (default),
- * 1 = 16-bit fixed point of the same deviation with S = 32767 / d_max (uniform
- * resolution; several times more precise for flowing states). */
+ * 1 = 16-bit fixed point of (f - w) * S / w with S = 32767 / d_max (default:
+ * uniform resolution, within 1e-3 of the max speed of an FP64 run after 1000
+ * steps of a 128^3 terrain brick), 0 = IEEE half of the same deviation with a
+ * power-of-two per-brick S (about 2e-3 on that brick). */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_fp16_format(int format);
 /* Per-cell force density field for a context (3 x cells floats, SoA order
  * fx[cells], fy[cells], fz[cells]; host pointer; null clears). */

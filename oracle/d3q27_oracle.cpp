@@ -49,6 +49,7 @@
 #include <cstring>
 #include <memory>
 #include <type_traits>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -103,11 +104,33 @@ typedef struct OracleD3Q27Params {
     int sponge;                    // 1: post-collision sponge toward rest in the 4 outer layers
     double state_nudge;            // runtime mode: 0.08 (velocity nudge toward the packet state, 8 outer layers)
     int runtime_mode;              // 1: benchmark mode off (jni.cpp:8037-8064, 1972-2047, 2191-2196)
+    int packet_has_source;         // 1: the packet carries the source channel (>= 10 channels); with 9 the
+                                   // transport's source comes from the fan channels (jni.cpp:1783-1797)
 } OracleD3Q27Params;
 
 }  // extern "C"
 
 namespace {
+
+// Loops over independent cells split by x-slab across the host's cores; the
+// results do not depend on the thread count (no cell reads another cell's
+// output of the same loop).
+template <typename F>
+void parallel_for(int n, F&& body) {
+    const int hw = int(std::max(1u, std::thread::hardware_concurrency()));
+    const int k = std::max(1, std::min(n, hw));
+    if (k == 1) {
+        for (int i = 0; i < n; ++i) body(i);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve(size_t(k));
+    for (int t = 0; t < k; ++t)
+        pool.emplace_back([&, t]() {
+            for (int i = t * n / k; i < (t + 1) * n / k; ++i) body(i);
+        });
+    for (auto& th : pool) th.join();
+}
 
 template <typename T>
 struct Lattice {
@@ -451,7 +474,7 @@ struct D3Q27Oracle {
         // effective_thermal_dt (jni.cpp:907-909): the update stride, 2 in runtime mode
         const T dt = T(p.runtime_mode ? 2.0f : 1.0f), cooling = T(0.0f);
         const T alpha = T(float(p.thermal_diffusivity));
-        for (int x = 0; x < nx; ++x)
+        parallel_for(nx, [&](int x) {
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     const size_t cell = cell_index(x, y, z);
@@ -460,7 +483,8 @@ struct D3Q27Oracle {
                     temperature_scratch[cell] = sample_trilinear(temperature, T(float(x)) - dt * ux[cell],
                                                                  T(float(y)) - dt * uy[cell], T(float(z)) - dt * uz[cell], tc);
                 }
-        for (int x = 0; x < nx; ++x)
+        });
+        parallel_for(nx, [&](int x) {
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     const size_t cell = cell_index(x, y, z);
@@ -470,7 +494,8 @@ struct D3Q27Oracle {
                                                     T(float(z)) + dt * uz[cell], temperature_scratch[cell]);
                     temperature_next[cell] = clampv(T(tc + T(0.5f) * (tc - back)), t_min, t_max);
                 }
-        for (int x = 0; x < nx; ++x)
+        });
+        parallel_for(nx, [&](int x) {
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     const size_t cell = cell_index(x, y, z);
@@ -491,6 +516,7 @@ struct D3Q27Oracle {
                                                    : alpha;
                     temperature_scratch[cell] = clampv(T(adv + dt * (a_loc * lap + src - cooling * adv)), t_min, t_max);
                 }
+        });
         temperature.swap(temperature_scratch);
         temperature_next = temperature;
     }
@@ -503,7 +529,7 @@ struct D3Q27Oracle {
         }
         const T dt = T(1.0f), cooling = T(0.0f);
         const T alpha = T(float(p.thermal_diffusivity));
-        for (int x = 0; x < nx; ++x)
+        parallel_for(nx, [&](int x) {
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     const size_t cell = cell_index(x, y, z);
@@ -522,6 +548,7 @@ struct D3Q27Oracle {
                     const T t_next = adv + dt * (alpha * lap + src - cooling * adv);
                     temperature_next[cell] = clampv(t_next, t_min, t_max);
                 }
+        });
         temperature.swap(temperature_next);
         temperature_next = temperature;
     }
@@ -657,7 +684,9 @@ struct D3Q27Oracle {
         const T ms = T(p.max_speed);
         const T tau_s_base = T(p.tau_shear), tau_n_base = T(p.tau_normal);
         const T sgs_c2 = T(p.sgs_c2);
-        for (size_t cell = 0; cell < cells; ++cell) {
+        parallel_for(nx, [&](int x) {
+            const size_t slab = size_t(ny) * size_t(nz);
+            for (size_t cell = size_t(x) * slab; cell < size_t(x + 1) * slab; ++cell) {
             if (obstacle[cell]) {
                 rho[cell] = T(1); ux[cell] = uy[cell] = uz[cell] = T(0);
                 for (int q = 0; q < 27; ++q) f_post[di(cell, q)] = f[di(cell, q)];
@@ -803,11 +832,12 @@ struct D3Q27Oracle {
                 }
             }
         }
+        });
     }
 
     // ---- stream_and_bounce (native/src/aero_lbm_jni.cpp:2415-2452)
     void stream() {
-        for (int x = 0; x < nx; ++x)
+        parallel_for(nx, [&](int x) {
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     const size_t cell = cell_index(x, y, z);
@@ -828,6 +858,7 @@ struct D3Q27Oracle {
                     }
                     for (int q = 0; q < 27; ++q) f[di(cell, q)] = fl[q];
                 }
+        });
     }
 
     // macro readout used by write_output / extract (native/src/aero_lbm_jni.cpp:2535-2581, 9385-9446)
@@ -926,7 +957,10 @@ struct D3Q27Oracle {
             const float t = std::min(1.0f, std::max(-1.0f, v[4]));
             if (p.thermal_transport) {
                 ref_temperature[cell] = T(t);
-                thermal_source[cell] = T(std::min(0.006f, std::max(-0.006f, v[5])));
+                // thermal_source_term reads the stored source only when the
+                // packet has a source channel; otherwise it recomputes the
+                // fan-driven source, which an overlay does not touch
+                if (p.packet_has_source) thermal_source[cell] = T(std::min(0.006f, std::max(-0.006f, v[5])));
             } else {
                 temperature[cell] = T(t);
             }

@@ -90,6 +90,7 @@ class OracleParams(ctypes.Structure):
         ("sponge", ctypes.c_int),
         ("state_nudge", ctypes.c_double),
         ("runtime_mode", ctypes.c_int),
+        ("packet_has_source", ctypes.c_int),
     ]
 
 
@@ -186,6 +187,7 @@ def derive_params(cfg: dict) -> OracleParams:
     p.initial_temperature = float(f32(cfg.get("initial_temperature", 0.0)))
     p.internal_thermal_source = 1 if cfg.get("thermal_source", False) else 0
     p.packet_has_temperature = 1 if int(cfg.get("packet_channels", 11)) > 10 else 0
+    p.packet_has_source = 1 if int(cfg.get("packet_channels", 11)) > 9 else 0
     p.cylinder_force = 1 if int(cfg.get("preset", 0)) == PRESET_CYLINDER_2D else 0
     # fan forcing, fan noise and the sponge: off unless the config clears their
     # DISABLE flags (the default config sets them)
@@ -629,6 +631,25 @@ def fan_thermal_source(pk: np.ndarray) -> np.ndarray:
     n = np.sqrt((f[0] * f[0] + f[1] * f[1]) + f[2] * f[2]).astype(np.float32)
     capped = np.minimum(np.float32(0.006), np.maximum(np.float32(0), (n * np.float32(0.0012)).astype(np.float32)))
     return np.where((m > 0) & (n > np.float32(1e-8)), (m * capped).astype(np.float32), np.float32(0)).astype(np.float32)
+
+
+def short_packet_script(packet: np.ndarray, seed: int = 5):
+    """Steps of a 9/10-channel packet, two of them with sparse overlays on
+    fan cells and other fluid cells (non-zero source values), reading the
+    flow and the temperature state in between."""
+    rng = np.random.default_rng(seed)
+    pk = np.asarray(packet, np.float32)
+    fans = np.nonzero((pk[:, 1] > 0) & (pk[:, 0] <= 0.5))[0]
+    fluid = np.nonzero(pk[:, 0] <= 0.5)[0]
+    cells = np.concatenate([fans[:12], rng.choice(fluid, 12, replace=False)]).astype(np.int32)
+    k = cells.size
+    vals = np.stack([rng.uniform(-0.05, 0.05, k), rng.uniform(-0.05, 0.05, k), rng.uniform(-0.05, 0.05, k),
+                     rng.uniform(-0.01, 0.01, k), rng.uniform(-0.5, 0.5, k), rng.uniform(-0.01, 0.01, k)],
+                    axis=1).astype(np.float32)
+    ov = (cells, np.ascontiguousarray(vals))
+    # overlays on even calls: runtime mode transports the temperature on those
+    return [("step",)] * 4 + [("flow",), ("temp",)] + [("step", ov), ("step",), ("step", ov), ("step",)] + \
+        [("flow",), ("temp",)]
 
 
 def run_script_oracle(o: "Oracle", cfg: dict, packet: np.ndarray, script):

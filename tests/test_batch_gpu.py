@@ -110,17 +110,84 @@ def test_graph_replay_is_bit_identical(gpu):
     c.close()
 
 
-def test_publish_atlas_quantisation(gpu):
+def quantize_signed(v, range_):
+    """quantize_signed (native/src/aero_lbm_simulation_bridge.cpp:3122-3128)
+    in float32: lround(clamp(v / range, -1, 1) * 32767), non-finite -> 0."""
+    v = np.asarray(v, np.float32)
+    x = np.clip(v / np.float32(range_), np.float32(-1.0), np.float32(1.0)) * np.float32(32767.0)
+    q = (np.sign(x) * np.floor(np.abs(x) + np.float32(0.5))).astype(np.int16)
+    return np.where(np.isfinite(v), q, np.int16(0)).astype(np.int16)
+
+
+def sampled(flow, dims, stride):
+    nx, ny, nz = dims
+    f = flow.reshape(nx, ny, nz, 4)
+    ix = [min(nx - 1, a * stride) for a in range((nx + stride - 1) // stride)]
+    iy = [min(ny - 1, a * stride) for a in range((ny + stride - 1) // stride)]
+    iz = [min(nz - 1, a * stride) for a in range((nz + stride - 1) // stride)]
+    return f[np.ix_(ix, iy, iz)].reshape(-1, 4)
+
+
+def test_publish_atlas_is_the_reference_quantisation_bit_exact(gpu):
+    """The device publish equals the reference's int16 quantisation of the
+    brick's own float output at the sampled cells, count for count."""
+    specs = brick_specs()
+    b = make_batch(gpu, specs)
+    b.tick(10)
+    for i, s in enumerate(specs):
+        v = sampled(b.flow(i), s["dims"], 4)
+        want = np.stack([quantize_signed(v[:, 0] * np.float32(20.0), 5.6), quantize_signed(v[:, 1] * np.float32(20.0), 5.6),
+                         quantize_signed(v[:, 2] * np.float32(20.0), 5.6), quantize_signed(v[:, 3], 0.03)], axis=1)
+        got = b.atlas(i).reshape(-1, 4)
+        assert got.shape == want.shape
+        assert np.array_equal(got, want), (i, int(np.count_nonzero(got != want)))
+        assert np.count_nonzero(got) > 0
+    b.close()
+
+
+def test_publish_atlas_against_oracle(gpu):
+    """The atlas against the quantised oracle run: the FP32 bricks' factorised
+    collision rounds differently from the oracle's reference order, so a
+    sample may land one count away."""
     specs = brick_specs()[:2]
     b = make_batch(gpu, specs)
     b.tick(10)
     for i, s in enumerate(specs):
         ref = oracle_run(s, 10, "f32").atlas(4)
-        want = np.stack([quantize(ref[:, 0] * 20.0, 5.6), quantize(ref[:, 1] * 20.0, 5.6),
-                         quantize(ref[:, 2] * 20.0, 5.6), quantize(ref[:, 3], 0.03)], axis=1)
-        got = b.atlas(i)
-        assert got.shape == want.shape
+        want = np.stack([quantize_signed(ref[:, 0] * np.float32(20.0), 5.6), quantize_signed(ref[:, 1] * np.float32(20.0), 5.6),
+                         quantize_signed(ref[:, 2] * np.float32(20.0), 5.6), quantize_signed(ref[:, 3], 0.03)], axis=1)
+        got = b.atlas(i).reshape(-1, 4)
         assert np.max(np.abs(got.astype(np.int32) - want.astype(np.int32))) <= 1
+    b.close()
+
+
+def test_batch_brick_sizes_of_the_batched_config(gpu):
+    """A batch with the batched config's brick sizes (32^3, 64^3, 128^3), FP32
+    and FP16 storage, against the oracle (FP32: 1e-5; FP16 vs FP64: 1e-3)."""
+    rng = np.random.default_rng(33)
+    specs = []
+    for n, prec in ((32, 0), (64, 1), (128, 0), (32, 1)):
+        dims = (n, n, n)
+        obst = (rng.random(dims) < rng.uniform(0.0, 0.15)).astype(np.uint8)
+        obst[:, :, 0] = 1
+        u = [np.where(obst == 0, np.float32(v), np.float32(0)).astype(np.float32) for v in (0.05, 0.01, 0.0)]
+        specs.append(dict(dims=dims, precision=prec, faces=[PER, PER, PER, PER, BB, BB], obstacle=obst, u=u,
+                          tau=float(rng.uniform(0.51, 0.6)), force=rng.uniform(-1e-5, 1e-5, 3).astype(np.float32)))
+    b = make_batch(gpu, specs)
+    ticks = 12
+    b.tick(ticks)
+    for i, s in enumerate(specs):
+        flow = b.flow(i)
+        if s["precision"] == 0:
+            e = O.flow_errors(flow, oracle_run(s, ticks, "f32").output())
+            assert e["u"] <= 1e-5 and e["rho"] <= 1e-5, (i, e)
+        else:
+            e = O.flow_errors(flow, oracle_run(s, ticks, "f64").output())
+            assert e["u"] <= 1e-3 and e["rho"] <= 1e-4, (i, e)
+        v = sampled(flow, s["dims"], 4)
+        want = np.stack([quantize_signed(v[:, k] * np.float32(20.0), 5.6) for k in range(3)] +
+                        [quantize_signed(v[:, 3], 0.03)], axis=1)
+        assert np.array_equal(b.atlas(i).reshape(-1, 4), want)
     b.close()
 
 

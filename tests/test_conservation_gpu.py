@@ -59,5 +59,5 @@ def test_periodic_brick_conserves_mass(gpu, solver_mode, fmt, tol):
         m1 = ctx.conservation_sums()[0]
     finally:
         gpu.aero_lbm_set_realtime_solver_mode(0)
-        gpu.aero_lbm_b200_set_fp16_format(0)
+        gpu.aero_lbm_b200_set_fp16_format(1)
     assert abs(m1 - m0) / m0 < tol, (m0, m1)

@@ -337,9 +337,10 @@ def test_runtime_mode_matches_reference_golden(gpu, collision):
 @pytest.mark.parametrize("channels", [9, 10])
 def test_short_packets_match_oracle(gpu, channels):
     """Runtime mode with 9- or 10-channel packets: no temperature channel, and
-    with 9 channels the temperature source derived from the fan channels."""
+    with 9 channels the temperature source derived from the fan channels
+    (sparse overlays on fan cells keep it)."""
     cfg, pk, pre = O.runtime_case(12, 77, True, channels)
-    script = [("step",)] * 3 + [("flow",), ("temp",)] + [("step",)] * 2 + [("flow",), ("temp",)]
+    script = O.short_packet_script(pk)
     res = run_script_gpu(gpu, (12, 12, 12), cfg, pk, script, key=910 + channels, streaming=0, temperature_state=pre)
     o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f32")
     o.set_temperature(pre)

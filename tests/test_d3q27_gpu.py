@@ -59,10 +59,19 @@ def test_c1_32_1000_bit_identical_to_reference(gpu, mode):
     assert_bits(out, g["out"])
 
 
-def test_tunnel_bit_identical_to_reference(gpu):
+@pytest.mark.parametrize("streaming,cpt", [(1, 2), (2, 1), (2, 2)])
+def test_tunnel_bit_identical_to_reference(gpu, streaming, cpt):
+    """Velocity inlet, convective outflow and symmetry faces around a sphere:
+    the two-buffer layout pulls the face values from the post-collision
+    state, the in-place layout from the slots its end-of-call fill wrote."""
     g = np.load(GOLDEN / "tunnel_16_60.npz")
     obst, u, cfg = lbm_cases.tunnel_case(16)
-    out, ctx = lbm_cases.run_product(gpu, (16, 16, 16), cfg, O.packet_from(obst, *u), int(g["steps"]))
+    assert gpu.aero_lbm_b200_set_cells_per_thread(cpt) == 1
+    try:
+        out, ctx = lbm_cases.run_product(gpu, (16, 16, 16), cfg, O.packet_from(obst, *u), int(g["steps"]),
+                                         streaming_mode=streaming)
+    finally:
+        gpu.aero_lbm_b200_set_cells_per_thread(2)
     assert_bits(out, g["out"])
 
 
@@ -79,8 +88,9 @@ def test_factorised_collision_within_tolerance(gpu):
     gpu.aero_lbm_b200_set_collision_mode(0)
 
 
+@pytest.mark.parametrize("streaming", [1, 2])
 @pytest.mark.parametrize("faces", ["pressure_outlet", "closed", "inherit_game", "periodic_all"])
-def test_faces_match_oracle(gpu, faces):
+def test_faces_match_oracle(gpu, faces, streaming):
     n = 12
     rng = np.random.default_rng(11)
     obst = (rng.random((n, n, n)) < 0.08).astype(np.uint8)
@@ -97,7 +107,7 @@ def test_faces_match_oracle(gpu, faces):
     }
     cfg = {"reynolds": 60.0, "initial_velocity": (0.04, 0.0, 0.0), "faces": table[faces], "sgs": True, "buoyancy": False}
     pk = O.packet_from(obst, *u, pressure=p)
-    out, ctx = lbm_cases.run_product(gpu, (n, n, n), cfg, pk, 40)
+    out, ctx = lbm_cases.run_product(gpu, (n, n, n), cfg, pk, 40, streaming_mode=streaming)
     o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
     o.set_fields(obst, *u, pressure=p)
     o.step(40)

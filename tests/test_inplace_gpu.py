@@ -228,6 +228,6 @@ def test_sixteen_bit_formats_against_fp64(gpu, fmt):
     try:
         out16, _ = _fp16_run(gpu, case, 200, key=45 + fmt)
     finally:
-        gpu.aero_lbm_b200_set_fp16_format(0)
+        gpu.aero_lbm_b200_set_fp16_format(1)
     e = O.flow_errors(out16, _oracle_run(case, 200, "f64"))
     assert e["u"] <= (3e-4 if fmt else 1e-3) and e["rho"] <= 1e-4, e

@@ -364,9 +364,10 @@ def test_oracle_runtime_halo_matches_reference_live(every):
 def test_oracle_short_packets_match_reference_live(channels):
     """Packets without the temperature channel (10) or also without the source
     channel (9): the reference temperature is 0 and, with 9 channels, the
-    transport's source comes from the fan channels."""
+    transport's source comes from the fan channels, also on cells a sparse
+    overlay rewrites (the overlay's source value is ignored then)."""
     cfg, pk, pre = O.runtime_case(12, 77, True, channels)
-    script = [("step",)] * 3 + [("flow",), ("temp",)] + [("step",)] * 2 + [("flow",), ("temp",)]
+    script = O.short_packet_script(pk)
     o = O.Oracle((12, 12, 12), O.derive_params(cfg), "f32")
     o.set_temperature(pre)
     res = O.run_script_oracle(o, cfg, pk, script)

@@ -64,7 +64,7 @@ def _run(gpu, storage, streamed, dims, seed, periodic_x, force, steps=24, key=30
         gpu.aero_lbm_b200_set_streamed_step(0)
         gpu.aero_lbm_set_realtime_solver_mode(0)
         gpu.aero_lbm_b200_set_collision_mode(0)
-        gpu.aero_lbm_b200_set_fp16_format(0)
+        gpu.aero_lbm_b200_set_fp16_format(1)
         gpu.aero_lbm_b200_set_physics_overrides(-1.0, -1.0, -1)
     return out, state
 

@@ -154,3 +154,30 @@ def test_bfecc_transport_matches_reference_golden(gpu, streaming, cpt):
     out, t = _run(gpu, n, cfg, [(0, pk)], steps, streaming, preload, key=680 + streaming, cpt=cpt)
     assert_bits(out, g["out"])
     assert np.array_equal(t.view(np.uint32), np.asarray(g["temperature"], np.float32).view(np.uint32))
+
+
+@pytest.mark.parametrize("collision,cpt", [(0, 1), (0, 2), (1, 2)])
+def test_fused_transport_equals_separate_pass(gpu, collision, cpt):
+    """The in-place step computing the transport itself (default) against the
+    separate transport pass, on the thermal case with mask changes between
+    calls (cells opening up take their temperature from the step, then
+    collide in the transition kernel): flow and temperature bit for bit."""
+    n, steps = 20, 16
+    obst, u, temp, src, cfg, preload = O.thermal_case(n, 41)
+    rng = np.random.default_rng(42)
+    obst2 = obst.copy()
+    obst2[(rng.random(obst.shape) < 0.03) & (obst == 0)] = 1
+    obst2[(rng.random(obst.shape) < 0.5) & (obst == 1)] = 0
+    pk1 = O.packet_from(obst, *u, temperature=temp, source=src)
+    pk2 = O.packet_from(obst2, *u, temperature=temp, source=src)
+    res = []
+    for fused in (1, 0):
+        assert gpu.aero_lbm_b200_set_fused_transport(fused) == 1
+        try:
+            res.append(_run(gpu, n, cfg, [(0, pk1), (7, pk2)], steps, 2, preload, key=640 + fused, cpt=cpt,
+                            collision=collision))
+        finally:
+            gpu.aero_lbm_b200_set_fused_transport(1)
+    (out_f, t_f), (out_s, t_s) = res
+    assert_bits(out_f, out_s)
+    assert np.array_equal(t_f.view(np.uint32), t_s.view(np.uint32))
