@@ -44,12 +44,25 @@ constexpr int kMaxDevices = 64;
 double* g_scratch_ptr[kMaxDevices] = {nullptr};
 std::mutex g_setup_mutex;
 
-// Device address of the scratch array for the current device (looked up once).
-double* scratch_for_current_device(std::string& err) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+// Device address of the scratch array on the context's device `dev` (looked
+// up once per device, with that device current). The call is rejected when
+// another device is current: the context's memory, the library stream and
+// the scratch all live on `dev`.
+double* scratch_for_device(int dev, std::string& err) {
+    if (dev < 0 || dev >= kMaxDevices) {
+        err = "the context's device " + std::to_string(dev) + " is outside the first " + std::to_string(kMaxDevices) +
+              " devices the scratch table covers";
+        return nullptr;
+    }
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) {
         err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+        return nullptr;
+    }
+    if (cur != dev) {
+        err = "device " + std::to_string(cur) + " is current but the context lives on device " + std::to_string(dev) +
+              "; make that device current first";
         return nullptr;
     }
     std::lock_guard<std::mutex> lk(g_setup_mutex);
@@ -191,7 +204,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums_noalloc(long long conte
         return 0;
     }
     std::string err;
-    double* scratch = scratch_for_current_device(err);
+    double* scratch = scratch_for_device(c->device, err);
     if (!scratch) {
         set_error("conservation_sums_noalloc: " + err);
         return 0;

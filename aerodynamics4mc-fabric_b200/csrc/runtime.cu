@@ -459,6 +459,7 @@ bool Context::allocate(int nx_, int ny_, int nz_) {
     release_device();
     nx = nx_; ny = ny_; nz = nz_;
     cells = (long long)nx * ny * nz;
+    if (cudaGetDevice(&device) != cudaSuccess) device = -1;
     const size_t c = (size_t)cells;
     auto al = [&](void** p, size_t bytes) { return cuda_ok(cudaMalloc(p, bytes + kCopySlack), "cudaMalloc"); };
     bool ok = true;
@@ -725,8 +726,23 @@ static float thermal_diffusivity() {
 }
 
 // One step of a context. packet may be null (cached step); out may be null.
+static bool step_context_body(Context& ctx, const float* packet, float* out, float scale, bool host_packet,
+                              const SparseOverlays* overlays, const DeviceFill* fill);
+
 bool step_context(Context& ctx, const float* packet, float* out, float scale, bool host_packet,
                   const SparseOverlays* overlays, const DeviceFill* fill) {
+    const bool ok = step_context_body(ctx, packet, out, scale, host_packet, overlays, fill);
+    if (!ok && host_packet && !fill && (packet || (overlays && overlays->count > 0))) {
+        // the caller owns its host buffers again when the call returns, also
+        // after a failure: wait for the host-to-device copies queued before it
+        // (a pinned buffer is read by DMA after cudaMemcpyAsync returns)
+        cudaStreamSynchronize(current_stream());
+    }
+    return ok;
+}
+
+static bool step_context_body(Context& ctx, const float* packet, float* out, float scale, bool host_packet,
+                              const SparseOverlays* overlays, const DeviceFill* fill) {
     cudaStream_t s = current_stream();
     const BrickDims d{ctx.nx, ctx.ny, ctx.nz, 0, ctx.cells};
     const FaceParams face_now = current_face_params();

@@ -25,6 +25,7 @@ constexpr size_t kCopySlack = 256;
 struct Context {
     int nx = 0, ny = 0, nz = 0;
     long long cells = 0;
+    int device = -1;  // CUDA device the context's memory lives on (current at allocation)
     float* g[2] = {nullptr, nullptr};
     uint8_t* obstacle[2] = {nullptr, nullptr};
     float* ref_p[2] = {nullptr, nullptr};

@@ -3,19 +3,27 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Workload (one GPU): the 128^3 terrain brick with Boussinesq buoyancy (seeded
-4-octave heightmap, inflow (0.08, 0.02, 0), Smagorinsky C = 0.1, g*beta = 1e-4
-along +z), stepped by the library's fused pull-stream + cumulant-collide kernel.
-Inputs are seeded synthetic data of the benchmark's shape (no dataset exists).
+4-octave heightmap, inflow (0.08, 0.02, 0) at x-, convective outflow at x+,
+far-field lid, Smagorinsky C = 0.1, g*beta = 1e-4 along +z, the temperature
+transported before every collision), stepped by the library's fused
+pull-stream + cumulant-collide kernel with 16-bit fixed-point deviation
+storage (the default format of the FP16 solver mode). Inputs are seeded
+synthetic data of the benchmark's shape (no dataset exists).
 
 value : device-resident MLUPS (state in HBM, one fused launch per step, CUDA
-        events on the launching stream; the 2 x 226 MB state is larger than L2).
+        events on the launching stream; the state is larger than L2). Each
+        variant's window of K steps is repeated until the windows cover at
+        least a second; the median window is reported.
 e2e   : the same metric through the reference-facing C ABI with host buffers:
         every step uploads the 11-channel packet from pinned memory
         (aero_lbm_step_rect) and reads back the stride-4 velocity atlas
-        (aero_lbm_extract_flow_atlas_rect).
+        (aero_lbm_extract_flow_atlas_rect). config.e2e_resident: the cached
+        step (aero_lbm_step_rect_cached) + atlas; config.brick_world: the
+        native brick-world service (aero_lbm_simulation_*) on the same terrain
+        as eight 64^3 bricks, a tick + eight int16 atlases per step.
 --impl reference: the reference's own CPU step (oracle/_ref, built from the
         reference sources) on the box's host cores, one single-threaded process
-        per core, each on a 64^3 window of the same workload.
+        per core, each stepping the same 128^3 brick.
 
 With torchrun (N > 1) every rank steps its own brick (bricks are independent
 work units; no data-path collective), timing is the max over ranks and value
@@ -25,6 +33,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import dataclasses
 import importlib.util
 import json
 import multiprocessing as mp
@@ -100,7 +109,7 @@ class ClockSampler:
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -135,105 +144,120 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- reference arm (CPU)
+# Steps per reference process: each is ~5 s of one core on the 128^3 brick, so
+# a run of K steps is bounded to keep the arm within a few minutes.
+REF_MAX_STEPS = 20
+
+
+def host_cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.lower().startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def _ref_worker(args):
-    """One process: the reference CPU step on a 64^3 window of the workload."""
-    steps, warmup, q = args
+    """One process: the reference CPU step on the benchmark's 128^3 brick
+    (same packet, configuration and starting temperature as our arm)."""
+    steps, warmup, n = args
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
     cases = load_cases()
-    case = cases.c2_terrain_boussinesq(128)
-    w = 64
-    obst = np.ascontiguousarray(case.obstacle[:w, :w, :w])
-    u = [np.ascontiguousarray(a[:w, :w, :w]) for a in case.u]
-    temp = np.ascontiguousarray(case.temperature[:w, :w, :w])
+    case = cases.c2_terrain_boussinesq(n)
     cfg = case.config_dict()
-    cfg["faces"] = case.faces
     ref = O.RefLib()
     lib = ref.lib
-    lib.aero_lbm_init_rect(w, w, w, 11, 4)
+    lib.aero_lbm_init_rect(n, n, n, 11, 4)
     c = O.config_struct(O.RefBenchmarkConfig, cfg, lib.aero_lbm_benchmark_default_config)
     lib.aero_lbm_benchmark_set_config(ctypes.byref(c))
-    # the window's temperature field as the starting state (as our arm loads it)
-    lib.aero_lbm_set_temperature_state_rect(w, w, w, 1, np.ascontiguousarray(temp.reshape(-1)).ctypes.data)
-    pk = O.packet_from(obst, *u, temperature=temp)
+    lib.aero_lbm_set_temperature_state_rect(n, n, n, 1, np.ascontiguousarray(case.temperature.reshape(-1)).ctypes.data)
+    pk = np.ascontiguousarray(case.packet())
     for _ in range(warmup):
-        lib.aero_lbm_step_rect(pk.ctypes.data, w, w, w, 1, None)
-    q.put("ready")
+        lib.aero_lbm_step_rect(pk.ctypes.data, n, n, n, 1, None)
     t0 = time.perf_counter()
     for _ in range(steps):
-        lib.aero_lbm_step_rect(pk.ctypes.data, w, w, w, 1, None)
+        lib.aero_lbm_step_rect(pk.ctypes.data, n, n, n, 1, None)
     dt = time.perf_counter() - t0
-    return w ** 3 * steps / dt / 1e6
+    return n ** 3 * steps / dt / 1e6
 
 
-def run_reference_arm(steps: int, warmup: int, procs: int | None = None) -> dict:
+def _run_ref_processes(procs: int, steps: int, warmup: int, n: int) -> tuple[list, float]:
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        t0 = time.perf_counter()
+        per = pool.map(_ref_worker, [(steps, warmup, n)] * procs)
+        wall = time.perf_counter() - t0
+    return per, wall
+
+
+def run_reference_arm(steps: int, warmup: int, n: int = 128, procs: int | None = None) -> dict:
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
     if not O.REF_LIB.exists():
         return {"impl": "reference", "unavailable": "oracle/_ref/libaero_lbm_ref.so was not built (reference sources absent)"}
     cores = procs or max(1, min(os.cpu_count() or 1, 16))
-    ctx = mp.get_context("spawn")
-    with ctx.Manager() as m:
-        q = m.Queue()
-        with ctx.Pool(cores) as pool:
-            t0 = time.perf_counter()
-            per = pool.map(_ref_worker, [(steps, warmup, q)] * cores)
-            wall = time.perf_counter() - t0
+    ref_steps = max(1, min(steps, REF_MAX_STEPS))
+    per, wall = _run_ref_processes(cores, ref_steps, min(warmup, 1), n)
     value = float(sum(per))
+    cpu = host_cpu_model()
     return {
         "impl": "reference",
         "metric": METRIC,
         "value": value,
         "unit": "MLUPS",
         "n_gpus": 0,
-        "steps": steps,
-        "warmup": warmup,
-        "ms_per_step": 64 ** 3 / (value / cores * 1e6) * 1e3,
+        "steps": ref_steps,
+        "warmup": min(warmup, 1),
+        "ms_per_step": n ** 3 / (value / cores * 1e6) * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded terrain, heightmap, temperature field)",
-        "config": {"workload": "d3q27-terrain-boussinesq 64^3 window of the 128^3 brick, reference CPU step",
-                   "processes": cores},
-        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": cores, "kind": "reference",
-                         "sample": f"{cores} processes x {steps} steps of a 64^3 window ({wall:.1f}s wall)"},
+        "config": {"workload": f"d3q27-cumulant {n}^3 terrain brick, SGS C=0.1, Boussinesq g*beta=1e-4, "
+                               "outflow x+, temperature transport; reference CPU step",
+                   "processes": cores, "same_config": True, "host_cpu": cpu},
+        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": cores, "kind": "reference", "host_cpu": cpu,
+                         "sample": f"{cores} single-threaded processes x {ref_steps} steps of the {n}^3 brick "
+                                   f"(steps bounded to {REF_MAX_STEPS}; {wall:.1f}s wall)"},
         "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
-def cpu_baseline_single(seconds: float = 15.0) -> dict | None:
-    """Reference CPU step, one core, bounded sample of the same workload."""
+def cpu_baseline_single(n: int = 128, steps: int = 3) -> dict | None:
+    """Reference CPU step, one core, a bounded sample of the same workload
+    (a few steps of the 128^3 brick, ~15-20 s)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
     if not O.REF_LIB.exists():
         return None
-    ctx = mp.get_context("spawn")
-    est_steps = max(2, int(seconds / 1.0))
-    with ctx.Manager() as m:
-        q = m.Queue()
-        with ctx.Pool(1) as pool:
-            v = pool.map(_ref_worker, [(est_steps, 1, q)])[0]
-    return {"value": v, "unit": "MLUPS", "cores": 1, "kind": "reference",
-            "sample": f"{est_steps} steps of a 64^3 window of the workload, single-threaded reference CPU step"}
+    per, wall = _run_ref_processes(1, steps, 1, n)
+    return {"value": per[0], "unit": "MLUPS", "cores": 1, "kind": "reference", "host_cpu": host_cpu_model(),
+            "sample": f"{steps} steps of the {n}^3 brick after one warm-up step, single-threaded reference CPU step "
+                      f"({wall:.1f}s wall)"}
 
 
 # ---------------------------------------------------------------- our arm
 # Temperature transport per cell and step: state read + write (2 x 4 B) and
 # the previous collision's velocity written by the collision and read by the
-# transport (2 x 12 B).
+# transport (2 x 12 B); since the transport runs inside the step kernel these
+# bytes are part of that kernel's traffic.
 THERMAL_BYTES = 2 * 4 + 2 * 12
 VARIANTS = {
-    # name: (realtime solver mode, collision mode, bytes per cell-step, storage note)
-    "fp16": (3, 1, 27 * 2 * 2 + 1, "fp16 deviation storage, in-place esoteric pull, factorised collision, "
-                                   "two cells per thread in packed FP32"),
-    "i16": (3, 1, 27 * 2 * 2 + 1, "16-bit fixed-point deviation storage, in-place esoteric pull, factorised collision"),
-    "fp32_exact": (0, 0, 27 * 4 * 2 + 1, "fp32, in-place esoteric pull, reference-order collision (bit-exact)"),
-    "fp32_fast": (0, 1, 27 * 4 * 2 + 1, "fp32, in-place esoteric pull, factorised collision"),
+    # name: (realtime solver mode, collision mode, 16-bit format, bytes per cell-step, storage note)
+    "i16": (3, 1, 1, 27 * 2 * 2 + 1, "16-bit fixed-point deviation storage (the FP16 mode's default format), "
+                                     "in-place esoteric pull, factorised collision, two cells per thread in packed FP32"),
+    "fp16": (3, 1, 0, 27 * 2 * 2 + 1, "IEEE-half deviation storage, in-place esoteric pull, factorised collision"),
+    "fp32_exact": (0, 0, 1, 27 * 4 * 2 + 1, "fp32, in-place esoteric pull, reference-order collision (bit-exact)"),
+    "fp32_fast": (0, 1, 1, 27 * 4 * 2 + 1, "fp32, in-place esoteric pull, factorised collision"),
 }
+HEADLINE = "i16"
 
 
 def setup_context(aero, lib, case, variant: str, key: int, streaming: int, thermal: int = -1):
@@ -243,9 +267,9 @@ def setup_context(aero, lib, case, variant: str, key: int, streaming: int, therm
     temperature field is loaded as the starting state."""
     import torch
 
-    solver_mode, collision, _, _ = VARIANTS[variant]
+    solver_mode, collision, fmt, _, _ = VARIANTS[variant]
     lib.aero_lbm_set_realtime_solver_mode(solver_mode)
-    lib.aero_lbm_b200_set_fp16_format(1 if variant == "i16" else 0)
+    lib.aero_lbm_b200_set_fp16_format(fmt)
     lib.aero_lbm_b200_set_collision_mode(collision)
     lib.aero_lbm_b200_set_physics_overrides(case.smagorinsky_c, case.buoyancy_beta, case.gravity_axis)
     lib.aero_lbm_b200_set_streaming_mode(streaming)
@@ -273,8 +297,52 @@ def setup_context(aero, lib, case, variant: str, key: int, streaming: int, therm
         raise RuntimeError(aero.last_error(lib))
     lib.aero_lbm_set_realtime_solver_mode(0)
     lib.aero_lbm_b200_set_collision_mode(0)
-    lib.aero_lbm_b200_set_fp16_format(0)
+    lib.aero_lbm_b200_set_fp16_format(1)
     return ctx, packet, pk_ptr
+
+
+def run_brick_world_leg(aero, lib, case, ticks: int, warmup: int, stride: int = 4) -> dict:
+    """The native brick-world service (aero_lbm_simulation_*, what the mod's
+    ClientL2Solver calls through JNI) on the benchmark's terrain split into
+    eight 64^3 bricks (a 2 x 2 x 2 world): the reference service's game-runtime
+    physics in its classic solver mode (fans, edge nudge, sponge, the
+    every-other-tick temperature transport, halo exchanges between the bricks).
+    A step = one tick + the eight stride-4 int16 atlases read back."""
+    n = case.dims[0] // 2
+    svc = aero.BrickWorldService(lib)
+    try:
+        svc.ensure_world(1, n, dx=1.0, dt=0.05, solver_mode=1)
+        coords = [(bx, by, bz) for bx in range(2) for by in range(2) for bz in range(2)]
+        svc.set_hints(1, coords)
+        flow = np.zeros(case.dims + (4,), np.float32)
+        for a in range(3):
+            flow[..., a] = case.u[a]
+        for (bx, by, bz) in coords:
+            sl = (slice(bx * n, (bx + 1) * n), slice(by * n, (by + 1) * n), slice(bz * n, (bz + 1) * n))
+            svc.upload_static(1, (bx, by, bz), case.obstacle[sl])
+            svc.upload_dynamic(1, (bx, by, bz), flow[sl], case.temperature[sl])
+        res = (n + stride - 1) // stride
+        atlases = [np.zeros(res ** 3 * 4, np.int16) for _ in coords]
+        for _ in range(warmup):
+            svc.step(1, 1)
+        launches0 = lib.aero_lbm_b200_launch_count()
+        t0 = time.perf_counter()
+        for _ in range(ticks):
+            svc.step(1, 1)
+            for c, out in zip(coords, atlases):
+                svc.atlas(1, c, stride, out)
+        dt = time.perf_counter() - t0
+        launches = lib.aero_lbm_b200_launch_count() - launches0
+        status = svc.status(1).tolist()
+    finally:
+        svc.release()
+    cells = len(coords) * n ** 3
+    return {"workload": f"brick world 2x2x2 of {n}^3 bricks (the terrain brick split), classic solver mode, "
+                        "game-runtime physics, exact hints",
+            "api": "aero_lbm_simulation_step_brick_world_runtime + copy_brick_world_packed_flow_atlas (stride 4)",
+            "cells_per_tick": cells, "ticks": ticks, "ms_per_tick": dt / ticks * 1e3,
+            "mlups": cells * ticks / dt / 1e6, "d2h_bytes_per_tick": int(sum(a.nbytes for a in atlases)),
+            "h2d_bytes_per_tick": 0, "launches_per_tick": launches / ticks, "status": status}
 
 
 def run_batch_leg(aero, lib, torch, stream, ticks: int, warmup: int) -> dict:
@@ -439,103 +507,128 @@ def run_ours(args) -> dict | None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def timed(variant: str, key: int, steps: int, sample_clocks: bool):
+    def timed(variant: str, key: int, steps: int):
+        """Windows of `steps` device-resident steps, repeated until they cover
+        at least a second (3..5000 windows, the same count on every rank);
+        the median window, each window's time the max over ranks."""
         ctx, packet, pk_ptr = setup_context(aero, lib, case, variant, key, args.streaming)
         for _ in range(args.warmup):
             ctx.advance(1)
         barrier()
-        launches0 = lib.aero_lbm_b200_launch_count()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        window_ms, launches = [], 0
         lib.aero_lbm_b200_kernel_timer(1)  # events around each step-kernel launch, on the library's stream
         with ClockSampler(local) as clk:
-            start.record(stream)
-            for _ in range(steps):
-                ctx.advance(1)
-            end.record(stream)
-            barrier()
-        launches = lib.aero_lbm_b200_launch_count() - launches0
+            windows = 3
+            while len(window_ms) < windows:
+                launches0 = lib.aero_lbm_b200_launch_count()
+                barrier()
+                start.record(stream)
+                for _ in range(steps):
+                    ctx.advance(1)
+                end.record(stream)
+                barrier()
+                launches = lib.aero_lbm_b200_launch_count() - launches0
+                window_ms.append(max_over_ranks(start.elapsed_time(end)))
+                if len(window_ms) == 1:
+                    windows = int(max_over_ranks(float(min(5000, max(3, -(-1000.0 // max(window_ms[0], 1e-3)))))))
         kms, kn = ctypes.c_double(0.0), ctypes.c_int(0)
         lib.aero_lbm_b200_kernel_time(ctypes.byref(kms), ctypes.byref(kn))
         lib.aero_lbm_b200_kernel_timer(0)
         kernel_ms = max_over_ranks(kms.value / max(1, kn.value))
-        ms = max_over_ranks(start.elapsed_time(end))
-        return ctx, packet, pk_ptr, ms, launches, clk.summary() if sample_clocks else None, kernel_ms
+        ms = statistics.median(window_ms)
+        return ctx, packet, pk_ptr, ms, launches, clk.summary(), kernel_ms, window_ms
 
     results = {}
-    head_ctx = None
-    for variant in ("fp16", "fp32_exact", "fp32_fast", "i16"):
-        if variant != "fp16" and variant not in args.variants:
-            continue
-        steps = args.steps if variant == "fp16" else max(10, args.steps // 2)
-        ctx, packet, pk_ptr, ms, launches, clocks, kernel_ms = timed(variant, 1 + rank * 8 + len(results), steps,
-                                                                     variant == "fp16")
+    head = None
+    for variant in [HEADLINE] + [v for v in args.variants if v != HEADLINE]:
+        steps = args.steps
+        ctx, packet, pk_ptr, ms, launches, clocks, kernel_ms, windows = timed(variant, 1 + rank * 8 + len(results), steps)
         ms_step = ms / steps
-        # achieved_gbs: the stream-collide kernel's algorithmic population
-        # bytes over its own launch time; step_gbs: every algorithmic byte of
-        # the step (populations + temperature transport) over the step time.
+        nbytes = VARIANTS[variant][3]
+        # achieved_gbs: the stream-collide kernel's algorithmic bytes (the
+        # populations, plus the transport's fields, which it computes in
+        # place) over its own launch time; step_gbs: the same bytes over the
+        # step time (the kernel plus the per-call boundary fill).
         results[variant] = {"mlups": cells * world * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms_step,
                             "launches": launches, "clocks": clocks, "steps": steps, "kernel_ms": kernel_ms,
-                            "achieved_gbs": VARIANTS[variant][2] * cells / (kernel_ms * 1e-3) / 1e9,
-                            "step_gbs": (VARIANTS[variant][2] + THERMAL_BYTES) * cells / (ms_step * 1e-3) / 1e9}
-        if variant == "fp16":
-            head_ctx = (ctx, packet, pk_ptr)
+                            "windows": len(windows), "window_ms_min": min(windows), "window_ms_max": max(windows),
+                            "achieved_gbs": (nbytes + THERMAL_BYTES) * cells / (kernel_ms * 1e-3) / 1e9,
+                            "population_gbs": nbytes * cells / (kernel_ms * 1e-3) / 1e9,
+                            "step_gbs": (nbytes + THERMAL_BYTES) * cells / (ms_step * 1e-3) / 1e9}
+        if variant == HEADLINE:
+            head = (ctx, packet, pk_ptr)
         else:
             ctx.release()
 
-    # e2e through the C ABI with host buffers (FP16 brick): per step the
+    # e2e through the C ABI with host buffers (headline brick): per step the
     # pinned 11-channel packet goes up (aero_lbm_step_rect) and the stride-4
     # velocity atlas comes back (aero_lbm_extract_flow_atlas_rect).
-    ctx, packet, pk_ptr = head_ctx
+    ctx, packet, pk_ptr = head
     stride = 4
     atlas = np.zeros(((n + stride - 1) // stride) ** 3 * 4, np.float32)
     e2e_steps = max(3, min(args.steps, 50))
-    for _ in range(2):
-        lib.aero_lbm_step_rect(pk_ptr, n, n, n, ctx.key, None)
-        lib.aero_lbm_extract_flow_atlas_rect(n, n, n, ctx.key, stride, aero.fptr(atlas), atlas.size)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        if not lib.aero_lbm_step_rect(pk_ptr, n, n, n, ctx.key, None):
-            raise RuntimeError(aero.last_error(lib))
-        if not lib.aero_lbm_extract_flow_atlas_rect(n, n, n, ctx.key, stride, aero.fptr(atlas), atlas.size):
-            raise RuntimeError(aero.last_error(lib))
-    barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = cells * world * e2e_steps / e2e_s / 1e6
+
+    def e2e_run(cached: bool) -> float:
+        for _ in range(2):
+            ok = (lib.aero_lbm_step_rect_cached(n, n, n, ctx.key, None) if cached
+                  else lib.aero_lbm_step_rect(pk_ptr, n, n, n, ctx.key, None))
+            if not ok or not lib.aero_lbm_extract_flow_atlas_rect(n, n, n, ctx.key, stride, aero.fptr(atlas), atlas.size):
+                raise RuntimeError(aero.last_error(lib))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ok = (lib.aero_lbm_step_rect_cached(n, n, n, ctx.key, None) if cached
+                  else lib.aero_lbm_step_rect(pk_ptr, n, n, n, ctx.key, None))
+            if not ok or not lib.aero_lbm_extract_flow_atlas_rect(n, n, n, ctx.key, stride, aero.fptr(atlas), atlas.size):
+                raise RuntimeError(aero.last_error(lib))
+        barrier()
+        return cells * world * e2e_steps / max_over_ranks(time.perf_counter() - t0) / 1e6
+
+    e2e_value = e2e_run(False)
+    e2e_resident = e2e_run(True)
     ctx.release()
 
-    # Accuracy leg: every variant after `accuracy_steps` calls from the same
-    # inputs against the FP64 run of the same scheme (the adjoint module's
-    # forward in double precision, every fluid cell probed), and FP16
-    # against the bit-exact FP32 step.
+    # Accuracy: every variant after `accuracy_steps` calls from the same
+    # inputs against the FP64 run of the same scheme on the GPU (the adjoint
+    # module's forward in double precision, every fluid cell probed). That
+    # forward holds the temperature fixed and has no outflow face, so this leg
+    # runs the brick with an equilibrium x+ face and without the transport;
+    # the configured case (outflow, transport) is checked against the
+    # oracle's FP64 run at 64^3 x 1000 in tests/test_fp16_c2_gpu.py.
     acc = None
     if args.accuracy_steps > 0:
+        far = {"kind": 4, "velocity": case.u_ref}
+        acase = dataclasses.replace(case, faces=[case.faces[0], far] + list(case.faces[2:]))
         outs = {}
-        # The FP64 reference run (the adjoint module's forward) takes the
-        # temperature as a fixed field, so the variants run without the
-        # temperature transport here: the leg measures storage precision.
-        for k, variant in enumerate(("fp16", "i16", "fp32_fast", "fp32_exact")):
-            c, _, _ = setup_context(aero, lib, case, variant, 90 + 8 * rank + k, args.streaming, thermal=0)
+        for k, variant in enumerate(("i16", "fp16", "fp32_fast", "fp32_exact")):
+            c, _, _ = setup_context(aero, lib, acase, variant, 90 + 8 * rank + k, args.streaming, thermal=0)
             c.advance(args.accuracy_steps - 1)
             outs[variant] = c.flow_state()
             c.release()
         lib.aero_lbm_b200_set_thermal_transport(-1)
-        fluid = np.flatnonzero(case.obstacle.reshape(-1) == 0).astype(np.int32)
-        ab = aero.AdjointBrick(case.obstacle, case.temperature, lib=lib, face_kind=[f["kind"] for f in case.faces],
-                               tau=case.tau, smagorinsky_c=case.smagorinsky_c, buoyancy_beta=case.buoyancy_beta,
+        fluid = np.flatnonzero(acase.obstacle.reshape(-1) == 0).astype(np.int32)
+        ab = aero.AdjointBrick(acase.obstacle, acase.temperature, lib=lib, face_kind=[f["kind"] for f in acase.faces],
+                               tau=acase.tau, smagorinsky_c=acase.smagorinsky_c, buoyancy_beta=acase.buoyancy_beta,
                                steps=args.accuracy_steps, checkpoint_every=20)
         ab.set_probes(fluid, np.zeros((fluid.size, 3), np.float32))
-        _, u64 = ab.forward(None, case.u_ref, precision=1)
+        _, u64 = ab.forward(None, acase.u_ref, precision=1)
         ab.close()
         speed64 = float(np.max(np.linalg.norm(u64.astype(np.float64), axis=1)))
         ref = outs["fp32_exact"].astype(np.float64)
         speed = float(np.max(np.linalg.norm(ref[:, :3], axis=1)))
         acc = {"steps": args.accuracy_steps,
                **{f"{v}_vs_fp64_u": float(np.max(np.abs(outs[v][fluid, :3] - u64))) / speed64 for v in outs},
-               "fp16_vs_fp32_u": float(np.max(np.abs(outs["fp16"][:, :3] - ref[:, :3]))) / speed,
-               "fp16_vs_fp32_rho": float(np.max(np.abs(outs["fp16"][:, 3] - ref[:, 3]))) / float(np.max(1 + ref[:, 3])),
-               "metric": "max |u - u64| / max |u64| over fluid cells"}
+               **{f"{v}_vs_fp32_exact_u": float(np.max(np.abs(outs[v][:, :3] - ref[:, :3]))) / speed
+                  for v in ("i16", "fp16", "fp32_fast")},
+               "i16_vs_fp32_exact_rho": float(np.max(np.abs(outs["i16"][:, 3] - ref[:, 3]))) / float(np.max(1 + ref[:, 3])),
+               "metric": "max |u - u64| / max |u64| over fluid cells",
+               "fp64_reference": "the library's double-precision forward (adjoint module) on the GPU",
+               "case": f"the {n}^3 terrain brick with an equilibrium x+ face and the temperature held fixed",
+               "configured_case_check": "tests/test_fp16_c2_gpu.py: default 16-bit format vs the oracle's FP64 run, "
+                                        "64^3, outflow x+, temperature transport, 1000 steps, bound 1e-3"}
 
+    brick_world = run_brick_world_leg(aero, lib, case, max(5, min(args.steps, 40)), args.warmup) if args.brick_world else None
     batch = None
     if args.batch_ticks > 0:
         batch = run_batch_leg(aero, lib, torch, stream, args.batch_ticks, args.warmup)
@@ -556,7 +649,7 @@ def run_ours(args) -> dict | None:
     if meso is not None:
         for k in ("fp32", "fp32_packed", "fp16", "i16"):
             meso[f"{k}_frac_of_peak"] = meso[f"{k}_achieved_gbs"] / peak
-    h = results["fp16"]
+    h = results[HEADLINE]
     achieved = h["achieved_gbs"]
     out = {
         "metric": METRIC,
@@ -569,28 +662,36 @@ def run_ours(args) -> dict | None:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "fp16-store/f32-compute",
+        "dtype": "i16-store/f32-compute",
         "data": "synthetic (seeded 4-octave terrain, temperature lapse + warm bubble)",
-        "config": {"workload": f"d3q27-cumulant {n}^3 terrain brick, SGS C=0.1, Boussinesq g*beta=1e-4, FP16 in-place",
-                   "bricks_per_gpu": 1, "cells_per_gpu": cells, "storage": VARIANTS["fp16"][3],
-                   "l2": "inputs larger than L2 (fp16 state 119 MB + fields; fp32 state 238 MB); no flush",
+        "config": {"workload": f"d3q27-cumulant {n}^3 terrain brick, inflow x-, convective outflow x+, SGS C=0.1, "
+                               "Boussinesq g*beta=1e-4 with the temperature transport, 16-bit fixed-point in-place",
+                   "bricks_per_gpu": 1, "cells_per_gpu": cells, "storage": VARIANTS[HEADLINE][4],
+                   "l2": "inputs larger than L2 (16-bit state 119 MB + fields; fp32 state 238 MB); no flush",
                    "parallelism": f"bricks x{world}",
-                   **{f"{v}_mlups": results[v]["mlups"] for v in results if v != "fp16"},
-                   **{f"fp16_over_{v}": h["mlups"] / results[v]["mlups"] for v in results if v != "fp16"},
-                   **{f"{v}_frac_of_peak": results[v]["achieved_gbs"] / peak for v in results if v != "fp16"},
+                   "timing": f"windows of {h['steps']} steps repeated to >= 1 s (median of {h['windows']}: "
+                             f"{h['window_ms_min']:.2f}..{h['window_ms_max']:.2f} ms)",
+                   **{f"{v}_mlups": results[v]["mlups"] for v in results if v != HEADLINE},
+                   **{f"{HEADLINE}_over_{v}": h["mlups"] / results[v]["mlups"] for v in results if v != HEADLINE},
+                   **{f"{v}_frac_of_peak": results[v]["achieved_gbs"] / peak for v in results},
                    **{f"{v}_kernel_us": results[v]["kernel_ms"] * 1e3 for v in results},
                    **{f"{v}_step_gbs": results[v]["step_gbs"] for v in results},
-                   "temperature_transport": "the reference's benchmark-mode scalar update before every collision "
-                                            "(buoyancy on); the case's field loaded as the starting state",
+                   "temperature_transport": "the reference's benchmark-mode scalar update before every collision, "
+                                            "computed inside the step kernel; the case's field loaded as the starting state",
+                   "e2e_resident": {"value": e2e_resident, "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                                    "d2h_bytes_per_step": int(atlas.nbytes), "steps": e2e_steps,
+                                    "api": "aero_lbm_step_rect_cached + aero_lbm_extract_flow_atlas_rect(stride 4)"},
+                   "brick_world": brick_world,
                    "accuracy": acc,
                    "batch": batch,
                    "meso_d3q19": meso,
                    "adjoint": adjoint},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic_record(f"step_ip2_fp16@{n}"), "peak_source": peak_kind,
-                     "bytes_per_cell": VARIANTS["fp16"][2], "kernel": "step_ip2_kernel<StoreF16Dev>",
+                     "traffic": traffic_record(f"step_ip2_i16@{n}"), "peak_source": peak_kind,
+                     "bytes_per_cell": VARIANTS[HEADLINE][3] + THERMAL_BYTES,
+                     "kernel": "step_ip2_kernel<StoreI16Dev> (temperature transport fused)",
                      "kernel_us": h["kernel_ms"] * 1e3,
-                     "timing": "CUDA events around each step-kernel launch on the library's stream, timed region"},
+                     "timing": "CUDA events around each step-kernel launch on the library's stream, timed windows"},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": int(packet.numel() * 4),
                 "d2h_bytes_per_step": int(atlas.nbytes), "steps": e2e_steps,
                 "api": "aero_lbm_step_rect (pinned packet) + aero_lbm_extract_flow_atlas_rect(stride 4)"},
@@ -598,26 +699,28 @@ def run_ours(args) -> dict | None:
         "clocks": h["clocks"],
     }
     if not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline_single()
+        out["cpu_baseline"] = cpu_baseline_single(n)
     return out
 
 
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--streaming", type=int, default=0, help="0 auto, 1 two-buffer, 2 in-place")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-ticks", type=int, default=500, help="ticks of the 512-brick batch leg (0 skips it)")
-    ap.add_argument("--variants", default="fp32_exact,fp32_fast,i16",
-                    help="FP32 variants measured beside the FP16 headline (comma list, may be empty)")
+    ap.add_argument("--variants", default="fp16,fp32_exact,fp32_fast",
+                    help="variants measured beside the 16-bit fixed-point headline (comma list, may be empty)")
     ap.add_argument("--meso-steps", type=int, default=2000, help="steps of the D3Q19 mesoscale leg (0 skips it)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false", help="skip the adjoint (gradient) leg")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
-                    help="steps of the FP16-vs-FP32 accuracy leg (0 skips it)")
+                    help="steps of the 16-bit-vs-FP64 accuracy leg (0 skips it)")
+    ap.add_argument("--no-brick-world", dest="brick_world", action="store_false",
+                    help="skip the brick-world service leg")
     args = ap.parse_args()
     args.variants = [v for v in args.variants.split(",") if v]
     if args.warmup < 3:
@@ -625,8 +728,7 @@ def main() -> int:
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0
-        ref_steps = max(1, min(args.steps, 10))
-        print(json.dumps(run_reference_arm(ref_steps, min(args.warmup, 1))))
+        print(json.dumps(run_reference_arm(args.steps, args.warmup, args.n)))
         return 0
     res = run_ours(args)
     if res is not None:

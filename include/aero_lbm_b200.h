@@ -300,9 +300,10 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums(long long context_key, 
  * allocation that synchronises the device; an embedding with a fixed device
  * memory budget). No counterpart in the reference. Its scratch is a static
  * 256 KiB device array, so contexts of at most 2,097,152 cells (128^3) are
- * accepted; larger ones return 0 with an error. The first call on a device
- * looks up the array's address; make it before any stream capture. Calls
- * share the array: overlapping calls on the GPU race. */
+ * accepted; larger ones return 0 with an error. Call it with the context's
+ * device current (another current device is rejected with an error). The
+ * first call on a device looks up the array's address; make it before any
+ * stream capture. Calls share the array: overlapping calls on the GPU race. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums_noalloc(long long context_key, double* out4);
 /* FP32 collision arithmetic: 0 = the reference's operation order, no
  * multiply-add contraction (bit-identical to the reference CPU step; default),

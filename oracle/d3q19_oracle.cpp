@@ -25,6 +25,8 @@
 #include <memory>
 #include <vector>
 
+#include "parallel_for.h"
+
 namespace {
 
 constexpr int Q = 19;
@@ -240,7 +242,7 @@ struct Meso {
         std::vector<T> pf(f.size()), pg(g.size()), ndeep(cells), nsurf(cells);
         const T fx = T(opt.body_force[0]), fy = T(opt.body_force[1]), fz = T(opt.body_force[2]);
         const bool forced = fx != T(0) || fy != T(0) || fz != T(0);
-        for (int x = 0; x < nx; ++x)
+        oracle_par::parallel_for(nx, [&](int x) {
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     const int i = idx(x, y, z);
@@ -303,7 +305,8 @@ struct Meso {
                         pg[od] = gep - gop;
                     }
                 }
-        for (int x = 0; x < nx; ++x)
+        });
+        oracle_par::parallel_for(nx, [&](int x) {
             for (int y = 0; y < ny; ++y)
                 for (int z = 0; z < nz; ++z) {
                     const int i = idx(x, y, z);
@@ -379,6 +382,7 @@ struct Meso {
                         gn[d] = gv;
                     }
                 }
+        });
         f.swap(fn);
         g.swap(gn);
         deep.swap(ndeep);

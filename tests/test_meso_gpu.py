@@ -229,3 +229,35 @@ def test_hydro_packed_open_boundaries_mask_change_odd_nz(gpu):
             pass
         e_u, e_rho = _errors(*last)
         assert e_u <= 1e-4 and e_rho <= 1e-5, (dims, e_u, e_rho)
+
+
+@pytest.fixture(scope="module")
+def c3_shaped_fp64():
+    """The mesoscale configuration's construction on a 64 x 32 x 64 grid, the
+    full 2000 steps, run by the oracle in double precision (once per module)."""
+    c = c3_small(64, 32, 64, seed=8)
+    ref = O.MesoOracle(c.dims, dx=c.dx_m, dt=c.dt_s, precision="f64", options=oracle_options(c.options))
+    want = None
+    for _ in range(2000):
+        want = ref.step(c.forcing)
+    return c, want
+
+
+@pytest.mark.parametrize("storage,collision,bound", [(0, 1, 1e-4), (1, 1, 2.5e-3), (2, 1, 1e-3)])
+def test_hydro_storages_vs_fp64_c3_shaped_2000(gpu, c3_shaped_fp64, storage, collision, bound):
+    """Each storage of the hydrodynamic D3Q19 step (FP32 packed, IEEE half,
+    16-bit fixed point) after 2000 steps against the FP64 run: wind error
+    relative to the largest wind, density error."""
+    c, want = c3_shaped_fp64
+    ctx = aero_b200.MesoscaleContext(c.dims, dx_m=c.dx_m, dt_s=c.dt_s,
+                                     options={**c.options, "storage": storage, "collision": collision})
+    ctx.step(c.forcing)
+    ctx.advance(1999)
+    got = ctx.state()
+    ctx.release()
+    umax = float(np.abs(want[:, 3:]).max())
+    err_u = float(np.abs(got[:, 3:] - want[:, 3:]).max()) / umax
+    err_rho = float(np.abs(got[:, 0] - want[:, 0]).max())
+    print(f"D3Q19 storage {storage} vs FP64 after 2000 steps: wind {err_u:.3e}, rho {err_rho:.3e}")
+    assert err_u <= bound, err_u
+    assert err_rho <= 1e-4, err_rho
