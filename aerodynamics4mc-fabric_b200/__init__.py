@@ -245,6 +245,7 @@ SIGNATURES = {
     "aero_lbm_b200_kernel_time": (_I, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
     "aero_lbm_b200_set_fp16_format": (_I, [_I]),
     "aero_lbm_b200_set_fused_transport": (_I, [_I]),
+    "aero_lbm_b200_reset_tuning": (None, []),
     "aero_lbm_b200_conservation_sums": (_I, [_LL, ctypes.POINTER(ctypes.c_double)]),
     "aero_lbm_b200_conservation_sums_noalloc": (_I, [_LL, ctypes.POINTER(ctypes.c_double)]),
     "aero_lbm_b200_set_force_field": (_I, [_LL, _F32P, _I]),

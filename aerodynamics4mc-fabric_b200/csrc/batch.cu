@@ -578,7 +578,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_batch_add_brick(long long handle, int nx,
         berr("batch_add_brick: batch already finalized");
         return 0;
     }
-    if (nx <= 0 || ny <= 0 || nz <= 0 || (long long)(nx + 2) * (ny + 2) * (nz + 2) * 27 >= (1LL << 31)) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || (long long)(nx + 2) * (ny + 2) * pad_row(nz) * 27 >= (1LL << 31)) {
         berr("batch_add_brick: invalid or too large brick dimensions");
         return 0;
     }

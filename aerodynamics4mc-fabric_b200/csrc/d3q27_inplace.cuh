@@ -2,11 +2,12 @@
 // population storage (FP32 or FP16 deviation) and the collision arithmetic
 // (reference order or factorised). See inplace27.cuh for the slot maps.
 //
-// The in-place layout supports the faces whose pulled value is local to the
-// pulling cell: periodic, bounce-back and the equilibrium faces (velocity,
-// pressure, moving wall). Symmetry and convective outflow read other cells'
-// post-collision populations, which the in-place update overwrites within the
-// step; contexts with such faces use the two-buffer kernels.
+// The step kernels resolve periodic and bounce-back faces themselves; every
+// other face kind (equilibrium faces, symmetry, convective outflow) has its
+// pulled values written into the ghost layer by face_fill_ip_kernel after the
+// previous call's step, from the post-collision populations that step left
+// (ip_face_source). An axis that is periodic on one side only has no in-place
+// form.
 #pragma once
 
 #include "d3q27_step.cuh"
@@ -42,6 +43,12 @@ struct IpArgs {
     // come back when the cell opens again. Stored at a canonical parity:
     // entry (p ? opp(q) : q) holds population q at a step of parity p.
     float* solid_f;
+    // Slot offsets of the launch's parity relative to a cell's own padded
+    // index, for cells none of whose neighbours wraps (in_offset / out_offset
+    // of inplace27.cuh, filled by the launcher): incoming [q][bounce],
+    // outgoing [q]. Launch-uniform, read from the parameter space.
+    int off_in[27][2];
+    int off_out[27];
 };
 
 
@@ -183,14 +190,14 @@ __device__ __forceinline__ void fused_transport(const IpArgs& a, int x, int y, i
                                         fused_sv, reinterpret_cast<unsigned char*>(fused_sv + 9 * W));
 }
 
-template <class S, bool kExact, int kParity>
+template <class S, bool kExact, int kParity, bool kTransport>
 __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom G = a.g;
     int x, y, z;
     long long cell;
     const bool in_line = line_cell(G, x, y, z, cell);
     float tn[1] = {0.0f};
-    if (a.transport) {
+    if (kTransport) {
         const int z_begin = blockIdx.x * blockDim.x;
         const int zs[1] = {z};
         fused_transport<1>(a, x, y, z_begin, min((int)blockDim.x, G.nz - z_begin), zs, tn);
@@ -211,7 +218,7 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
         fl[q] = S::load(f + (d * G.pcells + c), q, a.sc);
     }
     if (a.obstacle_cur[cell]) record_u(a.cur, cell, 0.0f, 0.0f, 0.0f);
-    if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell, x, y, z, a.transport ? tn : nullptr)) {
+    if (!a.obstacle_cur[cell] && !collide_cell<kExact>(fl, a.cp, a.cur, a.force, cell, x, y, z, kTransport ? tn : nullptr)) {
         reseed_push<S>(f, a, cell, x, y, z, kParity);
         return;
     }
@@ -223,7 +230,9 @@ __global__ void __launch_bounds__(128) step_ip_kernel(typename S::T* __restrict_
     }
 }
 
-// Loads and stores of two cells' populations of one direction.
+// Loads and stores of two cells' populations of one direction: at two
+// addresses, or (load2 / store2) as one aligned 2-element vector at p (the
+// first cell's slot; the second cell's is the next element).
 template <class S>
 struct PairIO;
 template <>
@@ -231,40 +240,81 @@ struct PairIO<StoreF32> {
     __device__ __forceinline__ static F2 load(const float* p0, const float* p1, int, const Fp16Scale&) {
         return f2(__ldg(p0), __ldg(p1));
     }
+    __device__ __forceinline__ static F2 load2(const float* p, int, const Fp16Scale&) {
+        return F2{__ldg(reinterpret_cast<const float2*>(p))};
+    }
     __device__ __forceinline__ static void store(float* p0, float* p1, bool s0, bool s1, int, F2 v, const Fp16Scale&) {
         if (s0) *p0 = v.v.x;
         if (s1) *p1 = v.v.y;
     }
+    __device__ __forceinline__ static void store2(float* p, int, F2 v, const Fp16Scale&) {
+        *reinterpret_cast<float2*>(p) = v.v;
+    }
 };
 template <>
 struct PairIO<StoreF16Dev> {
-    __device__ __forceinline__ static F2 load(const __half* p0, const __half* p1, int q, const Fp16Scale& s) {
-        const float2 h = make_float2(__half2float(__ldg(p0)), __half2float(__ldg(p1)));
+    __device__ __forceinline__ static F2 decode(float2 h, int q, const Fp16Scale& s) {
         const float w = q_w(q), k = w * s.inv_scale;
         return F2{__ffma2_rn(h, make_float2(k, k), make_float2(w, w))};
     }
-    __device__ __forceinline__ static void store(__half* p0, __half* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
+    __device__ __forceinline__ static float2 encode(F2 v, int q, const Fp16Scale& s) {
         const float k = s.scale * (1.0f / q_w(q));
-        const float2 h = __ffma2_rn(v.v, make_float2(k, k), make_float2(-s.scale, -s.scale));
+        return __ffma2_rn(v.v, make_float2(k, k), make_float2(-s.scale, -s.scale));
+    }
+    __device__ __forceinline__ static F2 load(const __half* p0, const __half* p1, int q, const Fp16Scale& s) {
+        return decode(make_float2(__half2float(__ldg(p0)), __half2float(__ldg(p1))), q, s);
+    }
+    __device__ __forceinline__ static F2 load2(const __half* p, int q, const Fp16Scale& s) {
+        return decode(__half22float2(__ldg(reinterpret_cast<const __half2*>(p))), q, s);
+    }
+    __device__ __forceinline__ static void store(__half* p0, __half* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
+        const float2 h = encode(v, q, s);
         if (s0) *p0 = __float2half_rn(h.x);
         if (s1) *p1 = __float2half_rn(h.y);
+    }
+    __device__ __forceinline__ static void store2(__half* p, int q, F2 v, const Fp16Scale& s) {
+        const float2 h = encode(v, q, s);
+        *reinterpret_cast<__half2*>(p) = __floats2half2_rn(h.x, h.y);
     }
 };
 
 template <>
 struct PairIO<StoreI16Dev> {
-    __device__ __forceinline__ static F2 load(const short* p0, const short* p1, int q, const Fp16Scale& s) {
-        const float2 h = make_float2((float)__ldg(p0), (float)__ldg(p1));
+    __device__ __forceinline__ static F2 decode(float2 h, int q, const Fp16Scale& s) {
         const float w = q_w(q), k = w * s.inv_scale;
         return F2{__ffma2_rn(h, make_float2(k, k), make_float2(w, w))};
     }
-    __device__ __forceinline__ static void store(short* p0, short* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
+    __device__ __forceinline__ static float2 encode(F2 v, int q, const Fp16Scale& s) {
         const float k = s.scale * (1.0f / q_w(q));
-        const float2 h = __ffma2_rn(v.v, make_float2(k, k), make_float2(-s.scale, -s.scale));
+        return __ffma2_rn(v.v, make_float2(k, k), make_float2(-s.scale, -s.scale));
+    }
+    __device__ __forceinline__ static F2 load(const short* p0, const short* p1, int q, const Fp16Scale& s) {
+        return decode(make_float2((float)__ldg(p0), (float)__ldg(p1)), q, s);
+    }
+    __device__ __forceinline__ static F2 load2(const short* p, int q, const Fp16Scale& s) {
+        const short2 r = __ldg(reinterpret_cast<const short2*>(p));
+        return decode(make_float2((float)r.x, (float)r.y), q, s);
+    }
+    __device__ __forceinline__ static void store(short* p0, short* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
+        const float2 h = encode(v, q, s);
         if (s0) *p0 = sat_round_s16(h.x);
         if (s1) *p1 = sat_round_s16(h.y);
     }
+    __device__ __forceinline__ static void store2(short* p, int q, F2 v, const Fp16Scale& s) {
+        const float2 h = encode(v, q, s);
+        *reinterpret_cast<short2*>(p) = make_short2(sat_round_s16(h.x), sat_round_s16(h.y));
+    }
 };
+
+// Whether the slot pair of direction q at a launch-uniform offset from an
+// even padded index is 2-element aligned (slot planes are pcells apart, an
+// even count): incoming slots sit in the cell's own memory (positive q and
+// the rest slot) or in the memory of the cell at -c_q, whose padded offset is
+// odd exactly when c_z != 0 (a bounce-back read takes the other slot of the
+// same memory cell, so the same rule holds); outgoing slots sit in the own
+// memory (negative q and rest) or at +c_q.
+__host__ __device__ constexpr bool in_pair_aligned(int q) { return q == kRest27 || q_positive(q) || q_cz(q) == 0; }
+__host__ __device__ constexpr bool out_pair_aligned(int q) { return q == kRest27 || !q_positive(q) || q_cz(q) == 0; }
 
 // Step with two z-adjacent cells per thread and the collision in packed FP32:
 // the factorised collision (collide27_x2.cuh), or with kExact the
@@ -283,13 +333,13 @@ struct PairIO<StoreI16Dev> {
 #ifndef AERO_IP2X_MIN_BLOCKS
 #define AERO_IP2X_MIN_BLOCKS 4
 #endif
-template <class S, bool kExact, int kParity>
+template <class S, bool kExact, int kParity, bool kTransport>
 __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_MIN_BLOCKS) step_ip2_kernel(typename S::T* __restrict__ f, IpArgs a) {
     const PadGeom& G = a.g;
     const int z0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int y = blockIdx.y, x = blockIdx.z;
     float tn[2] = {0.0f, 0.0f};
-    if (a.transport) {
+    if (kTransport) {
         const int z_begin = 2 * blockIdx.x * blockDim.x;
         const int zs[2] = {z0, z0 + 1};
         fused_transport<2>(a, x, y, z_begin, min(2 * (int)blockDim.x, G.nz - z_begin), zs, tn);
@@ -315,10 +365,28 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
     typename S::T* __restrict__ base0 = f + own0;
     F2 fl[27];
     if (flat) {
+        // own0 is even (even z0, even row starts): equal bounce bits and an
+        // aligned direction read both cells' slots as one vector. A warp none
+        // of whose flat lanes has a bounce-back link reads every slot at its
+        // launch-uniform offset without per-lane selects.
+        constexpr uint32_t kBounceBits = (1u << 27) - 1u;
+        if (__all_sync(__activemask(), ((w0 | w1) & kBounceBits) == 0u)) {
 #pragma unroll
-        for (int q = 0; q < 27; ++q)
-            fl[q] = PairIO<S>::load(base0 + in_offset(G, q, kParity, (w0 >> q) & 1u),
-                                    base0 + 1 + in_offset(G, q, kParity, (w1 >> q) & 1u), q, a.sc);
+            for (int q = 0; q < 27; ++q) {
+                const int o = a.off_in[q][0];
+                fl[q] = in_pair_aligned(q) ? PairIO<S>::load2(base0 + o, q, a.sc)
+                                           : PairIO<S>::load(base0 + o, base0 + 1 + o, q, a.sc);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 27; ++q) {
+                const bool b0 = (w0 >> q) & 1u, b1 = (w1 >> q) & 1u;
+                const int o0 = b0 ? a.off_in[q][1] : a.off_in[q][0];
+                const int o1 = b1 ? a.off_in[q][1] : a.off_in[q][0];
+                if (b0 == b1 && in_pair_aligned(q)) fl[q] = PairIO<S>::load2(base0 + o0, q, a.sc);
+                else fl[q] = PairIO<S>::load(base0 + o0, base0 + 1 + o1, q, a.sc);
+            }
+        }
     } else {
         const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
         const NeighbourOffsets o1 = neighbour_offsets(G, x, y, has1 ? z0 + 1 : z0);
@@ -332,7 +400,7 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
     }
     const float* temp = a.cur.temperature;
     const F2 t = !a.cp.enable_buoyancy ? f2(0.0f)
-                 : a.transport         ? f2(tn[0], tn[1])
+                 : kTransport          ? f2(tn[0], tn[1])
                                        : f2(temp[cell0], has1 ? temp[cell0 + 1] : 0.0f);
     F2 cfx = f2(0.0f), cfy = f2(0.0f), cfz = f2(0.0f);
     if (a.force.fx) {
@@ -368,8 +436,9 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
     if (flat) {
 #pragma unroll
         for (int q = 0; q < 27; ++q) {
-            const int off = out_offset(G, q, kParity);
-            PairIO<S>::store(base0 + off, base0 + off + 1, st0, st1, q, fl[q], a.sc);
+            const int off = a.off_out[q];
+            if (out_pair_aligned(q) && st0 && st1) PairIO<S>::store2(base0 + off, q, fl[q], a.sc);
+            else PairIO<S>::store(base0 + off, base0 + off + 1, st0, st1, q, fl[q], a.sc);
         }
         return;
     }

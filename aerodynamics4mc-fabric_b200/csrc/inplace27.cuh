@@ -20,7 +20,10 @@
 // updated and hold the in-transit populations of links that cross a
 // non-periodic face (bounce-back faces read them back; equilibrium faces
 // ignore them). Periodic axes wrap instead. Padded index:
-//   p(x, y, z) = ((x + 1) * (ny + 2) + (y + 1)) * (nz + 2) + (z + 1).
+//   p(x, y, z) = ((x + 1) * (ny + 2) + (y + 1)) * pz + (z + 2),
+// with a row length pz = nz + 3 rounded up to even (one unused element
+// before the z = -1 ghost): every row starts at an even element, so the
+// slots of an even z and of z + 1 form one aligned 2-element vector.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -96,16 +99,18 @@ __host__ __device__ __forceinline__ int solid_slot(int q, int parity) { return p
 // Geometry of one padded brick and the per-axis wrap rule.
 struct PadGeom {
     int nx, ny, nz;
-    int py, pz;            // padded ny + 2, nz + 2
-    int pcells;            // (nx + 2) (ny + 2) (nz + 2)
+    int py, pz;            // padded ny + 2; row length nz + 3 rounded up to even
+    int pcells;            // (nx + 2) (ny + 2) pz
     int wrap[3];           // axis wraps (periodic on both faces)
 };
+
+__host__ __device__ constexpr int pad_row(int nz) { return (nz + 4) & ~1; }
 
 __host__ __device__ inline PadGeom make_pad_geom(int nx, int ny, int nz, int periodic_mask) {
     PadGeom g;
     g.nx = nx; g.ny = ny; g.nz = nz;
-    g.py = ny + 2; g.pz = nz + 2;
-    g.pcells = (nx + 2) * (ny + 2) * (nz + 2);
+    g.py = ny + 2; g.pz = pad_row(nz);
+    g.pcells = (nx + 2) * (ny + 2) * g.pz;
     g.wrap[0] = (periodic_mask >> 0) & 1;
     g.wrap[1] = (periodic_mask >> 1) & 1;
     g.wrap[2] = (periodic_mask >> 2) & 1;
@@ -113,7 +118,7 @@ __host__ __device__ inline PadGeom make_pad_geom(int nx, int ny, int nz, int per
 }
 
 __device__ __forceinline__ int pad_index(const PadGeom& g, int x, int y, int z) {
-    return ((x + 1) * g.py + (y + 1)) * g.pz + (z + 1);
+    return ((x + 1) * g.py + (y + 1)) * g.pz + (z + 2);
 }
 
 // Neighbour coordinate along one axis: wrapped on periodic axes, else may be
@@ -136,7 +141,7 @@ __device__ __forceinline__ NeighbourOffsets neighbour_offsets(const PadGeom& g, 
     for (int k = 0; k < 3; ++k) {
         o.X[k] = (axis_neighbour(x, k - 1, g.nx, g.wrap[0]) + 1) * g.py * g.pz;
         o.Y[k] = (axis_neighbour(y, k - 1, g.ny, g.wrap[1]) + 1) * g.pz;
-        o.Z[k] = axis_neighbour(z, k - 1, g.nz, g.wrap[2]) + 1;
+        o.Z[k] = axis_neighbour(z, k - 1, g.nz, g.wrap[2]) + 2;
     }
     return o;
 }
@@ -159,15 +164,15 @@ __device__ __forceinline__ void incoming_slot(const NeighbourOffsets& o, int own
 // Slot offsets relative to a cell's own padded index, for a cell none of
 // whose neighbours wraps around a periodic axis (the neighbour along c is
 // then own + link_offset(c)); launch-uniform apart from the bounce choice.
-__device__ __forceinline__ int link_offset(const PadGeom& g, int q) { return (q_cx(q) * g.py + q_cy(q)) * g.pz + q_cz(q); }
+__host__ __device__ __forceinline__ int link_offset(const PadGeom& g, int q) { return (q_cx(q) * g.py + q_cy(q)) * g.pz + q_cz(q); }
 // bounce: the parity-flipped slot of the same memory cell
-__device__ __forceinline__ int in_offset(const PadGeom& g, int q, int p, bool bounce = false) {
+__host__ __device__ __forceinline__ int in_offset(const PadGeom& g, int q, int p, bool bounce = false) {
     const bool even = (p == 0) != bounce;
     const int dir = q == kRest27 ? kRest27 : (even ? q_opp(q) : q);
     const int cell = (q == kRest27 || q_positive(q)) ? 0 : -link_offset(g, q);
     return dir * g.pcells + cell;
 }
-__device__ __forceinline__ int out_offset(const PadGeom& g, int q, int p) {
+__host__ __device__ __forceinline__ int out_offset(const PadGeom& g, int q, int p) {
     const int dir = q == kRest27 ? kRest27 : (p == 0 ? q : q_opp(q));
     const int cell = (q == kRest27 || !q_positive(q)) ? 0 : link_offset(g, q);
     return dir * g.pcells + cell;

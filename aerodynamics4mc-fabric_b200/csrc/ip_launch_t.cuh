@@ -9,6 +9,16 @@
 
 namespace aero {
 
+// The launch-uniform slot offsets of the parity a.parity (IpArgs::off_in,
+// off_out) for the packed step's cells without periodic wraps.
+inline void fill_slot_offsets(IpArgs& a) {
+    for (int q = 0; q < 27; ++q) {
+        a.off_in[q][0] = in_offset(a.g, q, a.parity, false);
+        a.off_in[q][1] = in_offset(a.g, q, a.parity, true);
+        a.off_out[q] = out_offset(a.g, q, a.parity);
+    }
+}
+
 template <class S, bool kExact>
 struct IpLaunch {
     static cudaError_t init(typename S::T* f, const IpArgs& a, cudaStream_t s) {
@@ -36,13 +46,27 @@ struct IpLaunch {
         } else if (cpt == 2) {
             const int lb = line_block((a.g.nz + 1) / 2);
             const size_t smem = a.transport ? fused_smem_bytes(std::min(2 * lb, a.g.nz)) : 0;
-            if (a.parity == 0) step_ip2_kernel<S, kExact, 0><<<line_grid(a.g, lb, 2), lb, smem, s>>>(f, a);
-            else step_ip2_kernel<S, kExact, 1><<<line_grid(a.g, lb, 2), lb, smem, s>>>(f, a);
+            IpArgs b = a;
+            fill_slot_offsets(b);
+            const dim3 grid = line_grid(a.g, lb, 2);
+            if (a.transport) {
+                if (a.parity == 0) step_ip2_kernel<S, kExact, 0, true><<<grid, lb, smem, s>>>(f, b);
+                else step_ip2_kernel<S, kExact, 1, true><<<grid, lb, smem, s>>>(f, b);
+            } else {
+                if (a.parity == 0) step_ip2_kernel<S, kExact, 0, false><<<grid, lb, 0, s>>>(f, b);
+                else step_ip2_kernel<S, kExact, 1, false><<<grid, lb, 0, s>>>(f, b);
+            }
         } else {
             const int lb = line_block(a.g.nz);
             const size_t smem = a.transport ? fused_smem_bytes(std::min(lb, a.g.nz)) : 0;
-            if (a.parity == 0) step_ip_kernel<S, kExact, 0><<<line_grid(a.g, lb), lb, smem, s>>>(f, a);
-            else step_ip_kernel<S, kExact, 1><<<line_grid(a.g, lb), lb, smem, s>>>(f, a);
+            const dim3 grid = line_grid(a.g, lb);
+            if (a.transport) {
+                if (a.parity == 0) step_ip_kernel<S, kExact, 0, true><<<grid, lb, smem, s>>>(f, a);
+                else step_ip_kernel<S, kExact, 1, true><<<grid, lb, smem, s>>>(f, a);
+            } else {
+                if (a.parity == 0) step_ip_kernel<S, kExact, 0, false><<<grid, lb, 0, s>>>(f, a);
+                else step_ip_kernel<S, kExact, 1, false><<<grid, lb, 0, s>>>(f, a);
+            }
         }
         step_timer_end(s);
         count_launch();

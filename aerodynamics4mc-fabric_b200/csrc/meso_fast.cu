@@ -14,6 +14,8 @@
 // per-cell pull of the reference-order kernel.
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "collide27_x2.cuh"
 #include "d3q27_kernels.cuh"
 #include "lattice.cuh"
@@ -204,9 +206,16 @@ struct MesoPair<MesoI16> {
     }
 };
 
-template <class S>
-__global__ void __launch_bounds__(128) meso_hydro2_kernel(HydroArgs A) {
+// kWide: 64-bit slot offsets (grids of 19 x cells >= 2^31 elements); else
+// the launch-uniform offsets of a direction are 32-bit and every slot address
+// is the pair's own address plus one of them.
+#ifndef AERO_MESO2_MIN_BLOCKS
+#define AERO_MESO2_MIN_BLOCKS 6
+#endif
+template <class S, bool kWide>
+__global__ void __launch_bounds__(128, AERO_MESO2_MIN_BLOCKS) meso_hydro2_kernel(HydroArgs A) {
     using T = typename S::T;
+    using Off = typename std::conditional<kWide, long long, int>::type;
     const int nx = A.nx, ny = A.ny, nz = A.nz;
     const int z0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (z0 >= nz) return;
@@ -215,19 +224,42 @@ __global__ void __launch_bounds__(128) meso_hydro2_kernel(HydroArgs A) {
     const long long i0 = ((long long)x * ny + y) * nz + z0;
     const T* __restrict__ src = static_cast<const T*>(A.src);
     const uint32_t w0 = A.flags_prev[i0], w1 = A.flags_prev[i0 + 1];
-    const bool wrap_free = !A.periodic_sides || (x > 0 && x < nx - 1 && z0 > 0 && z0 + 1 < nz - 1);
     F2 f[19];
-    if (wrap_free && !((w0 | w1) & (kHydroSelfSolid | kHydroSlow))) {
+    if (!((w0 | w1) & (kHydroSelfSolid | kHydroSlow))) {
         // i0, cells and nz are even: a pair's normal source is 2-aligned
-        // when c_z = 0, its bounce-back source always
+        // when c_z = 0, its bounce-back source always. Periodic sides wrap the
+        // sources: along x for the whole line (both cells alike), along z for
+        // the first cell of the line's first pair and the second cell of its
+        // last pair only.
+        const T* __restrict__ own = src + i0;
+        const Off plane = (Off)cells;
+        const bool xlo = A.periodic_sides && x == 0, xhi = A.periodic_sides && x == nx - 1;
+        const bool zlo = A.periodic_sides && z0 == 0, zhi = A.periodic_sides && z0 + 2 == nz;
         typename MesoPair<S>::Raw raw[19];
+        // a warp none of whose lanes bounces back or wraps along z reads
+        // every slot at its line-uniform offset
+        if (__all_sync(__activemask(), ((w0 | w1) & ((1u << 19) - 1u)) == 0u && !zlo && !zhi)) {
 #pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            const long long off = ((long long)mcx(q) * ny + mcy(q)) * nz + mcz(q);
-            const long long n0 = (long long)q * cells + i0 - off, b0 = (long long)mopp(q) * cells + i0;
-            const bool bb0 = (w0 >> q) & 1u, bb1 = (w1 >> q) & 1u;
-            if (bb0 == bb1) raw[q] = MesoPair<S>::raw(src + (bb0 ? b0 : n0), bb0 || mcz(q) == 0);
-            else raw[q] = MesoPair<S>::raw2(src + (bb0 ? b0 : n0), src + (bb1 ? b0 : n0) + 1);
+            for (int q = 0; q < 19; ++q) {
+                Off n0 = (Off)q * plane - (((Off)mcx(q) * ny + mcy(q)) * nz + mcz(q));
+                if (mcx(q) == 1 && xlo) n0 += plane;
+                if (mcx(q) == -1 && xhi) n0 -= plane;
+                raw[q] = MesoPair<S>::raw(own + n0, mcz(q) == 0);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                Off n0 = (Off)q * plane - (((Off)mcx(q) * ny + mcy(q)) * nz + mcz(q));
+                if (mcx(q) == 1 && xlo) n0 += plane;
+                if (mcx(q) == -1 && xhi) n0 -= plane;
+                const Off na = n0 + ((mcz(q) == 1 && zlo) ? (Off)nz : (Off)0);
+                const Off nb = n0 - ((mcz(q) == -1 && zhi) ? (Off)nz : (Off)0);
+                const Off b0 = (Off)mopp(q) * plane;
+                const bool bb0 = (w0 >> q) & 1u, bb1 = (w1 >> q) & 1u;
+                const Off o0 = bb0 ? b0 : na, o1 = bb1 ? b0 : nb;
+                if (o0 == o1) raw[q] = MesoPair<S>::raw(own + o0, bb0 || mcz(q) == 0);
+                else raw[q] = MesoPair<S>::raw2(own + o0, own + o1 + 1);
+            }
         }
 #pragma unroll
         for (int q = 0; q < 19; ++q) f[q] = MesoPair<S>::decode(raw[q], q, A.inv_scale);
@@ -299,9 +331,9 @@ __global__ void __launch_bounds__(128) meso_hydro2_kernel(HydroArgs A) {
     trt_pair<13>(f, H, rho, tux, tuy, tuz, uu, om_e, pref, uf);
     trt_pair<15>(f, H, rho, tux, tuy, tuz, uu, om_e, pref, uf);
     trt_pair<17>(f, H, rho, tux, tuy, tuz, uu, om_e, pref, uf);
-    T* __restrict__ dst = static_cast<T*>(A.dst);
+    T* __restrict__ dst = static_cast<T*>(A.dst) + i0;
 #pragma unroll
-    for (int q = 0; q < 19; ++q) MesoPair<S>::store(dst + (long long)q * cells + i0, q, f[q], A.scale);
+    for (int q = 0; q < 19; ++q) MesoPair<S>::store(dst + (Off)q * (Off)cells, q, f[q], A.scale);
 }
 
 }  // namespace
@@ -312,9 +344,17 @@ cudaError_t meso_hydro_fast_step(const meso::HydroArgs& a, int storage, cudaStre
     const int pairs = a.nz / 2;
     const int block = pairs >= 128 ? 128 : ((pairs + 31) / 32) * 32;
     const dim3 grid((unsigned)((pairs + block - 1) / block), (unsigned)a.ny, (unsigned)a.nx);
-    if (storage == kMesoStoreF16) meso::meso_hydro2_kernel<meso::MesoF16><<<grid, block, 0, s>>>(a);
-    else if (storage == kMesoStoreI16) meso::meso_hydro2_kernel<meso::MesoI16><<<grid, block, 0, s>>>(a);
-    else meso::meso_hydro2_kernel<meso::MesoF32><<<grid, block, 0, s>>>(a);
+    const bool wide = 19LL * a.nx * a.ny * a.nz >= (1LL << 31);
+    if (storage == kMesoStoreF16) {
+        if (wide) meso::meso_hydro2_kernel<meso::MesoF16, true><<<grid, block, 0, s>>>(a);
+        else meso::meso_hydro2_kernel<meso::MesoF16, false><<<grid, block, 0, s>>>(a);
+    } else if (storage == kMesoStoreI16) {
+        if (wide) meso::meso_hydro2_kernel<meso::MesoI16, true><<<grid, block, 0, s>>>(a);
+        else meso::meso_hydro2_kernel<meso::MesoI16, false><<<grid, block, 0, s>>>(a);
+    } else {
+        if (wide) meso::meso_hydro2_kernel<meso::MesoF32, true><<<grid, block, 0, s>>>(a);
+        else meso::meso_hydro2_kernel<meso::MesoF32, false><<<grid, block, 0, s>>>(a);
+    }
     count_launch();
     return cudaGetLastError();
 }

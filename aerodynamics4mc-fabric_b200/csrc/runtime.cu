@@ -51,9 +51,11 @@ struct TimingStats {
 
 RuntimeConfig g_cfg;
 std::recursive_mutex g_mutex;  // guards every entry point (the caller is one worker thread)
+// Tuning knobs (aero_lbm_b200_set_*), at their defaults; reset_tuning()
+// restores exactly these values.
 int g_thermal_mode = -1;      // temperature transport: -1 with buoyancy, 0 never (packet field), 1 always
 int g_streamed_step = 0;      // factorised two-cell in-place step: bulk-copy streamed kernel where eligible (opt-in)
-int g_fused_transport = 1;    // in-place steps compute the first-order temperature transport themselves
+int g_fused_transport = 0;    // in-place steps compute the first-order temperature transport themselves (opt-in)
 int g_cells_per_thread = 2;    // in-place step: 1 one cell per thread, 2 two cells per thread (packed collision)
 int g_fp16_format = 1;         // 16-bit storage: 0 IEEE half deviations, 1 fixed-point deviations (default)
 std::unordered_map<long long, std::unique_ptr<Context>> g_contexts;
@@ -909,8 +911,8 @@ static bool step_context_body(Context& ctx, const float* packet, float* out, flo
         ctx.cur = 1 - ctx.cur;
     } else {
         if (ctx.initialized && !inplace_faces_ok(face_now)) {
-            set_error("in-place context: the faces changed to a kind that needs the two-buffer layout "
-                      "(symmetry or convective outflow); release and re-create the context");
+            set_error("in-place context: the faces changed to an axis periodic on one side only (or the cylinder "
+                      "preset), which needs the two-buffer layout; release and re-create the context");
             return false;
         }
         if (!join_fill(ctx, s)) return false;
@@ -975,7 +977,10 @@ static bool step_context_body(Context& ctx, const float* packet, float* out, flo
                 return false;
             ctx.fill_recorded = true;
         }
-        if (ctx.shell_count > 0) {
+        // the reference reads the shell in its FP16 in-place step only
+        // (jni.cpp:6779-6790): a call in another solver mode keeps it unapplied
+        if (ctx.shell_count > 0 &&
+            g_realtime_solver_mode == AERO_LBM_REALTIME_SOLVER_D3Q27_FP16_INPLACE_EXPERIMENTAL) {
             if (!join_fill(ctx, s)) return false;
             IpArgs a = ip_args(ctx, new_slot, new_slot, cp);
             a.parity = ctx.parity;
@@ -1570,8 +1575,8 @@ AERO_LBM_B200_EXPORT int aero_lbm_patch_d3q27_f16_static_cells_rect(int nx, int 
 // upload_d3q27_f16_boundary_shell (jni.cpp:6449-6540): fluid cells within
 // shell_layers of a face in face_mask (bit i: x-, x+, y-, y+, z-, z+) get a
 // layer (1 outermost) and a target (the flow state's velocity, speed-clamped,
-// and pressure, rounded to half precision); after every later call their
-// state is relaxed toward it (edits.cuh). Needs an in-place context that has
+// and pressure, rounded to half precision); after every later call made in
+// the FP16 in-place solver mode their state is relaxed toward it (edits.cuh). Needs an in-place context that has
 // stepped. A zero mask, layer count or relaxation clears the shell.
 AERO_LBM_B200_EXPORT int aero_lbm_set_d3q27_f16_boundary_shell_rect(int nx, int ny, int nz, long long key,
                                                                     const float* flow, int channels, int face_mask,
@@ -1791,7 +1796,7 @@ AERO_LBM_B200_EXPORT const char* aero_lbm_memory_info(void) {
                                      (c.u_last ? n * 12ull : 0);
         temp += t;
         if (c.layout == 1 && c.ip) {
-            const unsigned long long pc = (unsigned long long)(c.nx + 2) * (c.ny + 2) * (c.nz + 2);
+            const unsigned long long pc = (unsigned long long)(c.nx + 2) * (c.ny + 2) * pad_row(c.nz);
             ip_dist += pc * 27ull * (c.ip_variant == kIpF32Exact || c.ip_variant == kIpF32Fast ? 4ull : 2ull);
             ip_solid += 2ull * n;
             ip_class += 2ull * n * 4ull;
@@ -1971,6 +1976,20 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_advance_rect(long long key, int steps) {
     for (int i = 0; i < steps; ++i)
         if (!step_context(*c, nullptr, nullptr, 1.0f, true)) return 0;
     return 1;
+}
+
+AERO_LBM_B200_EXPORT void aero_lbm_b200_reset_tuning(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    g_thermal_mode = -1;
+    g_streamed_step = 0;
+    g_fused_transport = 0;
+    g_cells_per_thread = 2;
+    g_fp16_format = 1;
+    g_stream_mode = 0;
+    g_collision_mode = 0;
+    g_smagorinsky_c = -1.0f;
+    g_buoyancy_beta_override = -1.0f;
+    g_gravity_axis = -1;
 }
 
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streaming_mode(int mode) {

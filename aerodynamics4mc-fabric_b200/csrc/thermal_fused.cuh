@@ -82,18 +82,71 @@ __device__ __forceinline__ void stage_entry(const FusedTransport& tr, const uint
 // Stage the nine rows of a block's z-segment [z_begin, z_begin + span) plus a
 // one-cell halo in z: entry (dx, dy, k) at ((dx + 1) * 3 + dy + 1) * W + k,
 // W = span + 2, k = z - z_begin + 1. Every thread of the block takes part.
-__device__ __forceinline__ void stage_rows(const FusedTransport& tr, const uint8_t* obstacle, int nx, int ny, int nz, int x,
-                                           int y, int z_begin, int span, float* sv, unsigned char* sc) {
-    const int W = span + 2;
-    for (int i = threadIdx.x; i < 9 * W; i += blockDim.x) {
-        const int r = i / W, k = i - r * W;
-        stage_entry(tr, obstacle, nx, ny, nz, x + r / 3 - 1, y + r % 3 - 1, z_begin - 1 + k, sv[i], sc[i]);
+// Tagged staging (no Neumann face): an entry that stands for the querying
+// cell's own value (code 1) holds this NaN payload, which no float operation
+// produces, and the code array is not read.
+constexpr unsigned kOwnTag = 0x7fbadbadu;
+
+__device__ __forceinline__ bool no_neumann(const ThermalFaces& F) {
+    bool none = true;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) none = none && F.kind[f] != kThermalNeumann;
+    return none;
+}
+
+template <bool kTagged>
+__device__ __forceinline__ void put_entry(float* sv, unsigned char* sc, int i, float v, unsigned char code) {
+    if (kTagged) {
+        sv[i] = code == 1 ? __uint_as_float(kOwnTag) : v;
+    } else {
+        sv[i] = v;
+        sc[i] = code;
     }
 }
 
+// A line whose eight neighbour lines lie inside the brick (the block-uniform
+// common case) reads its rows directly: the span's own entries are cells of
+// the brick (per entry one mask byte and one temperature, kept for a fluid
+// cell), and the 18 z-halo entries (one per thread) take the face rules.
+template <bool kTagged>
+__device__ __forceinline__ void stage_rows(const FusedTransport& tr, const uint8_t* obstacle, int nx, int ny, int nz, int x,
+                                           int y, int z_begin, int span, float* sv, unsigned char* sc) {
+    const int W = span + 2;
+    if (x > 0 && x < nx - 1 && y > 0 && y < ny - 1) {
+#pragma unroll 1
+        for (int r = 0; r < 9; ++r) {
+            const long long row = ((long long)(x + r / 3 - 1) * ny + (y + r % 3 - 1)) * nz + z_begin - 1;
+            const uint8_t* ob = obstacle + row;
+            const float* t = tr.t + row;
+            for (int k = 1 + threadIdx.x; k <= span; k += blockDim.x) {
+                const unsigned char code = ob[k] ? 1 : 0;
+                const float v = __ldg(t + k);
+                put_entry<kTagged>(sv, sc, r * W + k, code ? 0.0f : v, code);
+            }
+        }
+        for (int i = threadIdx.x; i < 18; i += blockDim.x) {
+            const int r = i >> 1, k = (i & 1) ? span + 1 : 0;
+            float v;
+            unsigned char code;
+            stage_entry(tr, obstacle, nx, ny, nz, x + r / 3 - 1, y + r % 3 - 1, z_begin - 1 + k, v, code);
+            put_entry<kTagged>(sv, sc, r * W + k, v, code);
+        }
+        return;
+    }
+    for (int i = threadIdx.x; i < 9 * W; i += blockDim.x) {
+        const int r = i / W, k = i - r * W;
+        float v;
+        unsigned char code;
+        stage_entry(tr, obstacle, nx, ny, nz, x + r / 3 - 1, y + r % 3 - 1, z_begin - 1 + k, v, code);
+        put_entry<kTagged>(sv, sc, i, v, code);
+    }
+}
+
+template <bool kTagged>
 __device__ __forceinline__ float at(const float* sv, const unsigned char* sc, int i, float self) {
-    const int c = sc[i];
     const float v = sv[i];
+    if (kTagged) return __float_as_uint(v) == kOwnTag ? self : v;
+    const int c = sc[i];
     return c == 0 ? v : (c == 1 ? self : exact::rclamp(__fadd_rn(self, v), -1.0f, 1.0f));
 }
 
@@ -124,6 +177,7 @@ static __device__ __noinline__ float sample_far(const FusedTransport tr, const u
 // The updated temperature of fluid cell (x, y, z) (update_cell of the
 // separate pass): semi-Lagrangian sample at x - u, 6-point Laplacian, source;
 // k = z - z_begin + 1 indexes the staged rows.
+template <bool kTagged>
 __device__ __forceinline__ float update(const FusedTransport& tr, const uint8_t* obstacle, int nx, int ny, int nz,
                                         const float* sv, const unsigned char* sc, int W, int k, int x, int y, int z,
                                         long long cell) {
@@ -141,14 +195,14 @@ __device__ __forceinline__ float update(const FusedTransport& tr, const uint8_t*
         const float fx = __fsub_rn(px, (float)x0), fy = __fsub_rn(py, (float)y0), fz = __fsub_rn(pz, (float)z0);
         // corner (x0, y0, z0): rows step by 3 W in x and W in y
         const int b = ((x0 - x + 1) * 3 + (y0 - y + 1)) * W + k + (z0 - z);
-        const float c000 = at(sv, sc, b, tc);
-        const float c100 = at(sv, sc, b + 3 * W, tc);
-        const float c010 = at(sv, sc, b + W, tc);
-        const float c110 = at(sv, sc, b + 4 * W, tc);
-        const float c001 = at(sv, sc, b + 1, tc);
-        const float c101 = at(sv, sc, b + 3 * W + 1, tc);
-        const float c011 = at(sv, sc, b + W + 1, tc);
-        const float c111 = at(sv, sc, b + 4 * W + 1, tc);
+        const float c000 = at<kTagged>(sv, sc, b, tc);
+        const float c100 = at<kTagged>(sv, sc, b + 3 * W, tc);
+        const float c010 = at<kTagged>(sv, sc, b + W, tc);
+        const float c110 = at<kTagged>(sv, sc, b + 4 * W, tc);
+        const float c001 = at<kTagged>(sv, sc, b + 1, tc);
+        const float c101 = at<kTagged>(sv, sc, b + 3 * W + 1, tc);
+        const float c011 = at<kTagged>(sv, sc, b + W + 1, tc);
+        const float c111 = at<kTagged>(sv, sc, b + 4 * W + 1, tc);
         const float c00 = __fadd_rn(c000, __fmul_rn(__fsub_rn(c100, c000), fx));
         const float c10 = __fadd_rn(c010, __fmul_rn(__fsub_rn(c110, c010), fx));
         const float c01 = __fadd_rn(c001, __fmul_rn(__fsub_rn(c101, c001), fx));
@@ -160,11 +214,11 @@ __device__ __forceinline__ float update(const FusedTransport& tr, const uint8_t*
         adv = sample_far(tr, obstacle, nx, ny, nz, px, py, pz, tc);
     }
     // neighbours in the reference's order: +x, -x, +y, -y, +z, -z
-    float t_sum = __fadd_rn(at(sv, sc, ctr + 3 * W, tc), at(sv, sc, ctr - 3 * W, tc));
-    t_sum = __fadd_rn(t_sum, at(sv, sc, ctr + W, tc));
-    t_sum = __fadd_rn(t_sum, at(sv, sc, ctr - W, tc));
-    t_sum = __fadd_rn(t_sum, at(sv, sc, ctr + 1, tc));
-    t_sum = __fadd_rn(t_sum, at(sv, sc, ctr - 1, tc));
+    float t_sum = __fadd_rn(at<kTagged>(sv, sc, ctr + 3 * W, tc), at<kTagged>(sv, sc, ctr - 3 * W, tc));
+    t_sum = __fadd_rn(t_sum, at<kTagged>(sv, sc, ctr + W, tc));
+    t_sum = __fadd_rn(t_sum, at<kTagged>(sv, sc, ctr - W, tc));
+    t_sum = __fadd_rn(t_sum, at<kTagged>(sv, sc, ctr + 1, tc));
+    t_sum = __fadd_rn(t_sum, at<kTagged>(sv, sc, ctr - 1, tc));
     const float lap = __fsub_rn(t_sum, __fmul_rn(6.0f, tc));
     const float rate = __fsub_rn(__fadd_rn(__fmul_rn(tr.alpha, lap), src), __fmul_rn(cooling, adv));
     return exact::rclamp(__fadd_rn(adv, __fmul_rn(dt, rate)), -1.0f, 1.0f);
@@ -178,7 +232,9 @@ template <int kCells>
 __device__ __forceinline__ void update_cells(const FusedTransport& tr, const uint8_t* obstacle, int nx, int ny, int nz,
                                              int x, int y, int z_begin, int span, const int (&zs)[kCells],
                                              float (&tn)[kCells], float* sv, unsigned char* sc) {
-    stage_rows(tr, obstacle, nx, ny, nz, x, y, z_begin, span, sv, sc);
+    const bool tagged = no_neumann(tr.faces);
+    if (tagged) stage_rows<true>(tr, obstacle, nx, ny, nz, x, y, z_begin, span, sv, sc);
+    else stage_rows<false>(tr, obstacle, nx, ny, nz, x, y, z_begin, span, sv, sc);
     __syncthreads();
     const int W = span + 2;
 #pragma unroll
@@ -187,7 +243,9 @@ __device__ __forceinline__ void update_cells(const FusedTransport& tr, const uin
         const int z = zs[i];
         if (z >= nz) continue;
         const long long cell = ((long long)x * ny + y) * nz + z;
-        if (!obstacle[cell]) tn[i] = update(tr, obstacle, nx, ny, nz, sv, sc, W, z - z_begin + 1, x, y, z, cell);
+        if (!obstacle[cell])
+            tn[i] = tagged ? update<true>(tr, obstacle, nx, ny, nz, sv, sc, W, z - z_begin + 1, x, y, z, cell)
+                           : update<false>(tr, obstacle, nx, ny, nz, sv, sc, W, z - z_begin + 1, x, y, z, cell);
         tr.t_next[cell] = tn[i];
     }
 }

@@ -246,9 +246,10 @@ def cpu_baseline_single(n: int = 128, steps: int = 3) -> dict | None:
 # ---------------------------------------------------------------- our arm
 # Temperature transport per cell and step: state read + write (2 x 4 B) and
 # the previous collision's velocity written by the collision and read by the
-# transport (2 x 12 B); since the transport runs inside the step kernel these
-# bytes are part of that kernel's traffic.
-THERMAL_BYTES = 2 * 4 + 2 * 12
+# transport (2 x 12 B). With the transport inside the step kernel all of them
+# are that kernel's traffic; with the separate pass the step kernel reads the
+# new temperature and writes the velocity (4 + 12 B).
+THERMAL_BYTES = {True: 2 * 4 + 2 * 12, False: 4 + 12}
 VARIANTS = {
     # name: (realtime solver mode, collision mode, 16-bit format, bytes per cell-step, storage note)
     "i16": (3, 1, 1, 27 * 2 * 2 + 1, "16-bit fixed-point deviation storage (the FP16 mode's default format), "
@@ -490,6 +491,7 @@ def run_ours(args) -> dict | None:
     lib.aero_lbm_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
     if not lib.aero_lbm_init_rect(args.n, args.n, args.n, 11, 4):
         raise RuntimeError(aero.last_error(lib))
+    lib.aero_lbm_b200_set_fused_transport(args.fused_transport)
 
     case = cases.c2_terrain_boussinesq(args.n)
     n = args.n
@@ -547,15 +549,17 @@ def run_ours(args) -> dict | None:
         ms_step = ms / steps
         nbytes = VARIANTS[variant][3]
         # achieved_gbs: the stream-collide kernel's algorithmic bytes (the
-        # populations, plus the transport's fields, which it computes in
-        # place) over its own launch time; step_gbs: the same bytes over the
-        # step time (the kernel plus the per-call boundary fill).
+        # populations plus its share of the transport's fields) over its own
+        # launch time; step_gbs: the whole step's bytes (populations and every
+        # transport byte) over the step time (kernel, transport pass if
+        # separate, per-call boundary fill).
+        kb = nbytes + THERMAL_BYTES[bool(args.fused_transport)]
         results[variant] = {"mlups": cells * world * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms_step,
                             "launches": launches, "clocks": clocks, "steps": steps, "kernel_ms": kernel_ms,
                             "windows": len(windows), "window_ms_min": min(windows), "window_ms_max": max(windows),
-                            "achieved_gbs": (nbytes + THERMAL_BYTES) * cells / (kernel_ms * 1e-3) / 1e9,
+                            "achieved_gbs": kb * cells / (kernel_ms * 1e-3) / 1e9,
                             "population_gbs": nbytes * cells / (kernel_ms * 1e-3) / 1e9,
-                            "step_gbs": (nbytes + THERMAL_BYTES) * cells / (ms_step * 1e-3) / 1e9}
+                            "step_gbs": (nbytes + THERMAL_BYTES[True]) * cells / (ms_step * 1e-3) / 1e9}
         if variant == HEADLINE:
             head = (ctx, packet, pk_ptr)
         else:
@@ -669,6 +673,7 @@ def run_ours(args) -> dict | None:
                    "bricks_per_gpu": 1, "cells_per_gpu": cells, "storage": VARIANTS[HEADLINE][4],
                    "l2": "inputs larger than L2 (16-bit state 119 MB + fields; fp32 state 238 MB); no flush",
                    "parallelism": f"bricks x{world}",
+                   "fused_transport": bool(args.fused_transport),
                    "timing": f"windows of {h['steps']} steps repeated to >= 1 s (median of {h['windows']}: "
                              f"{h['window_ms_min']:.2f}..{h['window_ms_max']:.2f} ms)",
                    **{f"{v}_mlups": results[v]["mlups"] for v in results if v != HEADLINE},
@@ -677,7 +682,9 @@ def run_ours(args) -> dict | None:
                    **{f"{v}_kernel_us": results[v]["kernel_ms"] * 1e3 for v in results},
                    **{f"{v}_step_gbs": results[v]["step_gbs"] for v in results},
                    "temperature_transport": "the reference's benchmark-mode scalar update before every collision, "
-                                            "computed inside the step kernel; the case's field loaded as the starting state",
+                                            + ("computed inside the step kernel" if args.fused_transport else
+                                               "computed by a separate kernel before the step kernel")
+                                            + "; the case's field loaded as the starting state",
                    "e2e_resident": {"value": e2e_resident, "unit": "MLUPS", "h2d_bytes_per_step": 0,
                                     "d2h_bytes_per_step": int(atlas.nbytes), "steps": e2e_steps,
                                     "api": "aero_lbm_step_rect_cached + aero_lbm_extract_flow_atlas_rect(stride 4)"},
@@ -688,8 +695,9 @@ def run_ours(args) -> dict | None:
                    "adjoint": adjoint},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic_record(f"step_ip2_i16@{n}"), "peak_source": peak_kind,
-                     "bytes_per_cell": VARIANTS[HEADLINE][3] + THERMAL_BYTES,
-                     "kernel": "step_ip2_kernel<StoreI16Dev> (temperature transport fused)",
+                     "bytes_per_cell": VARIANTS[HEADLINE][3] + THERMAL_BYTES[bool(args.fused_transport)],
+                     "kernel": "step_ip2_kernel<StoreI16Dev>" + (" (temperature transport fused)" if args.fused_transport
+                                                                  else " (temperature transport as a separate kernel)"),
                      "kernel_us": h["kernel_ms"] * 1e3,
                      "timing": "CUDA events around each step-kernel launch on the library's stream, timed windows"},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": int(packet.numel() * 4),
@@ -711,6 +719,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--streaming", type=int, default=0, help="0 auto, 1 two-buffer, 2 in-place")
+    ap.add_argument("--fused-transport", type=int, choices=[0, 1], default=0,
+                    help="temperature transport as a separate pass (0, default) or inside the step kernel (1)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-ticks", type=int, default=500, help="ticks of the 512-brick batch leg (0 skips it)")
     ap.add_argument("--variants", default="fp16,fp32_exact,fp32_fast",

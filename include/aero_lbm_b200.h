@@ -189,8 +189,9 @@ AERO_LBM_B200_EXPORT int aero_lbm_patch_d3q27_f16_static_cells_rect(int nx, int 
                                                                     const uint8_t* fan_dir_values);
 /* native/include/aero_lbm_capi.h:183-193 (jni.cpp:6449-6540, 9962-10022) — a
  * boundary-reference shell: fluid cells within shell_layers of the faces in
- * face_mask (bit i: x-, x+, y-, y+, z-, z+) are relaxed after every call
- * toward the given flow state (flow_channels >= 4: ux, uy, uz, p) with
+ * face_mask (bit i: x-, x+, y-, y+, z-, z+) are relaxed after every call made
+ * in the FP16 in-place solver mode (3; the reference's FP16 step is the only
+ * one that reads the shell) toward the given flow state (flow_channels >= 4: ux, uy, uz, p) with
  * strength relaxation (<= 0.5) x (1 - (layer - 1) / layers)^2. In-place
  * contexts that have stepped; a zero mask, layer count or relaxation clears. */
 AERO_LBM_B200_EXPORT int aero_lbm_set_d3q27_f16_boundary_shell_rect(int nx, int ny, int nz, long long context_key,
@@ -331,11 +332,15 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_set_thermal_transport(int mode);
  * arithmetic, bit-identical results. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_streamed_step(int on);
 /* Where the first-order temperature transport of in-place contexts runs:
- * 1 (default) inside the step kernel, each cell updating its own temperature
- * right before its collision; 0 as a separate pass before the step. Same
+ * 0 (default) as a separate pass before the step; 1 inside the step kernel,
+ * each cell updating its own temperature right before its collision. Same
  * arithmetic, bit-identical results; the heated-cavity and game-runtime
  * (BFECC) transports always run as separate passes. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_set_fused_transport(int on);
+/* Restore every aero_lbm_b200_set_* tuning knob (streaming mode, collision
+ * mode, cells per thread, thermal transport, streamed step, fused transport,
+ * 16-bit format, physics overrides) to its default. */
+AERO_LBM_B200_EXPORT void aero_lbm_b200_reset_tuning(void);
 /* Format of the 16-bit deviation storage chosen by
  * aero_lbm_set_realtime_solver_mode(3), for contexts created afterwards:
  * 1 = 16-bit fixed point of (f - w) * S / w with S = 32767 / d_max (default:

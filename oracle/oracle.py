@@ -691,6 +691,11 @@ def run_script_oracle(o: "Oracle", cfg: dict, packet: np.ndarray, script):
             o.patch_cells(act[1], act[2])
         elif kind == "shell":
             o.set_shell(act[1], act[2], act[3], act[4])
+        elif kind == "mode":
+            # the realtime solver mode of the product's later calls; the shell
+            # restatement above models calls in the FP16 in-place mode (3),
+            # the only mode whose step reads the shell (jni.cpp:6779-6790)
+            pass
         elif kind == "flow":
             results.append(o.output())
         elif kind == "temp":

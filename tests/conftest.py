@@ -55,6 +55,20 @@ def lib():
     return aero_b200.load_library()
 
 
+@pytest.fixture(autouse=True)
+def _default_tuning():
+    """Every test starts from the library's default tuning knobs, solver mode
+    and benchmark configuration (they are process-global; a test that changes
+    one must not leak it into the next)."""
+    import aero_b200
+    lib = aero_b200._lib
+    if lib is not None:
+        lib.aero_lbm_b200_reset_tuning()
+        lib.aero_lbm_set_realtime_solver_mode(0)
+        lib.aero_lbm_benchmark_reset_config()
+    yield
+
+
 @pytest.fixture(scope="session")
 def gpu(lib):
     if not cuda_available():

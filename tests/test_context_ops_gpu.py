@@ -73,6 +73,8 @@ def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mod
                 assert gpu.aero_lbm_patch_d3q27_f16_static_cells_rect(nx, ny, nz, key, int(c.size), c.ctypes.data,
                                                                       sv.ctypes.data, fan.ctypes.data) == 1, \
                     aero_b200.last_error(gpu)
+            elif kind == "mode":
+                gpu.aero_lbm_set_realtime_solver_mode(act[1])
             elif kind == "shell":
                 fl = np.ascontiguousarray(act[1], np.float32)
                 assert gpu.aero_lbm_set_d3q27_f16_boundary_shell_rect(nx, ny, nz, key, _fp(fl), fl.shape[1], act[2],
@@ -107,7 +109,7 @@ def run_script_gpu(gpu, dims, cfg, pk, script, key, streaming, cpt=2, solver_mod
         gpu.aero_lbm_b200_set_cells_per_thread(2)
         gpu.aero_lbm_set_realtime_solver_mode(0)
         gpu.aero_lbm_b200_set_collision_mode(0)
-    assert len(results) == sum(1 for a in script if a[0] not in ("step", "shift", "cached", "patch", "shell"))
+    assert len(results) == sum(1 for a in script if a[0] not in ("step", "shift", "cached", "patch", "shell", "mode"))
     return results
 
 
@@ -152,7 +154,7 @@ def test_context_ops_fp16_against_fp64(gpu):
     o = O.Oracle((n, n, n), O.derive_params(cfg), "f64")
     o.set_temperature(pre)
     ref = O.run_script_oracle(o, cfg, pk, script)
-    kinds = [a[0] for a in script if a[0] not in ("step", "shift", "cached", "patch", "shell")]
+    kinds = [a[0] for a in script if a[0] not in ("step", "shift", "cached", "patch", "shell", "mode")]
     for kind, a, b in zip(kinds, res, ref):
         if kind == "flow":
             e = O.flow_errors(a, b)
@@ -217,15 +219,33 @@ def test_block_edits_and_shell_match_oracle(gpu, cpt):
     """In-place FP32 (reference-order collision): block edits between calls
     (cached steps after them, duplicates, out-of-range indices, solid cells
     opened and fluid ones closed) and the boundary shell, bit-identical to
-    the oracle's restatement of the same operations."""
+    the oracle's restatement of the same operations. The context is created
+    by a classic-mode call (FP32 storage); the later calls run in the FP16
+    in-place solver mode, the only mode whose step applies the shell."""
     n = 12
     obst, u, temp, src, cfg, pre = O.thermal_case(n, 41)
     pk = O.packet_from(obst, *u, temperature=temp, source=src)
-    script = O.edits_script(n)
+    ops = O.edits_script(n)
+    script = ops[:1] + [("mode", 3)] + ops[1:]
     res = run_script_gpu(gpu, (n, n, n), cfg, pk, script, key=860 + cpt, streaming=2, cpt=cpt, temperature_state=pre)
     o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
     o.set_temperature(pre)
     flags = O.results_equal(res, O.run_script_oracle(o, cfg, pk, script))
+    assert all(flags), flags
+
+
+def test_shell_ignored_outside_the_fp16_mode(gpu):
+    """Calls in the classic solver mode leave the shell unapplied (the
+    reference reads it in its FP16 in-place step only): the edit script with
+    its shells, run in mode 0, equals the oracle's run without them."""
+    n = 12
+    obst, u, temp, src, cfg, pre = O.thermal_case(n, 41)
+    pk = O.packet_from(obst, *u, temperature=temp, source=src)
+    script = O.edits_script(n)
+    res = run_script_gpu(gpu, (n, n, n), cfg, pk, script, key=869, streaming=2, cpt=2, temperature_state=pre)
+    o = O.Oracle((n, n, n), O.derive_params(cfg), "f32")
+    o.set_temperature(pre)
+    flags = O.results_equal(res, O.run_script_oracle(o, cfg, pk, [a for a in script if a[0] != "shell"]))
     assert all(flags), flags
 
 
