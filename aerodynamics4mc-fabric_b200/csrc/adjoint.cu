@@ -164,7 +164,13 @@ __global__ void adj_probe_kernel(Geo G, const T* __restrict__ s, T ux_in, T uy_i
 }
 
 // Scatter of a pre-collision adjoint along the transposed pull; velocity-face
-// pulls add to the inflow gradient.
+// pulls add to the inflow gradient. Every fluid cell's slot of the output is
+// the source of exactly one pull of the forward step (a neighbour's slot
+// pull, or the cell's own bounce-back), except the slot (opp q, cell) of a
+// direction q that the cell pulls from a velocity face: nothing reads that
+// population, so its adjoint is zero, written here. With kAccumulate false
+// the launch therefore writes every fluid slot of lam_prev exactly once and
+// needs no clearing pass (solid cells' slots are never read).
 template <bool kAccumulate>
 __device__ __forceinline__ void scatter(const Geo& G, long long i, int x, int y, int z, const float (&lam)[27],
                                         const float (&uin)[3], float* __restrict__ lam_prev, double (&du)[3]) {
@@ -178,6 +184,7 @@ __device__ __forceinline__ void scatter(const Geo& G, long long i, int x, int y,
             du[0] += (double)lam[q] * d[0];
             du[1] += (double)lam[q] * d[1];
             du[2] += (double)lam[q] * d[2];
+            if (!kAccumulate) lam_prev[(long long)q_opp(q) * G.cells + i] = 0.0f;
             continue;
         }
         float* slot = k == kPullSlot ? lam_prev + (long long)q * G.cells + src : lam_prev + (long long)q_opp(q) * G.cells + i;
@@ -238,8 +245,11 @@ __global__ void adj_seed_kernel(Geo G, const float* __restrict__ s, float ux_in,
 
 // One reverse call: lambda_n (cell-local read) -> lambda_{n-1} (scatter),
 // body-force gradient of the cell, inflow gradient.
+#ifndef AERO_ADJ_REV_MIN_BLOCKS
+#define AERO_ADJ_REV_MIN_BLOCKS 5
+#endif
 template <bool kInit>
-__global__ void __launch_bounds__(128) adj_reverse_kernel(StepArgs<float> A, const float* __restrict__ lam_n,
+__global__ void __launch_bounds__(128, AERO_ADJ_REV_MIN_BLOCKS) adj_reverse_kernel(StepArgs<float> A, const float* __restrict__ lam_n,
                                                           float* __restrict__ lam_prev, double* __restrict__ grad_f,
                                                           double* __restrict__ du_part) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -647,7 +657,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_gradient(long long handle, const 
         for (int n = last; ok && n >= first; --n) {
             const int m = n - first;  // input state of call n is states[m]
             StepArgs<float> a = step_args<float>(*b, inflow, states[m], nullptr);
-            if (!adj_ok(cudaMemsetAsync(b->lam[lc ^ 1], 0, bytes, s), "lambda clear")) { ok = false; break; }
+            // the reverse launch writes every fluid slot of lam[lc ^ 1] (scatter)
             if (n == 1)
                 adj_reverse_kernel<true><<<blocks_for(b->cells, 128), 128, 0, s>>>(a, b->lam[lc], b->lam[lc ^ 1], b->grad_f,
                                                                                    b->du_part);

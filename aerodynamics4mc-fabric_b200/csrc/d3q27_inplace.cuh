@@ -243,6 +243,11 @@ struct PairIO<StoreF32> {
     __device__ __forceinline__ static F2 load2(const float* p, int, const Fp16Scale&) {
         return F2{__ldg(reinterpret_cast<const float2*>(p))};
     }
+    __device__ __forceinline__ static F2 load2p(const float* p, const float* p1, bool fix, int, const Fp16Scale&) {
+        float2 r = __ldg(reinterpret_cast<const float2*>(p));
+        if (fix) r.y = __ldg(p1);
+        return F2{r};
+    }
     __device__ __forceinline__ static void store(float* p0, float* p1, bool s0, bool s1, int, F2 v, const Fp16Scale&) {
         if (s0) *p0 = v.v.x;
         if (s1) *p1 = v.v.y;
@@ -266,6 +271,12 @@ struct PairIO<StoreF16Dev> {
     }
     __device__ __forceinline__ static F2 load2(const __half* p, int q, const Fp16Scale& s) {
         return decode(__half22float2(__ldg(reinterpret_cast<const __half2*>(p))), q, s);
+    }
+    __device__ __forceinline__ static F2 load2p(const __half* p, const __half* p1, bool fix, int q, const Fp16Scale& s) {
+        const __half2 r = __ldg(reinterpret_cast<const __half2*>(p));
+        __half y = __high2half(r);
+        if (fix) y = __ldg(p1);
+        return decode(make_float2(__low2float(r), __half2float(y)), q, s);
     }
     __device__ __forceinline__ static void store(__half* p0, __half* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
         const float2 h = encode(v, q, s);
@@ -295,6 +306,12 @@ struct PairIO<StoreI16Dev> {
         const short2 r = __ldg(reinterpret_cast<const short2*>(p));
         return decode(make_float2((float)r.x, (float)r.y), q, s);
     }
+    __device__ __forceinline__ static F2 load2p(const short* p, const short* p1, bool fix, int q, const Fp16Scale& s) {
+        const short2 r = __ldg(reinterpret_cast<const short2*>(p));
+        short y = r.y;
+        if (fix) y = __ldg(p1);
+        return decode(make_float2((float)r.x, (float)y), q, s);
+    }
     __device__ __forceinline__ static void store(short* p0, short* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
         const float2 h = encode(v, q, s);
         if (s0) *p0 = sat_round_s16(h.x);
@@ -313,8 +330,22 @@ struct PairIO<StoreI16Dev> {
 // odd exactly when c_z != 0 (a bounce-back read takes the other slot of the
 // same memory cell, so the same rule holds); outgoing slots sit in the own
 // memory (negative q and rest) or at +c_q.
-__host__ __device__ constexpr bool in_pair_aligned(int q) { return q == kRest27 || q_positive(q) || q_cz(q) == 0; }
-__host__ __device__ constexpr bool out_pair_aligned(int q) { return q == kRest27 || !q_positive(q) || q_cz(q) == 0; }
+// AERO_PAIR_VECTOR_LOADS / _STORES select the vector form per build. Measured
+// on the 128^3 terrain brick (B200): vector stores shorten the step, vector
+// loads lengthen it (more load latency exposed: 136 us against 104 us for the
+// 16-bit step), so loads stay scalar by default.
+#ifndef AERO_PAIR_VECTOR_LOADS
+#define AERO_PAIR_VECTOR_LOADS 0
+#endif
+#ifndef AERO_PAIR_VECTOR_STORES
+#define AERO_PAIR_VECTOR_STORES 1
+#endif
+__host__ __device__ constexpr bool in_pair_aligned(int q) {
+    return AERO_PAIR_VECTOR_LOADS && (q == kRest27 || q_positive(q) || q_cz(q) == 0);
+}
+__host__ __device__ constexpr bool out_pair_aligned(int q) {
+    return AERO_PAIR_VECTOR_STORES && (q == kRest27 || !q_positive(q) || q_cz(q) == 0);
+}
 
 // Step with two z-adjacent cells per thread and the collision in packed FP32:
 // the factorised collision (collide27_x2.cuh), or with kExact the
@@ -365,27 +396,18 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
     typename S::T* __restrict__ base0 = f + own0;
     F2 fl[27];
     if (flat) {
-        // own0 is even (even z0, even row starts): equal bounce bits and an
-        // aligned direction read both cells' slots as one vector. A warp none
-        // of whose flat lanes has a bounce-back link reads every slot at its
-        // launch-uniform offset without per-lane selects.
-        constexpr uint32_t kBounceBits = (1u << 27) - 1u;
-        if (__all_sync(__activemask(), ((w0 | w1) & kBounceBits) == 0u)) {
+        // own0 is even (even z0, even row starts): with vector loads built in,
+        // an aligned direction reads both cells' slots as one vector at the
+        // first cell's offset; when the bounce-back bits differ the second
+        // lane is replaced by a scalar load from its own slot (a predicated
+        // load, no branch)
 #pragma unroll
-            for (int q = 0; q < 27; ++q) {
-                const int o = a.off_in[q][0];
-                fl[q] = in_pair_aligned(q) ? PairIO<S>::load2(base0 + o, q, a.sc)
-                                           : PairIO<S>::load(base0 + o, base0 + 1 + o, q, a.sc);
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 27; ++q) {
-                const bool b0 = (w0 >> q) & 1u, b1 = (w1 >> q) & 1u;
-                const int o0 = b0 ? a.off_in[q][1] : a.off_in[q][0];
-                const int o1 = b1 ? a.off_in[q][1] : a.off_in[q][0];
-                if (b0 == b1 && in_pair_aligned(q)) fl[q] = PairIO<S>::load2(base0 + o0, q, a.sc);
-                else fl[q] = PairIO<S>::load(base0 + o0, base0 + 1 + o1, q, a.sc);
-            }
+        for (int q = 0; q < 27; ++q) {
+            const bool b0 = (w0 >> q) & 1u, b1 = (w1 >> q) & 1u;
+            const int o0 = b0 ? a.off_in[q][1] : a.off_in[q][0];
+            const int o1 = b1 ? a.off_in[q][1] : a.off_in[q][0];
+            if (in_pair_aligned(q)) fl[q] = PairIO<S>::load2p(base0 + o0, base0 + 1 + o1, b0 != b1, q, a.sc);
+            else fl[q] = PairIO<S>::load(base0 + o0, base0 + 1 + o1, q, a.sc);
         }
     } else {
         const NeighbourOffsets o0 = neighbour_offsets(G, x, y, z0);
@@ -434,11 +456,19 @@ __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_
     if (live0 && !ok[0] && !pass0) reseed_push<S>(f, a, cell0, x, y, z0, kParity);
     if (live1 && !ok[1] && !pass1) reseed_push<S>(f, a, cell0 + 1, x, y, z0 + 1, kParity);
     if (flat) {
+        if (st0 && st1) {
 #pragma unroll
-        for (int q = 0; q < 27; ++q) {
-            const int off = a.off_out[q];
-            if (out_pair_aligned(q) && st0 && st1) PairIO<S>::store2(base0 + off, q, fl[q], a.sc);
-            else PairIO<S>::store(base0 + off, base0 + off + 1, st0, st1, q, fl[q], a.sc);
+            for (int q = 0; q < 27; ++q) {
+                const int off = a.off_out[q];
+                if (out_pair_aligned(q)) PairIO<S>::store2(base0 + off, q, fl[q], a.sc);
+                else PairIO<S>::store(base0 + off, base0 + off + 1, true, true, q, fl[q], a.sc);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 27; ++q) {
+                const int off = a.off_out[q];
+                PairIO<S>::store(base0 + off, base0 + off + 1, st0, st1, q, fl[q], a.sc);
+            }
         }
         return;
     }

@@ -161,11 +161,18 @@ __device__ __forceinline__ void trt_pair(F2 (&f)[19], const HydroRates& H, F2 rh
 // pair's own index i0 is even (nz even) and so is every q * cells.
 template <class S>
 struct MesoPair;
+// AERO_MESO_VECTOR_LOADS selects 2-element vector loads for aligned pairs.
+// Measured on the 256 x 64 x 256 grid (B200), scalar loads are faster
+// (FP16 31.5 against 24.5 GLUPS), so they are the default; stores stay
+// vectors.
+#ifndef AERO_MESO_VECTOR_LOADS
+#define AERO_MESO_VECTOR_LOADS 0
+#endif
 template <>
 struct MesoPair<MesoF32> {
     using Raw = float2;
     __device__ __forceinline__ static Raw raw(const float* p, bool aligned) {
-        return aligned ? __ldg(reinterpret_cast<const float2*>(p)) : make_float2(__ldg(p), __ldg(p + 1));
+        return (AERO_MESO_VECTOR_LOADS && aligned) ? __ldg(reinterpret_cast<const float2*>(p)) : make_float2(__ldg(p), __ldg(p + 1));
     }
     __device__ __forceinline__ static Raw raw2(const float* p0, const float* p1) { return make_float2(__ldg(p0), __ldg(p1)); }
     __device__ __forceinline__ static F2 decode(Raw r, int, float) { return F2{r}; }
@@ -175,7 +182,7 @@ template <>
 struct MesoPair<MesoF16> {
     using Raw = __half2;
     __device__ __forceinline__ static Raw raw(const __half* p, bool aligned) {
-        return aligned ? __ldg(reinterpret_cast<const __half2*>(p)) : __halves2half2(__ldg(p), __ldg(p + 1));
+        return (AERO_MESO_VECTOR_LOADS && aligned) ? __ldg(reinterpret_cast<const __half2*>(p)) : __halves2half2(__ldg(p), __ldg(p + 1));
     }
     __device__ __forceinline__ static Raw raw2(const __half* p0, const __half* p1) { return __halves2half2(__ldg(p0), __ldg(p1)); }
     __device__ __forceinline__ static F2 decode(Raw r, int q, float inv_scale) {
@@ -192,7 +199,7 @@ template <>
 struct MesoPair<MesoI16> {
     using Raw = short2;
     __device__ __forceinline__ static Raw raw(const short* p, bool aligned) {
-        return aligned ? __ldg(reinterpret_cast<const short2*>(p)) : make_short2(__ldg(p), __ldg(p + 1));
+        return (AERO_MESO_VECTOR_LOADS && aligned) ? __ldg(reinterpret_cast<const short2*>(p)) : make_short2(__ldg(p), __ldg(p + 1));
     }
     __device__ __forceinline__ static Raw raw2(const short* p0, const short* p1) { return make_short2(__ldg(p0), __ldg(p1)); }
     __device__ __forceinline__ static F2 decode(Raw r, int q, float inv_scale) {
