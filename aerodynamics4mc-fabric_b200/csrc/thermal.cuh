@@ -39,6 +39,19 @@ struct ThermalFaces {
     float heat_flux[6];     // Neumann increment
 };
 
+// Tagged staging of the transport's neighbourhood (bricks without a Neumann
+// face): an entry that stands for the querying cell's own value (a solid cell
+// or a face that returns the cell's value) holds this NaN payload, which no
+// float operation produces, instead of a separate code.
+constexpr unsigned kOwnTag = 0x7fbadbadu;
+
+__host__ __device__ __forceinline__ bool no_neumann(const ThermalFaces& F) {
+    bool none = true;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) none = none && F.kind[f] != kThermalNeumann;
+    return none;
+}
+
 struct ThermalArgs {
     int nx, ny, nz;
     long long cells;

@@ -79,14 +79,16 @@ __device__ __forceinline__ float th_sample(const ThermalArgs& a, const float* fi
 constexpr int kTZ = 32, kTY = 8, kTX = 4;  // cells per block: z x y x x
 constexpr int kSY = kTZ + 2, kSX = (kTY + 2) * (kTZ + 2), kTile = (kTX + 2) * kSX;
 
-enum TileKind { kTileClean = 0, kTileSolid = 1, kTileAny = 2 };
+// kTileTagged: codes 0 and 1 only, code 1 entries hold kOwnTag (bricks
+// without a Neumann face; the code array is not read).
+enum TileKind { kTileClean = 0, kTileTagged = 1, kTileAny = 2 };
 
 template <int kKind>
 __device__ __forceinline__ float tile_at(const float* sv, const unsigned char* sc, int i, float self) {
     const float v = sv[i];
     if (kKind == kTileClean) return v;
+    if (kKind == kTileTagged) return __float_as_uint(v) == kOwnTag ? self : v;
     const int c = sc[i];
-    if (kKind == kTileSolid) return c ? self : v;
     return c == 0 ? v : (c == 1 ? self : exact::rclamp(self + v, -1.0f, 1.0f));
 }
 
@@ -305,11 +307,27 @@ __device__ __forceinline__ void update_cell(const ThermalArgs& a, const float* s
 // updates the kTX cells of its (y, z) column. Loads are grouped so that many
 // are in flight at once (the kernel is latency-bound). Bricks stay below 2^31
 // cells (32-bit cell indices).
-__global__ void __launch_bounds__(kTZ * kTY, 5) thermal_update_kernel(ThermalArgs a) {
+__global__ void __launch_bounds__(kTZ * kTY, 4) thermal_update_kernel(ThermalArgs a) {
     __shared__ float sv[kTile];
     __shared__ unsigned char sc[kTile];
     const int zb = blockIdx.x * kTZ, yb = blockIdx.y * kTY, xb = blockIdx.z * kTX;
     const int tid = threadIdx.y * kTZ + threadIdx.x;
+    const bool tagged = no_neumann(a.faces);
+    // the cells' own velocity and source first: their loads overlap the
+    // staging loads instead of following the barrier
+    const int z = zb + threadIdx.x, y = yb + threadIdx.y;
+    const bool yz_own = y < a.ny && z < a.nz;
+    float u[kTX][3], src[kTX];
+#pragma unroll
+    for (int k = 0; k < kTX; ++k) {
+        const int x = xb + k;
+        const int cell = (x * a.ny + y) * a.nz + z;
+        const bool in = yz_own && x < a.nx;
+        u[k][0] = in ? __ldg(a.u + cell) : 0.0f;
+        u[k][1] = in ? __ldg(a.u + a.cells + cell) : 0.0f;
+        u[k][2] = in ? __ldg(a.u + 2 * a.cells + cell) : 0.0f;
+        src[k] = (in && a.source) ? exact::rclamp(__ldg(a.source + cell), -0.006f, 0.006f) : 0.0f;
+    }
     int seen = 0;  // bit c: some entry has code c
     // columns (iy, iz) of the halo tile, all kTX + 2 x-planes each
     for (int col = tid; col < kSX; col += kTZ * kTY) {
@@ -335,30 +353,19 @@ __global__ void __launch_bounds__(kTZ * kTY, 5) thermal_update_kernel(ThermalArg
             const int i = ix * kSX + col;
             if (yz_in && (unsigned)gx < (unsigned)a.nx) {
                 const unsigned char code = ob[ix] ? 1 : 0;
-                sv[i] = code ? 0.0f : tv[ix];
+                sv[i] = code ? (tagged ? __uint_as_float(kOwnTag) : 0.0f) : tv[ix];
                 sc[i] = code;
                 seen |= 1 << code;
             } else {
                 stage_outside(&a.faces, a.t, a.obstacle, a.nx, a.ny, a.nz, gx, gy, gz, &sv[i], &sc[i]);
+                if (tagged && sc[i] == 1) sv[i] = __uint_as_float(kOwnTag);
                 seen |= 1 << sc[i];
             }
         }
     }
     const int any_neumann = __syncthreads_or(seen & 4);
     const int any_self = __syncthreads_or(seen & 2);
-    const int z = zb + threadIdx.x, y = yb + threadIdx.y;
-    if (y >= a.ny || z >= a.nz) return;
-    float u[kTX][3], src[kTX];
-#pragma unroll
-    for (int k = 0; k < kTX; ++k) {
-        const int x = xb + k;
-        const int cell = (x * a.ny + y) * a.nz + z;
-        const bool in = x < a.nx;
-        u[k][0] = in ? __ldg(a.u + cell) : 0.0f;
-        u[k][1] = in ? __ldg(a.u + a.cells + cell) : 0.0f;
-        u[k][2] = in ? __ldg(a.u + 2 * a.cells + cell) : 0.0f;
-        src[k] = (in && a.source) ? exact::rclamp(__ldg(a.source + cell), -0.006f, 0.006f) : 0.0f;
-    }
+    if (!yz_own) return;
 #pragma unroll
     for (int k = 0; k < kTX; ++k) {
         const int x = xb + k;
@@ -370,7 +377,7 @@ __global__ void __launch_bounds__(kTZ * kTY, 5) thermal_update_kernel(ThermalArg
             continue;
         }
         if (!any_neumann && !any_self) update_cell<kTileClean>(a, sv, sc, c, x, y, z, cell, u[k], src[k]);
-        else if (!any_neumann) update_cell<kTileSolid>(a, sv, sc, c, x, y, z, cell, u[k], src[k]);
+        else if (tagged) update_cell<kTileTagged>(a, sv, sc, c, x, y, z, cell, u[k], src[k]);
         else update_cell<kTileAny>(a, sv, sc, c, x, y, z, cell, u[k], src[k]);
     }
 }

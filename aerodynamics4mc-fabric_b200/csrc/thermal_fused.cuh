@@ -82,17 +82,8 @@ __device__ __forceinline__ void stage_entry(const FusedTransport& tr, const uint
 // Stage the nine rows of a block's z-segment [z_begin, z_begin + span) plus a
 // one-cell halo in z: entry (dx, dy, k) at ((dx + 1) * 3 + dy + 1) * W + k,
 // W = span + 2, k = z - z_begin + 1. Every thread of the block takes part.
-// Tagged staging (no Neumann face): an entry that stands for the querying
-// cell's own value (code 1) holds this NaN payload, which no float operation
-// produces, and the code array is not read.
-constexpr unsigned kOwnTag = 0x7fbadbadu;
-
-__device__ __forceinline__ bool no_neumann(const ThermalFaces& F) {
-    bool none = true;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) none = none && F.kind[f] != kThermalNeumann;
-    return none;
-}
+// Tagged staging (no Neumann face, kOwnTag of thermal.cuh): the code array
+// is not read.
 
 template <bool kTagged>
 __device__ __forceinline__ void put_entry(float* sv, unsigned char* sc, int i, float v, unsigned char code) {
