@@ -74,13 +74,26 @@ __device__ __forceinline__ void cell_xyz(const Geo& G, long long i, int& x, int&
     cell_xyz32(i, G.ny, G.nz, x, y, z);
 }
 
+// pull_source for a cell none of whose neighbours lies outside the brick:
+// every source is the neighbour at -c_q (no face, no wrap), a slot pull unless
+// that neighbour is solid.
+__device__ __forceinline__ bool interior(const Geo& G, int x, int y, int z) {
+    return x > 0 && y > 0 && z > 0 && x < G.nx - 1 && y < G.ny - 1 && z < G.nz - 1;
+}
+__device__ __forceinline__ int pull_source_at(const Geo& G, bool in, long long i, int x, int y, int z, int q, long long& src) {
+    if (!in) return pull_source(G, x, y, z, q, src);
+    src = i - (((long long)q_cx(q) * G.ny + q_cy(q)) * G.nz + q_cz(q));
+    return G.solid[src] ? kPullBounce : kPullSlot;
+}
+
 template <class T>
 __device__ __forceinline__ void pull_cell(const Geo& G, const T* __restrict__ s, long long i, int x, int y, int z,
                                           const T (&uin)[3], T (&p)[27]) {
+    const bool in = interior(G, x, y, z);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         long long src = 0;
-        const int k = pull_source(G, x, y, z, q, src);
+        const int k = pull_source_at(G, in, i, x, y, z, q, src);
         p[q] = k == kPullSlot ? s[(long long)q * G.cells + src]
              : k == kPullBounce ? s[(long long)q_opp(q) * G.cells + i]
                                 : feq_t<T>(q, T(1), uin[0], uin[1], uin[2]);
@@ -174,10 +187,11 @@ __global__ void adj_probe_kernel(Geo G, const T* __restrict__ s, T ux_in, T uy_i
 template <bool kAccumulate>
 __device__ __forceinline__ void scatter(const Geo& G, long long i, int x, int y, int z, const float (&lam)[27],
                                         const float (&uin)[3], float* __restrict__ lam_prev, double (&du)[3]) {
+    const bool in = interior(G, x, y, z);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         long long src = 0;
-        const int k = pull_source(G, x, y, z, q, src);
+        const int k = pull_source_at(G, in, i, x, y, z, q, src);
         if (k == kPullFace) {
             float d[3];
             dfeq_du<float>(q, 1.0f, uin[0], uin[1], uin[2], d);

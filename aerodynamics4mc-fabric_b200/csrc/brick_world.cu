@@ -905,7 +905,10 @@ bool step_world(Service& svc, long long wkey, World& w, int steps) {
         Snapshots snaps;
         for (auto& [c, b] : w.bricks)
             if (solver_active(w, b) && b.has_dynamic) snaps[c] = Snapshot{b.cur, b.nonzero};
-        // face halos between neighbouring bricks (positive faces; the exchange copies both ways)
+        // face halos between neighbouring bricks (positive faces; the exchange
+        // copies both ways); the slabs of all pairs are disjoint, so their
+        // copies go out together
+        halo_batch_begin();
         for (auto& [c, b] : w.bricks) {
             if (!solver_active(w, b) || b.context == 0) continue;
             for (int f = 1; f < 6; f += 2) {
@@ -918,6 +921,10 @@ bool step_world(Service& svc, long long wkey, World& w, int steps) {
                 (void)aero_lbm_exchange_halo_layers_rect(n, n, n, kGhostLayers, b.context, nb.context, kFaceOffsets[f][0],
                                                          kFaceOffsets[f][1], kFaceOffsets[f][2]);
             }
+        }
+        if (!halo_batch_flush()) {
+            set_sim_error("step_brick_world_runtime: halo exchange failed: " + last_error());
+            return false;
         }
         std::vector<Fallback> fallbacks;
         SnapshotCache cache;

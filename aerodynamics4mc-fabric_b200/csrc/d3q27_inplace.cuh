@@ -515,20 +515,25 @@ __device__ __forceinline__ float ip_face_source(const typename S::T* __restrict_
         return S::load(f + (long long)pd * G.pcells + pc, q, a.sc);
     };
     auto solid = [&](int ix, int iy, int iz) { return a.obstacle_cur[((long long)ix * ny + iy) * nz + iz] != 0; };
+    // the mask bytes and the populations are loaded before any test (all
+    // inside the brick), so the loads of a cell's directions are in flight
+    // together instead of one dependent round trip after another
     if (kind == kHydroSymmetry) {
         const int ix = min(max(sx, 0), nx - 1), iy = min(max(sy, 0), ny - 1), iz = min(max(sz, 0), nz - 1);
-        return solid(ix, iy, iz) ? bounced : post(ix, iy, iz);
+        const bool si = solid(ix, iy, iz);
+        const float fi = post(ix, iy, iz);
+        return si ? bounced : fi;
     }
     if (kind == kHydroInheritGame && F.disable_convective) return bounced;
     const int dx = (sx < 0 || sx >= nx) ? q_cx(q) : 0;
     const int dy = (sy < 0 || sy >= ny) ? q_cy(q) : 0;
     const int dz = (sz < 0 || sz >= nz) ? q_cz(q) : 0;
     const int x1 = min(max(x + dx, 0), nx - 1), y1 = min(max(y + dy, 0), ny - 1), z1 = min(max(z + dz, 0), nz - 1);
-    if (solid(x1, y1, z1)) return bounced;
-    const float f1 = post(x1, y1, z1);
     const int x2 = min(max(x + 2 * dx, 0), nx - 1), y2 = min(max(y + 2 * dy, 0), ny - 1), z2 = min(max(z + 2 * dz, 0), nz - 1);
-    if (solid(x2, y2, z2)) return f1;
-    const float f2 = post(x2, y2, z2);
+    const bool s1 = solid(x1, y1, z1), s2 = solid(x2, y2, z2);
+    const float f1 = post(x1, y1, z1), f2 = post(x2, y2, z2);
+    if (s1) return bounced;
+    if (s2) return f1;
     return __fadd_rn(f1, __fmul_rn(0.15f, __fsub_rn(f1, f2)));
 }
 

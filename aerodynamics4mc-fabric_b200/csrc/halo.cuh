@@ -37,4 +37,24 @@ cudaError_t launch_materialise_ab(BrickDims d, const float* g, const uint32_t* f
 cudaError_t launch_halo_soa(const float* a, float* b, long long cells, int ny, int nz, int comps, const HaloSlab& ab,
                             cudaStream_t s);
 
+// Many exchanges in one launch: each job copies one slab in one direction.
+// The jobs live in device memory (the caller uploads them); jobs of one launch
+// must not write what another reads (true for the face slabs of a brick
+// world: writes go to the outermost layer along the exchange axis, reads come
+// from inner layers).
+struct HaloIpJob {
+    HaloIpSide src, dst;
+    HaloSlab slab;
+};
+struct HaloSoaJob {
+    const float* src;
+    float* dst;
+    long long cells;
+    int ny, nz;
+    HaloSlab slab;
+};
+// max_slab: the largest slab (cells) of the jobs (sets the grid).
+cudaError_t launch_halo_ip_batch(int storage, const HaloIpJob* jobs, int njobs, int max_slab, cudaStream_t s);
+cudaError_t launch_halo_soa_batch(const HaloSoaJob* jobs, int njobs, int max_slab, cudaStream_t s);
+
 }  // namespace aero

@@ -42,9 +42,8 @@ struct IpSide {
 };
 
 template <class S>
-__global__ void halo_ip_kernel(IpSide<S> src, IpSide<S> dst, HaloSlab slab) {
+__device__ __forceinline__ void halo_ip_cell(const IpSide<S>& src, const IpSide<S>& dst, const HaloSlab& slab, int i) {
     const int n_slab = slab.size[0] * slab.size[1] * slab.size[2];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_slab) return;
     const int lz = i % slab.size[2], ly = (i / slab.size[2]) % slab.size[1], lx = i / (slab.size[2] * slab.size[1]);
     const int sx = slab.src[0] + lx, sy = slab.src[1] + ly, sz = slab.src[2] + lz;
@@ -60,24 +59,43 @@ __global__ void halo_ip_kernel(IpSide<S> src, IpSide<S> dst, HaloSlab slab) {
     const NeighbourOffsets od = neighbour_offsets(dst.g, dx, dy, dz);
     const int own_s = pad_index(src.g, sx, sy, sz), own_d = pad_index(dst.g, dx, dy, dz);
     const long long scells = (long long)src.g.nx * src.g.ny * src.g.nz, dcells = (long long)dst.g.nx * dst.g.ny * dst.g.nz;
-#pragma unroll 1
+    // all 27 loads first (independent, in flight together), then the stores
+    float v[27];
+#pragma unroll
     for (int q = 0; q < 27; ++q) {
-        float v = q_w(q);
+        v[q] = q_w(q);
         if (!src_solid) {
             int c, d;
             incoming_slot(os, own_s, q, src.parity, (ws >> q) & 1u, c, d);
-            v = S::load(src.f + (long long)d * src.g.pcells + c, q, src.sc);
+            v[q] = S::load(src.f + (long long)d * src.g.pcells + c, q, src.sc);
         } else if (src.solid_f) {
-            v = src.solid_f[(long long)solid_slot(q, src.parity) * scells + scell];
+            v[q] = src.solid_f[(long long)solid_slot(q, src.parity) * scells + scell];
         }
+    }
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
         if (dst_solid) {
-            dst.solid_f[(long long)solid_slot(q, dst.parity) * dcells + dcell] = v;
+            dst.solid_f[(long long)solid_slot(q, dst.parity) * dcells + dcell] = v[q];
             continue;
         }
         int c, d;
         incoming_slot(od, own_d, q, dst.parity, (wd >> q) & 1u, c, d);
-        S::store(dst.f + (long long)d * dst.g.pcells + c, q, v, dst.sc);
+        S::store(dst.f + (long long)d * dst.g.pcells + c, q, v[q], dst.sc);
     }
+}
+
+template <class S>
+__global__ void halo_ip_kernel(IpSide<S> src, IpSide<S> dst, HaloSlab slab) {
+    halo_ip_cell(src, dst, slab, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// One job per blockIdx.y (jobs in device memory).
+template <class S>
+__global__ void halo_ip_batch_kernel(const HaloIpJob* __restrict__ jobs) {
+    const HaloIpJob& J = jobs[blockIdx.y];
+    const IpSide<S> src{static_cast<typename S::T*>(J.src.f), J.src.g, J.src.flags, J.src.parity, J.src.sc, J.src.solid_f};
+    const IpSide<S> dst{static_cast<typename S::T*>(J.dst.f), J.dst.g, J.dst.flags, J.dst.parity, J.dst.sc, J.dst.solid_f};
+    halo_ip_cell(src, dst, J.slab, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Two-buffer contexts: f = the pull of the post-collision state.
@@ -107,6 +125,18 @@ __global__ void halo_soa_kernel(const float* __restrict__ src, float* __restrict
     const long long scell = ((long long)(slab.src[0] + lx) * ny + slab.src[1] + ly) * nz + slab.src[2] + lz;
     const long long dcell = ((long long)(slab.dst[0] + lx) * ny + slab.dst[1] + ly) * nz + slab.dst[2] + lz;
     for (int k = 0; k < comps; ++k) dst[(long long)k * cells + dcell] = src[(long long)k * cells + scell];
+}
+
+__global__ void halo_soa_batch_kernel(const HaloSoaJob* __restrict__ jobs) {
+    const HaloSoaJob& J = jobs[blockIdx.y];
+    const HaloSlab& slab = J.slab;
+    const int n_slab = slab.size[0] * slab.size[1] * slab.size[2];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_slab) return;
+    const int lz = i % slab.size[2], ly = (i / slab.size[2]) % slab.size[1], lx = i / (slab.size[2] * slab.size[1]);
+    const long long scell = ((long long)(slab.src[0] + lx) * J.ny + slab.src[1] + ly) * J.nz + slab.src[2] + lz;
+    const long long dcell = ((long long)(slab.dst[0] + lx) * J.ny + slab.dst[1] + ly) * J.nz + slab.dst[2] + lz;
+    J.dst[dcell] = J.src[scell];
 }
 
 unsigned blocks_for(const HaloSlab& s) {
@@ -154,6 +184,24 @@ cudaError_t launch_halo_ip(int storage, const HaloIpSide& a, const HaloIpSide& b
     if (storage == 0) return halo_ip_t<StoreF32>(a, b, ab, ba, s);
     if (storage == 1) return halo_ip_t<StoreF16Dev>(a, b, ab, ba, s);
     return halo_ip_t<StoreI16Dev>(a, b, ab, ba, s);
+}
+
+cudaError_t launch_halo_ip_batch(int storage, const HaloIpJob* jobs, int njobs, int max_slab, cudaStream_t s) {
+    if (njobs <= 0 || max_slab <= 0) return cudaSuccess;
+    const dim3 grid((unsigned)((max_slab + 127) / 128), (unsigned)njobs);
+    if (storage == 0) halo_ip_batch_kernel<StoreF32><<<grid, 128, 0, s>>>(jobs);
+    else if (storage == 1) halo_ip_batch_kernel<StoreF16Dev><<<grid, 128, 0, s>>>(jobs);
+    else halo_ip_batch_kernel<StoreI16Dev><<<grid, 128, 0, s>>>(jobs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_halo_soa_batch(const HaloSoaJob* jobs, int njobs, int max_slab, cudaStream_t s) {
+    if (njobs <= 0 || max_slab <= 0) return cudaSuccess;
+    const dim3 grid((unsigned)((max_slab + 127) / 128), (unsigned)njobs);
+    halo_soa_batch_kernel<<<grid, 128, 0, s>>>(jobs);
+    count_launch();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_materialise_ab(BrickDims d, const float* g, const uint32_t* flags, const uint8_t* obstacle,

@@ -1061,6 +1061,84 @@ void record_timing(double copy_ms, double solver_ms, double readback_ms, double 
     else g_timing.full_packet_steps += 1;
 }
 
+// Deferred halo exchanges (halo_batch_begin / halo_batch_flush): the slab
+// copies of in-place contexts collect as jobs and go out as one launch per
+// storage kind plus one for the temperature slabs.
+struct HaloBatch {
+    bool open = false;
+    std::vector<HaloIpJob> ip[3];
+    std::vector<HaloSoaJob> soa;
+    int ip_max[3] = {0, 0, 0}, soa_max = 0;
+    int device = -1;
+    void* d_jobs = nullptr;       // device copy of the jobs of one flush
+    void* h_jobs = nullptr;       // pinned staging
+    size_t cap = 0;
+    cudaEvent_t staged = nullptr; // the last upload from h_jobs has finished
+};
+static HaloBatch g_halo;
+
+static int slab_cells(const HaloSlab& h) { return h.size[0] * h.size[1] * h.size[2]; }
+
+void halo_batch_begin() {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    g_halo.open = true;
+}
+
+bool halo_batch_flush() {
+    std::lock_guard<std::recursive_mutex> lk(g_mutex);
+    HaloBatch& B = g_halo;
+    B.open = false;
+    size_t bytes = B.soa.size() * sizeof(HaloSoaJob);
+    for (auto& v : B.ip) bytes += v.size() * sizeof(HaloIpJob);
+    if (bytes == 0) return true;
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "halo batch device")) return false;
+    if (B.device != dev || B.cap < bytes) {
+        if (B.staged) cudaEventSynchronize(B.staged);
+        if (B.d_jobs && B.device == dev) cudaFree(B.d_jobs);
+        if (B.h_jobs) cudaFreeHost(B.h_jobs);
+        B.d_jobs = B.h_jobs = nullptr;
+        const size_t cap = std::max<size_t>(bytes * 2, 16384);
+        if (!cuda_ok(cudaMalloc(&B.d_jobs, cap), "halo batch jobs") || !cuda_ok(cudaMallocHost(&B.h_jobs, cap), "halo batch staging")) {
+            B.cap = 0;
+            return false;
+        }
+        B.cap = cap;
+        B.device = dev;
+        if (!B.staged && !cuda_ok(cudaEventCreateWithFlags(&B.staged, cudaEventDisableTiming), "halo batch event")) return false;
+    } else if (!cuda_ok(cudaEventSynchronize(B.staged), "halo batch staging")) {
+        return false;
+    }
+    cudaStream_t s = current_stream();
+    char* h = static_cast<char*>(B.h_jobs);
+    size_t off = 0;
+    struct Part { int kind; size_t off; int n; int max; };
+    std::vector<Part> parts;
+    for (int k = 0; k < 3; ++k) {
+        if (B.ip[k].empty()) continue;
+        std::memcpy(h + off, B.ip[k].data(), B.ip[k].size() * sizeof(HaloIpJob));
+        parts.push_back({k, off, (int)B.ip[k].size(), B.ip_max[k]});
+        off += B.ip[k].size() * sizeof(HaloIpJob);
+    }
+    if (!B.soa.empty()) {
+        std::memcpy(h + off, B.soa.data(), B.soa.size() * sizeof(HaloSoaJob));
+        parts.push_back({3, off, (int)B.soa.size(), B.soa_max});
+        off += B.soa.size() * sizeof(HaloSoaJob);
+    }
+    bool ok = cuda_ok(cudaMemcpyAsync(B.d_jobs, B.h_jobs, off, cudaMemcpyHostToDevice, s), "halo batch upload") &&
+              cuda_ok(cudaEventRecord(B.staged, s), "halo batch event");
+    for (const Part& p : parts) {
+        if (!ok) break;
+        const char* d = static_cast<const char*>(B.d_jobs) + p.off;
+        ok = p.kind < 3 ? cuda_ok(launch_halo_ip_batch(p.kind, reinterpret_cast<const HaloIpJob*>(d), p.n, p.max, s), "halo_inplace")
+                        : cuda_ok(launch_halo_soa_batch(reinterpret_cast<const HaloSoaJob*>(d), p.n, p.max, s), "halo_temperature");
+    }
+    for (auto& v : B.ip) v.clear();
+    B.soa.clear();
+    B.ip_max[0] = B.ip_max[1] = B.ip_max[2] = B.soa_max = 0;
+    return ok;
+}
+
 }  // namespace aero
 
 // ====================================================================== C ABI
@@ -1326,7 +1404,13 @@ static bool exchange_halo(const char* who, int nx, int ny, int nz, int halo_laye
         };
         const int storage = a->ip_variant == kIpF16Fast ? 1 : (a->ip_variant == kIpI16Fast ? 2 : 0);
         if (!join_fill(*a, s) || !join_fill(*b, s)) return false;
-        if (!cuda_ok(launch_halo_ip(storage, side(*a), side(*b), ab, ba, s), "halo_inplace")) return false;
+        if (g_halo.open) {
+            g_halo.ip[storage].push_back(HaloIpJob{side(*a), side(*b), ab});
+            g_halo.ip[storage].push_back(HaloIpJob{side(*b), side(*a), ba});
+            g_halo.ip_max[storage] = std::max({g_halo.ip_max[storage], slab_cells(ab), slab_cells(ba)});
+        } else if (!cuda_ok(launch_halo_ip(storage, side(*a), side(*b), ab, ba, s), "halo_inplace")) {
+            return false;
+        }
     } else {
         for (Context* c : {a, b}) {
             if (c->f_ready) continue;
@@ -1346,6 +1430,12 @@ static bool exchange_halo(const char* who, int nx, int ny, int nz, int halo_laye
         return bench_active() || c->step_counter == 0 || (c->step_counter - 1) % 2 == 0;
     };
     if (updated_last(a) || updated_last(b)) {
+        if (g_halo.open && a->layout == 1) {
+            g_halo.soa.push_back(HaloSoaJob{a->temperature, b->temperature, a->cells, ny, nz, ab});
+            g_halo.soa.push_back(HaloSoaJob{b->temperature, a->temperature, b->cells, ny, nz, ba});
+            g_halo.soa_max = std::max({g_halo.soa_max, slab_cells(ab), slab_cells(ba)});
+            return true;
+        }
         if (!cuda_ok(launch_halo_soa(a->temperature, b->temperature, a->cells, ny, nz, 1, ab, s), "halo_temperature")) return false;
         if (!cuda_ok(launch_halo_soa(b->temperature, a->temperature, b->cells, ny, nz, 1, ba, s), "halo_temperature")) return false;
     }

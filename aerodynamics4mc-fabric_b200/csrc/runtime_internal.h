@@ -150,5 +150,10 @@ float i16_scale_for_speed(float umax);
 bool output_device(Context& ctx, OutBox box, int out_ch, float scale, float* dev_out);
 // Order stream s after the context's last equilibrium-face pre-fill.
 bool join_fill(Context& ctx, cudaStream_t s);
+// Collect the slab copies of the following exchange_halo calls (in-place
+// contexts) and launch them together at halo_batch_flush(); exchanges of one
+// batch must touch disjoint slabs (the face slabs of a brick world do).
+void halo_batch_begin();
+bool halo_batch_flush();
 
 }  // namespace aero
