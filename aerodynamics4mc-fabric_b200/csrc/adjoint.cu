@@ -74,26 +74,13 @@ __device__ __forceinline__ void cell_xyz(const Geo& G, long long i, int& x, int&
     cell_xyz32(i, G.ny, G.nz, x, y, z);
 }
 
-// pull_source for a cell none of whose neighbours lies outside the brick:
-// every source is the neighbour at -c_q (no face, no wrap), a slot pull unless
-// that neighbour is solid.
-__device__ __forceinline__ bool interior(const Geo& G, int x, int y, int z) {
-    return x > 0 && y > 0 && z > 0 && x < G.nx - 1 && y < G.ny - 1 && z < G.nz - 1;
-}
-__device__ __forceinline__ int pull_source_at(const Geo& G, bool in, long long i, int x, int y, int z, int q, long long& src) {
-    if (!in) return pull_source(G, x, y, z, q, src);
-    src = i - (((long long)q_cx(q) * G.ny + q_cy(q)) * G.nz + q_cz(q));
-    return G.solid[src] ? kPullBounce : kPullSlot;
-}
-
 template <class T>
 __device__ __forceinline__ void pull_cell(const Geo& G, const T* __restrict__ s, long long i, int x, int y, int z,
                                           const T (&uin)[3], T (&p)[27]) {
-    const bool in = interior(G, x, y, z);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         long long src = 0;
-        const int k = pull_source_at(G, in, i, x, y, z, q, src);
+        const int k = pull_source(G, x, y, z, q, src);
         p[q] = k == kPullSlot ? s[(long long)q * G.cells + src]
              : k == kPullBounce ? s[(long long)q_opp(q) * G.cells + i]
                                 : feq_t<T>(q, T(1), uin[0], uin[1], uin[2]);
@@ -187,11 +174,10 @@ __global__ void adj_probe_kernel(Geo G, const T* __restrict__ s, T ux_in, T uy_i
 template <bool kAccumulate>
 __device__ __forceinline__ void scatter(const Geo& G, long long i, int x, int y, int z, const float (&lam)[27],
                                         const float (&uin)[3], float* __restrict__ lam_prev, double (&du)[3]) {
-    const bool in = interior(G, x, y, z);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         long long src = 0;
-        const int k = pull_source_at(G, in, i, x, y, z, q, src);
+        const int k = pull_source(G, x, y, z, q, src);
         if (k == kPullFace) {
             float d[3];
             dfeq_du<float>(q, 1.0f, uin[0], uin[1], uin[2], d);
@@ -319,7 +305,8 @@ struct Brick {
     float* st[2] = {nullptr, nullptr};
     double* st64[2] = {nullptr, nullptr};
     std::vector<float*> ckpt;  // ckpt[j] = s_{jK} for j >= 1 (index 0 unused)
-    std::vector<float*> seg;   // K - 1 recomputed states of a segment
+    std::vector<float*> seg;   // two sets of K - 1 recomputed segment states
+    cudaStream_t side = nullptr;  // recomputation stream (overlaps the reverse launches)
     float* lam[2] = {nullptr, nullptr};
     double* grad_f = nullptr;
     double* probe_loss = nullptr;  // per probe
@@ -341,6 +328,7 @@ struct Brick {
             if (p) cudaFree(p);
         for (float* p : seg)
             if (p) cudaFree(p);
+        if (side) cudaStreamDestroy(side);
     }
 };
 
@@ -605,10 +593,11 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_gradient(long long handle, const 
     if (b->ckpt.empty()) {
         const int segments = (N + K - 1) / K;
         b->ckpt.assign(segments, nullptr);
-        b->seg.assign(std::max(0, K - 1), nullptr);
+        b->seg.assign(2 * std::max(0, K - 1), nullptr);
         bool got = true;
         for (int j = 1; got && j < segments; ++j) got = adj_ok(cudaMalloc(&b->ckpt[j], bytes), "checkpoint alloc");
-        for (int j = 0; got && j < K - 1; ++j) got = adj_ok(cudaMalloc(&b->seg[j], bytes), "segment alloc");
+        for (size_t j = 0; got && j < b->seg.size(); ++j) got = adj_ok(cudaMalloc(&b->seg[j], bytes), "segment alloc");
+        if (got && !b->side) got = adj_ok(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking), "side stream");
         if (!got) {
             for (float* p : b->ckpt)
                 if (p) cudaFree(p);
@@ -651,23 +640,54 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_gradient(long long handle, const 
         ok = adj_ok(cudaGetLastError(), "seed kernel");
     }
     // reverse sweep over segments: segment j covers calls jK+1 .. min((j+1)K, N)
-    // and needs s_{jK} .. s_{(j+1)K-1} (s_0 = the initial equilibrium)
+    // and needs s_{jK} .. s_{(j+1)K-1} (s_0 = the initial equilibrium). The
+    // states of segment j - 1 are recomputed on the side stream, into the
+    // other of two buffer sets, while segment j is reversed on s: the
+    // recomputation reads only checkpoint j - 1, so the two run side by side.
     int lc = 0;
     double rec_ms = 0.0, rev_ms = 0.0;
     const int segments = (N + K - 1) / K;
-    for (int j = segments - 1; ok && j >= 0; --j) {
+    const int per = std::max(0, K - 1);
+    cudaStream_t s2 = b->side;
+    std::vector<cudaEvent_t> evw(segments), evr(segments), eve(segments);  // on s: before / after the wait, after the reverse
+    cudaEvent_t rec_done[2], rev_done[2], fwd_done;
+    bool rev_used[2] = {false, false};
+    for (int k = 0; k < segments; ++k) {
+        cudaEventCreate(&evw[k]);
+        cudaEventCreate(&evr[k]);
+        cudaEventCreate(&eve[k]);
+    }
+    for (int k = 0; k < 2; ++k) {
+        cudaEventCreateWithFlags(&rec_done[k], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&rev_done[k], cudaEventDisableTiming);
+    }
+    cudaEventCreateWithFlags(&fwd_done, cudaEventDisableTiming);
+    // the side stream starts after the forward (force field, checkpoints)
+    ok = ok && adj_ok(cudaEventRecord(fwd_done, s), "sweep fork") && adj_ok(cudaStreamWaitEvent(s2, fwd_done, 0), "sweep fork");
+    auto recompute = [&](int j, int set) {
+        const int first = j * K + 1, last = std::min((j + 1) * K, N);
+        if (rev_used[set] && !adj_ok(cudaStreamWaitEvent(s2, rev_done[set], 0), "segment reuse")) return false;
+        const float* prev = j > 0 ? b->ckpt[j] : nullptr;
+        for (int m = 1; m <= last - first; ++m) {
+            float* dst = b->seg[(size_t)set * per + m - 1];
+            if (!(m == 1 && j == 0 ? launch_step<float>(*b, inflow, true, nullptr, dst, s2)
+                                   : launch_step<float>(*b, inflow, false, prev, dst, s2)))
+                return false;
+            prev = dst;
+        }
+        return adj_ok(cudaEventRecord(rec_done[set], s2), "segment done");
+    };
+    if (ok && segments > 0) ok = recompute(segments - 1, 0);
+    for (int j = segments - 1, idx = 0; ok && j >= 0; --j, ++idx) {
+        const int set = idx % 2;
+        if (j > 0) ok = recompute(j - 1, set ^ 1);
         const int first = j * K + 1, last = std::min((j + 1) * K, N);
         // states[m] = s_{jK + m} for m = 1 .. last - first (s_{jK} = ckpt[j])
         std::vector<const float*> states(last - first + 1, nullptr);
         states[0] = j > 0 ? b->ckpt[j] : nullptr;
-        cudaEventRecord(ev[2], s);
-        for (int m = 1; ok && m <= last - first; ++m) {
-            float* dst = b->seg[m - 1];
-            if (m == 1 && j == 0) ok = launch_step<float>(*b, inflow, true, nullptr, dst, s);
-            else ok = launch_step<float>(*b, inflow, false, states[m - 1], dst, s);
-            states[m] = dst;
-        }
-        cudaEventRecord(ev[3], s);
+        for (int m = 1; m <= last - first; ++m) states[m] = b->seg[(size_t)set * per + m - 1];
+        ok = ok && adj_ok(cudaEventRecord(evw[idx], s), "sweep event") && adj_ok(cudaStreamWaitEvent(s, rec_done[set], 0), "segment wait") &&
+             adj_ok(cudaEventRecord(evr[idx], s), "sweep event");
         for (int n = last; ok && n >= first; --n) {
             const int m = n - first;  // input state of call n is states[m]
             StepArgs<float> a = step_args<float>(*b, inflow, states[m], nullptr);
@@ -682,11 +702,24 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_gradient(long long handle, const 
             ok = adj_ok(cudaGetLastError(), "reverse kernel");
             lc ^= 1;
         }
-        cudaEventRecord(ev[4], s);
-        cudaEventSynchronize(ev[4]);
-        rec_ms += elapsed(ev[2], ev[3]);
-        rev_ms += elapsed(ev[3], ev[4]);
+        ok = ok && adj_ok(cudaEventRecord(eve[idx], s), "sweep event") && adj_ok(cudaEventRecord(rev_done[set], s), "sweep event");
+        rev_used[set] = true;
     }
+    if (ok) ok = adj_ok(cudaStreamSynchronize(s), "sweep sync");
+    for (int k = 0; ok && k < segments; ++k) {
+        rec_ms += elapsed(evw[k], evr[k]);
+        rev_ms += elapsed(evr[k], eve[k]);
+    }
+    for (int k = 0; k < segments; ++k) {
+        cudaEventDestroy(evw[k]);
+        cudaEventDestroy(evr[k]);
+        cudaEventDestroy(eve[k]);
+    }
+    for (int k = 0; k < 2; ++k) {
+        cudaEventDestroy(rec_done[k]);
+        cudaEventDestroy(rev_done[k]);
+    }
+    cudaEventDestroy(fwd_done);
     std::vector<double> pl(b->nprobe), du(3 * ((size_t)b->rev_blocks + 1));
     if (ok) ok = adj_ok(cudaMemcpyAsync(pl.data(), b->probe_loss, b->nprobe * sizeof(double), cudaMemcpyDeviceToHost, s),
                         "loss read") &&

@@ -508,7 +508,11 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_forward(long long handle, const f
 /* Loss and gradients (FP64): out_grad_force 3 x cells (SoA) or null, out_grad_inflow 3. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_gradient(long long handle, const float* force_soa, const float* inflow,
                                                         double* out_loss, double* out_grad_force, double* out_grad_inflow);
-/* Device ms per call of the last gradient run: forward, segment recomputation, reverse; and its wall ms. */
+/* Device ms per call of the last gradient run, and its wall ms. forward: the forward run with its
+ * checkpoints. The reverse sweep recomputes each segment's states on a second stream while the previous
+ * segment is reversed; recompute: the time the reverse stream waited for recomputed states (the part not
+ * hidden under reverse launches); reverse: the time of the reverse launches. recompute + reverse is the
+ * sweep's device time. */
 AERO_LBM_B200_EXPORT int aero_lbm_b200_adjoint_timing(long long handle, double* out_forward_ms_per_step,
                                                       double* out_recompute_ms_per_step, double* out_reverse_ms_per_step,
                                                       double* out_total_ms);
