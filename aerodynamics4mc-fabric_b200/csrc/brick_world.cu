@@ -402,6 +402,7 @@ void release_context(Service& svc, Brick& b) {
         aero_lbm_release_context(b.context);
         b.context = 0;
     }
+    b.stepped_context = 0;
     b.compact_active = false;
     b.stale = false;
     b.pending_patch_cells.clear();
@@ -766,9 +767,12 @@ bool step_brick(Service& svc, World& w, const Coord& c, Brick& b, Next& next, st
     }
     fa.ref_layers = std::max(1, std::min(kBoundaryReferenceLayers, n));
     fa.source_denominator = kSourceDenominator;
-    const DeviceFill fill{fill_launch, &fa};
+    // the mask comes from the static fields alone: unchanged since this
+    // context's last step, the step keeps its pull classification
+    const DeviceFill fill{fill_launch, &fa,
+                          had_context && b.stepped_context == b.context && b.stepped_version == b.static_version};
 
-    bool step_ok = false, compact_ok = false, have_summary = false;
+    bool step_ok = false, compact_ok = false, have_summary = false, fill_stepped = false;
     CompactSummary sum;
     if (experimental(w)) {
         HostDynamic tmp;
@@ -786,7 +790,7 @@ bool step_brick(Service& svc, World& w, const Coord& c, Brick& b, Next& next, st
         w.compact_last_nonfinite_cells = (uint64_t)std::max(0, sum.nonfinite);
         if (sum.supported && configure_compact(sum.v, n)) {
             if (had_context && b.compact_active) step_ok = aero_lbm_step_rect_cached(n, n, n, b.context, nullptr) != 0;
-            if (!step_ok) step_ok = step_rect_device(b.context, n, n, n, fill);
+            if (!step_ok) step_ok = fill_stepped = step_rect_device(b.context, n, n, n, fill);
             if (step_ok && aero_lbm_context_realtime_cached_initialized(b.context)) {
                 compact_ok = true;
                 w.compact_initial_steps++;
@@ -811,7 +815,7 @@ bool step_brick(Service& svc, World& w, const Coord& c, Brick& b, Next& next, st
         b.compact_active = false;
         w.d3q27_steps++;
         const bool fallback_faces = have_summary && configure_compact(sum.v, n);
-        step_ok = step_rect_device(b.context, n, n, n, fill);
+        step_ok = fill_stepped = step_rect_device(b.context, n, n, n, fill);
         aero_lbm_benchmark_reset_config();
         if (step_ok && fallback_faces && aero_lbm_context_realtime_cached_initialized(b.context)) {
             compact_ok = true;
@@ -825,6 +829,10 @@ bool step_brick(Service& svc, World& w, const Coord& c, Brick& b, Next& next, st
         release_context(svc, b);
         adopt_next(b, next);
         return false;
+    }
+    if (fill_stepped) {
+        b.stepped_version = b.static_version;
+        b.stepped_context = b.context;
     }
     if (compact_ok) {
         adopt_next(b, next);

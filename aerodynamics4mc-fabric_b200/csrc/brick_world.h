@@ -75,6 +75,10 @@ struct Brick {
     std::unique_ptr<StaticFields> stat;
     uint64_t static_version = 0;  // bumped on every change of stat
     uint64_t static_on_device = 0;  // version of the device copy (0: none)
+    // static version and context of the last step built from the static fields
+    // (its mask is the context's current one)
+    uint64_t stepped_version = 0;
+    long long stepped_context = 0;
 
     // dynamic state: buffer `cur` on the device, or a host copy not yet uploaded
     bool has_dynamic = false;

@@ -508,10 +508,17 @@ __device__ __forceinline__ float ip_face_source(const typename S::T* __restrict_
     int c, d;
     incoming_slot(o, own, q, p, true, c, d);
     const float bounced = S::load(f + (long long)d * G.pcells + c, q, a.sc);
-    // post-collision population q of cell (ix, iy, iz) after the last step
+    // post-collision population q of cell (ix, iy, iz) after the last step:
+    // outgoing_slot at parity p ^ 1 (the cell's own memory, or for positive q
+    // the memory of its neighbour at +c_q), without the full offset table
     auto post = [&](int ix, int iy, int iz) {
-        int pc, pd;
-        outgoing_slot(neighbour_offsets(G, ix, iy, iz), pad_index(G, ix, iy, iz), q, p ^ 1, pc, pd);
+        const int pd = q == kRest27 ? kRest27 : ((p ^ 1) == 0 ? q : q_opp(q));
+        int pc;
+        if (q != kRest27 && q_positive(q))
+            pc = pad_index(G, axis_neighbour(ix, q_cx(q), nx, G.wrap[0]), axis_neighbour(iy, q_cy(q), ny, G.wrap[1]),
+                           axis_neighbour(iz, q_cz(q), nz, G.wrap[2]));
+        else
+            pc = pad_index(G, ix, iy, iz);
         return S::load(f + (long long)pd * G.pcells + pc, q, a.sc);
     };
     auto solid = [&](int ix, int iy, int iz) { return a.obstacle_cur[((long long)ix * ny + iy) * nz + iz] != 0; };

@@ -136,6 +136,10 @@ __device__ __forceinline__ void ingest_cell(const float* p, int in_ch, long long
 struct DeviceFill {
     cudaError_t (*launch)(const CellFields& out, const BrickDims& d, cudaStream_t s, void* user);
     void* user;
+    // the caller guarantees that the obstacle mask this fill writes equals
+    // the mask of the context's last call: the pull classification is reused
+    // and no cell changes between fluid and solid
+    bool mask_unchanged = false;
 };
 
 struct ForceField {

@@ -778,6 +778,8 @@ static bool step_context_body(Context& ctx, const float* packet, float* out, flo
 
     int new_slot = ctx.slot;
     const bool face_changed = std::memcmp(&face_now, &ctx.face_prev, sizeof(FaceParams)) != 0;
+    // a device fill that rewrites the same mask keeps the classification
+    const bool same_mask = fill && fill->mask_unchanged && ctx.initialized && !face_changed && ctx.pending_slot < 0;
     if (have_packet) {
         new_slot = ctx.initialized ? 1 - ctx.slot : ctx.slot;
         const size_t bytes = (size_t)ctx.cells * in_ch * sizeof(float);
@@ -827,7 +829,16 @@ static bool step_context_body(Context& ctx, const float* packet, float* out, flo
                 return false;
         }
         if (host_packet && !cuda_ok(cudaEventRecord(ctx.copy_done, s), "copy event")) return false;
-        if (!classify(ctx, new_slot, face_now, d, s)) return false;
+        if (same_mask) {
+            ctx.h_face[new_slot] = face_now;
+            if (!cuda_ok(cudaMemcpyAsync(ctx.d_face[new_slot], ctx.d_face[ctx.slot], sizeof(FaceParams), cudaMemcpyDeviceToDevice, s),
+                         "copy faces") ||
+                !cuda_ok(cudaMemcpyAsync(ctx.flags[new_slot], ctx.flags[ctx.slot], (size_t)ctx.cells * sizeof(uint32_t),
+                                         cudaMemcpyDeviceToDevice, s), "copy classification"))
+                return false;
+        } else if (!classify(ctx, new_slot, face_now, d, s)) {
+            return false;
+        }
         ctx.has_inputs = true;
     } else if (ctx.pending_slot >= 0) {
         // block edits staged the mask of this call (aero_lbm_patch_d3q27_f16_static_cells_rect)
@@ -922,10 +933,14 @@ static bool step_context_body(Context& ctx, const float* packet, float* out, flo
             if (!cuda_ok(ip_init(ctx.ip_variant, ctx.ip, a, s), "init_inplace")) return false;
             ctx.parity = 1;
         } else {
-            const bool transitions = have_packet || ctx.pending_slot >= 0;
-            if (transitions && !ctx.solid_f) {
+            // a call with inputs can change the mask; one whose device fill
+            // keeps it has no transitions to apply
+            const bool inputs = have_packet || ctx.pending_slot >= 0;
+            const bool transitions = inputs && !same_mask;
+            if (inputs && !ctx.solid_f) {
                 // the first call that can change the mask: solid cells so far
-                // have been solid since initialisation and hold the rest state
+                // have been solid since initialisation and hold the rest state;
+                // from now on they keep (and exchange) their own populations
                 if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&ctx.solid_f), (size_t)ctx.cells * 27 * sizeof(float)),
                              "cudaMalloc(solid populations)") ||
                     !cuda_ok(launch_fill_rest(ctx.solid_f, ctx.cells, s), "fill solid populations"))

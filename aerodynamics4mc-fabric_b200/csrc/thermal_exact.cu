@@ -37,8 +37,10 @@ __device__ __forceinline__ float th_neighbour(const ThermalArgs& a, const float*
         return self;
     }
     const long long cell = ((long long)x * a.ny + y) * a.nz + z;
-    if (a.obstacle[cell]) return self;
-    return field[cell];
+    // both loads issued before the test (one round trip, not two)
+    const bool solid = a.obstacle[cell] != 0;
+    const float v = field[cell];
+    return solid ? self : v;
 }
 __device__ __forceinline__ float th_neighbour(const ThermalArgs& a, int x, int y, int z, float self) {
     return th_neighbour(a, a.t, x, y, z, self);
@@ -145,26 +147,45 @@ __device__ __noinline__ float th_sample_far(const ThermalArgs& a, float px, floa
 // neighbour; else C^2 |S| (capped at 5 nu0) from central differences of the
 // last collision's velocity, a solid or outside neighbour giving the centre's
 // value.
-__device__ __forceinline__ float vel_or_self(const ThermalArgs& a, const float* v, int x, int y, int z, float self) {
-    if (x < 0 || y < 0 || z < 0 || x >= a.nx || y >= a.ny || z >= a.nz) return self;
-    const long long c = ((long long)x * a.ny + y) * a.nz + z;
-    return a.obstacle[c] ? self : v[c];
-}
 __device__ __noinline__ float eddy_nu(const ThermalArgs& a, int x, int y, int z) {
+    // the six face neighbours (+x, -x, +y, -y, +z, -z): every mask byte and
+    // velocity is loaded before any test (outside neighbours read the cell
+    // itself), so the loads are in flight together
     const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    const long long cc = ((long long)x * a.ny + y) * a.nz + z;
+    bool inside[6];
+    long long nc[6];
+#pragma unroll
     for (int i = 0; i < 6; ++i) {
         const int p = x + off[i][0], q = y + off[i][1], r = z + off[i][2];
-        if (p < 0 || q < 0 || r < 0 || p >= a.nx || q >= a.ny || r >= a.nz) continue;
-        if (a.obstacle[((long long)p * a.ny + q) * a.nz + r]) return 0.0f;
+        inside[i] = !(p < 0 || q < 0 || r < 0 || p >= a.nx || q >= a.ny || r >= a.nz);
+        nc[i] = inside[i] ? ((long long)p * a.ny + q) * a.nz + r : cc;
     }
-    const long long cc = ((long long)x * a.ny + y) * a.nz + z;
-    float d[3][3];
+    bool solid[6];
+    float nv[3][6], sv[3];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) solid[i] = a.obstacle[nc[i]] != 0;
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float* v = a.u + (long long)k * a.cells;
-        const float self = v[cc];
-        d[k][0] = 0.5f * (vel_or_self(a, v, x + 1, y, z, self) - vel_or_self(a, v, x - 1, y, z, self));
-        d[k][1] = 0.5f * (vel_or_self(a, v, x, y + 1, z, self) - vel_or_self(a, v, x, y - 1, z, self));
-        d[k][2] = 0.5f * (vel_or_self(a, v, x, y, z + 1, self) - vel_or_self(a, v, x, y, z - 1, self));
+        sv[k] = v[cc];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) nv[k][i] = v[nc[i]];
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+        if (inside[i] && solid[i]) return 0.0f;
+    // the neighbour's velocity, the centre's for an outside one (a solid
+    // inside neighbour has returned above)
+    float d[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float w[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) w[i] = (inside[i] && !solid[i]) ? nv[k][i] : sv[k];
+        d[k][0] = 0.5f * (w[0] - w[1]);
+        d[k][1] = 0.5f * (w[2] - w[3]);
+        d[k][2] = 0.5f * (w[4] - w[5]);
     }
     const float sxx = d[0][0], syy = d[1][1], szz = d[2][2];
     const float sxy = 0.5f * (d[0][1] + d[1][0]);
