@@ -553,13 +553,17 @@ __device__ __forceinline__ float ip_face_source(const typename S::T* __restrict_
 // step that produced the post-collision populations it reads. One thread per
 // cell of the six boundary layers; cells on edges are visited once per face
 // and write identical values.
+// face_fill_count: threads of the fill (one per cell of each of the six faces).
+inline long long face_fill_count(const PadGeom& g) {
+    return 2LL * ((long long)g.ny * g.nz + (long long)g.nx * g.nz + (long long)g.nx * g.ny);
+}
+
 template <class S>
-__global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
-    const PadGeom G = a.g;
+__device__ __forceinline__ void face_fill_cell(typename S::T* __restrict__ f, const IpArgs& a, unsigned i) {
+    const PadGeom& G = a.g;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     // 32-bit index arithmetic: a face of a brick has far fewer than 2^31 cells
     const unsigned fx_n = (unsigned)ny * nz, fy_n = (unsigned)nx * nz, fz_n = (unsigned)nx * ny;
-    unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     int x, y, z;
     if (i < 2 * fx_n) {
         x = i < fx_n ? 0 : nx - 1;
@@ -594,6 +598,11 @@ __global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
         incoming_slot(o, own, q, a.parity, false, c, d);
         S::store(f + (long long)d * G.pcells + c, q, v, a.sc);
     }
+}
+
+template <class S>
+__global__ void face_fill_ip_kernel(typename S::T* __restrict__ f, IpArgs a) {
+    face_fill_cell<S>(f, a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Cells that were solid at the streaming call and are fluid now: start from

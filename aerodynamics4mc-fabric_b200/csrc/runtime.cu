@@ -51,6 +51,13 @@ struct TimingStats {
 
 RuntimeConfig g_cfg;
 std::recursive_mutex g_mutex;  // guards every entry point (the caller is one worker thread)
+// Arguments of each context's deferred face pre-fill (Context::fill_pending).
+std::unordered_map<const Context*, IpArgs> g_fill_args;
+void drop_pending_fill(Context& ctx) {
+    ctx.fill_pending = false;
+    g_fill_args.erase(&ctx);
+}
+
 // Tuning knobs (aero_lbm_b200_set_*), at their defaults; reset_tuning()
 // restores exactly these values.
 int g_thermal_mode = -1;      // temperature transport: -1 with buoyancy, 0 never (packet field), 1 always
@@ -442,12 +449,7 @@ void Context::release_device() {
     fr(reinterpret_cast<void*&>(fan_mask));
     if (copy_done) cudaEventDestroy(copy_done);
     copy_done = nullptr;
-    if (fill_done) cudaEventDestroy(fill_done);
-    if (fill_fork) cudaEventDestroy(fill_fork);
-    if (fill_stream) cudaStreamDestroy(fill_stream);
-    fill_done = fill_fork = nullptr;
-    fill_stream = nullptr;
-    fill_recorded = false;
+    drop_pending_fill(*this);
     fr(scratch);
     scratch_cap = 0;
     packet_cap = out_cap = 0;
@@ -570,8 +572,13 @@ static int ip_storage(const Context& ctx) {
 }
 
 bool join_fill(Context& ctx, cudaStream_t s) {
-    if (!ctx.fill_recorded) return true;
-    return cuda_ok(cudaStreamWaitEvent(s, ctx.fill_done, 0), "wait for the face pre-fill");
+    if (!ctx.fill_pending) return true;
+    auto it = g_fill_args.find(&ctx);
+    ctx.fill_pending = false;
+    if (it == g_fill_args.end()) return true;
+    const IpArgs a = it->second;
+    g_fill_args.erase(it);
+    return cuda_ok(ip_fill(ctx.ip_variant, ctx.ip, a, s), "face_fill_inplace");
 }
 
 static IpArgs ip_args(Context& ctx, int stream_slot, int cur_slot, const CollideParams& cp) {
@@ -899,7 +906,17 @@ static bool step_context_body(Context& ctx, const float* packet, float* out, flo
             transport.alpha = ta.alpha;
             transport.faces = ta.faces;
         } else if (update) {
-            if (!cuda_ok(launch_thermal_update(ta, s), "thermal_update")) return false;
+            auto pf = g_fill_args.find(&ctx);
+            if (ctx.fill_pending && ctx.layout == 1 && !ta.bfecc && pf != g_fill_args.end()) {
+                // the last call's face pre-fill rides in the same grid
+                const IpArgs fa = pf->second;
+                g_fill_args.erase(pf);
+                ctx.fill_pending = false;
+                if (!cuda_ok(launch_thermal_update_fill(ta, ip_storage(ctx), ctx.ip, fa, s), "thermal_update + face_fill"))
+                    return false;
+            } else if (!cuda_ok(launch_thermal_update(ta, s), "thermal_update")) {
+                return false;
+            }
             std::swap(ctx.temperature, ta.bfecc ? ctx.temperature_scratch : ctx.temperature_next);
         }
     }
@@ -976,21 +993,13 @@ static bool step_context_body(Context& ctx, const float* packet, float* out, flo
         // every incoming slot then holds the cell's streamed population (the
         // reference's f), which the halo exchange reads and writes.
         if (faces_need_fill(face_now)) {
-            // on the context's fill stream, forked after the step: it overlaps
-            // the next call's temperature update (the step waits for it)
-            if (!ctx.fill_stream &&
-                (!cuda_ok(cudaStreamCreateWithFlags(&ctx.fill_stream, cudaStreamNonBlocking), "fill stream") ||
-                 !cuda_ok(cudaEventCreateWithFlags(&ctx.fill_fork, cudaEventDisableTiming), "fill event") ||
-                 !cuda_ok(cudaEventCreateWithFlags(&ctx.fill_done, cudaEventDisableTiming), "fill event")))
-                return false;
+            // deferred: the next call's temperature update launches it in the
+            // same grid; anything else that reads the populations first
+            // launches it on its own (join_fill)
             IpArgs a = ip_args(ctx, new_slot, new_slot, cp);
             a.parity = ctx.parity;
-            if (!cuda_ok(cudaEventRecord(ctx.fill_fork, s), "fork fill") ||
-                !cuda_ok(cudaStreamWaitEvent(ctx.fill_stream, ctx.fill_fork, 0), "fork fill") ||
-                !cuda_ok(ip_fill(ctx.ip_variant, ctx.ip, a, ctx.fill_stream), "face_fill_inplace") ||
-                !cuda_ok(cudaEventRecord(ctx.fill_done, ctx.fill_stream), "join fill"))
-                return false;
-            ctx.fill_recorded = true;
+            g_fill_args[&ctx] = a;
+            ctx.fill_pending = true;
         }
         // the reference reads the shell in its FP16 in-place step only
         // (jni.cpp:6779-6790): a call in another solver mode keeps it unapplied

@@ -55,12 +55,11 @@ struct Context {
     int ip_variant = 0;      // IpVariant when layout == 1
     void* ip = nullptr;      // padded population array (float or __half)
     float* solid_f = nullptr;
-    // The equilibrium-face pre-fill at the end of a call runs on its own
-    // stream, overlapping the next call's temperature update; anything that
-    // touches the in-place populations joins it first (join_fill).
-    cudaStream_t fill_stream = nullptr;
-    cudaEvent_t fill_fork = nullptr, fill_done = nullptr;
-    bool fill_recorded = false;
+    // The face pre-fill a call leaves for the next one is deferred: the next
+    // call's temperature update launches it in the same grid (independent
+    // work), and anything else that touches the in-place populations first
+    // launches it on the library stream (join_fill).
+    bool fill_pending = false;
     cudaEvent_t copy_done = nullptr;  // a call's host-to-device input copies (returned only once read)
     float* fan_mask = nullptr;  // packet fan channels, 4 x cells (mask, ux, uy, uz), while fan forcing is on  // in-place: populations of solid cells (IpArgs::solid_f), from the first mask change on
     int parity = 0;          // slot-map parity of the next in-place step

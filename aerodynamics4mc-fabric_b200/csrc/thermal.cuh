@@ -72,6 +72,9 @@ struct ThermalArgs {
     int turbulent;              // add the local eddy diffusivity
     float sgs_c2;               // Smagorinsky C^2 of the eddy viscosity
     float nu0;                  // runtime molecular viscosity (its cap is 5 nu0)
+    int pairs;                  // set by the launch: z-pair vector access allowed (even nz, aligned fields)
+    int xchunk;                 // set by the launch: x-planes per transport block
+    int zero_bits;              // set by the launch: 0, a run-time zero for the packed products
 };
 
 // Runtime mode, every call after the first (apply_runtime_temperature_reference,
@@ -105,6 +108,11 @@ struct ThermalInitArgs {
 };
 
 cudaError_t launch_thermal_init(const ThermalInitArgs& a, cudaStream_t s);
+struct IpArgs;
+// The first-order transport (not BFECC) and, in the same launch, the face
+// pre-fill of an in-place context (storage: 0 FP32, 1 IEEE half, 2 16-bit
+// fixed point; f its populations, fill the fill's arguments).
+cudaError_t launch_thermal_update_fill(const ThermalArgs& a, int storage, void* f, const IpArgs& fill, cudaStream_t s);
 cudaError_t launch_thermal_update(const ThermalArgs& a, cudaStream_t s);
 
 }  // namespace aero

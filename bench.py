@@ -494,6 +494,9 @@ def run_ours(args) -> dict | None:
     lib.aero_lbm_b200_set_fused_transport(args.fused_transport)
 
     case = cases.c2_terrain_boussinesq(args.n)
+    if args.brick_world_only:
+        # profiling entry: the brick-world leg alone, its record printed
+        return {"brick_world": run_brick_world_leg(aero, lib, case, max(5, min(args.steps, 40)), args.warmup)}
     n = args.n
     cells = case.cells
 
@@ -736,6 +739,8 @@ def main() -> int:
                     help="steps of the 16-bit-vs-FP64 accuracy leg (0 skips it)")
     ap.add_argument("--no-brick-world", dest="brick_world", action="store_false",
                     help="skip the brick-world service leg")
+    ap.add_argument("--brick-world-only", action="store_true",
+                    help="run only the brick-world service leg and print its record (for profiling)")
     args = ap.parse_args()
     args.variants = [v for v in args.variants.split(",") if v]
     if args.warmup < 3:
