@@ -551,53 +551,66 @@ __device__ __forceinline__ float ip_face_source(const typename S::T* __restrict_
 // only the never-updated ghost would write). These slots are written by no
 // step and read by no other fill thread, so the fill runs right after the
 // step that produced the post-collision populations it reads. One thread per
-// cell of the six boundary layers; cells on edges are visited once per face
-// and write identical values.
-// face_fill_count: threads of the fill (one per cell of each of the six faces).
+// link: a cell of one of the six boundary layers and one of the nine
+// directions that pull across that face (c along the face's axis pointing
+// into the brick), consecutive threads along the face's cells, so that each
+// thread makes one round of independent loads. A link that crosses two or
+// three faces (edge and corner cells) is visited once per face; every visit
+// writes the same value.
+// face_fill_count: threads of the fill.
 inline long long face_fill_count(const PadGeom& g) {
-    return 2LL * ((long long)g.ny * g.nz + (long long)g.nx * g.nz + (long long)g.nx * g.ny);
+    return 9LL * 2 * ((long long)g.ny * g.nz + (long long)g.nx * g.nz + (long long)g.nx * g.ny);
 }
 
 template <class S>
 __device__ __forceinline__ void face_fill_cell(typename S::T* __restrict__ f, const IpArgs& a, unsigned i) {
     const PadGeom& G = a.g;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
-    // 32-bit index arithmetic: a face of a brick has far fewer than 2^31 cells
+    // 32-bit index arithmetic: 9 x the boundary layers of a brick stay far below 2^32
     const unsigned fx_n = (unsigned)ny * nz, fy_n = (unsigned)nx * nz, fz_n = (unsigned)nx * ny;
-    int x, y, z;
-    if (i < 2 * fx_n) {
-        x = i < fx_n ? 0 : nx - 1;
-        const unsigned r = i < fx_n ? i : i - fx_n;
-        y = (int)(r / (unsigned)nz); z = (int)(r - (unsigned)y * nz);
-    } else if ((i -= 2 * fx_n) < 2 * fy_n) {
-        y = i < fy_n ? 0 : ny - 1;
-        const unsigned r = i < fy_n ? i : i - fy_n;
-        x = (int)(r / (unsigned)nz); z = (int)(r - (unsigned)x * nz);
-    } else if ((i -= 2 * fy_n) < 2 * fz_n) {
-        z = i < fz_n ? 0 : nz - 1;
-        const unsigned r = i < fz_n ? i : i - fz_n;
-        x = (int)(r / (unsigned)ny); y = (int)(r - (unsigned)x * ny);
+    int x, y, z, q;
+    // slot s of the nine inward directions: the two other axes' components
+    // (s / 3 - 1, s % 3 - 1) in (x, y, z) order
+    if (i < 18 * fx_n) {
+        const unsigned s = i / (2 * fx_n), r = i - s * (2 * fx_n);
+        const bool hi = r >= fx_n;
+        const unsigned rr = hi ? r - fx_n : r;
+        x = hi ? nx - 1 : 0;
+        y = (int)(rr / (unsigned)nz);
+        z = (int)(rr - (unsigned)y * nz);
+        q = (hi ? 0 : 2) * 9 + (int)s;  // cx = -1 at x+, +1 at x-
+    } else if ((i -= 18 * fx_n) < 18 * fy_n) {
+        const unsigned s = i / (2 * fy_n), r = i - s * (2 * fy_n);
+        const bool hi = r >= fy_n;
+        const unsigned rr = hi ? r - fy_n : r;
+        y = hi ? ny - 1 : 0;
+        x = (int)(rr / (unsigned)nz);
+        z = (int)(rr - (unsigned)x * nz);
+        q = (int)(s / 3) * 9 + (hi ? 0 : 2) * 3 + (int)(s % 3);
+    } else if ((i -= 18 * fy_n) < 18 * fz_n) {
+        const unsigned s = i / (2 * fz_n), r = i - s * (2 * fz_n);
+        const bool hi = r >= fz_n;
+        const unsigned rr = hi ? r - fz_n : r;
+        z = hi ? nz - 1 : 0;
+        x = (int)(rr / (unsigned)ny);
+        y = (int)(rr - (unsigned)x * ny);
+        q = (int)(s / 3) * 9 + (int)(s % 3) * 3 + (hi ? 0 : 2);
     } else {
         return;
     }
     const long long cell = ((long long)x * ny + y) * nz + z;
     const uint32_t w = a.flags_prev[cell];
-    if ((w & kFlagSelfSolid) || !(w & kFlagFaceSpecial)) return;
+    if ((w & kFlagSelfSolid) || !(w & kFlagFaceSpecial) || ((w >> q) & 1u)) return;
+    const int sx = axis_neighbour(x, -q_cx(q), nx, G.wrap[0]);
+    const int sy = axis_neighbour(y, -q_cy(q), ny, G.wrap[1]);
+    const int sz = axis_neighbour(z, -q_cz(q), nz, G.wrap[2]);
+    if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) return;
     const NeighbourOffsets o = neighbour_offsets(G, x, y, z);
     const int own = pad_index(G, x, y, z);
-    // unrolled: the direction constants fold and the 27 tests issue independently
-#pragma unroll
-    for (int q = 0; q < 27; ++q) {
-        if ((w >> q) & 1u) continue;
-        const int sx = axis_neighbour(x, -q_cx(q), nx, G.wrap[0]);
-        const int sy = axis_neighbour(y, -q_cy(q), ny, G.wrap[1]);
-        const int sz = axis_neighbour(z, -q_cz(q), nz, G.wrap[2]);
-        if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) continue;
-        const float v = ip_face_source<S>(f, a, G, o, own, cell, x, y, z, q, sx, sy, sz, a.parity);
-        int c, d;
-        incoming_slot(o, own, q, a.parity, false, c, d);
-        S::store(f + (long long)d * G.pcells + c, q, v, a.sc);
-    }
+    const float v = ip_face_source<S>(f, a, G, o, own, cell, x, y, z, q, sx, sy, sz, a.parity);
+    int c, d;
+    incoming_slot(o, own, q, a.parity, false, c, d);
+    S::store(f + (long long)d * G.pcells + c, q, v, a.sc);
 }
 
 template <class S>

@@ -30,8 +30,8 @@ struct IpLaunch {
     // Pre-fill of equilibrium-face sources; needed when any face is an
     // equilibrium face (velocity, pressure, moving wall).
     static cudaError_t face_fill(typename S::T* f, const IpArgs& a, cudaStream_t s) {
-        const long long n = 2LL * ((long long)a.g.ny * a.g.nz + (long long)a.g.nx * a.g.nz + (long long)a.g.nx * a.g.ny);
-        face_fill_ip_kernel<S><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(f, a);
+        const long long n = face_fill_count(a.g);
+        face_fill_ip_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(f, a);
         count_launch();
         return cudaGetLastError();
     }
