@@ -49,6 +49,10 @@ struct IpArgs {
     // outgoing [q]. Launch-uniform, read from the parameter space.
     int off_in[27][2];
     int off_out[27];
+    // Faces the face pre-fill visits (bit f, faces x-, x+, y-, y+, z-, z+);
+    // 0 = all six. A face whose links are all bounce-back or periodic needs no
+    // visit: the deciding face of every link the fill writes is in the set.
+    unsigned fill_faces;
 };
 
 
@@ -558,45 +562,61 @@ __device__ __forceinline__ float ip_face_source(const typename S::T* __restrict_
 // three faces (edge and corner cells) is visited once per face; every visit
 // writes the same value.
 // face_fill_count: threads of the fill.
-inline long long face_fill_count(const PadGeom& g) {
-    return 9LL * 2 * ((long long)g.ny * g.nz + (long long)g.nx * g.nz + (long long)g.nx * g.ny);
+__host__ __device__ __forceinline__ unsigned fill_face_set(unsigned fill_faces) { return fill_faces ? fill_faces & 0x3Fu : 0x3Fu; }
+__host__ __device__ __forceinline__ long long face_area(const PadGeom& g, int face) {
+    const int axis = face >> 1;
+    return axis == 0 ? (long long)g.ny * g.nz : (axis == 1 ? (long long)g.nx * g.nz : (long long)g.nx * g.ny);
+}
+inline long long face_fill_count(const PadGeom& g, unsigned fill_faces) {
+    long long n = 0;
+    for (int f = 0; f < 6; ++f)
+        if ((fill_face_set(fill_faces) >> f) & 1u) n += 9 * face_area(g, f);
+    return n;
 }
 
 template <class S>
 __device__ __forceinline__ void face_fill_cell(typename S::T* __restrict__ f, const IpArgs& a, unsigned i) {
     const PadGeom& G = a.g;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
-    // 32-bit index arithmetic: 9 x the boundary layers of a brick stay far below 2^32
-    const unsigned fx_n = (unsigned)ny * nz, fy_n = (unsigned)nx * nz, fz_n = (unsigned)nx * ny;
-    int x, y, z, q;
+    const unsigned set = fill_face_set(a.fill_faces);
+    // the face of thread i (launch-uniform set; 32-bit indices: 9 x the
+    // boundary layers of a brick stay far below 2^32)
+    int face = -1;
+    unsigned area = 0;
+#pragma unroll
+    for (int fc = 0; fc < 6; ++fc) {
+        if (face >= 0 || !((set >> fc) & 1u)) continue;
+        const unsigned n = (unsigned)face_area(G, fc);
+        if (i < 9 * n) {
+            face = fc;
+            area = n;
+        } else {
+            i -= 9 * n;
+        }
+    }
+    if (face < 0) return;
     // slot s of the nine inward directions: the two other axes' components
-    // (s / 3 - 1, s % 3 - 1) in (x, y, z) order
-    if (i < 18 * fx_n) {
-        const unsigned s = i / (2 * fx_n), r = i - s * (2 * fx_n);
-        const bool hi = r >= fx_n;
-        const unsigned rr = hi ? r - fx_n : r;
+    // (s / 3 - 1, s % 3 - 1) in (x, y, z) order; consecutive threads along the
+    // face's cells
+    const unsigned s = i / area, r = i - s * area;
+    const bool hi = face & 1;
+    const int in = hi ? 0 : 2;  // component + 1 along the face's axis, pointing into the brick
+    int x, y, z, q;
+    if (face < 2) {
         x = hi ? nx - 1 : 0;
-        y = (int)(rr / (unsigned)nz);
-        z = (int)(rr - (unsigned)y * nz);
-        q = (hi ? 0 : 2) * 9 + (int)s;  // cx = -1 at x+, +1 at x-
-    } else if ((i -= 18 * fx_n) < 18 * fy_n) {
-        const unsigned s = i / (2 * fy_n), r = i - s * (2 * fy_n);
-        const bool hi = r >= fy_n;
-        const unsigned rr = hi ? r - fy_n : r;
+        y = (int)(r / (unsigned)nz);
+        z = (int)(r - (unsigned)y * nz);
+        q = in * 9 + (int)s;
+    } else if (face < 4) {
         y = hi ? ny - 1 : 0;
-        x = (int)(rr / (unsigned)nz);
-        z = (int)(rr - (unsigned)x * nz);
-        q = (int)(s / 3) * 9 + (hi ? 0 : 2) * 3 + (int)(s % 3);
-    } else if ((i -= 18 * fy_n) < 18 * fz_n) {
-        const unsigned s = i / (2 * fz_n), r = i - s * (2 * fz_n);
-        const bool hi = r >= fz_n;
-        const unsigned rr = hi ? r - fz_n : r;
-        z = hi ? nz - 1 : 0;
-        x = (int)(rr / (unsigned)ny);
-        y = (int)(rr - (unsigned)x * ny);
-        q = (int)(s / 3) * 9 + (int)(s % 3) * 3 + (hi ? 0 : 2);
+        x = (int)(r / (unsigned)nz);
+        z = (int)(r - (unsigned)x * nz);
+        q = (int)(s / 3) * 9 + in * 3 + (int)(s % 3);
     } else {
-        return;
+        z = hi ? nz - 1 : 0;
+        x = (int)(r / (unsigned)ny);
+        y = (int)(r - (unsigned)x * ny);
+        q = (int)(s / 3) * 9 + (int)(s % 3) * 3 + in;
     }
     const long long cell = ((long long)x * ny + y) * nz + z;
     const uint32_t w = a.flags_prev[cell];

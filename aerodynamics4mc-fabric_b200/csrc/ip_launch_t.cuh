@@ -30,7 +30,7 @@ struct IpLaunch {
     // Pre-fill of equilibrium-face sources; needed when any face is an
     // equilibrium face (velocity, pressure, moving wall).
     static cudaError_t face_fill(typename S::T* f, const IpArgs& a, cudaStream_t s) {
-        const long long n = face_fill_count(a.g);
+        const long long n = face_fill_count(a.g, a.fill_faces);
         face_fill_ip_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(f, a);
         count_launch();
         return cudaGetLastError();

@@ -555,15 +555,18 @@ static bool inplace_faces_ok(const FaceParams& f) {
 
 // Some face needs the end-of-call fill (a kind other than periodic and
 // bounce-back, which the step kernel resolves itself).
-static bool faces_need_fill(const FaceParams& f) {
+// fill_face_mask: those faces (bit f), the set the fill visits.
+static unsigned fill_face_mask(const FaceParams& f) {
+    unsigned m = 0;
     for (int i = 0; i < 6; ++i) {
         const int k = f.kind[i];
         if (k == kHydroPeriodic || k == kHydroBounceBack) continue;
         if (k == kHydroInheritGame && f.disable_convective) continue;
-        return true;
+        m |= 1u << i;
     }
-    return false;
+    return m;
 }
+static bool faces_need_fill(const FaceParams& f) { return fill_face_mask(f) != 0; }
 
 // Storage of an in-place context for the kernels that take it as a number:
 // 0 FP32, 1 IEEE-half deviations, 2 16-bit fixed point.
@@ -998,6 +1001,7 @@ static bool step_context_body(Context& ctx, const float* packet, float* out, flo
             // launches it on its own (join_fill)
             IpArgs a = ip_args(ctx, new_slot, new_slot, cp);
             a.parity = ctx.parity;
+            a.fill_faces = fill_face_mask(face_now);
             g_fill_args[&ctx] = a;
             ctx.fill_pending = true;
         }

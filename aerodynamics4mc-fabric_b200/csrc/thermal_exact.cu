@@ -683,10 +683,10 @@ __global__ void __launch_bounds__(kMThreads, kColumnBlocksPerSM) thermal_update_
 }
 
 // The transport's columns (the first `columns` blocks, numbered z-tile
-// fastest) and, in the remaining blocks, the face pre-fill of an in-place
-// context: two independent passes in one launch (the fill writes ghost-layer
-// slots from post-collision populations, the transport reads and writes
-// temperature).
+// fastest; about one wave of resident blocks) and, in the remaining blocks,
+// the face pre-fill of an in-place context: two independent passes in one
+// launch (the fill writes ghost-layer slots from post-collision populations,
+// the transport reads and writes temperature).
 template <class S, bool kTagged>
 __global__ void __launch_bounds__(kMThreads, kColumnBlocksPerSM) thermal_fill_kernel(const __grid_constant__ ThermalArgs a,
                                                                    typename S::T* __restrict__ f,
@@ -778,7 +778,7 @@ cudaError_t launch_thermal_update_fill(const ThermalArgs& a, int storage, void* 
     const unsigned gx = (unsigned)((a.nz + kMZ - 1) / kMZ), gy = (unsigned)((a.ny + kMY - 1) / kMY);
     const ThermalArgs ap = column_args(a, gx * gy);
     const unsigned columns = gx * gy * (unsigned)((a.nx + ap.xchunk - 1) / ap.xchunk);
-    const unsigned fill_blocks = (unsigned)((face_fill_count(fill.g) + kMThreads - 1) / kMThreads);
+    const unsigned fill_blocks = (unsigned)((face_fill_count(fill.g, fill.fill_faces) + kMThreads - 1) / kMThreads);
     const dim3 block(kMTZ, kMY), grid(fill_blocks + columns);
     const bool tagged = no_neumann(a.faces);
 #define AERO_THERMAL_FILL(S, T)                                                                                    \
