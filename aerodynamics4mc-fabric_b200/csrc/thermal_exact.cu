@@ -92,7 +92,7 @@ constexpr int kRowPairs = kPZ / 2;                // 18
 constexpr int kPairs = kRowPairs * (kMY + 2);     // staged z-pairs per plane: 180
 constexpr int kPlane = kPZ * (kMY + 2);           // staged entries per plane: 360
 constexpr int kRing = 4;                          // staged planes
-constexpr int kColumnBlocksPerSM = 6;             // resident column blocks per SM (80 registers)
+constexpr int kColumnBlocksPerSM = 7;             // resident column blocks per SM (72 registers)
 static_assert(kPairs <= 2 * kMThreads, "two staged pairs per thread and plane");
 
 // Lookups specialise on what the three planes of the window hold (block-
