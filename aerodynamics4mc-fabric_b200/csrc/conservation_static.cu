@@ -217,7 +217,7 @@ AERO_LBM_B200_EXPORT int aero_lbm_b200_conservation_sums_noalloc(long long conte
                                                                 c->obstacle[c->slot], c->ref_p[c->slot],
                                                                 c->d_face[c->slot], scratch, c->f_ready ? 1 : 0);
     } else {
-        if (!join_fill(*c, s)) return 0;  // the last call's face pre-fill runs on its own stream
+        if (!join_fill(*c, s)) return 0;  // the last call's pending face pre-fill first
         IpArgs a{};
         a.g = make_pad_geom(c->nx, c->ny, c->nz, c->periodic_mask);
         a.parity = c->parity;

@@ -83,9 +83,9 @@ __device__ __forceinline__ float ip_face_equilibrium(const FaceParams& F, int q,
     return feq27(q, rho, ux, uy, uz);
 }
 
-// Incoming populations of a fluid cell at parity p, read between calls: every
-// call ends with the equilibrium-face pre-fill, so each incoming slot (the
-// face sources included) holds the cell's streamed population.
+// Incoming populations of a fluid cell at parity p, read between calls: the
+// face pre-fill a call leaves runs before any such read, so each incoming
+// slot (the face sources included) holds the cell's streamed population.
 template <class S>
 __device__ __forceinline__ void ip_pull(const typename S::T* __restrict__ f, const IpArgs& a, const PadGeom& G,
                                         const NeighbourOffsets& o, int own, uint32_t w, int p, float (&fl)[27]) {

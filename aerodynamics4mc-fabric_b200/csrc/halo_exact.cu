@@ -10,8 +10,8 @@
 // populations (the reference's f) and its temperature.
 //
 // In-place contexts keep the streamed populations in the incoming slots of
-// the next step's parity between calls (the equilibrium-face sources are
-// pre-filled at the end of each call), so a cell's f is read and written
+// the next step's parity between calls (the equilibrium-face sources a call
+// leaves are pre-filled before anything reads them), so a cell's f is read and written
 // through the same slot map the step kernel pulls with (bounce-back bits of
 // the last classification). Solid cells of an in-place context keep their
 // populations beside the lattice (IpArgs::solid_f, at a canonical parity;

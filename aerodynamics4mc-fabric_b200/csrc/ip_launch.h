@@ -31,8 +31,9 @@ cudaError_t ip_fill_f16_fast(__half* f, const IpArgs& a, cudaStream_t s);
 cudaError_t ip_fill_i16_fast(short* f, const IpArgs& a, cudaStream_t s);
 
 // Equilibrium-face pre-fill for the step of parity a.parity (see
-// face_fill_ip_kernel); run at the end of every call, so that between calls
-// every incoming slot holds the cell's streamed population.
+// face_fill_ip_kernel); each call leaves one, run before anything reads the
+// populations, so that between calls every incoming slot holds the cell's
+// streamed population.
 inline cudaError_t ip_fill(int v, void* f, const IpArgs& a, cudaStream_t s) {
     if (v == kIpF32Exact) return ip_fill_f32_exact(static_cast<float*>(f), a, s);
     if (v == kIpF32Fast) return ip_fill_f32_fast(static_cast<float*>(f), a, s);

@@ -147,7 +147,8 @@ float fp16_scale_for_speed(float umax);
 float i16_scale_for_speed(float umax);
 // Device-side output into `dev_out` (no copy, no synchronisation).
 bool output_device(Context& ctx, OutBox box, int out_ch, float scale, float* dev_out);
-// Order stream s after the context's last equilibrium-face pre-fill.
+// Launches the face pre-fill the context's last call left pending (if any) on
+// stream s, before anything on s reads the populations.
 bool join_fill(Context& ctx, cudaStream_t s);
 // Collect the slab copies of the following exchange_halo calls (in-place
 // contexts) and launch them together at halo_batch_flush(); exchanges of one
