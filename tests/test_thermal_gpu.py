@@ -93,7 +93,7 @@ _EDGE_FACES = [{"kind": O.PERIODIC, "thermal": O.THERMAL_PERIODIC}, {"kind": O.P
 
 
 @pytest.mark.parametrize("variant,dims,steps", [("faces", (37, 19, 45), 6), ("periodic_x", (17, 9, 33), 6),
-                                                ("fast", (37, 19, 45), 2)])
+                                                ("fast", (37, 19, 45), 2), ("tiny", (5, 3, 7), 6)])
 @pytest.mark.parametrize("streaming", [1, 2])
 def test_thermal_transport_brick_edges_match_oracle(gpu, variant, dims, steps, streaming):
     """Non-cubic bricks: several x-chunks of the transport's column walk with
@@ -102,8 +102,9 @@ def test_thermal_transport_brick_edges_match_oracle(gpu, variant, dims, steps, s
     periodic x (the wrapped planes staged), symmetry and velocity faces, no
     Neumann face; fast: the same faces with packet speeds up to 0.6 and two
     cells beyond one cell per step (the out-of-window trilinear sample) for
-    the first update. Flow output and temperature state bit-identical to the
-    oracle, both layouts."""
+    the first update; tiny: periodic_x's faces on a brick smaller than one
+    tile in every axis (odd z extent: no z-pair vector access). Flow output
+    and temperature state bit-identical to the oracle, both layouts."""
     _, _, _, _, cfg, _ = O.thermal_case(12, 11)
     if variant != "faces":
         cfg = dict(cfg, faces=_EDGE_FACES)
@@ -114,6 +115,8 @@ def test_thermal_transport_brick_edges_match_oracle(gpu, variant, dims, steps, s
     u[0] += np.float32(0.04)
     if variant == "fast":
         u[0][5, 5, 5], u[1][20, 10, 30], u[2][36, 18, 44] = 1.5, -1.25, -1.0
+    if variant == "tiny":
+        obst[2, 1, 3] = 1
     temp = rng.uniform(-0.3, 0.3, dims).astype(np.float32)
     src = rng.uniform(-0.01, 0.01, dims).astype(np.float32)
     pre = np.full(int(np.prod(dims)), 0.5, np.float32)
