@@ -304,17 +304,16 @@ struct PairIO<StoreI16Dev> {
         return __ffma2_rn(v.v, make_float2(k, k), make_float2(-s.scale, -s.scale));
     }
     __device__ __forceinline__ static F2 load(const short* p0, const short* p1, int q, const Fp16Scale& s) {
-        return decode(make_float2((float)__ldg(p0), (float)__ldg(p1)), q, s);
+        const unsigned r = (unsigned)(unsigned short)__ldg(p0) | ((unsigned)(unsigned short)__ldg(p1) << 16);
+        return decode(s16x2_to_float2(r), q, s);
     }
     __device__ __forceinline__ static F2 load2(const short* p, int q, const Fp16Scale& s) {
-        const short2 r = __ldg(reinterpret_cast<const short2*>(p));
-        return decode(make_float2((float)r.x, (float)r.y), q, s);
+        return decode(s16x2_to_float2(__ldg(reinterpret_cast<const unsigned*>(p))), q, s);
     }
     __device__ __forceinline__ static F2 load2p(const short* p, const short* p1, bool fix, int q, const Fp16Scale& s) {
-        const short2 r = __ldg(reinterpret_cast<const short2*>(p));
-        short y = r.y;
-        if (fix) y = __ldg(p1);
-        return decode(make_float2((float)r.x, (float)y), q, s);
+        unsigned r = __ldg(reinterpret_cast<const unsigned*>(p));
+        if (fix) r = (r & 0xFFFFu) | ((unsigned)(unsigned short)__ldg(p1) << 16);
+        return decode(s16x2_to_float2(r), q, s);
     }
     __device__ __forceinline__ static void store(short* p0, short* p1, bool s0, bool s1, int q, F2 v, const Fp16Scale& s) {
         const float2 h = encode(v, q, s);

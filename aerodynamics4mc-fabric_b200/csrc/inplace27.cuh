@@ -76,10 +76,23 @@ struct StoreF16Dev {
 // over the whole range instead of 11 significant bits: the deviations that
 // carry the flow (|f - w| / w ~ 0.1-1) are stored 5-10x more precisely. A
 // non-finite value stores 0 (the rest weight).
+// max.NaN keeps a NaN (which the conversion stores as 0) and lifts everything
+// below -32767 to it before the saturating conversion: the same result as
+// saturating to [-32768, 32767] and then raising -32768 to -32767.
 __device__ __forceinline__ short sat_round_s16(float x) {
+    float y;
+    asm("max.NaN.f32 %0, %1, 0fC6FFFE00;" : "=f"(y) : "f"(x));  // -32767.0
     short r;
-    asm("cvt.rni.sat.s16.f32 %0, %1;" : "=h"(r) : "f"(x));
-    return r < -32767 ? (short)-32767 : r;
+    asm("cvt.rni.sat.s16.f32 %0, %1;" : "=h"(r) : "f"(y));
+    return r;
+}
+// Exact int16 -> float of both halves of a 32-bit word (low half first):
+// 2^23 + 2^22 + h has h in its low mantissa bits for |h| < 2^22, so one
+// integer add and one packed float subtract replace two conversions.
+__device__ __forceinline__ float2 s16x2_to_float2(unsigned w) {
+    const int lo = (int)(short)(w & 0xFFFFu), hi = (int)w >> 16;
+    const float2 b = make_float2(__int_as_float(0x4B400000 + lo), __int_as_float(0x4B400000 + hi));
+    return __fadd2_rn(b, make_float2(-12582912.0f, -12582912.0f));
 }
 struct StoreI16Dev {
     using T = short;

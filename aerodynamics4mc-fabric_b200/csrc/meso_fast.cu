@@ -204,7 +204,8 @@ struct MesoPair<MesoI16> {
     __device__ __forceinline__ static Raw raw2(const short* p0, const short* p1) { return make_short2(__ldg(p0), __ldg(p1)); }
     __device__ __forceinline__ static F2 decode(Raw r, int q, float inv_scale) {
         const float w = mw(q), k = w * inv_scale;
-        return F2{__ffma2_rn(make_float2((float)r.x, (float)r.y), make_float2(k, k), make_float2(w, w))};
+        const unsigned bits = (unsigned)(unsigned short)r.x | ((unsigned)(unsigned short)r.y << 16);
+        return F2{__ffma2_rn(s16x2_to_float2(bits), make_float2(k, k), make_float2(w, w))};
     }
     __device__ __forceinline__ static void store(short* p, int q, F2 v, float scale) {
         const float k = scale * (1.0f / mw(q));
