@@ -54,14 +54,38 @@ __device__ __forceinline__ float th_sample(const ThermalArgs& a, const float* fi
     const int x0 = (int)floorf(x), y0 = (int)floorf(y), z0 = (int)floorf(z);
     const int x1 = x0 + 1, y1 = y0 + 1, z1 = z0 + 1;
     const float fx = x - (float)x0, fy = y - (float)y0, fz = z - (float)z0;
-    const float c000 = th_neighbour(a, field, x0, y0, z0, fallback);
-    const float c100 = th_neighbour(a, field, x1, y0, z0, fallback);
-    const float c010 = th_neighbour(a, field, x0, y1, z0, fallback);
-    const float c110 = th_neighbour(a, field, x1, y1, z0, fallback);
-    const float c001 = th_neighbour(a, field, x0, y0, z1, fallback);
-    const float c101 = th_neighbour(a, field, x1, y0, z1, fallback);
-    const float c011 = th_neighbour(a, field, x0, y1, z1, fallback);
-    const float c111 = th_neighbour(a, field, x1, y1, z1, fallback);
+    float c000, c100, c010, c110, c001, c101, c011, c111;
+    if (x0 >= 0 && x1 < a.nx && y0 >= 0 && y1 < a.ny && z0 >= 0 && z1 < a.nz) {
+        // every corner inside the brick: the 16 loads issue together, then
+        // th_neighbour's solid rule
+        const int sy = a.nz, sx = a.ny * a.nz;
+        const int b = (x0 * a.ny + y0) * a.nz + z0;
+        const int o[8] = {0, sx, sy, sx + sy, 1, sx + 1, sy + 1, sx + sy + 1};
+        bool solid[8];
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            solid[k] = a.obstacle[b + o[k]] != 0;
+            v[k] = field[b + o[k]];
+        }
+        c000 = solid[0] ? fallback : v[0];
+        c100 = solid[1] ? fallback : v[1];
+        c010 = solid[2] ? fallback : v[2];
+        c110 = solid[3] ? fallback : v[3];
+        c001 = solid[4] ? fallback : v[4];
+        c101 = solid[5] ? fallback : v[5];
+        c011 = solid[6] ? fallback : v[6];
+        c111 = solid[7] ? fallback : v[7];
+    } else {
+        c000 = th_neighbour(a, field, x0, y0, z0, fallback);
+        c100 = th_neighbour(a, field, x1, y0, z0, fallback);
+        c010 = th_neighbour(a, field, x0, y1, z0, fallback);
+        c110 = th_neighbour(a, field, x1, y1, z0, fallback);
+        c001 = th_neighbour(a, field, x0, y0, z1, fallback);
+        c101 = th_neighbour(a, field, x1, y0, z1, fallback);
+        c011 = th_neighbour(a, field, x0, y1, z1, fallback);
+        c111 = th_neighbour(a, field, x1, y1, z1, fallback);
+    }
     const float c00 = c000 + (c100 - c000) * fx;
     const float c10 = c010 + (c110 - c010) * fx;
     const float c01 = c001 + (c101 - c001) * fx;
@@ -269,9 +293,32 @@ __global__ void __launch_bounds__(128) bfecc_final_kernel(const __grid_constant_
     const float tc = a.t[cell];
     const float ux = a.u[cell], uy = a.u[a.cells + cell], uz = a.u[2 * a.cells + cell];
     float adv = th_sample(a, a.t_next, (float)x - dt * ux, (float)y - dt * uy, (float)z - dt * uz, a.t_next[cell]);
-    const float n0 = th_neighbour(a, x + 1, y, z, tc), n1 = th_neighbour(a, x - 1, y, z, tc);
-    const float n2 = th_neighbour(a, x, y + 1, z, tc), n3 = th_neighbour(a, x, y - 1, z, tc);
-    const float n4 = th_neighbour(a, x, y, z + 1, tc), n5 = th_neighbour(a, x, y, z - 1, tc);
+    float n0, n1, n2, n3, n4, n5;
+    if (x >= 1 && x + 1 < a.nx && y >= 1 && y + 1 < a.ny && z >= 1 && z + 1 < a.nz) {
+        // all six face neighbours inside the brick: loads first, then the solid rule
+        const int sx = a.ny * a.nz, sy = a.nz;
+        const int o[6] = {sx, -sx, sy, -sy, 1, -1};
+        bool solid[6];
+        float v[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            solid[k] = a.obstacle[cell + o[k]] != 0;
+            v[k] = a.t[cell + o[k]];
+        }
+        n0 = solid[0] ? tc : v[0];
+        n1 = solid[1] ? tc : v[1];
+        n2 = solid[2] ? tc : v[2];
+        n3 = solid[3] ? tc : v[3];
+        n4 = solid[4] ? tc : v[4];
+        n5 = solid[5] ? tc : v[5];
+    } else {
+        n0 = th_neighbour(a, x + 1, y, z, tc);
+        n1 = th_neighbour(a, x - 1, y, z, tc);
+        n2 = th_neighbour(a, x, y + 1, z, tc);
+        n3 = th_neighbour(a, x, y - 1, z, tc);
+        n4 = th_neighbour(a, x, y, z + 1, tc);
+        n5 = th_neighbour(a, x, y, z - 1, tc);
+    }
     // local_temperature_bounds (jni.cpp:1883-1908): std::min / std::max in neighbour order
     float lo = tc, hi = tc;
     const float nb[6] = {n0, n1, n2, n3, n4, n5};
