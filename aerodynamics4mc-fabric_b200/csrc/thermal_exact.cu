@@ -55,7 +55,9 @@ __device__ __forceinline__ float th_sample(const ThermalArgs& a, const float* fi
     const int x1 = x0 + 1, y1 = y0 + 1, z1 = z0 + 1;
     const float fx = x - (float)x0, fy = y - (float)y0, fz = z - (float)z0;
     float c000, c100, c010, c110, c001, c101, c011, c111;
-    if (x0 >= 0 && x1 < a.nx && y0 >= 0 && y1 < a.ny && z0 >= 0 && z1 < a.nz) {
+    // x0 < nx - 1, not x1 < nx: a non-finite or huge position converts to
+    // INT_MAX, where x0 + 1 wraps
+    if (x0 >= 0 && x0 < a.nx - 1 && y0 >= 0 && y0 < a.ny - 1 && z0 >= 0 && z0 < a.nz - 1) {
         // every corner inside the brick: the 16 loads issue together, then
         // th_neighbour's solid rule
         const int sy = a.nz, sx = a.ny * a.nz;
