@@ -10,6 +10,7 @@
 // form.
 #pragma once
 
+#include "pdl.cuh"
 #include "d3q27_step.cuh"
 #include "collide27_x2.cuh"
 #include "collide27_exact_x2.cuh"
@@ -369,6 +370,9 @@ __host__ __device__ constexpr bool out_pair_aligned(int q) {
 #endif
 template <class S, bool kExact, int kParity, bool kTransport>
 __global__ void __launch_bounds__(128, kExact ? AERO_IP2X_MIN_BLOCKS : AERO_IP2_MIN_BLOCKS) step_ip2_kernel(typename S::T* __restrict__ f, IpArgs a) {
+    // launched after the transport (and the face pre-fill) with launch_pdl
+    pdl_trigger();
+    pdl_wait();
     const PadGeom& G = a.g;
     const int z0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int y = blockIdx.y, x = blockIdx.z;

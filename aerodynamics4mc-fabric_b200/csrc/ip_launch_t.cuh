@@ -53,8 +53,10 @@ struct IpLaunch {
                 if (a.parity == 0) step_ip2_kernel<S, kExact, 0, true><<<grid, lb, smem, s>>>(f, b);
                 else step_ip2_kernel<S, kExact, 1, true><<<grid, lb, smem, s>>>(f, b);
             } else {
-                if (a.parity == 0) step_ip2_kernel<S, kExact, 0, false><<<grid, lb, 0, s>>>(f, b);
-                else step_ip2_kernel<S, kExact, 1, false><<<grid, lb, 0, s>>>(f, b);
+                // may be scheduled under the tail of the transport launch (the kernel waits for it)
+                cudaError_t e = a.parity == 0 ? launch_pdl(step_ip2_kernel<S, kExact, 0, false>, grid, dim3(lb), 0, s, f, b)
+                                              : launch_pdl(step_ip2_kernel<S, kExact, 1, false>, grid, dim3(lb), 0, s, f, b);
+                if (e != cudaSuccess) return e;
             }
         } else {
             const int lb = line_block(a.g.nz);

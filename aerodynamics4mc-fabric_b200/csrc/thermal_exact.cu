@@ -5,6 +5,7 @@
 #include "collide27_exact.cuh"
 #include "collide27_exact_x2.cuh"
 #include "d3q27_inplace.cuh"
+#include "pdl.cuh"
 
 namespace aero {
 namespace {
@@ -728,6 +729,8 @@ __device__ __forceinline__ void thermal_column(const ThermalArgs& a, int bx, int
 // straight from the parameter space (no per-thread copy to local memory).
 template <bool kTagged>
 __global__ void __launch_bounds__(kMThreads, kColumnBlocksPerSM) thermal_update_kernel(const __grid_constant__ ThermalArgs a) {
+    pdl_trigger();
+    pdl_wait();  // launched with launch_pdl after the previous call's step
     thermal_column<kTagged>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -741,6 +744,8 @@ __global__ void __launch_bounds__(kMThreads, kColumnBlocksPerSM) thermal_fill_ke
                                                                    typename S::T* __restrict__ f,
                                                                    const __grid_constant__ IpArgs fa, unsigned columns,
                                                                    unsigned gx, unsigned gy) {
+    pdl_trigger();
+    pdl_wait();  // launched with launch_pdl after the previous call's step
     const unsigned b = blockIdx.x;
     if (b < columns) {
         thermal_column<kTagged>(a, (int)(b % gx), (int)((b / gx) % gy), (int)(b / (gx * gy)));
@@ -816,10 +821,10 @@ cudaError_t launch_thermal_update(const ThermalArgs& a, cudaStream_t s) {
     const unsigned gx = (unsigned)((a.nz + kMZ - 1) / kMZ), gy = (unsigned)((a.ny + kMY - 1) / kMY);
     const ThermalArgs ap = column_args(a, gx * gy);
     const dim3 grid(gx, gy, (unsigned)((a.nx + ap.xchunk - 1) / ap.xchunk));
-    if (no_neumann(a.faces)) thermal_update_kernel<true><<<grid, dim3(kMTZ, kMY), 0, s>>>(ap);
-    else thermal_update_kernel<false><<<grid, dim3(kMTZ, kMY), 0, s>>>(ap);
+    const cudaError_t e = no_neumann(a.faces) ? launch_pdl(thermal_update_kernel<true>, grid, dim3(kMTZ, kMY), 0, s, ap)
+                                              : launch_pdl(thermal_update_kernel<false>, grid, dim3(kMTZ, kMY), 0, s, ap);
     count_launch();
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_thermal_update_fill(const ThermalArgs& a, int storage, void* f, const IpArgs& fill, cudaStream_t s) {
@@ -831,12 +836,14 @@ cudaError_t launch_thermal_update_fill(const ThermalArgs& a, int storage, void* 
     const dim3 block(kMTZ, kMY), grid(fill_blocks + columns);
     const bool tagged = no_neumann(a.faces);
 #define AERO_THERMAL_FILL(S, T)                                                                                    \
-    (tagged ? (thermal_fill_kernel<S, true><<<grid, block, 0, s>>>(ap, static_cast<T*>(f), fill, columns, gx, gy), 0) \
-            : (thermal_fill_kernel<S, false><<<grid, block, 0, s>>>(ap, static_cast<T*>(f), fill, columns, gx, gy), 0))
-    if (storage == 1) AERO_THERMAL_FILL(StoreF16Dev, __half);
-    else if (storage == 2) AERO_THERMAL_FILL(StoreI16Dev, short);
-    else AERO_THERMAL_FILL(StoreF32, float);
+    (tagged ? launch_pdl(thermal_fill_kernel<S, true>, grid, block, 0, s, ap, static_cast<T*>(f), fill, columns, gx, gy) \
+            : launch_pdl(thermal_fill_kernel<S, false>, grid, block, 0, s, ap, static_cast<T*>(f), fill, columns, gx, gy))
+    cudaError_t e;
+    if (storage == 1) e = AERO_THERMAL_FILL(StoreF16Dev, __half);
+    else if (storage == 2) e = AERO_THERMAL_FILL(StoreI16Dev, short);
+    else e = AERO_THERMAL_FILL(StoreF32, float);
 #undef AERO_THERMAL_FILL
+    if (e != cudaSuccess) return e;
     count_launch();
     return cudaGetLastError();
 }
