@@ -122,16 +122,14 @@ constexpr int kRing = 4;                          // staged planes
 constexpr int kColumnBlocksPerSM = 7;             // resident column blocks per SM (72 registers)
 static_assert(kPairs <= 2 * kMThreads, "two staged pairs per thread and plane");
 
-// Lookups specialise on what the three planes of the window hold (block-
-// uniform): only code 0 (most of the air above a terrain), codes 0 and 1 with
-// code 1 entries holding kOwnTag (bricks without a Neumann face; the code
-// array is not read), or any code.
-enum TileKind { kTileClean = 0, kTileTagged = 1, kTileAny = 2 };
+// Lookups specialise on the brick's faces (launch-uniform): without a Neumann
+// face only codes 0 and 1 occur and code 1 entries hold kOwnTag (the code
+// array is not read); otherwise any code.
+enum TileKind { kTileTagged = 1, kTileAny = 2 };
 
 template <int kKind>
 __device__ __forceinline__ float tile_at(const float* sv, const unsigned char* sc, int i, float self) {
     const float v = sv[i];
-    if (kKind == kTileClean) return v;
     if (kKind == kTileTagged) return __float_as_uint(v) == kOwnTag ? self : v;
     const int c = sc[i];
     return c == 0 ? v : (c == 1 ? self : exact::rclamp(self + v, -1.0f, 1.0f));
