@@ -468,6 +468,24 @@ def run_adjoint_leg(aero, lib, torch) -> dict:
                           "gradient_equal_to_checkpointed": bool(np.array_equal(gf1, gf) and np.array_equal(gu1, gu))}}
 
 
+def rank_max(value: float, world: int, dist_mod=None, device=None) -> float:
+    """The maximum of `value` over the ranks of the process group (every rank
+    calls it with its own value); one rank returns its value untouched."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
+    return float(t.item())
+
+
+def window_count(first_window_ms: float, world: int, dist_mod=None, device=None) -> int:
+    """Timed windows of a variant: enough to cover about a second at the
+    first window's length (3..5000), the same count on every rank."""
+    own = float(min(5000, max(3, -(-1000.0 // max(first_window_ms, 1e-3)))))
+    return int(rank_max(own, world, dist_mod, device))
+
+
 def run_ours(args) -> dict | None:
     import torch
     import torch.distributed as dist
@@ -506,11 +524,7 @@ def run_ours(args) -> dict | None:
         torch.cuda.synchronize(dev)
 
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(v, world, dist, dev)
 
     def timed(variant: str, key: int, steps: int):
         """Windows of `steps` device-resident steps (one library call that
@@ -537,7 +551,7 @@ def run_ours(args) -> dict | None:
                 launches = lib.aero_lbm_b200_launch_count() - launches0
                 window_ms.append(max_over_ranks(start.elapsed_time(end)))
                 if len(window_ms) == 1:
-                    windows = int(max_over_ranks(float(min(5000, max(3, -(-1000.0 // max(window_ms[0], 1e-3)))))))
+                    windows = window_count(window_ms[0], world, dist, dev)
         lib.aero_lbm_b200_kernel_timer(1)  # events around each step-kernel launch, on the library's stream
         for _ in range(3):
             ctx.advance(steps)
