@@ -141,3 +141,74 @@ def test_fill_links_cover_each_face_link_once(dims, faces):
         start += n
         assert len(set(block)) == n
         assert set(block) == {(x, y, z, q) for (ff, x, y, z, q) in want if ff == f}
+
+
+# ---- th_sample's interior test (thermal_exact.cu): x0 < n - 1, overflow-free
+INT_MAX, INT_MIN = 2 ** 31 - 1, -2 ** 31
+
+
+@pytest.mark.parametrize("dims", [(1, 1, 1), (2, 3, 5), (12, 10, 70), (128, 128, 128)])
+def test_sample_interior_test_keeps_every_corner_inside(dims):
+    """Saturated conversions (a non-finite or huge position gives INT_MAX /
+    INT_MIN) never pass the interior test, and every accepted lower corner
+    keeps all eight corners inside the brick."""
+    nx, ny, nz = dims
+    cells = nx * ny * nz
+    probe = lambda n: sorted({INT_MIN, -1, 0, max(0, n - 2), n - 1, n, INT_MAX})
+    for x0, y0, z0 in itertools.product(probe(nx), probe(ny), probe(nz)):
+        inside = 0 <= x0 < nx - 1 and 0 <= y0 < ny - 1 and 0 <= z0 < nz - 1
+        if x0 in (INT_MIN, INT_MAX) or y0 in (INT_MIN, INT_MAX) or z0 in (INT_MIN, INT_MAX):
+            assert not inside
+        if inside:
+            b = (x0 * ny + y0) * nz + z0
+            assert b >= 0 and b + ny * nz + nz + 1 < cells
+
+
+# ---- the per-block halo source table against th_neighbour's per-entry rule
+PERIODIC, DIRICHLET, NEUMANN, ADIABATIC = 2, 4, 5, 3
+
+
+def _entry_rule(kinds, dims, x, y, z):
+    """th_neighbour without the querying cell: periodic axes wrap first, then
+    the first face crossed in the order x, y, z decides; ('cell', x, y, z) or
+    ('face', f)."""
+    n = dims
+    p = [x, y, z]
+    for a in range(3):
+        if (p[a] < 0 or p[a] >= n[a]) and kinds[2 * a + (0 if p[a] < 0 else 1)] == PERIODIC:
+            p[a] %= n[a]
+    for a in range(3):
+        if p[a] < 0:
+            return ("face", 2 * a)
+        if p[a] >= n[a]:
+            return ("face", 2 * a + 1)
+    return ("cell", *p)
+
+
+def _table_rule(kinds, dims, x, y, z):
+    """resolve_x, then resolve_yz (the column kernel's split)."""
+    nx, ny, nz = dims
+    if not 0 <= x < nx:
+        if kinds[0 if x < 0 else 1] != PERIODIC:
+            return ("face", 0 if x < 0 else 1)
+        x %= nx
+    if (y < 0 or y >= ny) and kinds[2 if y < 0 else 3] == PERIODIC:
+        y %= ny
+    if (z < 0 or z >= nz) and kinds[4 if z < 0 else 5] == PERIODIC:
+        z %= nz
+    if 0 <= y < ny and 0 <= z < nz:
+        return ("cell", x, y, z)
+    return ("face", 2 if y < 0 else (3 if y >= ny else (4 if z < 0 else 5)))
+
+
+@pytest.mark.parametrize("kinds", [(DIRICHLET, NEUMANN, PERIODIC, PERIODIC, ADIABATIC, DIRICHLET),
+                                   (PERIODIC, PERIODIC, ADIABATIC, NEUMANN, DIRICHLET, PERIODIC),
+                                   (PERIODIC, PERIODIC, PERIODIC, PERIODIC, PERIODIC, PERIODIC),
+                                   (ADIABATIC,) * 6])
+@pytest.mark.parametrize("dims", [(3, 2, 5), (5, 9, 4)])
+def test_source_table_matches_the_entry_rule(kinds, dims):
+    nx, ny, nz = dims
+    # every staged coordinate the column walk can touch: planes -1..nx, rows
+    # -1..ny+8 (a partial last tile), z from -2 to nz+33
+    for x, y, z in itertools.product(range(-1, nx + 1), range(-1, ny + 9), range(-2, nz + 34)):
+        assert _table_rule(kinds, dims, x, y, z) == _entry_rule(kinds, dims, x, y, z), (x, y, z)
